@@ -1,0 +1,195 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so): the checker of the parity tests.
+
+The oracle is test infrastructure; nothing in autan_b200/ imports it."""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB = Path(__file__).resolve().parent.parent / "oracle" / "liboracle.so"
+i32, i64, f64, P = C.c_int32, C.c_int64, C.c_double, C.POINTER
+
+
+class OracleMesh(C.Structure):
+    _fields_ = [(n, i32) for n in ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+                                   "n_owned_interior_faces", "n_owned_faces")] + [
+        ("owner", P(i32)), ("neighbour", P(i32)), ("cell_face_offsets", P(i64)),
+        ("cell_faces", P(i32)), ("ghost_owner", P(i32)), ("face_normal", P(f64)),
+        ("face_area_magnitude", P(f64)), ("face_centroid", P(f64)), ("face_moment", P(f64)),
+        ("cell_centroid", P(f64)), ("cell_volume", P(f64)), ("stencil_offsets", P(i64)),
+        ("stencil", P(i32)), ("stencil_lsq_weight", P(f64)),
+    ]  # fmt: skip
+
+
+class OracleScheme(C.Structure):
+    _fields_ = [(n, i32) for n in ("flux", "second_order", "limiter", "precision", "planar")] + [
+        (n, f64) for n in ("gamma", "gas_constant", "venkat_k", "length", "mach_ref")
+    ] + [("scale", f64 * 5), ("reference", f64 * 5)]  # fmt: skip
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(str(LIB))
+        vp = C.c_void_p
+        L.oracle_create.restype = vp
+        L.oracle_create.argtypes = [P(OracleMesh), P(OracleScheme), P(C.c_uint8), P(f64), P(f64)]
+        L.oracle_free.argtypes = [vp]
+        L.oracle_set_second_order.argtypes = [vp, i32]
+        L.oracle_residual.argtypes = [vp, P(f64), P(f64)]
+        L.oracle_arrays.argtypes = [vp] + [P(f64)] * 6
+        L.oracle_spectral_radius.argtypes = [vp, P(f64)]
+        L.oracle_step.restype = i64
+        L.oracle_step.argtypes = [vp, P(f64), i32, f64, f64, i32, P(f64), P(f64)]
+        L.oracle_norms.argtypes = [P(f64), i32, i32, P(f64)]
+        L.oracle_exact_sum.restype = f64
+        L.oracle_exact_sum.argtypes = [P(f64), i64]
+        L.oracle_first_invalid.restype = i64
+        L.oracle_first_invalid.argtypes = [vp, P(f64), P(f64)]
+        for n in ("oracle_flux",):
+            getattr(L, n).argtypes = [P(OracleScheme), P(f64), P(f64), P(f64), P(f64)]
+        L.oracle_boundary_value.argtypes = [P(OracleScheme), P(f64), f64, P(f64), P(f64), P(f64)]
+        L.oracle_to_primitive.argtypes = [P(OracleScheme), P(f64), P(f64)]
+        _lib = L
+    return _lib
+
+
+def _p(a, t=f64):
+    return None if a is None else a.ctypes.data_as(P(t))
+
+
+def scheme_struct(s: dict) -> OracleScheme:
+    o = OracleScheme()
+    for k in ("flux", "second_order", "limiter", "precision", "planar"):
+        setattr(o, k, int(s.get(k, 0)))
+    for k in ("gamma", "gas_constant", "venkat_k", "length", "mach_ref"):
+        setattr(o, k, float(s[k]))
+    o.scale[:] = [float(x) for x in s["scale"]]
+    o.reference[:] = [float(x) for x in s["reference"]]
+    return o
+
+
+class Oracle:
+    """The oracle over one mesh (a dict of arrays in the mesh contract's layout)."""
+
+    def __init__(self, mesh: dict, scheme: dict, bc_kind, bc, source=None):
+        self.keep = {}
+        m = OracleMesh()
+        for k in ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+                  "n_owned_interior_faces", "n_owned_faces"):  # fmt: skip
+            setattr(m, k, int(mesh[k]))
+        types = {"owner": i32, "neighbour": i32, "cell_faces": i32, "ghost_owner": i32,
+                 "stencil": i32, "cell_face_offsets": i64, "stencil_offsets": i64}  # fmt: skip
+        for k in ("owner", "neighbour", "cell_face_offsets", "cell_faces", "ghost_owner",
+                  "face_normal", "face_area_magnitude", "face_centroid", "face_moment",
+                  "cell_centroid", "cell_volume", "stencil_offsets", "stencil",
+                  "stencil_lsq_weight"):  # fmt: skip
+            t = types.get(k, f64)
+            dt = {i32: np.int32, i64: np.int64, f64: np.float64}[t]
+            a = np.ascontiguousarray(mesh[k], dtype=dt)
+            if a.size == 0:
+                a = np.zeros(1, dtype=dt)
+            self.keep[k] = a
+            setattr(m, k, _p(a, t))
+        self.mesh = m
+        self.n_cells = int(mesh["n_cells"])
+        self.n_faces = int(mesh["n_faces"])
+        self.n_owned = int(mesh["n_owned_cells"])
+        self.scheme = scheme_struct(scheme)
+        kind = np.ascontiguousarray(bc_kind, dtype=np.uint8)
+        bcd = np.ascontiguousarray(bc, dtype=np.float64)
+        src = None if source is None else np.ascontiguousarray(source, dtype=np.float64)
+        self.keep.update(kind=kind, bc=bcd, src=src)
+        self.h = lib().oracle_create(C.byref(m), C.byref(self.scheme), _p(kind, C.c_uint8),
+                                     _p(bcd), _p(src))  # fmt: skip
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_free(self.h)
+            self.h = None
+
+    def set_second_order(self, on: bool):
+        lib().oracle_set_second_order(self.h, int(on))
+
+    def residual(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        res = np.zeros((5, self.n_cells))
+        lib().oracle_residual(self.h, _p(u), _p(res))
+        return res
+
+    def arrays(self):
+        nc, nf = self.n_cells, self.n_faces
+        out = dict(prim=np.zeros((5, nc)), grad=np.zeros((15, nc)), phi=np.zeros((5, nc)),
+                   wmin=np.zeros((5, nc)), wmax=np.zeros((5, nc)), prim_b=np.zeros((5, nf)))  # fmt: skip
+        lib().oracle_arrays(self.h, *[_p(out[k]) for k in ("prim", "grad", "phi", "wmin", "wmax",
+                                                            "prim_b")])  # fmt: skip
+        return out
+
+    def spectral_radius(self):
+        lam = np.zeros(self.n_cells)
+        lib().oracle_spectral_radius(self.h, _p(lam))
+        return lam
+
+    def step(self, u, rk=3, cfl=0.5, dt=0.0, local=False):
+        """One step of u in place; returns (norms, dt, invalid cell or -1)."""
+        assert u.flags.c_contiguous and u.dtype == np.float64
+        norms = np.zeros(5)
+        h = np.zeros(1)
+        bad = lib().oracle_step(self.h, _p(u), rk, cfl, dt, int(local), _p(norms), _p(h))
+        return norms, float(h[0]), int(bad)
+
+    def first_invalid(self, u, res):
+        return int(lib().oracle_first_invalid(self.h, _p(np.ascontiguousarray(u)),
+                                              _p(np.ascontiguousarray(res))))  # fmt: skip
+
+
+def exact_sum(terms) -> float:
+    t = np.ascontiguousarray(terms, dtype=np.float64)
+    return float(lib().oracle_exact_sum(_p(t), t.size))
+
+
+def flux(scheme: dict, wl, wr, n):
+    s = scheme_struct(scheme)
+    out = np.zeros(5)
+    lib().oracle_flux(C.byref(s), _p(np.ascontiguousarray(wl, dtype=np.float64)),
+                      _p(np.ascontiguousarray(wr, dtype=np.float64)),
+                      _p(np.ascontiguousarray(n, dtype=np.float64)), _p(out))  # fmt: skip
+    return out
+
+
+def boundary_value(scheme: dict, w, kind, data, n):
+    s = scheme_struct(scheme)
+    out = np.zeros(5)
+    lib().oracle_boundary_value(C.byref(s), _p(np.ascontiguousarray(w, dtype=np.float64)),
+                                float(kind), _p(np.ascontiguousarray(data, dtype=np.float64)),
+                                _p(np.ascontiguousarray(n, dtype=np.float64)), _p(out))  # fmt: skip
+    return out
+
+
+def to_primitive(scheme: dict, dq):
+    s = scheme_struct(scheme)
+    out = np.zeros(5)
+    lib().oracle_to_primitive(C.byref(s), _p(np.ascontiguousarray(dq, dtype=np.float64)), _p(out))
+    return out
+
+
+def load_case(path) -> tuple[dict, dict, dict]:
+    """(mesh dict, scheme dict, everything else) of a golden case file."""
+    z = dict(np.load(path))
+    mesh_keys = ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+                 "n_owned_interior_faces", "n_owned_faces", "owner", "neighbour",
+                 "cell_face_offsets", "cell_faces", "ghost_owner", "face_normal",
+                 "face_area_magnitude", "face_centroid", "face_moment", "cell_centroid",
+                 "cell_volume", "stencil_offsets", "stencil", "stencil_lsq_weight")  # fmt: skip
+    mesh = {k: z[k] for k in mesh_keys}
+    for k in mesh_keys[:6]:
+        mesh[k] = int(mesh[k])
+    scheme = {k[len("scheme_"):]: (z[k].tolist()) for k in z if k.startswith("scheme_")}
+    rest = {k: v for k, v in z.items() if k not in mesh_keys and not k.startswith("scheme_")}
+    return mesh, scheme, rest
