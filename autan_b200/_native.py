@@ -125,6 +125,9 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_counters", C.c_int, vp, P(i64), C.c_char_p, sz)
         fn("autan_euler_device_gradients", C.c_int, vp, P(f64), P(f64), C.c_char_p, sz)
         fn("autan_euler_device_time_steps", C.c_int, vp, f64, P(f64), C.c_char_p, sz)
+        fn("autan_euler_device_history", C.c_int, vp, i64, P(f64), P(f64), C.c_char_p, sz)
+        fn("autan_euler_device_kernel_times", C.c_int, vp, f64, f64, i32, i32, i64, P(f64), P(i64),
+           C.c_char_p, sz)  # fmt: skip
 
 
 def lib() -> C.CDLL:

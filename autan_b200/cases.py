@@ -1,0 +1,112 @@
+"""The explicit-step workloads of the path: the convected isentropic vortex on periodic meshes.
+
+- `vortex_hex`: 64 x 64 x 2 hexahedra on [0,10] x [0,10] x [0,0.3125] (8192 cells), periodic in x
+  and y, symmetry (slip) in z; first-order Roe, classical RK4, CFL 0.5, FP64.
+- `vortex_tets`: Kuhn tetrahedra of a 240 x 240 x 6 lattice on [0,10]^2 x [0,0.25] (2 073 600
+  cells) whose nodes move by U(-0.2, 0.2) h (seed 0); second-order LSQ face2 gradient with the
+  Venkatakrishnan limiter (K = 5), HLLC, SSP-RK3, CFL 0.8; FP64 or fp32+acc64.
+
+Initial field: Shu's isentropic vortex of strength beta = 5 centred at (5, 5) on the freestream
+rho = p = 1, u = v = 1, w = 0, gamma = 1.4 (Shu 1998, Lecture Notes in Mathematics 1697, section
+5.2; the reference's vv/src/autan_vv/oracles/inviscid.py:105-181 states the same vortex scaled to
+c = 1): du = beta / (2 pi) e^((1 - r^2) / 2) (-dy, dx), T = 1 - (gamma - 1) beta^2 / (8 gamma pi^2)
+e^(1 - r^2), rho = T^(1 / (gamma - 1)), p = rho T, evaluated at the cell centroids.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from autan_b200 import mesh as M
+from autan_b200.euler import Scheme
+
+GAMMA = 1.4
+FREESTREAM = (1.0, 1.0, 1.0, 0.0, 1.0)  # rho, u, v, w, p
+
+
+def conserved(rho, u, v, w, p, gamma=GAMMA):
+    return np.stack([rho, rho * u, rho * v, rho * w, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)])
+
+
+def freestream_reference(gamma=GAMMA):
+    rho, u, v, w, p = FREESTREAM
+    return tuple(float(x) for x in conserved(np.array(rho), np.array(u), np.array(v), np.array(w),
+                                             np.array(p), gamma))  # fmt: skip
+
+
+def isentropic_vortex(mesh: M.Mesh, beta=5.0, centre=(5.0, 5.0), gamma=GAMMA) -> np.ndarray:
+    """The conserved state (5 x n_cells, images copied from their cells)."""
+    x = mesh.cell_centroid[0] - centre[0]
+    y = mesh.cell_centroid[1] - centre[1]
+    r2 = x * x + y * y
+    f = beta / (2.0 * np.pi) * np.exp(0.5 * (1.0 - r2))
+    u = FREESTREAM[1] - f * y
+    v = FREESTREAM[2] + f * x
+    t = 1.0 - (gamma - 1.0) * beta * beta / (8.0 * gamma * np.pi * np.pi) * np.exp(1.0 - r2)
+    rho = t ** (1.0 / (gamma - 1.0))
+    p = rho * t
+    U = conserved(rho, u, v, np.zeros_like(u), p, gamma)
+    if mesh.n_cells > mesh.n_owned_cells:
+        U[:, mesh.n_owned_cells :] = U[:, mesh.ghost_owner]
+    return np.ascontiguousarray(U)
+
+
+@dataclass
+class Case:
+    name: str
+    mesh: M.Mesh
+    scheme: Scheme
+    bc_kind: np.ndarray
+    bc_data: np.ndarray
+    u0: np.ndarray
+    rk: int
+    cfl: float
+    steps: int
+
+    @property
+    def n_cells(self) -> int:
+        return self.mesh.n_owned_cells
+
+
+def vortex_hex(nx=64, ny=64, nz=2, steps=200, precision="fp64") -> Case:
+    h = 10.0 / nx
+    mesh = M.periodic_box_hex(nx, ny, nz, extent=(10.0, 10.0 * ny / nx, h * nz))
+    scheme = Scheme(flux="roe", second_order=False, limiter=False, reference=freestream_reference(),
+                    precision=precision, planar=bool(mesh.all_planar))  # fmt: skip
+    kind = np.full(mesh.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
+    return Case("vortex-hex", mesh, scheme, kind, np.zeros((5, mesh.n_boundary_faces)),
+                isentropic_vortex(mesh), rk=4, cfl=0.5, steps=steps)  # fmt: skip
+
+
+def vortex_tets(nx=240, ny=240, nz=6, steps=100, precision="fp32+acc64", rcm=True,
+                extent=None) -> Case:  # fmt: skip
+    """The jittered-tetrahedra vortex; smaller lattices keep the cell size (h = 10 / 240) unless
+    `extent` is given, so that parity cases are the same problem on a smaller periodic box."""
+    if extent is None:
+        h = 10.0 / 240
+        extent = (nx * h, ny * h, nz * h)
+    mesh = M.jittered_tets(nx, ny, nz, extent=extent, rcm=rcm)
+    speed = float(np.hypot(FREESTREAM[1], FREESTREAM[2]))
+    scheme = Scheme(flux="hllc", second_order=True, limiter=True, venkat_k=5.0, length=1.0,
+                    scale=(FREESTREAM[0], speed, speed, speed, FREESTREAM[4]),
+                    reference=freestream_reference(), precision=precision,
+                    planar=bool(mesh.all_planar))  # fmt: skip
+    kind = np.full(mesh.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
+    centre = (extent[0] / 2.0, extent[1] / 2.0)
+    return Case("vortex-tets", mesh, scheme, kind, np.zeros((5, mesh.n_boundary_faces)),
+                isentropic_vortex(mesh, centre=centre), rk=3, cfl=0.8, steps=steps)  # fmt: skip
+
+
+def oracle_mesh_dict(case: Case) -> dict:
+    """The case's mesh arrays with its gradient weights, as the oracle takes them."""
+    m = case.mesh
+    d = {k: getattr(m, k) for k in ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+                                    "n_owned_interior_faces", "n_owned_faces")}  # fmt: skip
+    for k in ("owner", "neighbour", "cell_face_offsets", "cell_faces", "ghost_owner",
+              "face_normal", "face_area_magnitude", "face_centroid", "face_moment",
+              "cell_centroid", "cell_volume", "stencil_offsets", "stencil"):  # fmt: skip
+        d[k] = getattr(m, k)
+    d["stencil_lsq_weight"] = m.gradient_weights(case.bc_kind)
+    return d

@@ -1,0 +1,1661 @@
+// The explicit Euler residual-and-update path on B200 (sm_100a), behind the C ABI of
+// include/autan_euler_device.h.
+//
+// Data layout in HBM (owned cells only: a periodic image reads its owned cell's values, so the
+// reference's three ghost fills per residual disappear):
+//   cell arrays      structure of arrays, component k of cell c at k * n + c;
+//   stored states    three buffers S (float in fp32+acc64), rotating through the RK stages;
+//   FP64             u (conserved), stage, RK4 accumulator, residual, volume;
+//   stencil          face2 entries and LSQ weights in a sliced (ELLPACK, 32 cells per slice)
+//                    layout: entry j of cell c at start[c / 32] + 32 j + c % 32, so a warp
+//                    reading entry j of its 32 cells reads 128 contiguous bytes;
+//   incidences       each cell's faces in increasing face index (the reference's scatter order),
+//                    sliced the same way, coded 2 f + side (interior) or -(b + 1) (boundary);
+//   faces            left/right cells, normal, area, and rel(x_f, x_l), rel(x_r) already in the
+//                    compute type (what the bodies' rel() would compute), moments when warped.
+//
+// Kernels per RK stage (see DESIGN.md for the byte counts):
+//   boundary_states  prim_b of every boundary face;
+//   gradients        per cell: LSQ gradient over the stencil (FP64 sums), bounds, then the
+//                    Venkatakrishnan limiter over the cell's faces (fused: wmin/wmax never stored);
+//   faces            per cell: every face flux of the cell recomputed (gather-recompute: no float
+//                    atomics, no face scratch), summed from the source term in face order, then the
+//                    RK stage update in FP64 and the next stored state (fused).
+// Per step: the spectral radius with the global dt (atomicMin on its bits), and the exact-sum
+// residual norms of stage 0. All of it is captured in one CUDA graph per step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "autan_euler_device.h"
+#include "euler_bodies.cuh"
+#include "exact_sum.cuh"
+
+namespace autan_b200 {
+
+struct Fp64 {
+  using C = double;  // compute
+  using S = double;  // state storage
+  using G = double;  // gradient storage
+  using GV = double; // geometry read as values
+};
+struct Fp32Acc64 {
+  using C = float;
+  using S = float;
+  using G = float;
+  using GV = float;
+};
+
+constexpr int kSlice = 32;
+constexpr int kHistory = 4096;
+constexpr int kBlock = 256;
+
+// Step control in device memory: written by the kernels, read by the host after a batch.
+struct Control {
+  unsigned long long dt_bits;    // atomicMin of the positive local steps' bits
+  unsigned long long bad_state;  // least cell with an invalid state (~0: none)
+  unsigned long long bad_res;    // least cell with a non-finite residual
+  long long step;                // steps taken since the last reset
+  double dt;                     // the global step of the current step
+  double rms[5];
+  unsigned long long words[5][kWords];
+  double hist_rms[kHistory][5];
+  double hist_dt[kHistory];
+};
+// The part of Control a step's result needs (read back after every step call).
+constexpr size_t kControlHead = offsetof(Control, words);
+
+template <class P>
+struct Dev {
+  using C = typename P::C;
+  using S = typename P::S;
+  using G = typename P::G;
+  using GV = typename P::GV;
+  int n;      // owned cells
+  int nb;     // boundary faces
+  int n_if;   // owned interior faces
+  long long st_total, inc_total;
+  Params<C> p;
+  double ref[5];
+  // states
+  const S* s;  // stored state read this stage
+  S* s_next;   // stored state written this stage
+  G* grad;
+  S* phi;
+  S* prim_b;
+  // FP64
+  double* u;
+  double* stage;
+  double* racc;
+  double* res;
+  const double* volume;
+  double* dt_local;
+  const S* source;
+  // stencil (sliced)
+  const int* st_start;
+  const int* st_len;
+  const int* st_e;
+  const GV* st_w;
+  // incidences (sliced)
+  const int* inc_start;
+  const int* inc_len;
+  const int* inc_code;
+  // interior faces
+  const int* f_l;
+  const int* f_r;
+  const GV* f_n;
+  const GV* f_a;
+  const C* f_rl;
+  const C* f_rr;
+  const GV* f_m;
+  // boundary faces
+  const int* b_own;
+  const unsigned char* b_kind;
+  const S* b_data;
+  const GV* b_n;
+  const GV* b_a;
+  const C* b_r;
+  const GV* b_m;
+  Control* ctl;
+};
+
+template <class T, class S>
+__device__ __forceinline__ void load5(const S* a, long long stride, long long i, T* v) {
+#pragma unroll
+  for (int k = 0; k < 5; ++k) v[k] = static_cast<T>(__ldg(a + k * stride + i));
+}
+
+template <class P>
+__device__ __forceinline__ void prim_of(const Dev<P>& d, const typename P::S* s, int c,
+                                        typename P::C* w) {
+  typename P::C q[5];
+  load5(s, d.n, c, q);
+  to_primitive(q, d.p, w);
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Euler<P>::state (physics/src/euler.cpp:925-932): s = State(u - U_ref).
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typename P::S* s) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const long long i = static_cast<long long>(k) * d.n + c;
+    s[i] = static_cast<typename P::S>(u[i] - d.ref[k]);
+  }
+}
+
+// boundary_states (kernels/euler.py:455-466): prim_b of every boundary face.
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
+  using C = typename P::C;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  C w[5], data[5], n[3], out[5];
+  prim_of(d, d.s, __ldg(d.b_own + b), w);
+  load5(d.b_data, d.nb, b, data);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
+  boundary_value(w, static_cast<C>(__ldg(d.b_kind + b)), data, n, d.p, out);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) d.prim_b[k * d.nb + b] = static_cast<typename P::S>(out[k]);
+}
+
+// The value across incidence `code` of cell c (a neighbour's primitives or the boundary state),
+// with the face normal and area.
+template <class P>
+__device__ __forceinline__ void across(const Dev<P>& d, int c, int code, typename P::C* wn,
+                                       typename P::C* n, typename P::C& area,
+                                       const typename P::C* rel_unused = nullptr) {
+  using C = typename P::C;
+  if (code >= 0) {
+    const int f = code >> 1;
+    const int o = (code & 1) ? __ldg(d.f_l + f) : __ldg(d.f_r + f);
+    prim_of(d, d.s, o, wn);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.f_n + static_cast<long long>(a) * d.n_if + f));
+    area = static_cast<C>(__ldg(d.f_a + f));
+  } else {
+    const int b = -code - 1;
+    load5(d.prim_b, d.nb, b, wn);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
+    area = static_cast<C>(__ldg(d.b_a + b));
+  }
+  (void)c;
+  (void)rel_unused;
+}
+
+// gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the
+// LSQ gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell,
+// then phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)).
+template <class P, bool LIMIT>
+__global__ void __launch_bounds__(kBlock) k_gradients(Dev<P> d) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  C wc[5];
+  prim_of(d, d.s, c, wc);
+  double acc[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+  C lo[5], hi[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    lo[k] = C(INFINITY);
+    hi[k] = -C(INFINITY);
+  }
+  const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
+  const int len = __ldg(d.st_len + c);
+  for (int j = 0; j < len; ++j) {
+    const long long idx = base + static_cast<long long>(j) * kSlice;
+    const int e = __ldg(d.st_e + idx);
+    C wn[5];
+    if (e >= 0) {
+      prim_of(d, d.s, e, wn);
+    } else {
+      load5(d.prim_b, d.nb, -e - 1, wn);
+    }
+    const C w0 = static_cast<C>(__ldg(d.st_w + idx));
+    const C w1 = static_cast<C>(__ldg(d.st_w + d.st_total + idx));
+    const C w2 = static_cast<C>(__ldg(d.st_w + 2 * d.st_total + idx));
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const C dw = wn[i] - wc[i];
+      acc[3 * i] += static_cast<double>(dw * w0);
+      acc[3 * i + 1] += static_cast<double>(dw * w1);
+      acc[3 * i + 2] += static_cast<double>(dw * w2);
+    }
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      if (wn[i] < lo[i]) lo[i] = wn[i];
+      if (wn[i] > hi[i]) hi[i] = wn[i];
+    }
+  }
+  // include_own_value (:517-521)
+  C g[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) {
+    g[k] = static_cast<C>(acc[k]);
+    d.grad[static_cast<long long>(k) * d.n + c] = static_cast<typename P::G>(g[k]);
+  }
+  if constexpr (LIMIT) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      lo[i] = minv(lo[i], wc[i]);
+      hi[i] = maxv(hi[i], wc[i]);
+    }
+    const C vol = static_cast<C>(static_cast<typename P::GV>(__ldg(d.volume + c)));
+    C phi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
+    const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+    const int il = __ldg(d.inc_len + c);
+    for (int j = 0; j < il; ++j) {
+      const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+      C r[3];
+      if (code >= 0) {
+        const int f = code >> 1;
+        const C* rr = (code & 1) ? d.f_rr : d.f_rl;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = __ldg(rr + static_cast<long long>(a) * d.n_if + f);
+      } else {
+        const int b = -code - 1;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = __ldg(d.b_r + a * d.nb + b);
+      }
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+        const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+        if (v < phi[i]) phi[i] = v;
+      }
+    }
+    // at_most_one (:591-593)
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+      d.phi[static_cast<long long>(i) * d.n + c] = static_cast<typename P::S>(minv(phi[i], C(1.0)));
+  }
+}
+
+// spectral_radius (kernels/euler.py:1103-1112) and the CFL step of each cell
+// (device_stepper.cuh:84-89): lambda_c = sum over its faces of max(|v . n| + c) A (FP64 sum,
+// stored as State), dt_c = (cfl V) / lambda_c; the global step is their minimum (atomicMin on the
+// bits of positive doubles, exact and order-free).
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int local,
+                                                     double* dt_out) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  C wc[5];
+  prim_of(d, d.s, c, wc);
+  double acc = 0.0;
+  const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+  const int il = __ldg(d.inc_len + c);
+  for (int j = 0; j < il; ++j) {
+    const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+    C wn[5], n[3], area;
+    across(d, c, code, wn, n, area);
+    acc += static_cast<double>(wave_speed(wc, wn, n, area, d.p.g, d.p.pref));
+  }
+  const double lam = static_cast<double>(static_cast<typename P::S>(acc));
+  const double dt = cfl * d.volume[c] / lam;
+  if (local && d.dt_local != nullptr) d.dt_local[c] = dt;
+  if (dt_out != nullptr) dt_out[c] = dt;
+  if (d.ctl != nullptr && dt > 0.0)
+    atomicMin(&d.ctl->dt_bits, static_cast<unsigned long long>(__double_as_longlong(dt)));
+}
+
+enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
+
+// The faces of one owned cell (roe/hllc/ausm _faces and _boundaries, kernels/euler.py:687-1049),
+// gathered: every face flux of the cell recomputed here, added in increasing face index from the
+// source term -V s, as the reference's scatter adds them (emit_cpu.py emit_loop); then, in the RK
+// modes, the stage update in FP64 and the next stored state.
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage, double wa,
+                                                  double wb, int local, int last) {
+  using C = typename P::C;
+  using S = typename P::S;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  C wc[5], gc[15], pc[5];
+  prim_of(d, d.s, c, wc);
+  if constexpr (SECOND) {
+#pragma unroll
+    for (int k = 0; k < 15; ++k) gc[k] = static_cast<C>(__ldg(d.grad + static_cast<long long>(k) * d.n + c));
+    load5(d.phi, d.n, c, pc);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 15; ++k) gc[k] = C(0.0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) pc[k] = C(0.0);
+  }
+  const double vol = __ldg(d.volume + c);
+  // sources (:611-616): res = -V s, computed in the compute type, stored in FP64.
+  double res[5];
+  {
+    const C nv = -static_cast<C>(static_cast<typename P::GV>(vol));
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const C s = d.source != nullptr ? static_cast<C>(__ldg(d.source + static_cast<long long>(k) * d.n + c)) : C(0.0);
+      res[k] = static_cast<double>(nv * s);
+    }
+  }
+  const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+  const int il = __ldg(d.inc_len + c);
+  for (int j = 0; j < il; ++j) {
+    const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+    C out[5];
+    if (code >= 0) {
+      const int f = code >> 1;
+      const bool left = (code & 1) == 0;
+      const int o = left ? __ldg(d.f_r + f) : __ldg(d.f_l + f);
+      C wo[5], go[15], po[5];
+      prim_of(d, d.s, o, wo);
+      if constexpr (SECOND) {
+#pragma unroll
+        for (int k = 0; k < 15; ++k) go[k] = static_cast<C>(__ldg(d.grad + static_cast<long long>(k) * d.n + o));
+        load5(d.phi, d.n, o, po);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 15; ++k) go[k] = C(0.0);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) po[k] = C(0.0);
+      }
+      C n[3], rl[3], rr[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const long long i = static_cast<long long>(a) * d.n_if + f;
+        n[a] = static_cast<C>(__ldg(d.f_n + i));
+        rl[a] = __ldg(d.f_rl + i);
+        rr[a] = __ldg(d.f_rr + i);
+      }
+      const C area = static_cast<C>(__ldg(d.f_a + f));
+      const C* wl = left ? wc : wo;
+      const C* gl = left ? gc : go;
+      const C* pl = left ? pc : po;
+      const C* wr = left ? wo : wc;
+      const C* gr = left ? go : gc;
+      const C* pr = left ? po : pc;
+      C fl[5], fr[5], fx[5];
+      reconstruct(wl, gl, pl, rl, d.p.pref, fl);
+      reconstruct(wr, gr, pr, rr, d.p.pref, fr);
+      numerical_flux<FLUX>(fl, fr, n, d.p, fx);
+      if constexpr (PLANAR) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
+      } else {
+        C m[9], avg[5], wt[5];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) m[q] = static_cast<C>(__ldg(d.f_m + static_cast<long long>(q) * d.n_if + f));
+#pragma unroll
+        for (int k = 0; k < 5; ++k) avg[k] = C(0.5) * (fl[k] + fr[k]);
+        warp_term(avg, gl, pl, gr, pr, m, d.p.g, d.p.pref, wt);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = area * fx[k] + wt[k];
+      }
+      if (left) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) res[k] -= static_cast<double>(out[k]);
+      }
+    } else {
+      const int b = -code - 1;
+      C n[3], r[3], data[5], wf[5], wbv[5];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
+        r[a] = __ldg(d.b_r + a * d.nb + b);
+      }
+      load5(d.b_data, d.nb, b, data);
+      const C kind = static_cast<C>(__ldg(d.b_kind + b));
+      const C area = static_cast<C>(__ldg(d.b_a + b));
+      reconstruct(wc, gc, pc, r, d.p.pref, wf);
+      const bool slip = (kind > C(1.5)) & (kind < C(2.5));
+      const bool wall = PLANAR ? slip : (slip | (kind > C(4.5)));
+      if (wall) {
+        const C wfl[5] = {C(0.0), wf[4] * n[0], wf[4] * n[1], wf[4] * n[2], C(0.0)};
+        if constexpr (PLANAR) {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) out[k] = area * wfl[k];
+        } else {
+          C m[9];
+#pragma unroll
+          for (int q = 0; q < 9; ++q) m[q] = static_cast<C>(__ldg(d.b_m + static_cast<long long>(q) * d.nb + b));
+          // wall_warp (:678-681): p_l M^T grad p.
+          C ww[5] = {C(0.0), C(0.0), C(0.0), C(0.0), C(0.0)};
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+            ww[1 + i] = pc[4] * (m[i] * gc[12] + m[3 + i] * gc[13] + m[6 + i] * gc[14]);
+#pragma unroll
+          for (int k = 0; k < 5; ++k) out[k] = area * wfl[k] + ww[k];
+        }
+      } else {
+        boundary_value(wf, kind, data, n, d.p, wbv);
+        C fx[5];
+        numerical_flux<FLUX>(wf, wbv, n, d.p, fx);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
+    }
+  }
+  if (mode == kResidual || stage == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
+  }
+  if (mode == kResidual) return;
+  const double h = local ? d.dt_local[c] : d.ctl->dt;
+  double nu[5];
+  if (mode == kRk3) {
+    // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const long long i = static_cast<long long>(k) * d.n + c;
+      const double uk = d.u[i];
+      const double sk = stage == 0 ? uk : d.stage[i];
+      const double next = sk - h / vol * res[k];
+      nu[k] = wa * uk + wb * next;
+    }
+  } else {
+    // Classical RK4: stage_s = u - ((c_s h) / V) R_s; u = u - ((h / 6) / V) (R_0 + 2 R_1 + 2 R_2 + R_3).
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const long long i = static_cast<long long>(k) * d.n + c;
+      const double uk = d.u[i];
+      double a;
+      if (stage == 0) {
+        a = res[k];
+      } else if (stage < 3) {
+        a = d.racc[i] + 2.0 * res[k];
+      } else {
+        a = d.racc[i] + res[k];
+      }
+      if (stage < 3) {
+        d.racc[i] = a;
+        nu[k] = uk - wa * h / vol * res[k];
+      } else {
+        nu[k] = uk - h / 6.0 / vol * a;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const long long i = static_cast<long long>(k) * d.n + c;
+    if (last) {
+      d.u[i] = nu[k];
+    } else if (mode == kRk3) {
+      d.stage[i] = nu[k];
+    }
+    d.s_next[i] = static_cast<S>(nu[k] - d.ref[k]);
+  }
+  if (last) {
+    // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
+    // it, in the compute type, then this stage's residual.
+    const C g = d.p.g;
+    const C r0 = static_cast<C>(d.ref[0]);
+    C dq[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(static_cast<S>(nu[k] - d.ref[k]));
+    const C rho = r0 + dq[0];
+    C dm_m = C(0), mr_mr = C(0);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const C mr = static_cast<C>(d.ref[k + 1]);
+      dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
+      mr_mr = mr_mr + mr * mr;
+    }
+    const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
+    const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
+    const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
+                     !(rho > C(0)) || !(pr > C(0));
+    if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
+    bool badr = false;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) badr = badr || !isfinite(res[k]);
+    if (badr) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(c));
+  }
+}
+
+// The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176).
+__global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, Control* ctl) {
+  __shared__ unsigned long long sh[5 * kWords];
+  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < n; base += stride) {
+    const long long c = base + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+      warp_exact_add(sh + k * kWords, r * r);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+    const unsigned long long v = sh[i];
+    if (v != 0) atomicAdd(&ctl->words[i / kWords][i % kWords], v);
+  }
+}
+
+// record_norms (euler_physics.cpp:1040-1054): rms_k = sqrt(sum / N); the step's history entry.
+__global__ void k_norm_finish(Control* ctl, int n, int record) {
+  const int k = threadIdx.x;
+  __shared__ double rms[5];
+  if (k < 5) rms[k] = sqrt(exact_value(ctl->words[k]) / static_cast<double>(n));
+  __syncthreads();
+  if (k == 0) {
+    const long long slot = ctl->step % kHistory;
+    for (int q = 0; q < 5; ++q) {
+      ctl->rms[q] = rms[q];
+      if (record) ctl->hist_rms[slot][q] = rms[q];
+    }
+    if (record) ctl->hist_dt[slot] = ctl->dt;
+  }
+}
+
+// The start of a step: clears the sums and the validity marks, sets the global step (fixed) or
+// prepares its minimum (CFL).
+__global__ void k_begin(Control* ctl, double dt_fixed) {
+  const int t = threadIdx.x;
+  for (int i = t; i < 5 * kWords; i += blockDim.x) (&ctl->words[0][0])[i] = 0;
+  if (t == 0) {
+    ctl->dt_bits = dt_fixed > 0.0 ? static_cast<unsigned long long>(__double_as_longlong(dt_fixed))
+                                  : 0x7ff0000000000000ULL;
+    ctl->bad_state = ~0ULL;
+    ctl->bad_res = ~0ULL;
+  }
+}
+
+// The global step from its minimum's bits.
+__global__ void k_take_dt(Control* ctl) {
+  if (threadIdx.x == 0) ctl->dt = __longlong_as_double(static_cast<long long>(ctl->dt_bits));
+}
+
+__global__ void k_end_step(Control* ctl) {
+  if (threadIdx.x == 0) ctl->step += 1;
+}
+
+template <class P>
+__global__ void k_to_double(const typename P::G* a, long long n, double* out) {
+  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (i < n) out[i] = static_cast<double>(a[i]);
+}
+
+// ---------------------------------------------------------------- host side
+
+struct Failure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+[[noreturn]] void fail(const std::string& what) { throw Failure(what); }
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(std::string("E1200: ") + what + ": " + cudaGetErrorString(e));
+}
+
+class Buffer {
+ public:
+  Buffer() = default;
+  explicit Buffer(size_t bytes) { alloc(bytes); }
+  Buffer(const Buffer&) = delete;
+  Buffer& operator=(const Buffer&) = delete;
+  Buffer(Buffer&& o) noexcept : p_(o.p_), n_(o.n_) {
+    o.p_ = nullptr;
+    o.n_ = 0;
+  }
+  Buffer& operator=(Buffer&& o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+    return *this;
+  }
+  ~Buffer() {
+    if (p_ != nullptr) cudaFree(p_);
+  }
+  void alloc(size_t bytes) {
+    if (p_ != nullptr) cudaFree(p_);
+    p_ = nullptr;
+    n_ = bytes;
+    if (bytes > 0) check(cudaMalloc(&p_, bytes), "cudaMalloc");
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p_);
+  }
+  void* ptr() const { return p_; }
+  size_t bytes() const { return n_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+template <class T>
+Buffer upload(const std::vector<T>& v, cudaStream_t s) {
+  Buffer b(v.size() * sizeof(T));
+  if (!v.empty()) check(cudaMemcpyAsync(b.as<void>(), v.data(), v.size() * sizeof(T),
+                                        cudaMemcpyHostToDevice, s), "upload");  // NOLINT
+  return b;
+}
+
+// Sliced (ELLPACK by slices of 32) positions of CSR rows.
+struct Sliced {
+  std::vector<int> start;  // per slice
+  std::vector<int> len;    // per row
+  long long total = 0;
+  long long at(int row, int j) const {
+    return static_cast<long long>(start[row / kSlice]) + static_cast<long long>(j) * kSlice +
+           row % kSlice;
+  }
+};
+
+Sliced slice_rows(const std::vector<long long>& off) {
+  Sliced s;
+  const int n = static_cast<int>(off.size()) - 1;
+  s.len.resize(n);
+  s.start.resize((n + kSlice - 1) / kSlice + 1);
+  long long run = 0;
+  for (int sl = 0; sl * kSlice < n; ++sl) {
+    long long longest = 0;
+    for (int l = 0; l < kSlice && sl * kSlice + l < n; ++l) {
+      const int r = sl * kSlice + l;
+      s.len[r] = static_cast<int>(off[r + 1] - off[r]);
+      longest = std::max(longest, off[r + 1] - off[r]);
+    }
+    if (run > std::numeric_limits<int>::max()) fail("E1101: stencil too large for int32 offsets");
+    s.start[sl] = static_cast<int>(run);
+    run += longest * kSlice;
+  }
+  s.start.back() = static_cast<int>(std::min<long long>(run, std::numeric_limits<int>::max()));
+  s.total = run;
+  if (run >= std::numeric_limits<int>::max()) fail("E1101: stencil too large for int32 offsets");
+  return s;
+}
+
+struct Counters {
+  long long launches = 0, steps = 0, residuals = 0;
+};
+
+class Stepper {
+ public:
+  virtual ~Stepper() = default;
+  virtual void set_boundary(const uint8_t* kind, const double* data) = 0;
+  virtual void set_boundary_data(const double* data) = 0;
+  virtual void set_source(const double* source) = 0;
+  virtual void set_second_order(bool on) = 0;
+  virtual void upload_state(const double* u) = 0;
+  virtual void download_state(double* u) = 0;
+  virtual void residual(const double* u, double* res) = 0;
+  virtual void step(double cfl, double dt, bool local, int rk, long long n, bool graph,
+                    autan_euler_step_result* out) = 0;
+  virtual void evaluate(autan_euler_step_result* out) = 0;
+  virtual void history(long long count, double* rms, double* dt) = 0;
+  virtual void gradients(double* grad, double* phi) = 0;
+  virtual void time_steps(double cfl, double* dt) = 0;
+  virtual long long device_bytes() const = 0;
+  virtual void kernel_times(double cfl, double dt, bool local, int rk, long long n, double* ms,
+                            long long* launches) = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  Counters counters;
+};
+
+template <class P>
+class Impl final : public Stepper {
+  using C = typename P::C;
+  using S = typename P::S;
+  using G = typename P::G;
+  using GV = typename P::GV;
+
+ public:
+  Impl(const autan_euler_mesh& m, const autan_euler_scheme& sc, cudaStream_t st)
+      : scheme_(sc), planar_(sc.planar != 0), second_(sc.second_order != 0),
+        limiter_(sc.limiter != 0) {
+    stream = st;
+    nc_ = m.n_cells;
+    n_ = m.n_owned_cells;
+    nf_ = m.n_faces;
+    ni_ = m.n_interior_faces;
+    nif_ = m.n_owned_interior_faces;
+    nb_ = m.n_faces - m.n_interior_faces;
+    validate(m);
+    // Value index of every mesh cell: owned cells themselves, images their owned cell.
+    std::vector<int> val(nc_);
+    for (int c = 0; c < n_; ++c) val[c] = c;
+    for (int g = n_; g < nc_; ++g) {
+      const int o = m.ghost_owner[g - n_];
+      if (o < 0 || o >= n_) fail("E1101: a ghost cell's owner is not an owned cell");
+      val[g] = o;
+    }
+    // Parameters (physics/src/euler.cpp:229-245).
+    const double* r = sc.reference;
+    if (!(r[0] > 0.0)) fail("E1101: reference density must be positive");
+    if (!(sc.mach_ref > 0.0)) fail("E1101: AUSM+-up needs a positive cut-off Mach number");
+    const double p_ref =
+        (sc.gamma - 1.0) * (r[4] - 0.5 * (r[1] * r[1] + r[2] * r[2] + r[3] * r[3]) / r[0]);
+    const double k3 = std::pow(sc.venkat_k / sc.length, 3);
+    Params<C>& p = d_.p;
+    p.g = static_cast<C>(sc.gamma);
+    p.rgas = static_cast<C>(sc.gas_constant);
+    p.pref = static_cast<C>(p_ref);
+    p.minf = static_cast<C>(sc.mach_ref);
+    for (int k = 0; k < 5; ++k) {
+      p.ur[k] = static_cast<C>(r[k]);
+      p.scale[k] = static_cast<C>(k3 * sc.scale[k] * sc.scale[k]);
+      d_.ref[k] = r[k];
+    }
+    if (planar_ && m.face_moment != nullptr) {
+      for (long long i = 0; i < 9LL * nf_; ++i)
+        if (m.face_moment[i] != 0.0)
+          fail("E1101: planar loops on a mesh with a face not proven planar");
+    }
+    // Interior faces touching owned cells.
+    std::vector<int> fl(nif_), fr(nif_);
+    std::vector<GV> fn(3LL * nif_), fa(nif_), fm(planar_ ? 0 : 9LL * nif_);
+    std::vector<C> frl(3LL * nif_), frr(3LL * nif_);
+    for (int f = 0; f < nif_; ++f) {
+      const int l = m.owner[f], rr = m.neighbour[f];
+      fl[f] = val[l];
+      fr[f] = val[rr];
+      for (int a = 0; a < 3; ++a) {
+        fn[a * static_cast<long long>(nif_) + f] = static_cast<GV>(m.face_normal[a * static_cast<long long>(nf_) + f]);
+        const double xf = m.face_centroid[a * static_cast<long long>(nf_) + f];
+        frl[a * static_cast<long long>(nif_) + f] = static_cast<C>(xf - m.cell_centroid[a * static_cast<long long>(nc_) + l]);
+        frr[a * static_cast<long long>(nif_) + f] = static_cast<C>(xf - m.cell_centroid[a * static_cast<long long>(nc_) + rr]);
+      }
+      fa[f] = static_cast<GV>(m.face_area_magnitude[f]);
+      if (!planar_)
+        for (int q = 0; q < 9; ++q)
+          fm[q * static_cast<long long>(nif_) + f] =
+              m.face_moment != nullptr ? static_cast<GV>(m.face_moment[q * static_cast<long long>(nf_) + f]) : GV(0);
+    }
+    // Boundary faces (all of them: the stencils of owned cells reach those of images).
+    std::vector<int> bown(nb_);
+    std::vector<GV> bn(3LL * nb_), ba(nb_), bm(planar_ ? 0 : 9LL * nb_);
+    std::vector<C> br(3LL * nb_);
+    for (int b = 0; b < nb_; ++b) {
+      const int f = ni_ + b;
+      const int o = m.owner[f];
+      bown[b] = val[o];
+      for (int a = 0; a < 3; ++a) {
+        bn[a * static_cast<long long>(nb_) + b] = static_cast<GV>(m.face_normal[a * static_cast<long long>(nf_) + f]);
+        br[a * static_cast<long long>(nb_) + b] = static_cast<C>(m.face_centroid[a * static_cast<long long>(nf_) + f] -
+                                                                 m.cell_centroid[a * static_cast<long long>(nc_) + o]);
+      }
+      ba[b] = static_cast<GV>(m.face_area_magnitude[f]);
+      if (!planar_)
+        for (int q = 0; q < 9; ++q)
+          bm[q * static_cast<long long>(nb_) + b] =
+              m.face_moment != nullptr ? static_cast<GV>(m.face_moment[q * static_cast<long long>(nf_) + f]) : GV(0);
+    }
+    // Incidences of owned cells, in increasing face index, sliced.
+    std::vector<long long> ioff(n_ + 1);
+    for (int c = 0; c <= n_; ++c) ioff[c] = m.cell_face_offsets[c];
+    inc_ = slice_rows(ioff);
+    std::vector<int> code(std::max<long long>(inc_.total, 1), 0);
+    for (int c = 0; c < n_; ++c) {
+      int prev = -1;
+      for (long long k = ioff[c]; k < ioff[c + 1]; ++k) {
+        const int f = m.cell_faces[k];
+        if (f <= prev) fail("E1101: cell_faces must list each cell's faces in increasing order");
+        prev = f;
+        int v;
+        if (f < ni_) {
+          if (f >= nif_) fail("E1101: an owned cell's interior face lies beyond the owned faces");
+          if (m.owner[f] == c) {
+            v = 2 * f;
+          } else if (m.neighbour[f] == c) {
+            v = 2 * f + 1;
+          } else {
+            fail("E1101: cell_faces lists a face of another cell");
+          }
+        } else {
+          if (f >= m.n_owned_faces) fail("E1101: an owned cell's boundary face lies beyond the owned faces");
+          if (m.owner[f] != c) fail("E1101: cell_faces lists a boundary face of another cell");
+          v = -(f - ni_ + 1);
+        }
+        code[inc_.at(c, static_cast<int>(k - ioff[c]))] = v;
+      }
+    }
+    // Stencil of owned cells, sliced: values at the owned cell of an image.
+    const bool has_stencil =
+        m.stencil != nullptr && m.stencil_offsets != nullptr && m.stencil_lsq_weight != nullptr;
+    std::vector<long long> soff(n_ + 1, 0);
+    if (has_stencil)
+      for (int c = 0; c <= n_; ++c) soff[c] = m.stencil_offsets[c] - m.stencil_offsets[0];
+    st_ = slice_rows(soff);
+    const long long nst = has_stencil ? m.stencil_offsets[nc_] : 0;
+    std::vector<int> ste(std::max<long long>(st_.total, 1), 0);
+    std::vector<GV> stw(3 * std::max<long long>(st_.total, 1), GV(0));
+    for (int c = 0; c < (has_stencil ? n_ : 0); ++c) {
+      for (long long k = m.stencil_offsets[c]; k < m.stencil_offsets[c + 1]; ++k) {
+        const int e = m.stencil[k];
+        int v;
+        if (e >= 0) {
+          if (e >= nc_) fail("E1101: a stencil entry is out of range");
+          v = val[e];
+        } else {
+          const int f = -e - 1;
+          if (f < ni_ || f >= nf_) fail("E1101: a stencil entry is not a boundary face");
+          v = -(f - ni_ + 1);
+        }
+        const long long at = st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
+        ste[at] = v;
+        for (int a = 0; a < 3; ++a)
+          stw[a * st_.total + at] = static_cast<GV>(m.stencil_lsq_weight[a * nst + k]);
+      }
+    }
+    std::vector<double> vol(m.cell_volume, m.cell_volume + n_);
+    // Device arrays.
+    const size_t n5 = 5ULL * n_;
+    for (auto& b : s_) b.alloc(n5 * sizeof(S));
+    grad_.alloc(15ULL * n_ * sizeof(G));
+    phi_.alloc(n5 * sizeof(S));
+    prim_b_.alloc(5ULL * std::max(nb_, 1) * sizeof(S));
+    u_.alloc(n5 * sizeof(double));
+    stage_.alloc(n5 * sizeof(double));
+    racc_.alloc(n5 * sizeof(double));
+    res_.alloc(n5 * sizeof(double));
+    dt_local_.alloc(std::max(n_, 1) * sizeof(double));
+    ctl_.alloc(sizeof(Control));
+    volume_ = upload(vol, stream);
+    st_start_ = upload(st_.start, stream);
+    st_len_ = upload(st_.len, stream);
+    st_e_ = upload(ste, stream);
+    st_w_ = upload(stw, stream);
+    inc_start_ = upload(inc_.start, stream);
+    inc_len_ = upload(inc_.len, stream);
+    inc_code_ = upload(code, stream);
+    f_l_ = upload(fl, stream);
+    f_r_ = upload(fr, stream);
+    f_n_ = upload(fn, stream);
+    f_a_ = upload(fa, stream);
+    f_rl_ = upload(frl, stream);
+    f_rr_ = upload(frr, stream);
+    f_m_ = upload(fm, stream);
+    b_own_ = upload(bown, stream);
+    b_n_ = upload(bn, stream);
+    b_a_ = upload(ba, stream);
+    b_r_ = upload(br, stream);
+    b_m_ = upload(bm, stream);
+    std::vector<unsigned char> kind(std::max(nb_, 1), 2);
+    b_kind_ = upload(kind, stream);
+    b_data_.alloc(5ULL * std::max(nb_, 1) * sizeof(S));
+    check(cudaMemsetAsync(b_data_.as<void>(), 0, b_data_.bytes(), stream), "memset");
+    for (auto* b : {&grad_, &phi_, &prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
+      check(cudaMemsetAsync(b->ptr(), 0, b->bytes(), stream), "memset");
+    for (auto& b : s_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
+    if (second_ && !limiter_) fill_phi_one();
+    d_.n = n_;
+    d_.nb = nb_;
+    d_.n_if = nif_;
+    d_.st_total = st_.total;
+    d_.inc_total = inc_.total;
+    d_.grad = grad_.as<G>();
+    d_.phi = phi_.as<S>();
+    d_.prim_b = prim_b_.as<S>();
+    d_.u = u_.as<double>();
+    d_.stage = stage_.as<double>();
+    d_.racc = racc_.as<double>();
+    d_.res = res_.as<double>();
+    d_.volume = volume_.as<double>();
+    d_.dt_local = dt_local_.as<double>();
+    d_.source = nullptr;
+    d_.st_start = st_start_.as<int>();
+    d_.st_len = st_len_.as<int>();
+    d_.st_e = st_e_.as<int>();
+    d_.st_w = st_w_.as<GV>();
+    d_.inc_start = inc_start_.as<int>();
+    d_.inc_len = inc_len_.as<int>();
+    d_.inc_code = inc_code_.as<int>();
+    d_.f_l = f_l_.as<int>();
+    d_.f_r = f_r_.as<int>();
+    d_.f_n = f_n_.as<GV>();
+    d_.f_a = f_a_.as<GV>();
+    d_.f_rl = f_rl_.as<C>();
+    d_.f_rr = f_rr_.as<C>();
+    d_.f_m = f_m_.as<GV>();
+    d_.b_own = b_own_.as<int>();
+    d_.b_kind = b_kind_.as<unsigned char>();
+    d_.b_data = b_data_.as<S>();
+    d_.b_n = b_n_.as<GV>();
+    d_.b_a = b_a_.as<GV>();
+    d_.b_r = b_r_.as<C>();
+    d_.b_m = b_m_.as<GV>();
+    d_.ctl = ctl_.as<Control>();
+    check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
+    check(cudaStreamSynchronize(stream), "create");
+  }
+
+  ~Impl() override {
+    drop_graph();
+    if (head_ != nullptr) cudaFreeHost(head_);
+  }
+
+  long long device_bytes() const override {
+    long long t = 0;
+    for (const Buffer* b : {&grad_, &phi_, &prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_,
+                            &ctl_, &volume_, &st_start_, &st_len_, &st_e_, &st_w_, &inc_start_,
+                            &inc_len_, &inc_code_, &f_l_, &f_r_, &f_n_, &f_a_, &f_rl_, &f_rr_,
+                            &f_m_, &b_own_, &b_kind_, &b_data_, &b_n_, &b_a_, &b_r_, &b_m_,
+                            &source_})
+      t += static_cast<long long>(b->bytes());
+    for (const auto& b : s_) t += static_cast<long long>(b.bytes());
+    return t;
+  }
+
+  void set_boundary(const uint8_t* kind, const double* data) override {
+    std::vector<unsigned char> k(std::max(nb_, 1), 2);
+    for (int b = 0; b < nb_; ++b) {
+      if (kind[b] > 5) fail("E1101: boundary code out of range");
+      k[b] = kind[b];
+    }
+    b_kind_ = upload(k, stream);
+    d_.b_kind = b_kind_.as<unsigned char>();
+    set_boundary_data(data);
+    drop_graph();
+  }
+
+  void set_boundary_data(const double* data) override {
+    std::vector<S> v(5ULL * std::max(nb_, 1), S(0));
+    for (long long i = 0; i < 5LL * nb_; ++i) v[i] = static_cast<S>(data[i]);
+    check(cudaMemcpyAsync(b_data_.as<void>(), v.data(), v.size() * sizeof(S),
+                          cudaMemcpyHostToDevice, stream), "boundary data");
+    check(cudaStreamSynchronize(stream), "boundary data");
+  }
+
+  void set_source(const double* source) override {
+    std::vector<S> v(5ULL * n_);
+    bool any = false;
+    for (int k = 0; k < 5; ++k)
+      for (int c = 0; c < n_; ++c) {
+        v[k * static_cast<long long>(n_) + c] = static_cast<S>(source[k * static_cast<long long>(nc_) + c]);
+        any = any || v[k * static_cast<long long>(n_) + c] != S(0);
+      }
+    if (!any) {
+      source_ = Buffer();
+      d_.source = nullptr;
+    } else {
+      source_ = upload(v, stream);
+      d_.source = source_.as<S>();
+      check(cudaStreamSynchronize(stream), "source");
+    }
+    drop_graph();
+  }
+
+  void set_second_order(bool on) override {
+    second_ = on;
+    // As the host (physics/src/euler.cpp:903-912): without reconstruction gradients and limiter
+    // are zero; unlimited, phi is 1.
+    check(cudaMemsetAsync(grad_.as<void>(), 0, grad_.bytes(), stream), "grad");
+    if (on && !limiter_) {
+      fill_phi_one();
+    } else {
+      check(cudaMemsetAsync(phi_.as<void>(), 0, phi_.bytes(), stream), "phi");
+    }
+    drop_graph();
+  }
+
+  // Host state (5 x n_cells, caller-owned; pinned memory makes the copies asynchronous DMA):
+  // one copy per component, of the owned cells.
+  void copy_in(const double* host, double* dev) {
+    const size_t per = static_cast<size_t>(n_) * sizeof(double);
+    for (int k = 0; k < 5; ++k)
+      check(cudaMemcpyAsync(dev + k * static_cast<long long>(n_), host + k * static_cast<long long>(nc_),
+                            per, cudaMemcpyHostToDevice, stream), "upload");
+  }
+  void copy_out(const double* dev, double* host) {
+    const size_t per = static_cast<size_t>(n_) * sizeof(double);
+    for (int k = 0; k < 5; ++k)
+      check(cudaMemcpyAsync(host + k * static_cast<long long>(nc_), dev + k * static_cast<long long>(n_),
+                            per, cudaMemcpyDeviceToHost, stream), "download");
+    check(cudaStreamSynchronize(stream), "download");
+    for (int k = 0; k < 5; ++k)
+      for (int g = n_; g < nc_; ++g)
+        host[k * static_cast<long long>(nc_) + g] = host[k * static_cast<long long>(nc_) + ghost_owner_[g - n_]];
+  }
+
+  void upload_state(const double* u) override {
+    copy_in(u, u_.as<double>());
+    launch_store(u_.as<double>(), s_[0].as<S>());
+    check(cudaStreamSynchronize(stream), "upload");
+  }
+
+  void download_state(double* u) override { copy_out(u_.as<double>(), u); }
+
+  void residual(const double* u, double* res) override {
+    copy_in(u, stage_.as<double>());
+    launch_store(stage_.as<double>(), s_[1].as<S>());
+    enqueue_residual(s_[1].as<S>());
+    copy_out(res_.as<double>(), res);
+    for (int k = 0; k < 5; ++k)
+      for (int g = n_; g < nc_; ++g) res[k * static_cast<long long>(nc_) + g] = 0.0;
+  }
+
+  void evaluate(autan_euler_step_result* out) override {
+    launch(k_begin, 1, 256, d_.ctl, 1.0);
+    enqueue_residual(s_[0].as<S>());
+    launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+    launch(k_norm_finish, 1, 32, d_.ctl, n_, 0);
+    Control h;
+    read_control(&h);
+    for (int k = 0; k < 5; ++k) out->residuals[k] = h.rms[k];
+    out->time_step = 0.0;
+    out->steps = 0;
+    // invalid(): the state, then the residual.
+    std::vector<double> u(5ULL * n_), r(5ULL * n_);
+    check(cudaMemcpyAsync(u.data(), u_.as<void>(), u.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
+    check(cudaMemcpyAsync(r.data(), res_.as<void>(), r.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
+    check(cudaStreamSynchronize(stream), "evaluate");
+    out->invalid_cell = first_invalid(u, r);
+  }
+
+  void step(double cfl, double dt, bool local, int rk, long long n, bool graph,
+            autan_euler_step_result* out) override {
+    if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
+    if (n < 1) fail("E1101: n_steps must be positive");
+    if (!(dt > 0.0) && !(cfl > 0.0)) fail("E1101: a positive dt or CFL is needed");
+    // Reset the step count so that the history holds this call's steps.
+    check(cudaMemsetAsync(&d_.ctl->step, 0, sizeof(long long), stream), "reset");
+    const StepKey key{cfl, dt, local, rk};
+    if (graph) {
+      if (!graph_exec_ || !(key == graph_key_)) capture(key);
+      for (long long i = 0; i < n; ++i) {
+        check(cudaGraphLaunch(graph_exec_, stream), "cudaGraphLaunch");
+        counters.launches += graph_nodes_;
+      }
+    } else {
+      for (long long i = 0; i < n; ++i) enqueue_step(key);
+    }
+    counters.steps += n;
+    // The result: the control's head (the last step's sums, step and marks) only.
+    Control* h = head_;
+    check(cudaMemcpyAsync(h, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
+    check(cudaStreamSynchronize(stream), "control");
+    for (int k = 0; k < 5; ++k) out->residuals[k] = h->rms[k];
+    out->time_step = h->dt;
+    out->steps = h->step;
+    out->invalid_cell = h->bad_state != ~0ULL ? static_cast<int64_t>(h->bad_state)
+                        : h->bad_res != ~0ULL ? static_cast<int64_t>(h->bad_res)
+                                              : -1;
+  }
+
+  void history(long long count, double* rms, double* dt) override {
+    Control h;
+    read_control(&h);
+    const long long n = std::min<long long>({count, h.step, kHistory});
+    for (long long i = 0; i < n; ++i) {
+      if (rms != nullptr)
+        for (int k = 0; k < 5; ++k) rms[5 * i + k] = h.hist_rms[i][k];
+      if (dt != nullptr) dt[i] = h.hist_dt[i];
+    }
+  }
+
+  void gradients(double* grad, double* phi) override {
+    Buffer tmp(15ULL * n_ * sizeof(double));
+    if (grad != nullptr) {
+      launch(k_to_double<P>, blocks(15LL * n_), kBlock, static_cast<const G*>(grad_.as<G>()), 15LL * n_, tmp.as<double>());
+      check(cudaMemcpyAsync(grad, tmp.as<void>(), 15ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "grad");
+    }
+    check(cudaStreamSynchronize(stream), "grad");
+    if (phi != nullptr) {
+      launch(k_to_double<P>, blocks(5LL * n_), kBlock, reinterpret_cast<const G*>(phi_.as<S>()), 5LL * n_, tmp.as<double>());
+      check(cudaMemcpyAsync(phi, tmp.as<void>(), 5ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "phi");
+    }
+    check(cudaStreamSynchronize(stream), "gradients");
+  }
+
+  void time_steps(double cfl, double* dt) override {
+    Buffer tmp(std::max(n_, 1) * sizeof(double));
+    launch(k_boundary_states<P>, blocks(nb_), kBlock, with_state(s_[0].as<S>()));
+    launch(k_spectral<P>, blocks(n_), kBlock, with_state(s_[0].as<S>()), cfl, 0, tmp.as<double>());
+    check(cudaMemcpyAsync(dt, tmp.as<void>(), n_ * sizeof(double), cudaMemcpyDeviceToHost, stream), "dt");
+    check(cudaStreamSynchronize(stream), "time steps");
+  }
+
+  std::vector<int> ghost_owner_;
+
+ private:
+  struct StepKey {
+    double cfl, dt;
+    bool local;
+    int rk;
+    bool operator==(const StepKey& o) const {
+      return cfl == o.cfl && dt == o.dt && local == o.local && rk == o.rk;
+    }
+  };
+
+  void validate(const autan_euler_mesh& m) {
+    if (m.n_owned_cells < 1 || m.n_cells < m.n_owned_cells || m.n_faces < m.n_interior_faces ||
+        m.n_owned_interior_faces > m.n_interior_faces || m.n_owned_faces > m.n_faces ||
+        m.n_owned_faces < m.n_interior_faces)
+      fail("E1101: inconsistent mesh counts");
+    if (m.owner == nullptr || m.cell_face_offsets == nullptr || m.cell_faces == nullptr ||
+        m.face_normal == nullptr || m.face_area_magnitude == nullptr ||
+        m.face_centroid == nullptr || m.cell_centroid == nullptr || m.cell_volume == nullptr ||
+        (m.n_interior_faces > 0 && m.neighbour == nullptr))
+      fail("E1101: a required mesh array is NULL");
+    if (m.n_cells > m.n_owned_cells && m.ghost_owner == nullptr)
+      fail("E1101: ghost cells need ghost_owner");
+    if (second_ && (m.stencil == nullptr || m.stencil_offsets == nullptr ||
+                    m.stencil_lsq_weight == nullptr))
+      fail("E1101: a second-order scheme needs the stencil and its weights");
+    if (scheme_.flux < 0 || scheme_.flux > 2) fail("E1101: unknown flux");
+    for (int c = 0; c < m.n_owned_cells; ++c)
+      if (!(m.cell_volume[c] > 0.0)) fail("E0121: an owned cell has a non-positive volume");
+    ghost_owner_.assign(m.ghost_owner, m.ghost_owner + (m.n_cells - m.n_owned_cells));
+  }
+
+  static int blocks(long long n) { return static_cast<int>(std::max<long long>(1, (n + kBlock - 1) / kBlock)); }
+  int norm_blocks() const { return std::min(blocks(n_), 148 * 8); }
+
+  // Kernel kinds of autan_euler_device_kernel_times.
+  enum Kind : int { kBoundary = 0, kGradients = 1, kSpectral = 2, kFaces = 3, kNorms = 4, kControl = 5 };
+
+  template <class K, class... A>
+  void launch(K kernel, int grid, int block, A... args) {
+    launch_as(kControl, kernel, grid, block, args...);
+  }
+
+  template <class K, class... A>
+  void launch_as(int kind, K kernel, int grid, int block, A... args) {
+    cudaEvent_t before = nullptr, after = nullptr;
+    if (timing_) {
+      check(cudaEventCreate(&before), "event");
+      check(cudaEventCreate(&after), "event");
+      check(cudaEventRecord(before, stream), "event");
+    }
+    kernel<<<grid, block, 0, stream>>>(args...);
+    check(cudaGetLastError(), "kernel launch");
+    ++counters.launches;
+    if (timing_) {
+      check(cudaEventRecord(after, stream), "event");
+      timed_.push_back({kind, before, after});
+    }
+  }
+
+ public:
+  // Runs n steps with CUDA events around every launch on the handle's stream; per kind the total
+  // milliseconds and the launches.
+  void kernel_times(double cfl, double dt, bool local, int rk, long long n, double* ms,
+                    long long* launches) override {
+    for (int k = 0; k < 6; ++k) {
+      ms[k] = 0.0;
+      launches[k] = 0;
+    }
+    timing_ = true;
+    const StepKey key{cfl, dt, local, rk};
+    try {
+      for (long long i = 0; i < n; ++i) enqueue_step(key);
+    } catch (...) {
+      timing_ = false;
+      throw;
+    }
+    timing_ = false;
+    check(cudaStreamSynchronize(stream), "kernel times");
+    for (const auto& t : timed_) {
+      float m = 0.0f;
+      check(cudaEventElapsedTime(&m, t.before, t.after), "elapsed");
+      ms[t.kind] += m;
+      launches[t.kind] += 1;
+      cudaEventDestroy(t.before);
+      cudaEventDestroy(t.after);
+    }
+    timed_.clear();
+    counters.steps += n;
+  }
+
+ private:
+
+  Dev<P> with_state(const S* s, S* s_next = nullptr) const {
+    Dev<P> d = d_;
+    d.s = s;
+    d.s_next = s_next;
+    return d;
+  }
+
+  void fill_phi_one() {
+    std::vector<S> one(5ULL * n_, S(1));
+    check(cudaMemcpyAsync(phi_.as<void>(), one.data(), one.size() * sizeof(S),
+                          cudaMemcpyHostToDevice, stream), "phi");
+    check(cudaStreamSynchronize(stream), "phi");
+  }
+
+  void launch_store(const double* u, S* s) { launch(k_store<P>, blocks(n_), kBlock, d_, u, s); }
+
+  void launch_faces(const Dev<P>& d, int mode, int stage, double wa, double wb, int local,
+                    int last) {
+    const int g = blocks(n_);
+    auto go = [&](auto kernel) { launch_as(kFaces, kernel, g, kBlock, d, mode, stage, wa, wb, local, last); };
+    const int f = scheme_.flux;
+    if (planar_) {
+      if (second_) {
+        if (f == 0) go(k_faces<P, 0, true, true>);
+        else if (f == 1) go(k_faces<P, 1, true, true>);
+        else go(k_faces<P, 2, true, true>);
+      } else {
+        if (f == 0) go(k_faces<P, 0, true, false>);
+        else if (f == 1) go(k_faces<P, 1, true, false>);
+        else go(k_faces<P, 2, true, false>);
+      }
+    } else {
+      if (second_) {
+        if (f == 0) go(k_faces<P, 0, false, true>);
+        else if (f == 1) go(k_faces<P, 1, false, true>);
+        else go(k_faces<P, 2, false, true>);
+      } else {
+        if (f == 0) go(k_faces<P, 0, false, false>);
+        else if (f == 1) go(k_faces<P, 1, false, false>);
+        else go(k_faces<P, 2, false, false>);
+      }
+    }
+  }
+
+  // The cell loops before the faces, on stored state s: boundary states, gradients, limiter.
+  void enqueue_cells(const S* s) {
+    const Dev<P> d = with_state(s);
+    launch_as(kBoundary, k_boundary_states<P>, blocks(nb_), kBlock, d);
+    if (second_) {
+      if (limiter_) {
+        launch_as(kGradients, k_gradients<P, true>, blocks(n_), kBlock, d);
+      } else {
+        launch_as(kGradients, k_gradients<P, false>, blocks(n_), kBlock, d);
+      }
+    }
+  }
+
+  void enqueue_residual(const S* s) {
+    enqueue_cells(s);
+    launch_faces(with_state(s), kResidual, 0, 0.0, 0.0, 0, 0);
+    ++counters.residuals;
+  }
+
+  // One step. Stored states rotate through three buffers so that a step starts and ends in s_[0]:
+  // RK3 0 -> 1 -> 2 -> 0; RK4 0 -> 1 -> 2 -> 1 -> 0.
+  void enqueue_step(const StepKey& k) {
+    const double dt_fixed = k.dt > 0.0 ? k.dt : 0.0;
+    const bool local = !(k.dt > 0.0) && k.local;
+    launch(k_begin, 1, 256, d_.ctl, dt_fixed);
+    S* s0 = s_[0].as<S>();
+    S* s1 = s_[1].as<S>();
+    S* s2 = s_[2].as<S>();
+    enqueue_cells(s0);
+    if (!(k.dt > 0.0))
+      launch_as(kSpectral, k_spectral<P>, blocks(n_), kBlock, with_state(s0), k.cfl, local ? 1 : 0,
+                static_cast<double*>(nullptr));
+    launch(k_take_dt, 1, 32, d_.ctl);
+    if (k.rk == 3) {
+      static const double w[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
+      S* in[3] = {s0, s1, s2};
+      S* out[3] = {s1, s2, s0};
+      for (int st = 0; st < 3; ++st) {
+        if (st > 0) enqueue_cells(in[st]);
+        launch_faces(with_state(in[st], out[st]), kRk3, st, w[st][0], w[st][1], local ? 1 : 0,
+                     st == 2 ? 1 : 0);
+        if (st == 0) {
+          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+          launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        }
+      }
+    } else {
+      static const double cs[4] = {0.5, 0.5, 1.0, 0.0};
+      S* in[4] = {s0, s1, s2, s1};
+      S* out[4] = {s1, s2, s1, s0};
+      for (int st = 0; st < 4; ++st) {
+        if (st > 0) enqueue_cells(in[st]);
+        launch_faces(with_state(in[st], out[st]), kRk4, st, cs[st], 0.0, local ? 1 : 0,
+                     st == 3 ? 1 : 0);
+        if (st == 0) {
+          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+          launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        }
+      }
+    }
+    launch(k_end_step, 1, 32, d_.ctl);
+  }
+
+  void capture(const StepKey& k) {
+    drop_graph();
+    const long long before = counters.launches;
+    check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      enqueue_step(k);
+    } catch (...) {
+      cudaGraph_t g;
+      cudaStreamEndCapture(stream, &g);
+      if (g != nullptr) cudaGraphDestroy(g);
+      throw;
+    }
+    check(cudaStreamEndCapture(stream, &graph_), "end capture");
+    check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "instantiate");
+    graph_nodes_ = counters.launches - before;
+    counters.launches = before;
+    graph_key_ = k;
+  }
+
+  void drop_graph() {
+    if (graph_exec_ != nullptr) cudaGraphExecDestroy(graph_exec_);
+    if (graph_ != nullptr) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+  }
+
+  void read_control(Control* h) {
+    check(cudaMemcpyAsync(h, d_.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control");
+    check(cudaStreamSynchronize(stream), "control");
+  }
+
+  long long first_invalid(const std::vector<double>& u, const std::vector<double>& r) const {
+    const double* ref = d_.ref;
+    const C g = static_cast<C>(scheme_.gamma);
+    const C r0 = static_cast<C>(ref[0]);
+    for (int c = 0; c < n_; ++c) {
+      C dq[5];
+      for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(static_cast<S>(u[k * static_cast<long long>(n_) + c] - ref[k]));
+      const C rho = r0 + dq[0];
+      C dm_m = 0, mr_mr = 0;
+      for (int k = 0; k < 3; ++k) {
+        const C mr = static_cast<C>(ref[k + 1]);
+        dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
+        mr_mr = mr_mr + mr * mr;
+      }
+      const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
+      const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d_.p.pref;
+      if (!std::isfinite(static_cast<double>(rho)) || !std::isfinite(static_cast<double>(pr)) ||
+          !(rho > C(0)) || !(pr > C(0)))
+        return c;
+    }
+    for (int c = 0; c < n_; ++c)
+      for (int k = 0; k < 5; ++k)
+        if (!std::isfinite(r[k * static_cast<long long>(n_) + c])) return c;
+    return -1;
+  }
+
+  autan_euler_scheme scheme_;
+  bool planar_, second_, limiter_;
+  int nc_ = 0, n_ = 0, nf_ = 0, ni_ = 0, nif_ = 0, nb_ = 0;
+  Sliced st_, inc_;
+  Dev<P> d_{};
+  Buffer s_[3];
+  Buffer grad_, phi_, prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
+  Buffer st_start_, st_len_, st_e_, st_w_, inc_start_, inc_len_, inc_code_;
+  Buffer f_l_, f_r_, f_n_, f_a_, f_rl_, f_rr_, f_m_;
+  Buffer b_own_, b_kind_, b_data_, b_n_, b_a_, b_r_, b_m_, source_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  long long graph_nodes_ = 0;
+  StepKey graph_key_{0.0, 0.0, false, 0};
+  Control* head_ = nullptr;  // pinned copy of the control's head
+  struct Timed {
+    int kind;
+    cudaEvent_t before, after;
+  };
+  bool timing_ = false;
+  std::vector<Timed> timed_;
+};
+
+int fail_to(char* err, size_t len, const std::string& what) {
+  if (err != nullptr && len > 0) {
+    std::strncpy(err, what.c_str(), len - 1);
+    err[len - 1] = '\0';
+  }
+  return 1;
+}
+
+template <class F>
+int guarded(char* err, size_t len, F&& body) {
+  try {
+    body();
+    return 0;
+  } catch (const Failure& e) {
+    return fail_to(err, len, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail_to(err, len, "E1103: out of host memory");
+  } catch (const std::exception& e) {
+    return fail_to(err, len, std::string("E1100: ") + e.what());
+  }
+}
+
+struct DeviceGuard {
+  int previous = -1;
+  explicit DeviceGuard(int device) {
+    cudaGetDevice(&previous);
+    if (device >= 0 && device != previous) check(cudaSetDevice(device), "cudaSetDevice");
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (previous >= 0 && now != previous) cudaSetDevice(previous);
+  }
+};
+
+Stepper* as_stepper(void* h) {
+  if (h == nullptr) fail("E1101: null handle");
+  return static_cast<Stepper*>(h);
+}
+
+}  // namespace autan_b200
+
+using namespace autan_b200;
+
+extern "C" {
+
+int autan_euler_device_create(const autan_euler_mesh* mesh, const autan_euler_scheme* scheme,
+                              int32_t device, void* stream, void** handle, char* err,
+                              size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (mesh == nullptr || scheme == nullptr || handle == nullptr) fail("E1101: null argument");
+    int count = 0;
+    check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    if (device >= count) fail("E1101: no such device");
+    int dev = device;
+    if (dev < 0) check(cudaGetDevice(&dev), "cudaGetDevice");
+    DeviceGuard guard(dev);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bool own = false;
+    if (s == nullptr) {
+      check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+      own = true;
+    }
+    std::unique_ptr<Stepper> h;
+    try {
+      if (scheme->precision == AUTAN_FP64) {
+        h = std::make_unique<Impl<Fp64>>(*mesh, *scheme, s);
+      } else if (scheme->precision == AUTAN_FP32_ACC64) {
+        h = std::make_unique<Impl<Fp32Acc64>>(*mesh, *scheme, s);
+      } else {
+        fail("E1102: unknown precision policy");
+      }
+    } catch (...) {
+      if (own) cudaStreamDestroy(s);
+      throw;
+    }
+    h->own_stream = own;
+    h->device = dev;
+    *handle = h.release();
+  });
+}
+
+void autan_euler_device_destroy(void* handle) {
+  if (handle == nullptr) return;
+  auto* h = static_cast<Stepper*>(handle);
+  DeviceGuard guard(h->device);
+  cudaStream_t s = h->stream;
+  const bool own = h->own_stream;
+  cudaStreamSynchronize(s);
+  delete h;
+  if (own) cudaStreamDestroy(s);
+}
+
+int autan_euler_device_set_boundary(void* handle, const uint8_t* kind, const double* data,
+                                    int64_t n_boundary, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (kind == nullptr || data == nullptr) fail("E1101: null boundary arrays");
+    (void)n_boundary;
+    h->set_boundary(kind, data);
+  });
+}
+
+int autan_euler_device_set_boundary_data(void* handle, const double* data, int64_t n_boundary,
+                                         char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (data == nullptr) fail("E1101: null boundary data");
+    (void)n_boundary;
+    h->set_boundary_data(data);
+  });
+}
+
+int autan_euler_device_set_source(void* handle, const double* source, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (source == nullptr) fail("E1101: null source");
+    h->set_source(source);
+  });
+}
+
+int autan_euler_device_set_second_order(void* handle, int32_t on, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    h->set_second_order(on != 0);
+  });
+}
+
+int autan_euler_device_upload(void* handle, const double* u, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (u == nullptr) fail("E1101: null state");
+    h->upload_state(u);
+  });
+}
+
+int autan_euler_device_download(void* handle, double* u, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (u == nullptr) fail("E1101: null state");
+    h->download_state(u);
+  });
+}
+
+int autan_euler_device_residual(void* handle, const double* u, double* res, char* err,
+                                size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (u == nullptr || res == nullptr) fail("E1101: null arrays");
+    h->residual(u, res);
+  });
+}
+
+int autan_euler_device_step(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                            int64_t n_steps, int32_t use_graph, autan_euler_step_result* out,
+                            char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    autan_euler_step_result r{};
+    h->step(cfl, dt, local != 0, rk, n_steps, use_graph != 0, &r);
+    if (out != nullptr) *out = r;
+  });
+}
+
+int autan_euler_device_evaluate(void* handle, autan_euler_step_result* out, char* err,
+                                size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    autan_euler_step_result r{};
+    h->evaluate(&r);
+    if (out != nullptr) *out = r;
+  });
+}
+
+int autan_euler_device_history(void* handle, int64_t count, double* rms, double* dt, char* err,
+                               size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    h->history(count, rms, dt);
+  });
+}
+
+int autan_euler_device_gradients(void* handle, double* grad, double* phi, char* err,
+                                 size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    h->gradients(grad, phi);
+  });
+}
+
+int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* err,
+                                  size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (dt == nullptr) fail("E1101: null output");
+    h->time_steps(cfl, dt);
+  });
+}
+
+int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                                    int64_t n_steps, double* ms, int64_t* launches, char* err,
+                                    size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    if (ms == nullptr || launches == nullptr) fail("E1101: null output");
+    if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
+    long long l[6];
+    h->kernel_times(cfl, dt, local != 0, rk, n_steps, ms, l);
+    for (int k = 0; k < 6; ++k) launches[k] = l[k];
+  });
+}
+
+int autan_euler_device_sync(void* handle, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    DeviceGuard guard(h->device);
+    check(cudaStreamSynchronize(h->stream), "sync");
+  });
+}
+
+void* autan_euler_device_stream(void* handle) {
+  return handle == nullptr ? nullptr : static_cast<void*>(static_cast<Stepper*>(handle)->stream);
+}
+
+int autan_euler_device_counters(void* handle, int64_t* counters, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    auto* h = as_stepper(handle);
+    counters[0] = h->counters.launches;
+    counters[1] = h->counters.steps;
+    counters[2] = h->counters.residuals;
+    counters[3] = h->device_bytes();
+  });
+}
+
+}  // extern "C"

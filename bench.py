@@ -1,0 +1,424 @@
+"""Benchmark of the explicit Euler residual-and-update path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tets|hex]
+
+Workload (default `tets`): the convected isentropic vortex on 2 073 600 jittered Kuhn tetrahedra
+(240 x 240 x 6 lattice, nodes moved by U(-0.2, 0.2) h, seed 0, periodic in x and y, slip in z),
+second-order LSQ face2 gradients with the Venkatakrishnan limiter (K = 5), HLLC, SSP-RK3 at CFL 0.8,
+fp32+acc64. A step is one SSP-RK3 step (three residual evaluations and updates, the CFL time step
+and the exact residual norms). Synthetic data: the vortex field is generated, no dataset is read.
+
+Metric: cell-iterations per second (cells x steps / s), whole job. `value` is device time (CUDA
+events on the stepper's stream) with the state resident in HBM; `e2e` is the same metric through
+the C ABI with the state in pinned host memory, copied in and out every step. With N > 1 (torchrun)
+each rank steps its own copy of the case (independent replicas, weak scaling); the time is the max
+over ranks.
+
+`--impl reference` times the reference algorithm on the host cores: the CPU oracle (a C
+restatement of the reference's residual and steps) on one thread per core, each thread stepping
+its own 240 x 24 x 6 slab of the same lattice (207 360 cells) per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+L2_BYTES = 126 * 2**20
+
+
+def measured_hbm_peak() -> tuple[float, str]:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ algorithmic bytes
+
+
+def kernel_bytes(case, rk: int) -> dict[str, float]:
+    """Algorithmic bytes of one step per kernel kind: every array a kernel touches, read or written
+    once, at its stored size (the rule of the reference's physics/bench/euler_bench.cu:321-372,
+    applied to this layout); re-reads of neighbours' values are not counted."""
+    m = case.mesh
+    fp32 = case.scheme.precision != "fp64"
+    sS = sG = sGV = sC = 4 if fp32 else 8
+    n = m.n_owned_cells
+    fi = m.n_owned_interior_faces
+    nb = m.n_faces - m.n_interior_faces
+    nbo = m.n_owned_faces - m.n_interior_faces
+    k = int(m.cell_face_offsets[n] - m.cell_face_offsets[0])
+    s = int(m.stencil_offsets[n] - m.stencil_offsets[0])
+    second = case.scheme.second_order
+    stages = 3 if rk == 3 else 4
+    inc = 4 * n + 4 * k  # lengths and codes
+    boundary = nb * (4 + 5 * sS + 3 * sGV + 1 + 5 * sS + 5 * sS)
+    grad = 0.0
+    if second:
+        grad = (5 * sS * n + 4 * n + 4 * s + 3 * sGV * s + 5 * sS * nb + inc + 6 * sC * fi
+                + 3 * sC * nbo + 8 * n + 15 * sG * n + 5 * sS * n)  # fmt: skip
+    spectral = (5 * sS * n + inc + 8 * fi + 4 * sGV * fi + 4 * sGV * nbo + 5 * sS * nbo + 8 * n)
+    face_common = (5 * sS * n + (20 * sS * n if second else 0) + 8 * n + inc + 8 * fi
+                   + 4 * sGV * fi + 6 * sC * fi + nbo * (3 * sGV + 3 * sC + 5 * sS + 1 + sGV))  # fmt: skip
+    faces = 0.0
+    for st in range(stages):
+        b = face_common + 40 * n + 40 * n + 5 * sS * n  # u read, stage/u write, next state write
+        if rk == 3 and st > 0:
+            b += 40 * n  # stage read
+        if rk == 4:
+            b += (40 * n if st > 0 else 0) + (40 * n if st < 3 else 0)  # accumulator
+        if st == 0:
+            b += 40 * n  # residual for the norms
+        faces += b
+    return {
+        "boundary_states": boundary * stages,
+        "gradients": grad * stages,
+        "spectral": spectral,
+        "faces": faces,
+        "norms": 40.0 * n,
+        "control": 0.0,
+    }
+
+
+# ------------------------------------------------------------------ clocks
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )  # fmt: skip
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, smax, reasons = [], [], set()
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                smax.append(float(r[1]))
+                for i, nme in enumerate(names):
+                    if r[3 + i].strip().lower() == "active":
+                        reasons.add(nme)
+            except (ValueError, IndexError):
+                continue
+        os.unlink(self.file.name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def gpu_uuid(device: int) -> str:
+    import torch
+
+    try:
+        u = str(torch.cuda.get_device_properties(device).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return str(device)
+
+
+# ------------------------------------------------------------------ CPU (oracle) throughput
+
+
+def cpu_throughput(steps: int, warmup: int, threads: int) -> tuple[float, str, int]:
+    """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
+    240 x 24 x 6 slab of the benchmark lattice (SSP-RK3, fp32+acc64); the rate of the whole host."""
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle as O
+    from autan_b200 import cases
+
+    case = cases.vortex_tets(240, 24, 6, steps=1, precision="fp32+acc64")
+    md = cases.oracle_mesh_dict(case)
+    sch = case.scheme.as_dict()
+    oracles = [O.Oracle(md, sch, case.bc_kind, case.bc_data) for _ in range(threads)]
+    states = [case.u0.copy() for _ in range(threads)]
+
+    def one_step(i):
+        oracles[i].step(states[i], rk=3, cfl=case.cfl)
+
+    def all_threads():
+        ts = [threading.Thread(target=one_step, args=(i,)) for i in range(threads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+
+    for _ in range(warmup):
+        all_threads()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        all_threads()
+    elapsed = time.perf_counter() - t0
+    cells = case.mesh.n_owned_cells
+    rate = cells * threads * steps / elapsed
+    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a 240x24x6 slab "
+              f"({cells} cells) of the benchmark lattice, CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
+    return rate, sample, threads
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ arms
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    threads = host_threads()
+    rate, sample, cores = cpu_throughput(args.steps, max(1, min(args.warmup, 1)), threads)
+    line = {
+        "impl": "reference",
+        "metric": "cell-iterations/s",
+        "value": rate,
+        "unit": "cell-iterations/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 accumulation)",
+        "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": rate, "unit": "cell-iterations/s", "cores": cores,
+                         "kind": "port", "sample": sample},  # fmt: skip
+        "e2e": {"value": rate, "unit": "cell-iterations/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},  # fmt: skip
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args) -> dict:
+    if args.workload == "hex":
+        return {"workload": "isentropic vortex, 64x64x2 periodic hexahedra (8192 cells), "
+                            "first-order Roe, classical RK4, CFL 0.5, fp64",
+                "cells": 8192, "l2": "inputs smaller than L2 (launch-bound case)"}  # fmt: skip
+    return {
+        "workload": "isentropic vortex, 2073600 jittered Kuhn tetrahedra (240x240x6, periodic x/y, "
+                    "slip z), LSQ face2 + Venkatakrishnan K=5, HLLC, SSP-RK3, CFL 0.8, fp32+acc64",
+        "cells": 2073600,
+        "parallelism": f"replicas x{args.gpus}",
+        "l2": "working set of every step (about 2 GB) larger than the 126 MB L2",
+    }
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from autan_b200 import cases
+    from autan_b200.euler import EulerDevice
+
+    if args.workload == "hex":
+        case = cases.vortex_hex()
+    else:
+        case = cases.vortex_tets(precision="fp32+acc64")
+    n = case.mesh.n_owned_cells
+    dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
+    dev.upload(case.u0)
+    stream = torch.cuda.ExternalStream(dev.stream)
+    # Warm-up (and graph capture).
+    dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.warmup, graph=True)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # -- device-timed steps, state resident in HBM
+    launches0 = dev.counters()["launches"]
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_uuid(local_rank)) as clocks:
+        start.record(stream)
+        r = dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.steps, graph=True)
+        end.record(stream)
+        end.synchronize()
+    barrier()
+    launches = dev.counters()["launches"] - launches0
+    ms = max_over_ranks(start.elapsed_time(end))
+    value = world * n * args.steps / (ms * 1e-3)
+    if r.invalid_cell is not None:
+        raise RuntimeError(f"invalid state at cell {r.invalid_cell}")
+
+    # -- end to end through the C ABI: pinned host state in and out every step
+    u_host = torch.empty((5, case.mesh.n_cells), dtype=torch.float64, pin_memory=True).numpy()
+    u_host[:] = dev.download()
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        dev.upload(u_host)
+        dev.step(cfl=case.cfl, rk=case.rk, n_steps=1, graph=True)
+        u_host[:] = dev.download()
+    t1 = time.perf_counter()
+    e2e_s = max_over_ranks(t1 - t0)
+    e2e = world * n * e2e_steps / e2e_s
+
+    # -- per-kernel times (CUDA events around every launch on the stepper's stream)
+    kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, n_steps=3)
+    alg = kernel_bytes(case, case.rk)
+    dominant = max((k for k in kt if kt[k][1] > 0), key=lambda k: kt[k][0])
+    per_step_launches = kt[dominant][1] / 3
+    avg_ms = kt[dominant][0] / kt[dominant][1]
+    bytes_per_launch = alg[dominant] / per_step_launches
+    achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_hbm_peak()
+    step_ms = ms / args.steps
+    step_bytes = sum(alg.values())
+    traffic = committed_traffic(dominant, n)
+    line = None
+    if rank == 0:
+        line = {
+            "metric": "cell-iterations/s",
+            "value": value,
+            "unit": "cell-iterations/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": step_ms,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (f64 accumulation)" if case.scheme.precision != "fp64" else "f64",
+            "data": "synthetic",
+            "config": workload_config(args),
+            "e2e": {"value": e2e, "unit": "cell-iterations/s",
+                    "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 40 * n + 128},  # fmt: skip
+            "gpu_launches": int(launches),
+            "roofline": {
+                "bound": "hbm",
+                "kernel": dominant,
+                "achieved": achieved,
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "avg_launch_ms": avg_ms,
+            },
+            "step_roofline": {"algorithmic_bytes": step_bytes,
+                              "achieved_gbs": step_bytes / (step_ms * 1e-3) / 1e9,
+                              "frac": step_bytes / (step_ms * 1e-3) / 1e9 / peak},  # fmt: skip
+            "kernels_ms_per_step": {k: v[0] / 3 for k, v in kt.items()},
+            "clocks": clocks.summary(),
+            "residual_rms": list(map(float, r.residuals)),
+        }
+    dev.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu:
+            rate, sample, cores = cpu_throughput(2, 1, host_threads())
+            line["cpu_baseline"] = {"value": rate, "unit": "cell-iterations/s", "cores": cores,
+                                    "kind": "port", "sample": sample}  # fmt: skip
+        print(json.dumps(line), flush=True)
+
+
+def committed_traffic(kernel: str, n_cells: int):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.md, a
+    line `traffic <kernel> <bytes per launch> <cells>` scaled to this case's cells), else None."""
+    p = REPO / "profiles" / "traffic.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        f = line.strip().strip("`").split()
+        if len(f) == 4 and f[0] == "traffic" and f[1] == kernel:
+            return float(f[2]) * n_cells / float(f[3])
+    return None
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["tets", "hex"], default="tets")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

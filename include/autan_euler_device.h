@@ -1,0 +1,177 @@
+/* C ABI of the B200-native explicit Euler residual-and-update path.
+ *
+ * It replaces, for one rank on one GPU, the reference's device stepper and host residual:
+ *   physics/include/autan/physics/euler_device.hpp:22-41   DeviceStepper<P>::{step, evaluate,
+ *                                                           residual, set_second_order, upload,
+ *                                                           download}
+ *   physics/include/autan/physics/euler_device.hpp:49-54   make_device_stepper<P>(...)
+ *   physics/include/autan/physics/euler.hpp:127-184        Euler<P>::{set_boundary,
+ *                                                           set_boundary_data, set_source,
+ *                                                           residual}
+ * with the conventions of the reference's own C ABI (physics/mms/capi.cpp:42-60,126-347): opaque
+ * handles, int return (0 success, 1 failure with "Exxxx: message" copied into err, err_len bytes,
+ * NUL-terminated), no exception across the boundary, caller-owned FP64 host arrays copied at the
+ * call, structure of arrays (component c of entity i at c * n + i).
+ *
+ * Meshes follow Autan's face-based mesh contract (docs/contracts/mesh.md): owned cells then ghost
+ * cells; interior faces sorted by (owner, neighbour), owner < neighbour, faces touching an owned
+ * cell first; boundary faces after the interior ones; cell_faces per cell in increasing face
+ * index. Ghost cells are periodic images of owned cells (a one-rank partition with self-exchange,
+ * partition/src/self_exchange.cpp:15-30): ghost g takes the values of owned cell ghost_owner[g].
+ * The device holds owned cells only and reads an image's values at its owned cell, so no ghost
+ * fill runs.
+ *
+ * Not thread-safe per handle; distinct handles may run concurrently. Every call is ordered on the
+ * handle's stream; calls that return host data synchronise it. */
+#ifndef AUTAN_EULER_DEVICE_H
+#define AUTAN_EULER_DEVICE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary condition codes (physics/include/autan/physics/euler.hpp:31-38, kernels/euler.py:55-60)
+ * and the meaning of each face's five data values. */
+enum autan_boundary_kind {
+  AUTAN_BC_STATE = 0,    /* W = (rho, u, v, w, p) given */
+  AUTAN_BC_FARFIELD = 1, /* freestream W; Riemann invariants normal to the face */
+  AUTAN_BC_SLIP = 2,     /* slip wall or symmetry plane; data unused */
+  AUTAN_BC_INLET = 3,    /* subsonic inflow normal to the face: (p0, T0, -, -, -) */
+  AUTAN_BC_OUTLET = 4,   /* subsonic outflow: (-, -, -, -, p) */
+  AUTAN_BC_WALL = 5      /* no-slip wall at rest: (T_wall or 0 when adiabatic, -, -, -, -) */
+};
+
+enum autan_flux { AUTAN_FLUX_ROE = 0, AUTAN_FLUX_HLLC = 1, AUTAN_FLUX_AUSM_UP = 2 };
+enum autan_precision { AUTAN_FP64 = 0, AUTAN_FP32_ACC64 = 1 };
+
+/* Scheme and gas (physics/include/autan/physics/euler.hpp:40-71, the real[] of
+ * autan_mms_euler_create). `planar` selects the loops without warped-face terms
+ * (Euler<P>::set_planar): refused unless every face moment is zero. */
+struct autan_euler_scheme {
+  int32_t flux;
+  int32_t second_order;
+  int32_t limiter;
+  int32_t precision;
+  int32_t planar;
+  double gamma;
+  double gas_constant;
+  double venkat_k;
+  double length;
+  double mach_ref;
+  double scale[5];
+  double reference[5]; /* conserved reference state U_ref; density > 0 */
+};
+
+/* The mesh, its FP64 geometry and gradient stencil, in the layouts of kernels::Topology
+ * (codegen/include/autan/kernels/runtime.hpp:167-216) and kernels::PackedGeometry
+ * (codegen/include/autan/kernels/geometry.hpp:16-42). face_moment may be NULL (all planar).
+ * stencil_lsq_weight: Euler<P>::gradient_weights() for the boundary kinds set_boundary will give. */
+struct autan_euler_mesh {
+  int32_t n_cells, n_owned_cells, n_faces, n_interior_faces, n_owned_interior_faces, n_owned_faces;
+  const int32_t* owner;             /* n_faces */
+  const int32_t* neighbour;         /* n_interior_faces */
+  const int64_t* cell_face_offsets; /* n_cells + 1 */
+  const int32_t* cell_faces;
+  const int32_t* ghost_owner;        /* n_cells - n_owned_cells */
+  const double* face_normal;         /* 3 x n_faces, unit, owner -> neighbour */
+  const double* face_area_magnitude; /* n_faces */
+  const double* face_centroid;       /* 3 x n_faces */
+  const double* face_moment;         /* 9 x n_faces, row-major per face, or NULL */
+  const double* cell_centroid;       /* 3 x n_cells, ghosts at their shifted positions */
+  const double* cell_volume;         /* n_cells */
+  const int64_t* stencil_offsets;    /* n_cells + 1 */
+  const int32_t* stencil;            /* cell, or -(f + 1) for boundary face f */
+  const double* stencil_lsq_weight;  /* 3 x stencil entries */
+};
+
+/* What one explicit step reports (DeviceStepper<P>::Result, euler_device.hpp:25-29). */
+struct autan_euler_step_result {
+  double residuals[5]; /* RMS of each residual component at the start of the last step */
+  double time_step;    /* the global step of the last step (the least, with local steps) */
+  int64_t invalid_cell; /* least owned cell with a non-finite or non-positive state or a
+                           non-finite residual after the last step, -1 if none */
+  int64_t steps;       /* steps taken */
+};
+
+/* make_device_stepper (euler_device.hpp:49-54, physics/src/euler_device.cu:8-23): copies the
+ * mesh, geometry and stencil to `device` (an ordinal; -1: the current device) and runs on
+ * `stream` (a cudaStream_t; NULL: a stream of the handle's own). Boundary kinds default to slip
+ * with zero data, the source to zero. */
+int autan_euler_device_create(const struct autan_euler_mesh* mesh,
+                              const struct autan_euler_scheme* scheme, int32_t device,
+                              void* stream, void** handle, char* err, size_t err_len);
+void autan_euler_device_destroy(void* handle);
+
+/* Euler<P>::set_boundary (euler.hpp:126-127): one code per boundary face (n_faces -
+ * n_interior_faces) and 5 x n_boundary data values. */
+int autan_euler_device_set_boundary(void* handle, const uint8_t* kind, const double* data,
+                                    int64_t n_boundary, char* err, size_t err_len);
+/* Euler<P>::set_boundary_data (euler.hpp:128-129). */
+int autan_euler_device_set_boundary_data(void* handle, const double* data, int64_t n_boundary,
+                                         char* err, size_t err_len);
+/* Euler<P>::set_source (euler.hpp:178-179): 5 x n_cells, per unit volume. */
+int autan_euler_device_set_source(void* handle, const double* source, char* err, size_t err_len);
+/* DeviceStepper<P>::set_second_order (euler_device.hpp:38). */
+int autan_euler_device_set_second_order(void* handle, int32_t on, char* err, size_t err_len);
+
+/* DeviceStepper<P>::upload / download (euler_device.hpp:39-40): the FP64 conserved state,
+ * 5 x n_cells (ghost entries ignored on upload, written as their owned cell's on download). */
+int autan_euler_device_upload(void* handle, const double* u, char* err, size_t err_len);
+int autan_euler_device_download(void* handle, double* u, char* err, size_t err_len);
+
+/* DeviceStepper<P>::residual (euler_device.hpp:37): R(state(u)) of a host FP64 state into a host
+ * FP64 residual, both 5 x n_cells (ghost entries of res set to zero). The device state is
+ * unchanged. */
+int autan_euler_device_residual(void* handle, const double* u, double* res, char* err,
+                                size_t err_len);
+
+/* DeviceStepper<P>::step (euler_device.hpp:33), `n_steps` times on the device state:
+ *   rk 3: SSP-RK3 (Shu and Osher 1988, eq. 2.18) as CudaStepper::step (device_stepper.cuh:313-345);
+ *   rk 4: classical RK4, stage_s = u - ((c_s dt) / V) R with c = (1/2, 1/2, 1), then
+ *         u - ((dt / 6) / V) (R_0 + 2 R_1 + 2 R_2 + R_3) (not in the reference);
+ *   dt > 0: that global step; else CFL: dt = min over owned cells of (cfl V) / lambda, lambda the
+ *   convective spectral radius (kernels/euler.py:1091-1112); `local` != 0: each cell its own.
+ * use_graph != 0 captures one step in a CUDA graph and replays it. The host reads nothing until
+ * the last step; *out describes the last step. */
+int autan_euler_device_step(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                            int64_t n_steps, int32_t use_graph,
+                            struct autan_euler_step_result* out, char* err, size_t err_len);
+/* DeviceStepper<P>::evaluate (euler_device.hpp:35): residual norms and validity of the state. */
+int autan_euler_device_evaluate(void* handle, struct autan_euler_step_result* out, char* err,
+                                size_t err_len);
+/* Per-step history of the last autan_euler_device_step call: for step i < min(steps, 4096),
+ * 5 RMS values at rms[5 i], the global step at dt[i]; either pointer may be NULL. */
+int autan_euler_device_history(void* handle, int64_t count, double* rms, double* dt, char* err,
+                               size_t err_len);
+
+/* After a residual or step: the reconstruction gradients (15 x n_owned_cells, row-major per cell
+ * (3 i + j) as Euler<P>::Arrays::grad) and limiter (5 x n_owned_cells) of the last evaluation, as
+ * FP64; either pointer may be NULL. */
+int autan_euler_device_gradients(void* handle, double* grad, double* phi, char* err,
+                                 size_t err_len);
+/* The CFL time step of each owned cell for the device state, (cfl V) / lambda (n_owned_cells). */
+int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* err, size_t err_len);
+
+/* Runs n_steps steps as autan_euler_device_step does, launching without a graph and recording a
+ * CUDA event pair around every kernel on the handle's stream; per kernel kind, ms[k] receives the
+ * summed durations and launches[k] the launches: 0 boundary states, 1 gradients and limiter,
+ * 2 spectral radius and time step, 3 faces and RK update, 4 residual norms, 5 step control. */
+int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                                    int64_t n_steps, double* ms, int64_t* launches, char* err,
+                                    size_t err_len);
+/* Waits for the handle's stream. */
+int autan_euler_device_sync(void* handle, char* err, size_t err_len);
+/* The handle's cudaStream_t. */
+void* autan_euler_device_stream(void* handle);
+/* Counters of the handle since creation: [0] kernels launched by the library, [1] steps taken,
+ * [2] residual evaluations, [3] device bytes held. */
+int autan_euler_device_counters(void* handle, int64_t* counters, char* err, size_t err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

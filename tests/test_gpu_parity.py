@@ -1,0 +1,185 @@
+"""The CUDA path against the CPU oracle and the reference-evaluated golden vectors, through the C
+ABI (include/autan_euler_device.h). Tolerances: bit-identical wherever the arithmetic is the same
+operation sequence (every body but the exp/log of farfield and inlet states); 1e-12 relative in
+fp64 otherwise; fp32+acc64 against the fp64 oracle within the bound stated per test."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from autan_b200 import cases
+from autan_b200.euler import EulerDevice, Scheme
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES = sorted(p.stem for p in GOLDEN.glob("*.npz") if p.stem != "bodies")
+EXP_LOG = {"chan_ausm2_f64", "chan_roe2_f64"}  # farfield and inlet faces: CUDA exp/log
+
+
+def bits_equal(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return np.array_equal(a, b) and np.array_equal(np.signbit(a), np.signbit(b))
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def device_of(mesh, scheme, bc_kind, bc, source=None):
+    dev = EulerDevice(mesh, Scheme.from_dict(scheme) if isinstance(scheme, dict) else scheme,
+                      bc_kind=bc_kind, bc_data=bc, weights=mesh["stencil_lsq_weight"])
+    if source is not None:
+        dev.set_source(source)
+    return dev
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_golden_residual(case):
+    mesh, scheme, z = O.load_case(GOLDEN / f"{case}.npz")
+    no = mesh["n_owned_cells"]
+    with device_of(mesh, scheme, z["bc_kind"], z["bc"], z["source"]) as dev:
+        res = dev.residual(z["u"])
+        grad, phi = dev.gradients()
+    if scheme["second_order"]:
+        assert bits_equal(grad, z["grad"][:, :no])
+        assert bits_equal(phi, z["phi"][:, :no])
+    if case in EXP_LOG:
+        assert rel_err(res[:, :no], z["res"][:, :no]) <= 1e-12
+    else:
+        assert bits_equal(res[:, :no], z["res"][:, :no]), rel_err(res[:, :no], z["res"][:, :no])
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c not in EXP_LOG])
+def test_golden_steps(case):
+    if case not in ("hex_roe1_f64", "tet_hllc2_f64", "tet_hllc2_f32"):
+        pytest.skip("no step vectors")
+    mesh, scheme, z = O.load_case(GOLDEN / f"{case}.npz")
+    no = mesh["n_owned_cells"]
+    for rk in (3, 4):
+        with device_of(mesh, scheme, z["bc_kind"], z["bc"], z["source"]) as dev:
+            dev.upload(z["u"])
+            r = dev.step(cfl=0.5, rk=rk, n_steps=1)
+            u = dev.download()
+        assert r.invalid_cell is None
+        assert r.time_step == float(z[f"step{rk}_dt"])
+        assert bits_equal(r.residuals, z[f"step{rk}_norms"])
+        assert bits_equal(u[:, :no], z[f"step{rk}_u"][:, :no])
+
+
+def run_device(case, steps, graph=True, local=False):
+    with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+        dev.upload(case.u0)
+        r = dev.step(cfl=case.cfl, rk=case.rk, n_steps=steps, graph=graph, local=local)
+        rms, dts = dev.history(steps)
+        return dev.download(), r, rms, dts
+
+
+def run_oracle(case, steps, local=False, precision=None):
+    scheme = case.scheme.as_dict()
+    if precision is not None:
+        scheme["precision"] = precision
+    o = O.Oracle(cases.oracle_mesh_dict(case), scheme, case.bc_kind, case.bc_data)
+    u = case.u0.copy()
+    norms, dts = [], []
+    bad = -1
+    for _ in range(steps):
+        n, dt, bad = o.step(u, rk=case.rk, cfl=case.cfl, local=local)
+        norms.append(n)
+        dts.append(dt)
+    return u, np.array(norms), np.array(dts), bad
+
+
+def test_vortex_hex_rk4_200_steps():
+    """The 8192-cell periodic vortex, first-order Roe, RK4, CFL 0.5, 200 steps, FP64: the final
+    state within 1e-12 relative of the oracle (and, by construction, bit for bit)."""
+    case = cases.vortex_hex()
+    u_d, r, rms_d, dt_d = run_device(case, case.steps)
+    u_o, rms_o, dt_o, bad = run_oracle(case, case.steps)
+    no = case.mesh.n_owned_cells
+    assert r.invalid_cell is None and bad == -1
+    assert rel_err(u_d[:, :no], u_o[:, :no]) <= 1e-12
+    assert bits_equal(u_d[:, :no], u_o[:, :no])
+    assert bits_equal(rms_d, rms_o)
+    assert bits_equal(dt_d, dt_o)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
+def test_vortex_tets_same_precision(precision):
+    """The jittered-tetrahedra vortex (HLLC, LSQ face2 + Venkatakrishnan, SSP-RK3, CFL 0.8) on a
+    24 x 24 x 6 lattice (20 736 cells), 10 steps: the device equals the oracle of the same precision
+    bit for bit (fp64 bound 1e-12 relative)."""
+    case = cases.vortex_tets(24, 24, 6, steps=10, precision=precision)
+    u_d, r, rms_d, dt_d = run_device(case, case.steps)
+    u_o, rms_o, dt_o, bad = run_oracle(case, case.steps)
+    no = case.mesh.n_owned_cells
+    assert rel_err(u_d[:, :no], u_o[:, :no]) <= 1e-12
+    assert bits_equal(u_d[:, :no], u_o[:, :no])
+    assert bits_equal(rms_d, rms_o)
+    assert bits_equal(dt_d, dt_o)
+
+
+def test_vortex_tets_fp32_against_fp64_oracle():
+    """fp32+acc64 against the FP64 oracle: after 10 steps the conserved state differs by at most
+    2e-6 of its largest magnitude (FP32 resolution of the gauge state, 6e-8, times the growth over
+    the steps)."""
+    case = cases.vortex_tets(24, 24, 6, steps=10, precision="fp32+acc64")
+    u_d, *_ = run_device(case, case.steps)
+    u_o, *_ = run_oracle(case, case.steps, precision=0)
+    no = case.mesh.n_owned_cells
+    err = rel_err(u_d[:, :no], u_o[:, :no])
+    print(f"fp32+acc64 vs fp64 oracle: {err:.3e}")
+    assert err <= 2e-6
+
+
+def test_graph_equals_eager_and_repeats():
+    """A captured step replays the eager launches bit for bit; two runs give the same bits."""
+    case = cases.vortex_tets(16, 16, 6, steps=4, precision="fp32+acc64")
+    a, *_ = run_device(case, case.steps, graph=True)
+    b, *_ = run_device(case, case.steps, graph=False)
+    c, *_ = run_device(case, case.steps, graph=True)
+    assert bits_equal(a, b)
+    assert bits_equal(a, c)
+
+
+def test_local_time_steps():
+    case = cases.vortex_tets(16, 16, 6, steps=3, precision="fp64")
+    u_d, *_ = run_device(case, case.steps, local=True)
+    u_o, *_ = run_oracle(case, case.steps, local=True)
+    no = case.mesh.n_owned_cells
+    assert bits_equal(u_d[:, :no], u_o[:, :no])
+
+
+def test_freestream_preserved_full_size():
+    """Size-independent property at the benchmark's full size (2 073 600 tetrahedra): a uniform
+    freestream is a steady state of the residual to round-off (acceptance gate freestream
+    preservation, docs/validation/acceptance.md:27): every |R| <= 64 eps (|F| A) per cell."""
+    case = cases.vortex_tets(precision="fp64")
+    u = np.repeat(np.array(cases.freestream_reference())[:, None], case.mesh.n_cells, axis=1)
+    with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+        res = dev.residual(u)
+    no = case.mesh.n_owned_cells
+    area = case.mesh.face_area_magnitude
+    scale = 3.5 * 2.0 * area.max() * 6
+    assert np.abs(res[:, :no]).max() <= 64 * np.finfo(np.float64).eps * scale
+
+
+def test_conservation_full_size():
+    """Size-independent property at full size: over 3 SSP-RK3 steps of the fp32+acc64 benchmark
+    case, total mass, x/y momentum and energy (sum of V u over the periodic box with slip walls)
+    change by at most 1e-12 relative (the FP64 update and the face-order gather conserve to
+    round-off)."""
+    case = cases.vortex_tets(precision="fp32+acc64")
+    vol = case.mesh.cell_volume[: case.mesh.n_owned_cells]
+    no = case.mesh.n_owned_cells
+    with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+        dev.upload(case.u0)
+        before = (case.u0[:, :no] * vol).sum(axis=1)
+        r = dev.step(cfl=case.cfl, rk=3, n_steps=3)
+        after = (dev.download()[:, :no] * vol).sum(axis=1)
+    assert r.invalid_cell is None
+    for k in (0, 1, 2, 4):
+        assert abs(after[k] - before[k]) <= 1e-12 * abs(before[k]), (k, after[k] - before[k])
