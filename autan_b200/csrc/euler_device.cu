@@ -3,26 +3,31 @@
 //
 // Data layout in HBM (owned cells only: a periodic image reads its owned cell's values, so the
 // reference's three ghost fills per residual disappear):
-//   cell arrays      structure of arrays, component k of cell c at k * n + c;
-//   stored states    three buffers S (float in fp32+acc64), rotating through the RK stages;
-//   FP64             u (conserved), stage, RK4 accumulator, residual, volume;
-//   stencil          face2 entries and LSQ weights in a sliced (ELLPACK, 32 cells per slice)
-//                    layout: entry j of cell c at start[c / 32] + 32 j + c % 32, so a warp
-//                    reading entry j of its 32 cells reads 128 contiguous bytes;
+//   cell records     one 32-element record per cell (128 B in fp32+acc64): primitives W at words
+//                    0-4, limiter phi at 8-12, gradient grad W at 13-27 (row-major 5 x 3): a
+//                    neighbour's whole reconstruction data is one cache line, read with 16-byte
+//                    vector loads; three record buffers rotate through the RK stages;
+//   FP64 SoA         u (conserved), RK stage, RK4 accumulator, residual, volume (streamed);
+//   stencil          face2 entries, each {w_x, w_y, w_z, cell or -(b + 1)} in 16 B (fp32), in a
+//                    sliced ELLPACK layout (32 cells per slice, entry j of cell c at
+//                    start[c / 32] + 32 j + c % 32): a warp reads entry j of its cells as 512
+//                    contiguous bytes;
 //   incidences       each cell's faces in increasing face index (the reference's scatter order),
 //                    sliced the same way, coded 2 f + side (interior) or -(b + 1) (boundary);
-//   faces            left/right cells, normal, area, and rel(x_f, x_l), rel(x_r) already in the
-//                    compute type (what the bodies' rel() would compute), moments when warped.
+//   face records     per interior face {n, A, rel(x_f, x_l), l, rel(x_f, x_r), r} (48 B), per
+//                    boundary face {n, A, rel(x_f, x_o), kind, data, owner} (64 B): the `rel`
+//                    offsets already in the compute type, as the bodies' rel() computes them;
+//                    moments (warped faces only) apart.
 //
-// Kernels per RK stage (see DESIGN.md for the byte counts):
-//   boundary_states  prim_b of every boundary face;
-//   gradients        per cell: LSQ gradient over the stencil (FP64 sums), bounds, then the
-//                    Venkatakrishnan limiter over the cell's faces (fused: wmin/wmax never stored);
-//   faces            per cell: every face flux of the cell recomputed (gather-recompute: no float
-//                    atomics, no face scratch), summed from the source term in face order, then the
-//                    RK stage update in FP64 and the next stored state (fused).
-// Per step: the spectral radius with the global dt (atomicMin on its bits), and the exact-sum
-// residual norms of stage 0. All of it is captured in one CUDA graph per step.
+// Kernels per RK stage:
+//   k_boundary_states  prim_b of every boundary face;
+//   k_gradients        per cell: LSQ gradient over the stencil (FP64 sums), bounds, then the
+//                      Venkatakrishnan limiter over the cell's faces (wmin/wmax never stored); at
+//                      stage 0 also the spectral radius, the CFL step and its block minimum;
+//   k_faces            per cell: every face flux of the cell recomputed (gather-recompute: no float
+//                      atomics, no face scratch), summed in face order from the source term, then
+//                      the RK stage update in FP64 and the next stage's primitives.
+// Per step: the exact-sum residual norms of stage 0. A step is captured in one CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,25 +48,29 @@
 namespace autan_b200 {
 
 struct Fp64 {
-  using C = double;  // compute
-  using S = double;  // state storage
-  using G = double;  // gradient storage
-  using GV = double; // geometry read as values
+  using C = double;  // compute, and storage of states, gradients and geometry values
+  using V = double2; // 16-byte vector of C
+  static constexpr int kVec = 2;
 };
 struct Fp32Acc64 {
   using C = float;
-  using S = float;
-  using G = float;
-  using GV = float;
+  using V = float4;
+  static constexpr int kVec = 4;
 };
 
 constexpr int kSlice = 32;
 constexpr int kHistory = 4096;
 constexpr int kBlock = 256;
+constexpr int kRec = 32;    // record width, elements
+constexpr int kPhi = 8;     // phi at words 8-12
+constexpr int kGrad = 13;   // grad at words 13-27
+constexpr int kFace = 12;   // interior face record width
+constexpr int kBface = 16;  // boundary face record width
+constexpr int kPrimB = 8;   // boundary state record width
 
 // Step control in device memory: written by the kernels, read by the host after a batch.
 struct Control {
-  unsigned long long dt_bits;    // atomicMin of the positive local steps' bits
+  unsigned long long dt_bits;    // atomicMin of the local steps' bits (positive doubles)
   unsigned long long bad_state;  // least cell with an invalid state (~0: none)
   unsigned long long bad_res;    // least cell with a non-finite residual
   long long step;                // steps taken since the last reset
@@ -77,83 +86,138 @@ constexpr size_t kControlHead = offsetof(Control, words);
 template <class P>
 struct Dev {
   using C = typename P::C;
-  using S = typename P::S;
-  using G = typename P::G;
-  using GV = typename P::GV;
-  int n;      // owned cells
-  int nb;     // boundary faces
-  int n_if;   // owned interior faces
-  long long st_total, inc_total;
+  int n;     // owned cells
+  int nb;    // boundary faces
+  int n_if;  // owned interior faces
   Params<C> p;
   double ref[5];
-  // states
-  const S* s;  // stored state read this stage
-  S* s_next;   // stored state written this stage
-  G* grad;
-  S* phi;
-  S* prim_b;
-  // FP64
+  const C* rec;    // records read this stage
+  C* rec_next;     // records whose primitives this stage writes
+  C* prim_b;       // kPrimB x nb
   double* u;
   double* stage;
   double* racc;
   double* res;
   const double* volume;
   double* dt_local;
-  const S* source;
-  // stencil (sliced)
+  const C* source;  // 5 x n, or null
   const int* st_start;
   const int* st_len;
-  const int* st_e;
-  const GV* st_w;
-  // incidences (sliced)
+  const C* st;      // 4 per entry, sliced
   const int* inc_start;
   const int* inc_len;
   const int* inc_code;
-  // interior faces
-  const int* f_l;
-  const int* f_r;
-  const GV* f_n;
-  const GV* f_a;
-  const C* f_rl;
-  const C* f_rr;
-  const GV* f_m;
-  // boundary faces
-  const int* b_own;
-  const unsigned char* b_kind;
-  const S* b_data;
-  const GV* b_n;
-  const GV* b_a;
-  const C* b_r;
-  const GV* b_m;
+  const C* face;    // kFace per owned interior face
+  const C* bface;   // kBface per boundary face
+  const C* f_m;     // 9 x n_if, warped meshes only
+  const C* b_m;     // 9 x nb
   Control* ctl;
 };
 
-template <class T, class S>
-__device__ __forceinline__ void load5(const S* a, long long stride, long long i, T* v) {
+__device__ __forceinline__ int index_of(float x) { return __float_as_int(x); }
+__device__ __forceinline__ int index_of(double x) {
+  return static_cast<int>(__double_as_longlong(x));
+}
+
+// 16-byte vector loads of a record's words [w, w + count), count a multiple of the vector width.
+template <class P>
+__device__ __forceinline__ void load_words(const typename P::C* base, int w, int count,
+                                           typename P::C* out) {
+  using V = typename P::V;
+  const V* v = reinterpret_cast<const V*>(base + w);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) v[k] = static_cast<T>(__ldg(a + k * stride + i));
+  for (int q = 0; q < count / P::kVec; ++q) {
+    const V x = __ldg(v + q);
+    if constexpr (P::kVec == 4) {
+      out[4 * q] = x.x;
+      out[4 * q + 1] = x.y;
+      out[4 * q + 2] = x.z;
+      out[4 * q + 3] = x.w;
+    } else {
+      out[2 * q] = x.x;
+      out[2 * q + 1] = x.y;
+    }
+  }
 }
 
 template <class P>
-__device__ __forceinline__ void prim_of(const Dev<P>& d, const typename P::S* s, int c,
-                                        typename P::C* w) {
-  typename P::C q[5];
-  load5(s, d.n, c, q);
-  to_primitive(q, d.p, w);
+__device__ __forceinline__ void store_words(typename P::C* base, int w, int count,
+                                            const typename P::C* in) {
+  using V = typename P::V;
+  V* v = reinterpret_cast<V*>(base + w);
+#pragma unroll
+  for (int q = 0; q < count / P::kVec; ++q) {
+    V x;
+    if constexpr (P::kVec == 4) {
+      x.x = in[4 * q];
+      x.y = in[4 * q + 1];
+      x.z = in[4 * q + 2];
+      x.w = in[4 * q + 3];
+    } else {
+      x.x = in[2 * q];
+      x.y = in[2 * q + 1];
+    }
+    v[q] = x;
+  }
+}
+
+// The primitives of cell c (words 0-4 of its record).
+template <class P>
+__device__ __forceinline__ void load_prim(const typename P::C* rec, int c, typename P::C* w) {
+  typename P::C t[8];
+  load_words<P>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) w[k] = t[k];
+}
+
+// Primitives, limiter and gradient of cell c.
+template <class P>
+__device__ __forceinline__ void load_recon(const typename P::C* rec, int c, typename P::C* w,
+                                           typename P::C* phi, typename P::C* g) {
+  typename P::C t[28];
+  const typename P::C* base = rec + static_cast<long long>(c) * kRec;
+  load_words<P>(base, 0, 8, t);
+  load_words<P>(base, 8, 20, t + 8);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) w[k] = t[k];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) phi[k] = t[kPhi + k];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) g[k] = t[kGrad + k];
+}
+
+// Writes the primitives of cell c (words 0-7, the padding 5-7 zero).
+template <class P>
+__device__ __forceinline__ void store_prim(typename P::C* rec, int c, const typename P::C* w) {
+  using C = typename P::C;
+  const C t[8] = {w[0], w[1], w[2], w[3], w[4], C(0), C(0), C(0)};
+  store_words<P>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+}
+
+// Euler<P>::state then to_primitive: W of the stored state S(u - U_ref) (euler.cpp:925-932,
+// kernels/euler.py:94-104, 433).
+template <class P>
+__device__ __forceinline__ void prim_of_state(const Dev<P>& d, const double* u, typename P::C* w,
+                                              typename P::C* dq) {
+  using C = typename P::C;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(u[k] - d.ref[k]);
+  to_primitive(dq, d.p, w);
 }
 
 // ---------------------------------------------------------------- kernels
 
-// Euler<P>::state (physics/src/euler.cpp:925-932): s = State(u - U_ref).
+// The primitives of a host state (upload, residual): records of u.
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typename P::S* s) {
+__global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typename P::C* rec) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.n) return;
+  double uc[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const long long i = static_cast<long long>(k) * d.n + c;
-    s[i] = static_cast<typename P::S>(u[i] - d.ref[k]);
-  }
+  for (int k = 0; k < 5; ++k) uc[k] = u[static_cast<long long>(k) * d.n + c];
+  typename P::C w[5], dq[5];
+  prim_of_state(d, uc, w, dq);
+  store_prim<P>(rec, c, w);
 }
 
 // boundary_states (kernels/euler.py:455-466): prim_b of every boundary face.
@@ -162,160 +226,181 @@ __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   using C = typename P::C;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
-  C w[5], data[5], n[3], out[5];
-  prim_of(d, d.s, __ldg(d.b_own + b), w);
-  load5(d.b_data, d.nb, b, data);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
-  boundary_value(w, static_cast<C>(__ldg(d.b_kind + b)), data, n, d.p, out);
-#pragma unroll
-  for (int k = 0; k < 5; ++k) d.prim_b[k * d.nb + b] = static_cast<typename P::S>(out[k]);
+  C r[kBface], w[5], out[8];
+  load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
+  load_prim<P>(d.rec, index_of(r[13]), w);
+  boundary_value(w, r[7], r + 8, r, d.p, out);
+  out[5] = out[6] = out[7] = C(0);
+  store_words<P>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
 }
 
-// The value across incidence `code` of cell c (a neighbour's primitives or the boundary state),
-// with the face normal and area.
+// The minimum over a block of positive doubles' bits, then one atomicMin. Every thread of the
+// block calls it.
+__device__ __forceinline__ void block_min_dt(double dt, bool valid, unsigned long long* target) {
+  __shared__ unsigned long long warp_min[kBlock / 32];
+  unsigned long long b = valid && dt > 0.0 ? static_cast<unsigned long long>(__double_as_longlong(dt))
+                                           : ~0ULL;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(0xffffffffu, b, off);
+    b = o < b ? o : b;
+  }
+  if ((threadIdx.x & 31) == 0) warp_min[threadIdx.x >> 5] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = warp_min[0];
+    for (int i = 1; i < static_cast<int>(blockDim.x >> 5); ++i) m = warp_min[i] < m ? warp_min[i] : m;
+    if (m != ~0ULL) atomicMin(target, m);
+  }
+}
+
+// spectral_radius (kernels/euler.py:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89):
+// lambda_c = sum over its faces of max(|v . n| + c) A (FP64 sum, stored as State), dt_c = (cfl V)
+// / lambda_c.
 template <class P>
-__device__ __forceinline__ void across(const Dev<P>& d, int c, int code, typename P::C* wn,
-                                       typename P::C* n, typename P::C& area,
-                                       const typename P::C* rel_unused = nullptr) {
+__device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const typename P::C* wc,
+                                                 double cfl) {
   using C = typename P::C;
-  if (code >= 0) {
-    const int f = code >> 1;
-    const int o = (code & 1) ? __ldg(d.f_l + f) : __ldg(d.f_r + f);
-    prim_of(d, d.s, o, wn);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.f_n + static_cast<long long>(a) * d.n_if + f));
-    area = static_cast<C>(__ldg(d.f_a + f));
-  } else {
-    const int b = -code - 1;
-    load5(d.prim_b, d.nb, b, wn);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
-    area = static_cast<C>(__ldg(d.b_a + b));
-  }
-  (void)c;
-  (void)rel_unused;
-}
-
-// gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the
-// LSQ gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell,
-// then phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)).
-template <class P, bool LIMIT>
-__global__ void __launch_bounds__(kBlock) k_gradients(Dev<P> d) {
-  using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n) return;
-  C wc[5];
-  prim_of(d, d.s, c, wc);
-  double acc[15];
-#pragma unroll
-  for (int k = 0; k < 15; ++k) acc[k] = 0.0;
-  C lo[5], hi[5];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    lo[k] = C(INFINITY);
-    hi[k] = -C(INFINITY);
-  }
-  const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
-  const int len = __ldg(d.st_len + c);
-  for (int j = 0; j < len; ++j) {
-    const long long idx = base + static_cast<long long>(j) * kSlice;
-    const int e = __ldg(d.st_e + idx);
-    C wn[5];
-    if (e >= 0) {
-      prim_of(d, d.s, e, wn);
-    } else {
-      load5(d.prim_b, d.nb, -e - 1, wn);
-    }
-    const C w0 = static_cast<C>(__ldg(d.st_w + idx));
-    const C w1 = static_cast<C>(__ldg(d.st_w + d.st_total + idx));
-    const C w2 = static_cast<C>(__ldg(d.st_w + 2 * d.st_total + idx));
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      const C dw = wn[i] - wc[i];
-      acc[3 * i] += static_cast<double>(dw * w0);
-      acc[3 * i + 1] += static_cast<double>(dw * w1);
-      acc[3 * i + 2] += static_cast<double>(dw * w2);
-    }
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      if (wn[i] < lo[i]) lo[i] = wn[i];
-      if (wn[i] > hi[i]) hi[i] = wn[i];
-    }
-  }
-  // include_own_value (:517-521)
-  C g[15];
-#pragma unroll
-  for (int k = 0; k < 15; ++k) {
-    g[k] = static_cast<C>(acc[k]);
-    d.grad[static_cast<long long>(k) * d.n + c] = static_cast<typename P::G>(g[k]);
-  }
-  if constexpr (LIMIT) {
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      lo[i] = minv(lo[i], wc[i]);
-      hi[i] = maxv(hi[i], wc[i]);
-    }
-    const C vol = static_cast<C>(static_cast<typename P::GV>(__ldg(d.volume + c)));
-    C phi[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
-    const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
-    const int il = __ldg(d.inc_len + c);
-    for (int j = 0; j < il; ++j) {
-      const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
-      C r[3];
-      if (code >= 0) {
-        const int f = code >> 1;
-        const C* rr = (code & 1) ? d.f_rr : d.f_rl;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = __ldg(rr + static_cast<long long>(a) * d.n_if + f);
-      } else {
-        const int b = -code - 1;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = __ldg(d.b_r + a * d.nb + b);
-      }
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-        const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
-        if (v < phi[i]) phi[i] = v;
-      }
-    }
-    // at_most_one (:591-593)
-#pragma unroll
-    for (int i = 0; i < 5; ++i)
-      d.phi[static_cast<long long>(i) * d.n + c] = static_cast<typename P::S>(minv(phi[i], C(1.0)));
-  }
-}
-
-// spectral_radius (kernels/euler.py:1103-1112) and the CFL step of each cell
-// (device_stepper.cuh:84-89): lambda_c = sum over its faces of max(|v . n| + c) A (FP64 sum,
-// stored as State), dt_c = (cfl V) / lambda_c; the global step is their minimum (atomicMin on the
-// bits of positive doubles, exact and order-free).
-template <class P>
-__global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int local,
-                                                     double* dt_out) {
-  using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n) return;
-  C wc[5];
-  prim_of(d, d.s, c, wc);
   double acc = 0.0;
   const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
   const int il = __ldg(d.inc_len + c);
   for (int j = 0; j < il; ++j) {
     const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
-    C wn[5], n[3], area;
-    across(d, c, code, wn, n, area);
-    acc += static_cast<double>(wave_speed(wc, wn, n, area, d.p.g, d.p.pref));
+    C wn[5], rec[kFace];
+    if (code >= 0) {
+      const int f = code >> 1;
+      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, rec);
+      const int o = (code & 1) ? index_of(rec[7]) : index_of(rec[11]);
+      load_prim<P>(d.rec, o, wn);
+    } else {
+      const int b = -code - 1;
+      load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, 4, rec);
+      C t[8];
+      load_words<P>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, t);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) wn[k] = t[k];
+    }
+    acc += static_cast<double>(wave_speed(wc, wn, rec, rec[3], d.p.g, d.p.pref));
   }
-  const double lam = static_cast<double>(static_cast<typename P::S>(acc));
-  const double dt = cfl * d.volume[c] / lam;
-  if (local && d.dt_local != nullptr) d.dt_local[c] = dt;
-  if (dt_out != nullptr) dt_out[c] = dt;
-  if (d.ctl != nullptr && dt > 0.0)
-    atomicMin(&d.ctl->dt_bits, static_cast<unsigned long long>(__double_as_longlong(dt)));
+  const double lam = static_cast<double>(static_cast<C>(acc));
+  return cfl * d.volume[c] / lam;
+}
+
+// gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the
+// LSQ gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell,
+// then phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)). With DT,
+// also the cell's CFL step and the block's minimum.
+template <class P, bool LIMIT, bool DT>
+__global__ void __launch_bounds__(kBlock) k_gradients(Dev<P> d, double cfl, int local) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n;
+  double dt = 0.0;
+  if (live) {
+    C wc[5];
+    load_prim<P>(d.rec, c, wc);
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
+    }
+    const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
+    const int len = __ldg(d.st_len + c);
+    for (int j = 0; j < len; ++j) {
+      C e4[4];
+      load_words<P>(d.st + 4 * (base + static_cast<long long>(j) * kSlice), 0, 4, e4);
+      const int e = index_of(e4[3]);
+      C wn[5];
+      if (e >= 0) {
+        load_prim<P>(d.rec, e, wn);
+      } else {
+        C t[8];
+        load_words<P>(d.prim_b + static_cast<long long>(-e - 1) * kPrimB, 0, 8, t);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) wn[k] = t[k];
+      }
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const C dw = wn[i] - wc[i];
+        acc[3 * i] += static_cast<double>(dw * e4[0]);
+        acc[3 * i + 1] += static_cast<double>(dw * e4[1]);
+        acc[3 * i + 2] += static_cast<double>(dw * e4[2]);
+      }
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        if (wn[i] < lo[i]) lo[i] = wn[i];
+        if (wn[i] > hi[i]) hi[i] = wn[i];
+      }
+    }
+    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
+    C out[20];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
+    const C* g = out + 5;
+    if constexpr (LIMIT) {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        lo[i] = minv(lo[i], wc[i]);
+        hi[i] = maxv(hi[i], wc[i]);
+      }
+      const C vol = static_cast<C>(__ldg(d.volume + c));
+      C phi[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
+      const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+      const int il = __ldg(d.inc_len + c);
+      for (int j = 0; j < il; ++j) {
+        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+        C r[4];
+        if (code >= 0) {
+          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, (code & 1) ? 8 : 4, 4, r);
+        } else {
+          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 4, 4, r);
+        }
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+          if (v < phi[i]) phi[i] = v;
+        }
+      }
+      // at_most_one (:591-593)
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
+    } else {
+      // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = C(1.0);
+    }
+    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+    if constexpr (DT) {
+      dt = cell_time_step(d, c, wc, cfl);
+      if (local) d.dt_local[c] = dt;
+    }
+  }
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+// The CFL step alone (first-order schemes), with the block minimum; `dt_out` for the host.
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int local,
+                                                     double* dt_out) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n;
+  double dt = 0.0;
+  if (live) {
+    C wc[5];
+    load_prim<P>(d.rec, c, wc);
+    dt = cell_time_step(d, c, wc, cfl);
+    if (local && d.dt_local != nullptr) d.dt_local[c] = dt;
+    if (dt_out != nullptr) dt_out[c] = dt;
+  }
+  if (d.ctl != nullptr) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
 enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
@@ -323,34 +408,31 @@ enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
 // The faces of one owned cell (roe/hllc/ausm _faces and _boundaries, kernels/euler.py:687-1049),
 // gathered: every face flux of the cell recomputed here, added in increasing face index from the
 // source term -V s, as the reference's scatter adds them (emit_cpu.py emit_loop); then, in the RK
-// modes, the stage update in FP64 and the next stored state.
+// modes, the stage update in FP64 and the next stage's primitives.
 template <class P, int FLUX, bool PLANAR, bool SECOND>
 __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage, double wa,
                                                   double wb, int local, int last) {
   using C = typename P::C;
-  using S = typename P::S;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.n) return;
   C wc[5], gc[15], pc[5];
-  prim_of(d, d.s, c, wc);
   if constexpr (SECOND) {
-#pragma unroll
-    for (int k = 0; k < 15; ++k) gc[k] = static_cast<C>(__ldg(d.grad + static_cast<long long>(k) * d.n + c));
-    load5(d.phi, d.n, c, pc);
+    load_recon<P>(d.rec, c, wc, pc, gc);
   } else {
+    load_prim<P>(d.rec, c, wc);
 #pragma unroll
     for (int k = 0; k < 15; ++k) gc[k] = C(0.0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) pc[k] = C(0.0);
   }
   const double vol = __ldg(d.volume + c);
-  // sources (:611-616): res = -V s, computed in the compute type, stored in FP64.
+  // sources (:611-616): res = -V s, in the compute type, stored in FP64.
   double res[5];
   {
-    const C nv = -static_cast<C>(static_cast<typename P::GV>(vol));
+    const C nv = -static_cast<C>(vol);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-      const C s = d.source != nullptr ? static_cast<C>(__ldg(d.source + static_cast<long long>(k) * d.n + c)) : C(0.0);
+      const C s = d.source != nullptr ? __ldg(d.source + static_cast<long long>(k) * d.n + c) : C(0.0);
       res[k] = static_cast<double>(nv * s);
     }
   }
@@ -362,47 +444,42 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
     if (code >= 0) {
       const int f = code >> 1;
       const bool left = (code & 1) == 0;
-      const int o = left ? __ldg(d.f_r + f) : __ldg(d.f_l + f);
+      C fr_[kFace];
+      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr_);
+      const int o = left ? index_of(fr_[11]) : index_of(fr_[7]);
       C wo[5], go[15], po[5];
-      prim_of(d, d.s, o, wo);
       if constexpr (SECOND) {
-#pragma unroll
-        for (int k = 0; k < 15; ++k) go[k] = static_cast<C>(__ldg(d.grad + static_cast<long long>(k) * d.n + o));
-        load5(d.phi, d.n, o, po);
+        load_recon<P>(d.rec, o, wo, po, go);
       } else {
+        load_prim<P>(d.rec, o, wo);
 #pragma unroll
         for (int k = 0; k < 15; ++k) go[k] = C(0.0);
 #pragma unroll
         for (int k = 0; k < 5; ++k) po[k] = C(0.0);
       }
-      C n[3], rl[3], rr[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const long long i = static_cast<long long>(a) * d.n_if + f;
-        n[a] = static_cast<C>(__ldg(d.f_n + i));
-        rl[a] = __ldg(d.f_rl + i);
-        rr[a] = __ldg(d.f_rr + i);
-      }
-      const C area = static_cast<C>(__ldg(d.f_a + f));
+      const C* n = fr_;
+      const C area = fr_[3];
+      const C* rl = fr_ + 4;
+      const C* rr = fr_ + 8;
       const C* wl = left ? wc : wo;
       const C* gl = left ? gc : go;
       const C* pl = left ? pc : po;
       const C* wr = left ? wo : wc;
       const C* gr = left ? go : gc;
       const C* pr = left ? po : pc;
-      C fl[5], fr[5], fx[5];
+      C fl[5], frr[5], fx[5];
       reconstruct(wl, gl, pl, rl, d.p.pref, fl);
-      reconstruct(wr, gr, pr, rr, d.p.pref, fr);
-      numerical_flux<FLUX>(fl, fr, n, d.p, fx);
+      reconstruct(wr, gr, pr, rr, d.p.pref, frr);
+      numerical_flux<FLUX>(fl, frr, n, d.p, fx);
       if constexpr (PLANAR) {
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
       } else {
         C m[9], avg[5], wt[5];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) m[q] = static_cast<C>(__ldg(d.f_m + static_cast<long long>(q) * d.n_if + f));
+        for (int q = 0; q < 9; ++q) m[q] = __ldg(d.f_m + static_cast<long long>(q) * d.n_if + f);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) avg[k] = C(0.5) * (fl[k] + fr[k]);
+        for (int k = 0; k < 5; ++k) avg[k] = C(0.5) * (fl[k] + frr[k]);
         warp_term(avg, gl, pl, gr, pr, m, d.p.g, d.p.pref, wt);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = area * fx[k] + wt[k];
@@ -416,16 +493,12 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
       }
     } else {
       const int b = -code - 1;
-      C n[3], r[3], data[5], wf[5], wbv[5];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        n[a] = static_cast<C>(__ldg(d.b_n + a * d.nb + b));
-        r[a] = __ldg(d.b_r + a * d.nb + b);
-      }
-      load5(d.b_data, d.nb, b, data);
-      const C kind = static_cast<C>(__ldg(d.b_kind + b));
-      const C area = static_cast<C>(__ldg(d.b_a + b));
-      reconstruct(wc, gc, pc, r, d.p.pref, wf);
+      C br[kBface], wf[5], wbv[5];
+      load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+      const C* n = br;
+      const C area = br[3];
+      const C kind = br[7];
+      reconstruct(wc, gc, pc, br + 4, d.p.pref, wf);
       const bool slip = (kind > C(1.5)) & (kind < C(2.5));
       const bool wall = PLANAR ? slip : (slip | (kind > C(4.5)));
       if (wall) {
@@ -436,7 +509,7 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
         } else {
           C m[9];
 #pragma unroll
-          for (int q = 0; q < 9; ++q) m[q] = static_cast<C>(__ldg(d.b_m + static_cast<long long>(q) * d.nb + b));
+          for (int q = 0; q < 9; ++q) m[q] = __ldg(d.b_m + static_cast<long long>(q) * d.nb + b);
           // wall_warp (:678-681): p_l M^T grad p.
           C ww[5] = {C(0.0), C(0.0), C(0.0), C(0.0), C(0.0)};
 #pragma unroll
@@ -446,7 +519,7 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
           for (int k = 0; k < 5; ++k) out[k] = area * wfl[k] + ww[k];
         }
       } else {
-        boundary_value(wf, kind, data, n, d.p, wbv);
+        boundary_value(wf, kind, br + 8, n, d.p, wbv);
         C fx[5];
         numerical_flux<FLUX>(wf, wbv, n, d.p, fx);
 #pragma unroll
@@ -503,16 +576,15 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
     } else if (mode == kRk3) {
       d.stage[i] = nu[k];
     }
-    d.s_next[i] = static_cast<S>(nu[k] - d.ref[k]);
   }
+  C w[5], dq[5];
+  prim_of_state(d, nu, w, dq);
+  store_prim<P>(d.rec_next, c, w);
   if (last) {
     // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
     // it, in the compute type, then this stage's residual.
     const C g = d.p.g;
     const C r0 = static_cast<C>(d.ref[0]);
-    C dq[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(static_cast<S>(nu[k] - d.ref[k]));
     const C rho = r0 + dq[0];
     C dm_m = C(0), mr_mr = C(0);
 #pragma unroll
@@ -592,10 +664,14 @@ __global__ void k_end_step(Control* ctl) {
   if (threadIdx.x == 0) ctl->step += 1;
 }
 
+// Gradients and limiter of the records, as FP64 SoA (15 x n, 5 x n).
 template <class P>
-__global__ void k_to_double(const typename P::G* a, long long n, double* out) {
-  const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (i < n) out[i] = static_cast<double>(a[i]);
+__global__ void k_unpack(const typename P::C* rec, int n, double* grad, double* phi) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const typename P::C* r = rec + static_cast<long long>(c) * kRec;
+  for (int k = 0; k < 15; ++k) grad[static_cast<long long>(k) * n + c] = static_cast<double>(r[kGrad + k]);
+  for (int k = 0; k < 5; ++k) phi[static_cast<long long>(k) * n + c] = static_cast<double>(r[kPhi + k]);
 }
 
 // ---------------------------------------------------------------- host side
@@ -648,9 +724,10 @@ class Buffer {
 
 template <class T>
 Buffer upload(const std::vector<T>& v, cudaStream_t s) {
-  Buffer b(v.size() * sizeof(T));
-  if (!v.empty()) check(cudaMemcpyAsync(b.as<void>(), v.data(), v.size() * sizeof(T),
-                                        cudaMemcpyHostToDevice, s), "upload");  // NOLINT
+  Buffer b(std::max<size_t>(v.size(), 1) * sizeof(T));
+  if (!v.empty())
+    check(cudaMemcpyAsync(b.ptr(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s),
+          "upload");
   return b;
 }
 
@@ -668,8 +745,8 @@ struct Sliced {
 Sliced slice_rows(const std::vector<long long>& off) {
   Sliced s;
   const int n = static_cast<int>(off.size()) - 1;
-  s.len.resize(n);
-  s.start.resize((n + kSlice - 1) / kSlice + 1);
+  s.len.assign(std::max(n, 1), 0);
+  s.start.assign((n + kSlice - 1) / kSlice + 1, 0);
   long long run = 0;
   for (int sl = 0; sl * kSlice < n; ++sl) {
     long long longest = 0;
@@ -678,14 +755,25 @@ Sliced slice_rows(const std::vector<long long>& off) {
       s.len[r] = static_cast<int>(off[r + 1] - off[r]);
       longest = std::max(longest, off[r + 1] - off[r]);
     }
-    if (run > std::numeric_limits<int>::max()) fail("E1101: stencil too large for int32 offsets");
     s.start[sl] = static_cast<int>(run);
     run += longest * kSlice;
+    if (run >= std::numeric_limits<int>::max() / 4) fail("E1101: stencil too large for int32 offsets");
   }
-  s.start.back() = static_cast<int>(std::min<long long>(run, std::numeric_limits<int>::max()));
+  s.start.back() = static_cast<int>(run);
   s.total = run;
-  if (run >= std::numeric_limits<int>::max()) fail("E1101: stencil too large for int32 offsets");
   return s;
+}
+
+template <class C>
+C index_bits(int i) {
+  C x;
+  if constexpr (sizeof(C) == 4) {
+    std::memcpy(&x, &i, 4);
+  } else {
+    const long long l = i;
+    std::memcpy(&x, &l, 8);
+  }
+  return x;
 }
 
 struct Counters {
@@ -720,9 +808,6 @@ class Stepper {
 template <class P>
 class Impl final : public Stepper {
   using C = typename P::C;
-  using S = typename P::S;
-  using G = typename P::G;
-  using GV = typename P::GV;
 
  public:
   Impl(const autan_euler_mesh& m, const autan_euler_scheme& sc, cudaStream_t st)
@@ -766,44 +851,45 @@ class Impl final : public Stepper {
         if (m.face_moment[i] != 0.0)
           fail("E1101: planar loops on a mesh with a face not proven planar");
     }
-    // Interior faces touching owned cells.
-    std::vector<int> fl(nif_), fr(nif_);
-    std::vector<GV> fn(3LL * nif_), fa(nif_), fm(planar_ ? 0 : 9LL * nif_);
-    std::vector<C> frl(3LL * nif_), frr(3LL * nif_);
+    const long long NF = nf_, NC = nc_;
+    // Interior face records.
+    std::vector<C> face(static_cast<size_t>(kFace) * std::max(nif_, 1), C(0));
+    std::vector<C> fm(planar_ ? 0 : 9LL * nif_);
     for (int f = 0; f < nif_; ++f) {
       const int l = m.owner[f], rr = m.neighbour[f];
-      fl[f] = val[l];
-      fr[f] = val[rr];
+      C* q = face.data() + static_cast<long long>(f) * kFace;
       for (int a = 0; a < 3; ++a) {
-        fn[a * static_cast<long long>(nif_) + f] = static_cast<GV>(m.face_normal[a * static_cast<long long>(nf_) + f]);
-        const double xf = m.face_centroid[a * static_cast<long long>(nf_) + f];
-        frl[a * static_cast<long long>(nif_) + f] = static_cast<C>(xf - m.cell_centroid[a * static_cast<long long>(nc_) + l]);
-        frr[a * static_cast<long long>(nif_) + f] = static_cast<C>(xf - m.cell_centroid[a * static_cast<long long>(nc_) + rr]);
+        q[a] = static_cast<C>(m.face_normal[a * NF + f]);
+        const double xf = m.face_centroid[a * NF + f];
+        q[4 + a] = static_cast<C>(xf - m.cell_centroid[a * NC + l]);
+        q[8 + a] = static_cast<C>(xf - m.cell_centroid[a * NC + rr]);
       }
-      fa[f] = static_cast<GV>(m.face_area_magnitude[f]);
+      q[3] = static_cast<C>(m.face_area_magnitude[f]);
+      q[7] = index_bits<C>(val[l]);
+      q[11] = index_bits<C>(val[rr]);
       if (!planar_)
-        for (int q = 0; q < 9; ++q)
-          fm[q * static_cast<long long>(nif_) + f] =
-              m.face_moment != nullptr ? static_cast<GV>(m.face_moment[q * static_cast<long long>(nf_) + f]) : GV(0);
+        for (int j = 0; j < 9; ++j)
+          fm[j * static_cast<long long>(nif_) + f] =
+              m.face_moment != nullptr ? static_cast<C>(m.face_moment[j * NF + f]) : C(0);
     }
-    // Boundary faces (all of them: the stencils of owned cells reach those of images).
-    std::vector<int> bown(nb_);
-    std::vector<GV> bn(3LL * nb_), ba(nb_), bm(planar_ ? 0 : 9LL * nb_);
-    std::vector<C> br(3LL * nb_);
+    // Boundary face records (all of them: the stencils of owned cells reach those of images).
+    bface_host_.assign(static_cast<size_t>(kBface) * std::max(nb_, 1), C(0));
+    std::vector<C> bm(planar_ ? 0 : 9LL * nb_);
     for (int b = 0; b < nb_; ++b) {
       const int f = ni_ + b;
       const int o = m.owner[f];
-      bown[b] = val[o];
+      C* q = bface_host_.data() + static_cast<long long>(b) * kBface;
       for (int a = 0; a < 3; ++a) {
-        bn[a * static_cast<long long>(nb_) + b] = static_cast<GV>(m.face_normal[a * static_cast<long long>(nf_) + f]);
-        br[a * static_cast<long long>(nb_) + b] = static_cast<C>(m.face_centroid[a * static_cast<long long>(nf_) + f] -
-                                                                 m.cell_centroid[a * static_cast<long long>(nc_) + o]);
+        q[a] = static_cast<C>(m.face_normal[a * NF + f]);
+        q[4 + a] = static_cast<C>(m.face_centroid[a * NF + f] - m.cell_centroid[a * NC + o]);
       }
-      ba[b] = static_cast<GV>(m.face_area_magnitude[f]);
+      q[3] = static_cast<C>(m.face_area_magnitude[f]);
+      q[7] = C(2);  // slip until set_boundary
+      q[13] = index_bits<C>(val[o]);
       if (!planar_)
-        for (int q = 0; q < 9; ++q)
-          bm[q * static_cast<long long>(nb_) + b] =
-              m.face_moment != nullptr ? static_cast<GV>(m.face_moment[q * static_cast<long long>(nf_) + f]) : GV(0);
+        for (int j = 0; j < 9; ++j)
+          bm[j * static_cast<long long>(nb_) + b] =
+              m.face_moment != nullptr ? static_cast<C>(m.face_moment[j * NF + f]) : C(0);
     }
     // Incidences of owned cells, in increasing face index, sliced.
     std::vector<long long> ioff(n_ + 1);
@@ -816,7 +902,7 @@ class Impl final : public Stepper {
         const int f = m.cell_faces[k];
         if (f <= prev) fail("E1101: cell_faces must list each cell's faces in increasing order");
         prev = f;
-        int v;
+        int v = 0;
         if (f < ni_) {
           if (f >= nif_) fail("E1101: an owned cell's interior face lies beyond the owned faces");
           if (m.owner[f] == c) {
@@ -834,7 +920,7 @@ class Impl final : public Stepper {
         code[inc_.at(c, static_cast<int>(k - ioff[c]))] = v;
       }
     }
-    // Stencil of owned cells, sliced: values at the owned cell of an image.
+    // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, value index or -(b + 1)}.
     const bool has_stencil =
         m.stencil != nullptr && m.stencil_offsets != nullptr && m.stencil_lsq_weight != nullptr;
     std::vector<long long> soff(n_ + 1, 0);
@@ -842,8 +928,7 @@ class Impl final : public Stepper {
       for (int c = 0; c <= n_; ++c) soff[c] = m.stencil_offsets[c] - m.stencil_offsets[0];
     st_ = slice_rows(soff);
     const long long nst = has_stencil ? m.stencil_offsets[nc_] : 0;
-    std::vector<int> ste(std::max<long long>(st_.total, 1), 0);
-    std::vector<GV> stw(3 * std::max<long long>(st_.total, 1), GV(0));
+    std::vector<C> ste(4 * std::max<long long>(st_.total, 1), C(0));
     for (int c = 0; c < (has_stencil ? n_ : 0); ++c) {
       for (long long k = m.stencil_offsets[c]; k < m.stencil_offsets[c + 1]; ++k) {
         const int e = m.stencil[k];
@@ -856,19 +941,16 @@ class Impl final : public Stepper {
           if (f < ni_ || f >= nf_) fail("E1101: a stencil entry is not a boundary face");
           v = -(f - ni_ + 1);
         }
-        const long long at = st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
-        ste[at] = v;
-        for (int a = 0; a < 3; ++a)
-          stw[a * st_.total + at] = static_cast<GV>(m.stencil_lsq_weight[a * nst + k]);
+        C* q = ste.data() + 4 * st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
+        for (int a = 0; a < 3; ++a) q[a] = static_cast<C>(m.stencil_lsq_weight[a * nst + k]);
+        q[3] = index_bits<C>(v);
       }
     }
     std::vector<double> vol(m.cell_volume, m.cell_volume + n_);
     // Device arrays.
     const size_t n5 = 5ULL * n_;
-    for (auto& b : s_) b.alloc(n5 * sizeof(S));
-    grad_.alloc(15ULL * n_ * sizeof(G));
-    phi_.alloc(n5 * sizeof(S));
-    prim_b_.alloc(5ULL * std::max(nb_, 1) * sizeof(S));
+    for (auto& b : rec_) b.alloc(static_cast<size_t>(kRec) * n_ * sizeof(C));
+    prim_b_.alloc(static_cast<size_t>(kPrimB) * std::max(nb_, 1) * sizeof(C));
     u_.alloc(n5 * sizeof(double));
     stage_.alloc(n5 * sizeof(double));
     racc_.alloc(n5 * sizeof(double));
@@ -879,38 +961,20 @@ class Impl final : public Stepper {
     st_start_ = upload(st_.start, stream);
     st_len_ = upload(st_.len, stream);
     st_e_ = upload(ste, stream);
-    st_w_ = upload(stw, stream);
     inc_start_ = upload(inc_.start, stream);
     inc_len_ = upload(inc_.len, stream);
     inc_code_ = upload(code, stream);
-    f_l_ = upload(fl, stream);
-    f_r_ = upload(fr, stream);
-    f_n_ = upload(fn, stream);
-    f_a_ = upload(fa, stream);
-    f_rl_ = upload(frl, stream);
-    f_rr_ = upload(frr, stream);
+    face_ = upload(face, stream);
     f_m_ = upload(fm, stream);
-    b_own_ = upload(bown, stream);
-    b_n_ = upload(bn, stream);
-    b_a_ = upload(ba, stream);
-    b_r_ = upload(br, stream);
+    bface_ = upload(bface_host_, stream);
     b_m_ = upload(bm, stream);
-    std::vector<unsigned char> kind(std::max(nb_, 1), 2);
-    b_kind_ = upload(kind, stream);
-    b_data_.alloc(5ULL * std::max(nb_, 1) * sizeof(S));
-    check(cudaMemsetAsync(b_data_.as<void>(), 0, b_data_.bytes(), stream), "memset");
-    for (auto* b : {&grad_, &phi_, &prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
+    for (Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
       check(cudaMemsetAsync(b->ptr(), 0, b->bytes(), stream), "memset");
-    for (auto& b : s_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
-    if (second_ && !limiter_) fill_phi_one();
+    for (auto& b : rec_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
     d_.n = n_;
     d_.nb = nb_;
     d_.n_if = nif_;
-    d_.st_total = st_.total;
-    d_.inc_total = inc_.total;
-    d_.grad = grad_.as<G>();
-    d_.phi = phi_.as<S>();
-    d_.prim_b = prim_b_.as<S>();
+    d_.prim_b = prim_b_.as<C>();
     d_.u = u_.as<double>();
     d_.stage = stage_.as<double>();
     d_.racc = racc_.as<double>();
@@ -920,25 +984,14 @@ class Impl final : public Stepper {
     d_.source = nullptr;
     d_.st_start = st_start_.as<int>();
     d_.st_len = st_len_.as<int>();
-    d_.st_e = st_e_.as<int>();
-    d_.st_w = st_w_.as<GV>();
+    d_.st = st_e_.as<C>();
     d_.inc_start = inc_start_.as<int>();
     d_.inc_len = inc_len_.as<int>();
     d_.inc_code = inc_code_.as<int>();
-    d_.f_l = f_l_.as<int>();
-    d_.f_r = f_r_.as<int>();
-    d_.f_n = f_n_.as<GV>();
-    d_.f_a = f_a_.as<GV>();
-    d_.f_rl = f_rl_.as<C>();
-    d_.f_rr = f_rr_.as<C>();
-    d_.f_m = f_m_.as<GV>();
-    d_.b_own = b_own_.as<int>();
-    d_.b_kind = b_kind_.as<unsigned char>();
-    d_.b_data = b_data_.as<S>();
-    d_.b_n = b_n_.as<GV>();
-    d_.b_a = b_a_.as<GV>();
-    d_.b_r = b_r_.as<C>();
-    d_.b_m = b_m_.as<GV>();
+    d_.face = face_.as<C>();
+    d_.bface = bface_.as<C>();
+    d_.f_m = f_m_.as<C>();
+    d_.b_m = b_m_.as<C>();
     d_.ctl = ctl_.as<Control>();
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     check(cudaStreamSynchronize(stream), "create");
@@ -951,65 +1004,56 @@ class Impl final : public Stepper {
 
   long long device_bytes() const override {
     long long t = 0;
-    for (const Buffer* b : {&grad_, &phi_, &prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_,
-                            &ctl_, &volume_, &st_start_, &st_len_, &st_e_, &st_w_, &inc_start_,
-                            &inc_len_, &inc_code_, &f_l_, &f_r_, &f_n_, &f_a_, &f_rl_, &f_rr_,
-                            &f_m_, &b_own_, &b_kind_, &b_data_, &b_n_, &b_a_, &b_r_, &b_m_,
-                            &source_})
+    for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
+                            &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
+                            &face_, &f_m_, &bface_, &b_m_, &source_})
       t += static_cast<long long>(b->bytes());
-    for (const auto& b : s_) t += static_cast<long long>(b.bytes());
+    for (const auto& b : rec_) t += static_cast<long long>(b.bytes());
     return t;
   }
 
   void set_boundary(const uint8_t* kind, const double* data) override {
-    std::vector<unsigned char> k(std::max(nb_, 1), 2);
     for (int b = 0; b < nb_; ++b) {
       if (kind[b] > 5) fail("E1101: boundary code out of range");
-      k[b] = kind[b];
+      bface_host_[static_cast<long long>(b) * kBface + 7] = static_cast<C>(kind[b]);
     }
-    b_kind_ = upload(k, stream);
-    d_.b_kind = b_kind_.as<unsigned char>();
     set_boundary_data(data);
     drop_graph();
   }
 
   void set_boundary_data(const double* data) override {
-    std::vector<S> v(5ULL * std::max(nb_, 1), S(0));
-    for (long long i = 0; i < 5LL * nb_; ++i) v[i] = static_cast<S>(data[i]);
-    check(cudaMemcpyAsync(b_data_.as<void>(), v.data(), v.size() * sizeof(S),
+    for (int b = 0; b < nb_; ++b)
+      for (int k = 0; k < 5; ++k)
+        bface_host_[static_cast<long long>(b) * kBface + 8 + k] =
+            static_cast<C>(data[k * static_cast<long long>(nb_) + b]);
+    check(cudaMemcpyAsync(bface_.ptr(), bface_host_.data(), bface_host_.size() * sizeof(C),
                           cudaMemcpyHostToDevice, stream), "boundary data");
     check(cudaStreamSynchronize(stream), "boundary data");
   }
 
   void set_source(const double* source) override {
-    std::vector<S> v(5ULL * n_);
+    std::vector<C> v(5ULL * n_);
     bool any = false;
     for (int k = 0; k < 5; ++k)
       for (int c = 0; c < n_; ++c) {
-        v[k * static_cast<long long>(n_) + c] = static_cast<S>(source[k * static_cast<long long>(nc_) + c]);
-        any = any || v[k * static_cast<long long>(n_) + c] != S(0);
+        v[k * static_cast<long long>(n_) + c] = static_cast<C>(source[k * static_cast<long long>(nc_) + c]);
+        any = any || v[k * static_cast<long long>(n_) + c] != C(0);
       }
     if (!any) {
       source_ = Buffer();
       d_.source = nullptr;
     } else {
       source_ = upload(v, stream);
-      d_.source = source_.as<S>();
+      d_.source = source_.as<C>();
       check(cudaStreamSynchronize(stream), "source");
     }
     drop_graph();
   }
 
   void set_second_order(bool on) override {
+    // As the host (physics/src/euler.cpp:903-912): without reconstruction the faces read no
+    // gradients or limiter; unlimited, phi is 1 (written by the gradient kernel).
     second_ = on;
-    // As the host (physics/src/euler.cpp:903-912): without reconstruction gradients and limiter
-    // are zero; unlimited, phi is 1.
-    check(cudaMemsetAsync(grad_.as<void>(), 0, grad_.bytes(), stream), "grad");
-    if (on && !limiter_) {
-      fill_phi_one();
-    } else {
-      check(cudaMemsetAsync(phi_.as<void>(), 0, phi_.bytes(), stream), "phi");
-    }
     drop_graph();
   }
 
@@ -1034,7 +1078,8 @@ class Impl final : public Stepper {
 
   void upload_state(const double* u) override {
     copy_in(u, u_.as<double>());
-    launch_store(u_.as<double>(), s_[0].as<S>());
+    launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
+           rec_[0].as<C>());
     check(cudaStreamSynchronize(stream), "upload");
   }
 
@@ -1042,8 +1087,9 @@ class Impl final : public Stepper {
 
   void residual(const double* u, double* res) override {
     copy_in(u, stage_.as<double>());
-    launch_store(stage_.as<double>(), s_[1].as<S>());
-    enqueue_residual(s_[1].as<S>());
+    launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(stage_.as<double>()),
+           rec_[1].as<C>());
+    enqueue_residual(1);
     copy_out(res_.as<double>(), res);
     for (int k = 0; k < 5; ++k)
       for (int g = n_; g < nc_; ++g) res[k * static_cast<long long>(nc_) + g] = 0.0;
@@ -1051,18 +1097,18 @@ class Impl final : public Stepper {
 
   void evaluate(autan_euler_step_result* out) override {
     launch(k_begin, 1, 256, d_.ctl, 1.0);
-    enqueue_residual(s_[0].as<S>());
+    enqueue_residual(0);
     launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
     launch(k_norm_finish, 1, 32, d_.ctl, n_, 0);
-    Control h;
-    read_control(&h);
-    for (int k = 0; k < 5; ++k) out->residuals[k] = h.rms[k];
+    check(cudaMemcpyAsync(head_, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
+    check(cudaStreamSynchronize(stream), "evaluate");
+    for (int k = 0; k < 5; ++k) out->residuals[k] = head_->rms[k];
     out->time_step = 0.0;
     out->steps = 0;
     // invalid(): the state, then the residual.
     std::vector<double> u(5ULL * n_), r(5ULL * n_);
-    check(cudaMemcpyAsync(u.data(), u_.as<void>(), u.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
-    check(cudaMemcpyAsync(r.data(), res_.as<void>(), r.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
+    check(cudaMemcpyAsync(u.data(), u_.ptr(), u.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
+    check(cudaMemcpyAsync(r.data(), res_.ptr(), r.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
     check(cudaStreamSynchronize(stream), "evaluate");
     out->invalid_cell = first_invalid(u, r);
   }
@@ -1076,7 +1122,7 @@ class Impl final : public Stepper {
     check(cudaMemsetAsync(&d_.ctl->step, 0, sizeof(long long), stream), "reset");
     const StepKey key{cfl, dt, local, rk};
     if (graph) {
-      if (!graph_exec_ || !(key == graph_key_)) capture(key);
+      if (graph_exec_ == nullptr || !(key == graph_key_)) capture(key);
       for (long long i = 0; i < n; ++i) {
         check(cudaGraphLaunch(graph_exec_, stream), "cudaGraphLaunch");
         counters.launches += graph_nodes_;
@@ -1085,113 +1131,51 @@ class Impl final : public Stepper {
       for (long long i = 0; i < n; ++i) enqueue_step(key);
     }
     counters.steps += n;
+    last_rec_ = rk == 3 ? 2 : 1;
     // The result: the control's head (the last step's sums, step and marks) only.
-    Control* h = head_;
-    check(cudaMemcpyAsync(h, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
+    check(cudaMemcpyAsync(head_, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
     check(cudaStreamSynchronize(stream), "control");
-    for (int k = 0; k < 5; ++k) out->residuals[k] = h->rms[k];
-    out->time_step = h->dt;
-    out->steps = h->step;
-    out->invalid_cell = h->bad_state != ~0ULL ? static_cast<int64_t>(h->bad_state)
-                        : h->bad_res != ~0ULL ? static_cast<int64_t>(h->bad_res)
-                                              : -1;
+    for (int k = 0; k < 5; ++k) out->residuals[k] = head_->rms[k];
+    out->time_step = head_->dt;
+    out->steps = head_->step;
+    out->invalid_cell = head_->bad_state != ~0ULL ? static_cast<int64_t>(head_->bad_state)
+                        : head_->bad_res != ~0ULL ? static_cast<int64_t>(head_->bad_res)
+                                                  : -1;
   }
 
   void history(long long count, double* rms, double* dt) override {
-    Control h;
-    read_control(&h);
-    const long long n = std::min<long long>({count, h.step, kHistory});
+    std::vector<Control> h(1);
+    check(cudaMemcpyAsync(h.data(), d_.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control");
+    check(cudaStreamSynchronize(stream), "control");
+    const long long n = std::min<long long>({count, h[0].step, kHistory});
     for (long long i = 0; i < n; ++i) {
       if (rms != nullptr)
-        for (int k = 0; k < 5; ++k) rms[5 * i + k] = h.hist_rms[i][k];
-      if (dt != nullptr) dt[i] = h.hist_dt[i];
+        for (int k = 0; k < 5; ++k) rms[5 * i + k] = h[0].hist_rms[i][k];
+      if (dt != nullptr) dt[i] = h[0].hist_dt[i];
     }
   }
 
   void gradients(double* grad, double* phi) override {
-    Buffer tmp(15ULL * n_ * sizeof(double));
-    if (grad != nullptr) {
-      launch(k_to_double<P>, blocks(15LL * n_), kBlock, static_cast<const G*>(grad_.as<G>()), 15LL * n_, tmp.as<double>());
-      check(cudaMemcpyAsync(grad, tmp.as<void>(), 15ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "grad");
-    }
-    check(cudaStreamSynchronize(stream), "grad");
-    if (phi != nullptr) {
-      launch(k_to_double<P>, blocks(5LL * n_), kBlock, reinterpret_cast<const G*>(phi_.as<S>()), 5LL * n_, tmp.as<double>());
-      check(cudaMemcpyAsync(phi, tmp.as<void>(), 5ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "phi");
-    }
+    Buffer g(15ULL * n_ * sizeof(double)), f(5ULL * n_ * sizeof(double));
+    launch(k_unpack<P>, blocks(n_), kBlock, static_cast<const C*>(rec_[last_rec_].as<C>()), n_,
+           g.as<double>(), f.as<double>());
+    if (grad != nullptr)
+      check(cudaMemcpyAsync(grad, g.ptr(), 15ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "grad");
+    if (phi != nullptr)
+      check(cudaMemcpyAsync(phi, f.ptr(), 5ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "phi");
     check(cudaStreamSynchronize(stream), "gradients");
   }
 
   void time_steps(double cfl, double* dt) override {
     Buffer tmp(std::max(n_, 1) * sizeof(double));
-    launch(k_boundary_states<P>, blocks(nb_), kBlock, with_state(s_[0].as<S>()));
-    launch(k_spectral<P>, blocks(n_), kBlock, with_state(s_[0].as<S>()), cfl, 0, tmp.as<double>());
-    check(cudaMemcpyAsync(dt, tmp.as<void>(), n_ * sizeof(double), cudaMemcpyDeviceToHost, stream), "dt");
+    Dev<P> d = with_rec(0, 0);
+    launch(k_boundary_states<P>, blocks(nb_), kBlock, d);
+    d.ctl = nullptr;
+    launch(k_spectral<P>, blocks(n_), kBlock, d, cfl, 0, tmp.as<double>());
+    check(cudaMemcpyAsync(dt, tmp.ptr(), n_ * sizeof(double), cudaMemcpyDeviceToHost, stream), "dt");
     check(cudaStreamSynchronize(stream), "time steps");
   }
 
-  std::vector<int> ghost_owner_;
-
- private:
-  struct StepKey {
-    double cfl, dt;
-    bool local;
-    int rk;
-    bool operator==(const StepKey& o) const {
-      return cfl == o.cfl && dt == o.dt && local == o.local && rk == o.rk;
-    }
-  };
-
-  void validate(const autan_euler_mesh& m) {
-    if (m.n_owned_cells < 1 || m.n_cells < m.n_owned_cells || m.n_faces < m.n_interior_faces ||
-        m.n_owned_interior_faces > m.n_interior_faces || m.n_owned_faces > m.n_faces ||
-        m.n_owned_faces < m.n_interior_faces)
-      fail("E1101: inconsistent mesh counts");
-    if (m.owner == nullptr || m.cell_face_offsets == nullptr || m.cell_faces == nullptr ||
-        m.face_normal == nullptr || m.face_area_magnitude == nullptr ||
-        m.face_centroid == nullptr || m.cell_centroid == nullptr || m.cell_volume == nullptr ||
-        (m.n_interior_faces > 0 && m.neighbour == nullptr))
-      fail("E1101: a required mesh array is NULL");
-    if (m.n_cells > m.n_owned_cells && m.ghost_owner == nullptr)
-      fail("E1101: ghost cells need ghost_owner");
-    if (second_ && (m.stencil == nullptr || m.stencil_offsets == nullptr ||
-                    m.stencil_lsq_weight == nullptr))
-      fail("E1101: a second-order scheme needs the stencil and its weights");
-    if (scheme_.flux < 0 || scheme_.flux > 2) fail("E1101: unknown flux");
-    for (int c = 0; c < m.n_owned_cells; ++c)
-      if (!(m.cell_volume[c] > 0.0)) fail("E0121: an owned cell has a non-positive volume");
-    ghost_owner_.assign(m.ghost_owner, m.ghost_owner + (m.n_cells - m.n_owned_cells));
-  }
-
-  static int blocks(long long n) { return static_cast<int>(std::max<long long>(1, (n + kBlock - 1) / kBlock)); }
-  int norm_blocks() const { return std::min(blocks(n_), 148 * 8); }
-
-  // Kernel kinds of autan_euler_device_kernel_times.
-  enum Kind : int { kBoundary = 0, kGradients = 1, kSpectral = 2, kFaces = 3, kNorms = 4, kControl = 5 };
-
-  template <class K, class... A>
-  void launch(K kernel, int grid, int block, A... args) {
-    launch_as(kControl, kernel, grid, block, args...);
-  }
-
-  template <class K, class... A>
-  void launch_as(int kind, K kernel, int grid, int block, A... args) {
-    cudaEvent_t before = nullptr, after = nullptr;
-    if (timing_) {
-      check(cudaEventCreate(&before), "event");
-      check(cudaEventCreate(&after), "event");
-      check(cudaEventRecord(before, stream), "event");
-    }
-    kernel<<<grid, block, 0, stream>>>(args...);
-    check(cudaGetLastError(), "kernel launch");
-    ++counters.launches;
-    if (timing_) {
-      check(cudaEventRecord(after, stream), "event");
-      timed_.push_back({kind, before, after});
-    }
-  }
-
- public:
   // Runs n steps with CUDA events around every launch on the handle's stream; per kind the total
   // milliseconds and the launches.
   void kernel_times(double cfl, double dt, bool local, int rk, long long n, double* ms,
@@ -1222,28 +1206,84 @@ class Impl final : public Stepper {
     counters.steps += n;
   }
 
- private:
+  std::vector<int> ghost_owner_;
 
-  Dev<P> with_state(const S* s, S* s_next = nullptr) const {
+ private:
+  struct StepKey {
+    double cfl, dt;
+    bool local;
+    int rk;
+    bool operator==(const StepKey& o) const {
+      return cfl == o.cfl && dt == o.dt && local == o.local && rk == o.rk;
+    }
+  };
+
+  // Kernel kinds of autan_euler_device_kernel_times.
+  enum Kind : int { kBoundary = 0, kGradients = 1, kSpectral = 2, kFaces = 3, kNorms = 4, kControl = 5 };
+
+  void validate(const autan_euler_mesh& m) {
+    if (m.n_owned_cells < 1 || m.n_cells < m.n_owned_cells || m.n_faces < m.n_interior_faces ||
+        m.n_owned_interior_faces > m.n_interior_faces || m.n_owned_faces > m.n_faces ||
+        m.n_owned_faces < m.n_interior_faces)
+      fail("E1101: inconsistent mesh counts");
+    if (m.owner == nullptr || m.cell_face_offsets == nullptr || m.cell_faces == nullptr ||
+        m.face_normal == nullptr || m.face_area_magnitude == nullptr ||
+        m.face_centroid == nullptr || m.cell_centroid == nullptr || m.cell_volume == nullptr ||
+        (m.n_interior_faces > 0 && m.neighbour == nullptr))
+      fail("E1101: a required mesh array is NULL");
+    if (m.n_cells > m.n_owned_cells && m.ghost_owner == nullptr)
+      fail("E1101: ghost cells need ghost_owner");
+    if (second_ && (m.stencil == nullptr || m.stencil_offsets == nullptr ||
+                    m.stencil_lsq_weight == nullptr))
+      fail("E1101: a second-order scheme needs the stencil and its weights");
+    if (scheme_.flux < 0 || scheme_.flux > 2) fail("E1101: unknown flux");
+    for (int c = 0; c < m.n_owned_cells; ++c)
+      if (!(m.cell_volume[c] > 0.0)) fail("E0121: an owned cell has a non-positive volume");
+    if (m.n_cells > m.n_owned_cells)
+      ghost_owner_.assign(m.ghost_owner, m.ghost_owner + (m.n_cells - m.n_owned_cells));
+    if (static_cast<long long>(m.n_owned_cells) >= (1LL << 30)) fail("E1101: mesh too large");
+  }
+
+  static int blocks(long long n) {
+    return static_cast<int>(std::max<long long>(1, (n + kBlock - 1) / kBlock));
+  }
+  int norm_blocks() const { return std::min(blocks(n_), 148 * 8); }
+
+  template <class K, class... A>
+  void launch(K kernel, int grid, int block, A... args) {
+    launch_as(kControl, kernel, grid, block, args...);
+  }
+
+  template <class K, class... A>
+  void launch_as(int kind, K kernel, int grid, int block, A... args) {
+    cudaEvent_t before = nullptr, after = nullptr;
+    if (timing_) {
+      check(cudaEventCreate(&before), "event");
+      check(cudaEventCreate(&after), "event");
+      check(cudaEventRecord(before, stream), "event");
+    }
+    kernel<<<grid, block, 0, stream>>>(args...);
+    check(cudaGetLastError(), "kernel launch");
+    ++counters.launches;
+    if (timing_) {
+      check(cudaEventRecord(after, stream), "event");
+      timed_.push_back({kind, before, after});
+    }
+  }
+
+  Dev<P> with_rec(int in, int out) const {
     Dev<P> d = d_;
-    d.s = s;
-    d.s_next = s_next;
+    d.rec = rec_[in].as<C>();
+    d.rec_next = rec_[out].as<C>();
     return d;
   }
-
-  void fill_phi_one() {
-    std::vector<S> one(5ULL * n_, S(1));
-    check(cudaMemcpyAsync(phi_.as<void>(), one.data(), one.size() * sizeof(S),
-                          cudaMemcpyHostToDevice, stream), "phi");
-    check(cudaStreamSynchronize(stream), "phi");
-  }
-
-  void launch_store(const double* u, S* s) { launch(k_store<P>, blocks(n_), kBlock, d_, u, s); }
 
   void launch_faces(const Dev<P>& d, int mode, int stage, double wa, double wb, int local,
                     int last) {
     const int g = blocks(n_);
-    auto go = [&](auto kernel) { launch_as(kFaces, kernel, g, kBlock, d, mode, stage, wa, wb, local, last); };
+    auto go = [&](auto kernel) {
+      launch_as(kFaces, kernel, g, kBlock, d, mode, stage, wa, wb, local, last);
+    };
     const int f = scheme_.flux;
     if (planar_) {
       if (second_) {
@@ -1268,64 +1308,57 @@ class Impl final : public Stepper {
     }
   }
 
-  // The cell loops before the faces, on stored state s: boundary states, gradients, limiter.
-  void enqueue_cells(const S* s) {
-    const Dev<P> d = with_state(s);
+  // The loops before the faces on record buffer `in`: boundary states, gradients and limiter;
+  // with `dt`, the spectral radius and the CFL step of the step too.
+  void enqueue_cells(int in, bool dt, double cfl, bool local) {
+    const Dev<P> d = with_rec(in, in);
     launch_as(kBoundary, k_boundary_states<P>, blocks(nb_), kBlock, d);
+    const int g = blocks(n_);
+    const int loc = local ? 1 : 0;
     if (second_) {
       if (limiter_) {
-        launch_as(kGradients, k_gradients<P, true>, blocks(n_), kBlock, d);
+        if (dt) launch_as(kGradients, k_gradients<P, true, true>, g, kBlock, d, cfl, loc);
+        else launch_as(kGradients, k_gradients<P, true, false>, g, kBlock, d, cfl, loc);
       } else {
-        launch_as(kGradients, k_gradients<P, false>, blocks(n_), kBlock, d);
+        if (dt) launch_as(kGradients, k_gradients<P, false, true>, g, kBlock, d, cfl, loc);
+        else launch_as(kGradients, k_gradients<P, false, false>, g, kBlock, d, cfl, loc);
       }
+    } else if (dt) {
+      launch_as(kSpectral, k_spectral<P>, g, kBlock, d, cfl, loc, static_cast<double*>(nullptr));
     }
   }
 
-  void enqueue_residual(const S* s) {
-    enqueue_cells(s);
-    launch_faces(with_state(s), kResidual, 0, 0.0, 0.0, 0, 0);
+  void enqueue_residual(int in) {
+    enqueue_cells(in, false, 0.0, false);
+    launch_faces(with_rec(in, in), kResidual, 0, 0.0, 0.0, 0, 0);
+    last_rec_ = in;
     ++counters.residuals;
   }
 
-  // One step. Stored states rotate through three buffers so that a step starts and ends in s_[0]:
+  // One step. Records rotate through three buffers so that a step starts and ends in buffer 0:
   // RK3 0 -> 1 -> 2 -> 0; RK4 0 -> 1 -> 2 -> 1 -> 0.
   void enqueue_step(const StepKey& k) {
-    const double dt_fixed = k.dt > 0.0 ? k.dt : 0.0;
-    const bool local = !(k.dt > 0.0) && k.local;
-    launch(k_begin, 1, 256, d_.ctl, dt_fixed);
-    S* s0 = s_[0].as<S>();
-    S* s1 = s_[1].as<S>();
-    S* s2 = s_[2].as<S>();
-    enqueue_cells(s0);
-    if (!(k.dt > 0.0))
-      launch_as(kSpectral, k_spectral<P>, blocks(n_), kBlock, with_state(s0), k.cfl, local ? 1 : 0,
-                static_cast<double*>(nullptr));
-    launch(k_take_dt, 1, 32, d_.ctl);
-    if (k.rk == 3) {
-      static const double w[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
-      S* in[3] = {s0, s1, s2};
-      S* out[3] = {s1, s2, s0};
-      for (int st = 0; st < 3; ++st) {
-        if (st > 0) enqueue_cells(in[st]);
-        launch_faces(with_state(in[st], out[st]), kRk3, st, w[st][0], w[st][1], local ? 1 : 0,
-                     st == 2 ? 1 : 0);
-        if (st == 0) {
-          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
-          launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
-        }
-      }
-    } else {
-      static const double cs[4] = {0.5, 0.5, 1.0, 0.0};
-      S* in[4] = {s0, s1, s2, s1};
-      S* out[4] = {s1, s2, s1, s0};
-      for (int st = 0; st < 4; ++st) {
-        if (st > 0) enqueue_cells(in[st]);
-        launch_faces(with_state(in[st], out[st]), kRk4, st, cs[st], 0.0, local ? 1 : 0,
-                     st == 3 ? 1 : 0);
-        if (st == 0) {
-          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
-          launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
-        }
+    const bool cfl_dt = !(k.dt > 0.0);
+    const bool local = cfl_dt && k.local;
+    launch(k_begin, 1, 256, d_.ctl, cfl_dt ? 0.0 : k.dt);
+    const int stages = k.rk == 3 ? 3 : 4;
+    static const int in3[3] = {0, 1, 2}, out3[3] = {1, 2, 0};
+    static const int in4[4] = {0, 1, 2, 1}, out4[4] = {1, 2, 1, 0};
+    static const double w3[3][2] = {{0.0, 1.0}, {0.75, 0.25}, {1.0 / 3.0, 2.0 / 3.0}};
+    static const double c4[4] = {0.5, 0.5, 1.0, 0.0};
+    for (int st = 0; st < stages; ++st) {
+      const int in = k.rk == 3 ? in3[st] : in4[st];
+      const int out = k.rk == 3 ? out3[st] : out4[st];
+      enqueue_cells(in, st == 0 && cfl_dt, k.cfl, local);
+      if (st == 0) launch(k_take_dt, 1, 32, d_.ctl);
+      const double wa = k.rk == 3 ? w3[st][0] : c4[st];
+      const double wb = k.rk == 3 ? w3[st][1] : 0.0;
+      launch_faces(with_rec(in, out), k.rk == 3 ? kRk3 : kRk4, st, wa, wb, local ? 1 : 0,
+                   st == stages - 1 ? 1 : 0);
+      if (st == 0) {
+        launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
+                  static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
       }
     }
     launch(k_end_step, 1, 32, d_.ctl);
@@ -1338,7 +1371,7 @@ class Impl final : public Stepper {
     try {
       enqueue_step(k);
     } catch (...) {
-      cudaGraph_t g;
+      cudaGraph_t g = nullptr;
       cudaStreamEndCapture(stream, &g);
       if (g != nullptr) cudaGraphDestroy(g);
       throw;
@@ -1357,18 +1390,13 @@ class Impl final : public Stepper {
     graph_ = nullptr;
   }
 
-  void read_control(Control* h) {
-    check(cudaMemcpyAsync(h, d_.ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream), "control");
-    check(cudaStreamSynchronize(stream), "control");
-  }
-
   long long first_invalid(const std::vector<double>& u, const std::vector<double>& r) const {
     const double* ref = d_.ref;
     const C g = static_cast<C>(scheme_.gamma);
     const C r0 = static_cast<C>(ref[0]);
     for (int c = 0; c < n_; ++c) {
       C dq[5];
-      for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(static_cast<S>(u[k * static_cast<long long>(n_) + c] - ref[k]));
+      for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(u[k * static_cast<long long>(n_) + c] - ref[k]);
       const C rho = r0 + dq[0];
       C dm_m = 0, mr_mr = 0;
       for (int k = 0; k < 3; ++k) {
@@ -1393,15 +1421,16 @@ class Impl final : public Stepper {
   int nc_ = 0, n_ = 0, nf_ = 0, ni_ = 0, nif_ = 0, nb_ = 0;
   Sliced st_, inc_;
   Dev<P> d_{};
-  Buffer s_[3];
-  Buffer grad_, phi_, prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
-  Buffer st_start_, st_len_, st_e_, st_w_, inc_start_, inc_len_, inc_code_;
-  Buffer f_l_, f_r_, f_n_, f_a_, f_rl_, f_rr_, f_m_;
-  Buffer b_own_, b_kind_, b_data_, b_n_, b_a_, b_r_, b_m_, source_;
+  Buffer rec_[3];
+  Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
+  Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_;
+  Buffer face_, f_m_, bface_, b_m_, source_;
+  std::vector<C> bface_host_;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   long long graph_nodes_ = 0;
   StepKey graph_key_{0.0, 0.0, false, 0};
+  int last_rec_ = 0;
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {
     int kind;
@@ -1436,13 +1465,13 @@ int guarded(char* err, size_t len, F&& body) {
 struct DeviceGuard {
   int previous = -1;
   explicit DeviceGuard(int device) {
-    cudaGetDevice(&previous);
+    if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
     if (device >= 0 && device != previous) check(cudaSetDevice(device), "cudaSetDevice");
   }
   ~DeviceGuard() {
     int now = -1;
-    cudaGetDevice(&now);
-    if (previous >= 0 && now != previous) cudaSetDevice(previous);
+    if (cudaGetDevice(&now) == cudaSuccess && previous >= 0 && now != previous)
+      cudaSetDevice(previous);
   }
 };
 
@@ -1504,11 +1533,16 @@ void autan_euler_device_destroy(void* handle) {
   if (own) cudaStreamDestroy(s);
 }
 
+#define AUTAN_CALL(body)             \
+  return guarded(err, err_len, [&] { \
+    auto* h = as_stepper(handle);    \
+    DeviceGuard guard(h->device);    \
+    body;                            \
+  })
+
 int autan_euler_device_set_boundary(void* handle, const uint8_t* kind, const double* data,
                                     int64_t n_boundary, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (kind == nullptr || data == nullptr) fail("E1101: null boundary arrays");
     (void)n_boundary;
     h->set_boundary(kind, data);
@@ -1517,9 +1551,7 @@ int autan_euler_device_set_boundary(void* handle, const uint8_t* kind, const dou
 
 int autan_euler_device_set_boundary_data(void* handle, const double* data, int64_t n_boundary,
                                          char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (data == nullptr) fail("E1101: null boundary data");
     (void)n_boundary;
     h->set_boundary_data(data);
@@ -1527,35 +1559,25 @@ int autan_euler_device_set_boundary_data(void* handle, const double* data, int64
 }
 
 int autan_euler_device_set_source(void* handle, const double* source, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (source == nullptr) fail("E1101: null source");
     h->set_source(source);
   });
 }
 
 int autan_euler_device_set_second_order(void* handle, int32_t on, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
-    h->set_second_order(on != 0);
-  });
+  AUTAN_CALL(h->set_second_order(on != 0));
 }
 
 int autan_euler_device_upload(void* handle, const double* u, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (u == nullptr) fail("E1101: null state");
     h->upload_state(u);
   });
 }
 
 int autan_euler_device_download(void* handle, double* u, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (u == nullptr) fail("E1101: null state");
     h->download_state(u);
   });
@@ -1563,9 +1585,7 @@ int autan_euler_device_download(void* handle, double* u, char* err, size_t err_l
 
 int autan_euler_device_residual(void* handle, const double* u, double* res, char* err,
                                 size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (u == nullptr || res == nullptr) fail("E1101: null arrays");
     h->residual(u, res);
   });
@@ -1574,9 +1594,7 @@ int autan_euler_device_residual(void* handle, const double* u, double* res, char
 int autan_euler_device_step(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                             int64_t n_steps, int32_t use_graph, autan_euler_step_result* out,
                             char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     autan_euler_step_result r{};
     h->step(cfl, dt, local != 0, rk, n_steps, use_graph != 0, &r);
     if (out != nullptr) *out = r;
@@ -1585,9 +1603,7 @@ int autan_euler_device_step(void* handle, double cfl, double dt, int32_t local, 
 
 int autan_euler_device_evaluate(void* handle, autan_euler_step_result* out, char* err,
                                 size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     autan_euler_step_result r{};
     h->evaluate(&r);
     if (out != nullptr) *out = r;
@@ -1596,27 +1612,17 @@ int autan_euler_device_evaluate(void* handle, autan_euler_step_result* out, char
 
 int autan_euler_device_history(void* handle, int64_t count, double* rms, double* dt, char* err,
                                size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
-    h->history(count, rms, dt);
-  });
+  AUTAN_CALL(h->history(count, rms, dt));
 }
 
 int autan_euler_device_gradients(void* handle, double* grad, double* phi, char* err,
                                  size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
-    h->gradients(grad, phi);
-  });
+  AUTAN_CALL(h->gradients(grad, phi));
 }
 
 int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* err,
                                   size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (dt == nullptr) fail("E1101: null output");
     h->time_steps(cfl, dt);
   });
@@ -1625,9 +1631,7 @@ int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* er
 int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                     int64_t n_steps, double* ms, int64_t* launches, char* err,
                                     size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
+  AUTAN_CALL({
     if (ms == nullptr || launches == nullptr) fail("E1101: null output");
     if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
     long long l[6];
@@ -1637,11 +1641,7 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {
-  return guarded(err, err_len, [&] {
-    auto* h = as_stepper(handle);
-    DeviceGuard guard(h->device);
-    check(cudaStreamSynchronize(h->stream), "sync");
-  });
+  AUTAN_CALL(check(cudaStreamSynchronize(h->stream), "sync"));
 }
 
 void* autan_euler_device_stream(void* handle) {

@@ -180,8 +180,11 @@ class EulerDevice:
         a = np.ascontiguousarray(u, dtype=np.float64).reshape(5, self.n_cells)
         self._call("autan_euler_device_upload", N.ptr(a, C.c_double))
 
-    def download(self) -> np.ndarray:
-        a = np.zeros((5, self.n_cells))
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The FP64 state (5 x n_cells); into `out` (C-contiguous FP64, e.g. pinned) if given."""
+        a = np.zeros((5, self.n_cells)) if out is None else out
+        if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != 5 * self.n_cells:
+            raise ValueError("out must be a C-contiguous float64 array of 5 x n_cells")
         self._call("autan_euler_device_download", N.ptr(a, C.c_double))
         return a
 

@@ -117,7 +117,7 @@ class ClockSampler:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=self.file, stderr=subprocess.DEVNULL,
             )  # fmt: skip
         except Exception:
@@ -313,14 +313,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     # -- end to end through the C ABI: pinned host state in and out every step
     u_host = torch.empty((5, case.mesh.n_cells), dtype=torch.float64, pin_memory=True).numpy()
-    u_host[:] = dev.download()
+    dev.download(out=u_host)
     e2e_steps = max(3, min(args.steps, 10))
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         dev.upload(u_host)
         dev.step(cfl=case.cfl, rk=case.rk, n_steps=1, graph=True)
-        u_host[:] = dev.download()
+        dev.download(out=u_host)
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(t1 - t0)
     e2e = world * n * e2e_steps / e2e_s

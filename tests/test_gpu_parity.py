@@ -45,8 +45,13 @@ def test_golden_residual(case):
         res = dev.residual(z["u"])
         grad, phi = dev.gradients()
     if scheme["second_order"]:
-        assert bits_equal(grad, z["grad"][:, :no])
-        assert bits_equal(phi, z["phi"][:, :no])
+        if case in EXP_LOG:
+            # farfield/inlet boundary states enter the limiter's bounds (and kept-face fits)
+            assert rel_err(grad, z["grad"][:, :no]) <= 1e-12
+            assert rel_err(phi, z["phi"][:, :no]) <= 1e-12
+        else:
+            assert bits_equal(grad, z["grad"][:, :no])
+            assert bits_equal(phi, z["phi"][:, :no])
     if case in EXP_LOG:
         assert rel_err(res[:, :no], z["res"][:, :no]) <= 1e-12
     else:
