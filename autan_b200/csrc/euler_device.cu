@@ -286,103 +286,192 @@ __device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const t
   return cfl * d.volume[c] / lam;
 }
 
-// gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the
-// LSQ gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell,
-// then phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)). With DT,
-// also the cell's CFL step and the block's minimum.
+// Shared memory of the slice-parallel kernels: arrays indexed [row][component][lane], so that the
+// 32 lanes of a warp (the 32 cells of a slice) touch consecutive words.
+constexpr int kCellRows = 35;  // wc 0-4, grad 5-19, lo 20-24, hi 25-29, phi 30-34
+
+template <class P>
+size_t gradient_smem(int s_max, int i_max) {
+  return (static_cast<size_t>(s_max) * 8 * 32 + kCellRows * 32 + static_cast<size_t>(i_max) * 5 * 32) *
+             sizeof(typename P::C) +
+         (static_cast<size_t>(i_max) * 32 + 32) * sizeof(double);
+}
+
+// gradients (kernels/euler.py:540-549) then limiter (:596-608) for the 32 cells of one slice per
+// block, entry-parallel: warp j gathers stencil entry j of the 32 cells into shared memory; one
+// thread per (cell, component) then reduces the entries in stencil order (FP64 sums; Min/Max ties
+// keeping the first), the order of the reference's serial cell_reduce (emit_cpu.py reduce_body);
+// warp j evaluates the limiter at face j of the cells, and one thread per (cell, component) takes
+// the ordered minimum (at_most_one caps it at 1). With DT, the faces' wave speeds
+// (spectral_radius, :1103-1112) are summed the same way into each cell's CFL step
+// (device_stepper.cuh:84-89) and the block's minimum goes to the global step.
 template <class P, bool LIMIT, bool DT>
-__global__ void __launch_bounds__(kBlock) k_gradients(Dev<P> d, double cfl, int local) {
+__global__ void __launch_bounds__(512) k_gradients(Dev<P> d, double cfl, int local, int s_max,
+                                                   int i_max) {
   using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* E = reinterpret_cast<C*>(smem_raw);
+  C* cell = E + static_cast<size_t>(s_max) * 8 * 32;
+  C* V = cell + kCellRows * 32;
+  double* W = reinterpret_cast<double*>(V + static_cast<size_t>(i_max) * 5 * 32);
+  double* dts = W + static_cast<size_t>(i_max) * 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int slice = blockIdx.x;
+  const int c = slice * 32 + lane;
   const bool live = c < d.n;
-  double dt = 0.0;
-  if (live) {
-    C wc[5];
-    load_prim<P>(d.rec, c, wc);
-    double acc[15];
+  const int len = live ? __ldg(d.st_len + c) : 0;
+  const int il = live ? __ldg(d.inc_len + c) : 0;
+  if (warp == 0) {
+    C w[5] = {C(0), C(0), C(0), C(0), C(0)};
+    if (live) load_prim<P>(d.rec, c, w);
 #pragma unroll
-    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
-    C lo[5], hi[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      lo[k] = C(INFINITY);
-      hi[k] = -C(INFINITY);
-    }
-    const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
-    const int len = __ldg(d.st_len + c);
-    for (int j = 0; j < len; ++j) {
-      C e4[4];
-      load_words<P>(d.st + 4 * (base + static_cast<long long>(j) * kSlice), 0, 4, e4);
+    for (int k = 0; k < 5; ++k) cell[k * 32 + lane] = w[k];
+  }
+  const int sb = __ldg(d.st_start + slice) + lane;
+  for (int j = warp; j < s_max; j += nw) {
+    if (j < len) {
+      C e4[4], wn[8];
+      load_words<P>(d.st + 4 * (sb + static_cast<long long>(j) * kSlice), 0, 4, e4);
       const int e = index_of(e4[3]);
-      C wn[5];
       if (e >= 0) {
-        load_prim<P>(d.rec, e, wn);
+        load_words<P>(d.rec + static_cast<long long>(e) * kRec, 0, 8, wn);
       } else {
-        C t[8];
-        load_words<P>(d.prim_b + static_cast<long long>(-e - 1) * kPrimB, 0, 8, t);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) wn[k] = t[k];
+        load_words<P>(d.prim_b + static_cast<long long>(-e - 1) * kPrimB, 0, 8, wn);
       }
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const C dw = wn[i] - wc[i];
-        acc[3 * i] += static_cast<double>(dw * e4[0]);
-        acc[3 * i + 1] += static_cast<double>(dw * e4[1]);
-        acc[3 * i + 2] += static_cast<double>(dw * e4[2]);
-      }
+      for (int k = 0; k < 5; ++k) E[(j * 8 + k) * 32 + lane] = wn[k];
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        if (wn[i] < lo[i]) lo[i] = wn[i];
-        if (wn[i] > hi[i]) hi[i] = wn[i];
-      }
-    }
-    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
-    C out[20];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
-    const C* g = out + 5;
-    if constexpr (LIMIT) {
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        lo[i] = minv(lo[i], wc[i]);
-        hi[i] = maxv(hi[i], wc[i]);
-      }
-      const C vol = static_cast<C>(__ldg(d.volume + c));
-      C phi[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
-      const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
-      const int il = __ldg(d.inc_len + c);
-      for (int j = 0; j < il; ++j) {
-        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
-        C r[4];
-        if (code >= 0) {
-          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, (code & 1) ? 8 : 4, 4, r);
-        } else {
-          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 4, 4, r);
-        }
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
-          if (v < phi[i]) phi[i] = v;
-        }
-      }
-      // at_most_one (:591-593)
-#pragma unroll
-      for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
-    } else {
-      // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
-#pragma unroll
-      for (int i = 0; i < 5; ++i) out[i] = C(1.0);
-    }
-    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
-    if constexpr (DT) {
-      dt = cell_time_step(d, c, wc, cfl);
-      if (local) d.dt_local[c] = dt;
+      for (int a = 0; a < 3; ++a) E[(j * 8 + 5 + a) * 32 + lane] = e4[a];
     }
   }
-  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+  __syncthreads();
+  for (int t = threadIdx.x; t < 25 * 32; t += blockDim.x) {
+    const int q = t >> 5, l = t & 31;
+    const int cc = slice * 32 + l;
+    if (cc >= d.n) continue;
+    const int ln = __ldg(d.st_len + cc);
+    if (q < 15) {
+      const int i = q / 3, a = q % 3;
+      const C wci = cell[i * 32 + l];
+      double acc = 0.0;
+      for (int j = 0; j < ln; ++j) {
+        const C dw = E[(j * 8 + i) * 32 + l] - wci;
+        acc += static_cast<double>(dw * E[(j * 8 + 5 + a) * 32 + l]);
+      }
+      cell[(5 + q) * 32 + l] = static_cast<C>(acc);  // include_own_value (:517-521)
+    } else if (q < 20) {
+      const int i = q - 15;
+      C lo = C(INFINITY);
+      for (int j = 0; j < ln; ++j) {
+        const C v = E[(j * 8 + i) * 32 + l];
+        if (v < lo) lo = v;
+      }
+      cell[(20 + i) * 32 + l] = minv(lo, cell[i * 32 + l]);
+    } else {
+      const int i = q - 20;
+      C hi = -C(INFINITY);
+      for (int j = 0; j < ln; ++j) {
+        const C v = E[(j * 8 + i) * 32 + l];
+        if (v > hi) hi = v;
+      }
+      cell[(25 + i) * 32 + l] = maxv(hi, cell[i * 32 + l]);
+    }
+  }
+  __syncthreads();
+  if constexpr (LIMIT || DT) {
+    const int ib = __ldg(d.inc_start + slice) + lane;
+    const C vol = live ? static_cast<C>(__ldg(d.volume + c)) : C(0);
+    for (int j = warp; j < i_max; j += nw) {
+      if (j < il) {
+        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+        C fr[kFace];
+        const C* r;
+        if (code >= 0) {
+          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
+          r = (code & 1) ? fr + 8 : fr + 4;
+        } else {
+          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 0, 8, fr);
+          r = fr + 4;
+        }
+        if constexpr (LIMIT) {
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            const C* g = cell + (5 + 3 * i) * 32 + lane;
+            const C dd = g[0] * r[0] + g[32] * r[1] + g[64] * r[2];
+            const C wci = cell[i * 32 + lane];
+            V[(j * 5 + i) * 32 + lane] = venkat(dd, cell[(25 + i) * 32 + lane] - wci,
+                                                cell[(20 + i) * 32 + lane] - wci, d.p.scale[i] * vol);
+          }
+        }
+        if constexpr (DT) {
+          C wn[8], wc[5];
+          if (code >= 0) {
+            const int o = (code & 1) ? index_of(fr[7]) : index_of(fr[11]);
+            load_words<P>(d.rec + static_cast<long long>(o) * kRec, 0, 8, wn);
+          } else {
+            load_words<P>(d.prim_b + static_cast<long long>(-code - 1) * kPrimB, 0, 8, wn);
+          }
+#pragma unroll
+          for (int k = 0; k < 5; ++k) wc[k] = cell[k * 32 + lane];
+          W[j * 32 + lane] = static_cast<double>(wave_speed(wc, wn, fr, fr[3], d.p.g, d.p.pref));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < 6 * 32; t += blockDim.x) {
+    const int q = t >> 5, l = t & 31;
+    const int cc = slice * 32 + l;
+    if (cc >= d.n) continue;
+    const int iln = __ldg(d.inc_len + cc);
+    if (q < 5) {
+      C phi = C(1.0);  // second order without limiter: phi = 1 (physics/src/euler.cpp:195)
+      if constexpr (LIMIT) {
+        phi = C(INFINITY);
+        for (int j = 0; j < iln; ++j) {
+          const C v = V[(j * 5 + q) * 32 + l];
+          if (v < phi) phi = v;
+        }
+        phi = minv(phi, C(1.0));  // at_most_one (:591-593)
+      }
+      cell[(30 + q) * 32 + l] = phi;
+    } else if constexpr (DT) {
+      double acc = 0.0;
+      for (int j = 0; j < iln; ++j) acc += W[j * 32 + l];
+      const double lam = static_cast<double>(static_cast<C>(acc));
+      const double dt = cfl * d.volume[cc] / lam;
+      if (local) d.dt_local[cc] = dt;
+      dts[l] = dt;
+    }
+  }
+  __syncthreads();
+  // Words 8-27 of the records: phi (8-12), then grad (13-27), as 16-byte vectors.
+  constexpr int nvec = 20 / P::kVec;
+  for (int t = threadIdx.x; t < nvec * 32; t += blockDim.x) {
+    const int v = t >> 5, l = t & 31;
+    const int cc = slice * 32 + l;
+    if (cc >= d.n) continue;
+    C x[P::kVec];
+#pragma unroll
+    for (int u = 0; u < P::kVec; ++u) {
+      const int w = 8 + v * P::kVec + u;
+      x[u] = w < kGrad ? cell[(30 + (w - kPhi)) * 32 + l] : cell[(5 + (w - kGrad)) * 32 + l];
+    }
+    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(cc) * kRec, 8 + v * P::kVec,
+                   P::kVec, x);
+  }
+  if constexpr (DT) {
+    if (warp == 0) {
+      unsigned long long b = ~0ULL;
+      if (live && dts[lane] > 0.0) b = static_cast<unsigned long long>(__double_as_longlong(dts[lane]));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(0xffffffffu, b, off);
+        b = o < b ? o : b;
+      }
+      if (lane == 0 && b != ~0ULL) atomicMin(&d.ctl->dt_bits, b);
+    }
+  }
 }
 
 // The CFL step alone (first-order schemes), with the block minimum; `dt_out` for the host.
@@ -405,45 +494,51 @@ __global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int l
 
 enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
 
-// The faces of one owned cell (roe/hllc/ausm _faces and _boundaries, kernels/euler.py:687-1049),
-// gathered: every face flux of the cell recomputed here, added in increasing face index from the
-// source term -V s, as the reference's scatter adds them (emit_cpu.py emit_loop); then, in the RK
-// modes, the stage update in FP64 and the next stage's primitives.
+template <class P>
+size_t faces_smem(int i_max) {
+  return static_cast<size_t>(i_max) * 5 * 32 * sizeof(typename P::C) + 5 * 32 * sizeof(double) +
+         static_cast<size_t>(i_max) * 32;
+}
+
+// The faces of the 32 cells of one slice per block (roe/hllc/ausm _faces and _boundaries,
+// kernels/euler.py:687-1049), face-parallel and gathered: warp j recomputes the flux of face j of
+// every cell (no float atomics, no face scratch in HBM); one thread per (cell, component) then
+// adds them in increasing face index from the source term -V s, the order in which the
+// reference's scatter adds them (emit_cpu.py emit_loop), and in the RK modes updates that
+// component in FP64; one thread per cell finally writes the next stage's primitives.
 template <class P, int FLUX, bool PLANAR, bool SECOND>
-__global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage, double wa,
-                                                  double wb, int local, int last) {
+__global__ void __launch_bounds__(256) k_faces(Dev<P> d, int mode, int stage, double wa,
+                                               double wb, int local, int last, int i_max) {
   using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n) return;
-  C wc[5], gc[15], pc[5];
-  if constexpr (SECOND) {
-    load_recon<P>(d.rec, c, wc, pc, gc);
-  } else {
-    load_prim<P>(d.rec, c, wc);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* F = reinterpret_cast<C*>(smem_raw);
+  double* NU = reinterpret_cast<double*>(F + static_cast<size_t>(i_max) * 5 * 32);
+  signed char* side = reinterpret_cast<signed char*>(NU + 5 * 32);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int slice = blockIdx.x;
+  const int c = slice * 32 + lane;
+  const bool live = c < d.n;
+  const int il = live ? __ldg(d.inc_len + c) : 0;
+  const int ib = __ldg(d.inc_start + slice) + lane;
+  for (int j = warp; j < i_max; j += nw) {
+    if (j >= il) continue;
+    C wc[5], gc[15], pc[5];
+    if constexpr (SECOND) {
+      load_recon<P>(d.rec, c, wc, pc, gc);
+    } else {
+      load_prim<P>(d.rec, c, wc);
 #pragma unroll
-    for (int k = 0; k < 15; ++k) gc[k] = C(0.0);
+      for (int k = 0; k < 15; ++k) gc[k] = C(0.0);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) pc[k] = C(0.0);
-  }
-  const double vol = __ldg(d.volume + c);
-  // sources (:611-616): res = -V s, in the compute type, stored in FP64.
-  double res[5];
-  {
-    const C nv = -static_cast<C>(vol);
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const C s = d.source != nullptr ? __ldg(d.source + static_cast<long long>(k) * d.n + c) : C(0.0);
-      res[k] = static_cast<double>(nv * s);
+      for (int k = 0; k < 5; ++k) pc[k] = C(0.0);
     }
-  }
-  const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
-  const int il = __ldg(d.inc_len + c);
-  for (int j = 0; j < il; ++j) {
     const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
     C out[5];
+    signed char sgn = 1;
     if (code >= 0) {
       const int f = code >> 1;
       const bool left = (code & 1) == 0;
+      sgn = left ? 1 : -1;
       C fr_[kFace];
       load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr_);
       const int o = left ? index_of(fr_[11]) : index_of(fr_[7]);
@@ -459,8 +554,6 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
       }
       const C* n = fr_;
       const C area = fr_[3];
-      const C* rl = fr_ + 4;
-      const C* rr = fr_ + 8;
       const C* wl = left ? wc : wo;
       const C* gl = left ? gc : go;
       const C* pl = left ? pc : po;
@@ -468,8 +561,8 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
       const C* gr = left ? go : gc;
       const C* pr = left ? po : pc;
       C fl[5], frr[5], fx[5];
-      reconstruct(wl, gl, pl, rl, d.p.pref, fl);
-      reconstruct(wr, gr, pr, rr, d.p.pref, frr);
+      reconstruct(wl, gl, pl, fr_ + 4, d.p.pref, fl);
+      reconstruct(wr, gr, pr, fr_ + 8, d.p.pref, frr);
       numerical_flux<FLUX>(fl, frr, n, d.p, fx);
       if constexpr (PLANAR) {
 #pragma unroll
@@ -483,13 +576,6 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
         warp_term(avg, gl, pl, gr, pr, m, d.p.g, d.p.pref, wt);
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = area * fx[k] + wt[k];
-      }
-      if (left) {
-#pragma unroll
-        for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
-      } else {
-#pragma unroll
-        for (int k = 0; k < 5; ++k) res[k] -= static_cast<double>(out[k]);
       }
     } else {
       const int b = -code - 1;
@@ -525,83 +611,93 @@ __global__ void __launch_bounds__(kBlock) k_faces(Dev<P> d, int mode, int stage,
 #pragma unroll
         for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
       }
-#pragma unroll
-      for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
     }
-  }
-  if (mode == kResidual || stage == 0) {
 #pragma unroll
-    for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
+    for (int k = 0; k < 5; ++k) F[(j * 5 + k) * 32 + lane] = out[k];
+    side[j * 32 + lane] = sgn;
   }
-  if (mode == kResidual) return;
-  const double h = local ? d.dt_local[c] : d.ctl->dt;
-  double nu[5];
-  if (mode == kRk3) {
-    // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const long long i = static_cast<long long>(k) * d.n + c;
-      const double uk = d.u[i];
+  __syncthreads();
+  for (int t = threadIdx.x; t < 5 * 32; t += blockDim.x) {
+    const int k = t >> 5, l = t & 31;
+    const int cc = slice * 32 + l;
+    if (cc >= d.n) continue;
+    const int iln = __ldg(d.inc_len + cc);
+    const double vol = __ldg(d.volume + cc);
+    const long long i = static_cast<long long>(k) * d.n + cc;
+    // sources (:611-616): res = -V s, in the compute type, stored in FP64.
+    const C s = d.source != nullptr ? __ldg(d.source + i) : C(0.0);
+    double res = static_cast<double>(-static_cast<C>(vol) * s);
+    for (int j = 0; j < iln; ++j) {
+      const double o = static_cast<double>(F[(j * 5 + k) * 32 + l]);
+      if (side[j * 32 + l] > 0) {
+        res += o;
+      } else {
+        res -= o;
+      }
+    }
+    if (mode == kResidual || stage == 0) d.res[i] = res;
+    if (mode == kResidual) continue;
+    const double h = local ? d.dt_local[cc] : d.ctl->dt;
+    const double uk = d.u[i];
+    double nu;
+    if (mode == kRk3) {
+      // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
       const double sk = stage == 0 ? uk : d.stage[i];
-      const double next = sk - h / vol * res[k];
-      nu[k] = wa * uk + wb * next;
-    }
-  } else {
-    // Classical RK4: stage_s = u - ((c_s h) / V) R_s; u = u - ((h / 6) / V) (R_0 + 2 R_1 + 2 R_2 + R_3).
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const long long i = static_cast<long long>(k) * d.n + c;
-      const double uk = d.u[i];
+      const double next = sk - h / vol * res;
+      nu = wa * uk + wb * next;
+      if (!last) d.stage[i] = nu;
+    } else {
+      // Classical RK4: stage_s = u - ((c_s h) / V) R_s; u = u - ((h / 6) / V) (R_0 + 2 R_1 +
+      // 2 R_2 + R_3).
       double a;
       if (stage == 0) {
-        a = res[k];
+        a = res;
       } else if (stage < 3) {
-        a = d.racc[i] + 2.0 * res[k];
+        a = d.racc[i] + 2.0 * res;
       } else {
-        a = d.racc[i] + res[k];
+        a = d.racc[i] + res;
       }
       if (stage < 3) {
         d.racc[i] = a;
-        nu[k] = uk - wa * h / vol * res[k];
+        nu = uk - wa * h / vol * res;
       } else {
-        nu[k] = uk - h / 6.0 / vol * a;
+        nu = uk - h / 6.0 / vol * a;
       }
     }
-  }
-#pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    const long long i = static_cast<long long>(k) * d.n + c;
     if (last) {
-      d.u[i] = nu[k];
-    } else if (mode == kRk3) {
-      d.stage[i] = nu[k];
+      d.u[i] = nu;
+      if (!isfinite(res)) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(cc));
     }
+    NU[k * 32 + l] = nu;
   }
-  C w[5], dq[5];
-  prim_of_state(d, nu, w, dq);
-  store_prim<P>(d.rec_next, c, w);
-  if (last) {
-    // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
-    // it, in the compute type, then this stage's residual.
-    const C g = d.p.g;
-    const C r0 = static_cast<C>(d.ref[0]);
-    const C rho = r0 + dq[0];
-    C dm_m = C(0), mr_mr = C(0);
+  if (mode == kResidual) return;
+  __syncthreads();
+  if (warp == 0 && live) {
+    double nu[5];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const C mr = static_cast<C>(d.ref[k + 1]);
-      dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
-      mr_mr = mr_mr + mr * mr;
+    for (int k = 0; k < 5; ++k) nu[k] = NU[k * 32 + lane];
+    C w[5], dq[5];
+    prim_of_state(d, nu, w, dq);
+    store_prim<P>(d.rec_next, c, w);
+    if (last) {
+      // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will
+      // read it, in the compute type.
+      const C g = d.p.g;
+      const C r0 = static_cast<C>(d.ref[0]);
+      const C rho = r0 + dq[0];
+      C dm_m = C(0), mr_mr = C(0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const C mr = static_cast<C>(d.ref[k + 1]);
+        dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
+        mr_mr = mr_mr + mr * mr;
+      }
+      const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
+      const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
+      const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
+                       !(rho > C(0)) || !(pr > C(0));
+      if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
     }
-    const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
-    const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
-    const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
-                     !(rho > C(0)) || !(pr > C(0));
-    if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
-    bool badr = false;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) badr = badr || !isfinite(res[k]);
-    if (badr) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(c));
   }
 }
 
@@ -947,6 +1043,14 @@ class Impl final : public Stepper {
       }
     }
     std::vector<double> vol(m.cell_volume, m.cell_volume + n_);
+    for (int c = 0; c < n_; ++c) {
+      s_max_ = std::max(s_max_, st_.len[c]);
+      i_max_ = std::max(i_max_, inc_.len[c]);
+    }
+    grad_warps_ = std::min(16, std::max(8, (s_max_ + 1) / 2));
+    face_warps_ = std::min(8, std::max(i_max_, 5));
+    if (gradient_smem<P>(s_max_, i_max_) > 200 * 1024)
+      fail("E1101: a stencil row is too long for the gradient kernel's shared memory");
     // Device arrays.
     const size_t n5 = 5ULL * n_;
     for (auto& b : rec_) b.alloc(static_cast<size_t>(kRec) * n_ * sizeof(C));
@@ -1244,6 +1348,8 @@ class Impl final : public Stepper {
     if (static_cast<long long>(m.n_owned_cells) >= (1LL << 30)) fail("E1101: mesh too large");
   }
 
+  int slices() const { return std::max(1, (n_ + kSlice - 1) / kSlice); }
+
   static int blocks(long long n) {
     return static_cast<int>(std::max<long long>(1, (n + kBlock - 1) / kBlock));
   }
@@ -1256,13 +1362,21 @@ class Impl final : public Stepper {
 
   template <class K, class... A>
   void launch_as(int kind, K kernel, int grid, int block, A... args) {
+    launch_smem(kind, kernel, grid, block, 0, args...);
+  }
+
+  template <class K, class... A>
+  void launch_smem(int kind, K kernel, int grid, int block, size_t smem, A... args) {
     cudaEvent_t before = nullptr, after = nullptr;
+    if (smem > 48 * 1024)
+      check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)), "shared memory");
     if (timing_) {
       check(cudaEventCreate(&before), "event");
       check(cudaEventCreate(&after), "event");
       check(cudaEventRecord(before, stream), "event");
     }
-    kernel<<<grid, block, 0, stream>>>(args...);
+    kernel<<<grid, block, smem, stream>>>(args...);
     check(cudaGetLastError(), "kernel launch");
     ++counters.launches;
     if (timing_) {
@@ -1280,9 +1394,11 @@ class Impl final : public Stepper {
 
   void launch_faces(const Dev<P>& d, int mode, int stage, double wa, double wb, int local,
                     int last) {
-    const int g = blocks(n_);
+    const int g = slices();
+    const size_t smem = faces_smem<P>(i_max_);
     auto go = [&](auto kernel) {
-      launch_as(kFaces, kernel, g, kBlock, d, mode, stage, wa, wb, local, last);
+      launch_smem(kFaces, kernel, g, 32 * face_warps_, smem, d, mode, stage, wa, wb, local, last,
+                  i_max_);
     };
     const int f = scheme_.flux;
     if (planar_) {
@@ -1316,12 +1432,14 @@ class Impl final : public Stepper {
     const int g = blocks(n_);
     const int loc = local ? 1 : 0;
     if (second_) {
+      const int gs = slices(), bs = 32 * grad_warps_;
+      const size_t smem = gradient_smem<P>(s_max_, i_max_);
       if (limiter_) {
-        if (dt) launch_as(kGradients, k_gradients<P, true, true>, g, kBlock, d, cfl, loc);
-        else launch_as(kGradients, k_gradients<P, true, false>, g, kBlock, d, cfl, loc);
+        if (dt) launch_smem(kGradients, k_gradients<P, true, true>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
+        else launch_smem(kGradients, k_gradients<P, true, false>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
       } else {
-        if (dt) launch_as(kGradients, k_gradients<P, false, true>, g, kBlock, d, cfl, loc);
-        else launch_as(kGradients, k_gradients<P, false, false>, g, kBlock, d, cfl, loc);
+        if (dt) launch_smem(kGradients, k_gradients<P, false, true>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
+        else launch_smem(kGradients, k_gradients<P, false, false>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
       }
     } else if (dt) {
       launch_as(kSpectral, k_spectral<P>, g, kBlock, d, cfl, loc, static_cast<double*>(nullptr));
@@ -1431,6 +1549,8 @@ class Impl final : public Stepper {
   long long graph_nodes_ = 0;
   StepKey graph_key_{0.0, 0.0, false, 0};
   int last_rec_ = 0;
+  int s_max_ = 1, i_max_ = 1;        // longest stencil and incidence rows
+  int grad_warps_ = 8, face_warps_ = 4;  // warps per block of the slice-parallel kernels
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {
     int kind;

@@ -274,13 +274,22 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if args.workload == "hex":
         case = cases.vortex_hex()
     else:
-        case = cases.vortex_tets(precision="fp32+acc64")
+        nx, ny, nz = (int(v) for v in args.lattice.split(","))
+        case = cases.vortex_tets(nx, ny, nz, precision="fp32+acc64")
     n = case.mesh.n_owned_cells
     dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
     dev.upload(case.u0)
     stream = torch.cuda.ExternalStream(dev.stream)
     # Warm-up (and graph capture).
     dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.warmup, graph=True)
+    if args.profile:
+        # Eager launches for a profiler: the warm-up above, then `steps` steps kernel by kernel.
+        t0 = time.perf_counter()
+        r = dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.steps, graph=False)
+        print(json.dumps({"profile": True, "cells": n, "steps": args.steps,
+                          "wall_s": time.perf_counter() - t0, "rms": list(r.residuals)}))  # fmt: skip
+        dev.close()
+        return
 
     def barrier():
         torch.cuda.synchronize()
@@ -408,6 +417,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["tets", "hex"], default="tets")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
