@@ -126,6 +126,10 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_gradients", C.c_int, vp, P(f64), P(f64), C.c_char_p, sz)
         fn("autan_euler_device_time_steps", C.c_int, vp, f64, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_history", C.c_int, vp, i64, P(f64), P(f64), C.c_char_p, sz)
+        fn("autan_euler_device_set_tuning", C.c_int, vp, P(i32), i32, C.c_char_p, sz)
+        fn("autan_euler_device_get_tuning", C.c_int, vp, P(i32), i32, C.c_char_p, sz)
+        fn("autan_euler_device_autotune", C.c_int, vp, f64, f64, i32, i32, i32, P(i32), P(f64),
+           C.c_char_p, sz)  # fmt: skip
         fn("autan_euler_device_kernel_times", C.c_int, vp, f64, f64, i32, i32, i64, P(f64), P(i64),
            C.c_char_p, sz)  # fmt: skip
 

@@ -39,6 +39,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "autan_euler_device.h"
@@ -286,198 +287,140 @@ __device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const t
   return cfl * d.volume[c] / lam;
 }
 
-// Shared memory of the slice-parallel kernels: arrays indexed [row][component][lane], so that the
-// 32 lanes of a warp (the 32 cells of a slice) touch consecutive words.
-constexpr int kCellRows = 35;  // wc 0-4, grad 5-19, lo 20-24, hi 25-29, phi 30-34
-
+// The primitives of a cell (words 0-4) or of a boundary face's state, five values only.
 template <class P>
-size_t gradient_smem(int s_max, int i_max) {
-  return (static_cast<size_t>(s_max) * 8 * 32 + kCellRows * 32 + static_cast<size_t>(i_max) * 5 * 32) *
-             sizeof(typename P::C) +
-         (static_cast<size_t>(i_max) * 32 + 32) * sizeof(double);
+__device__ __forceinline__ void load5(const typename P::C* src, typename P::C* w) {
+  using C = typename P::C;
+  if constexpr (P::kVec == 4) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+    w[0] = a.x;
+    w[1] = a.y;
+    w[2] = a.z;
+    w[3] = a.w;
+    w[4] = __ldg(src + 4);
+  } else {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(src));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(src) + 1);
+    w[0] = a.x;
+    w[1] = a.y;
+    w[2] = b.x;
+    w[3] = b.y;
+    w[4] = __ldg(src + 4);
+  }
+  (void)sizeof(C);
 }
 
-// gradients (kernels/euler.py:540-549) then limiter (:596-608) for the 32 cells of one slice per
-// block, entry-parallel: warp j gathers stencil entry j of the 32 cells into shared memory; one
-// thread per (cell, component) then reduces the entries in stencil order (FP64 sums; Min/Max ties
-// keeping the first), the order of the reference's serial cell_reduce (emit_cpu.py reduce_body);
-// warp j evaluates the limiter at face j of the cells, and one thread per (cell, component) takes
-// the ordered minimum (at_most_one caps it at 1). With DT, the faces' wave speeds
-// (spectral_radius, :1103-1112) are summed the same way into each cell's CFL step
-// (device_stepper.cuh:84-89) and the block's minimum goes to the global step.
-template <class P, bool LIMIT, bool DT>
-__global__ void __launch_bounds__(512) k_gradients(Dev<P> d, double cfl, int local, int s_max,
-                                                   int i_max) {
+// gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the LSQ
+// gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell, then
+// phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
+// are read CHUNK at a time (their loads, then the neighbours' loads, all in flight together) and
+// added in stencil order. With DT, also the cell's CFL step and the block's minimum.
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* E = reinterpret_cast<C*>(smem_raw);
-  C* cell = E + static_cast<size_t>(s_max) * 8 * 32;
-  C* V = cell + kCellRows * 32;
-  double* W = reinterpret_cast<double*>(V + static_cast<size_t>(i_max) * 5 * 32);
-  double* dts = W + static_cast<size_t>(i_max) * 32;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int slice = blockIdx.x;
-  const int c = slice * 32 + lane;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < d.n;
-  const int len = live ? __ldg(d.st_len + c) : 0;
-  const int il = live ? __ldg(d.inc_len + c) : 0;
-  if (warp == 0) {
-    C w[5] = {C(0), C(0), C(0), C(0), C(0)};
-    if (live) load_prim<P>(d.rec, c, w);
+  double dt = 0.0;
+  if (live) {
+    C wc[5];
+    load5<P>(d.rec + static_cast<long long>(c) * kRec, wc);
+    double acc[15];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) cell[k * 32 + lane] = w[k];
-  }
-  const int sb = __ldg(d.st_start + slice) + lane;
-  for (int j = warp; j < s_max; j += nw) {
-    if (j < len) {
-      C e4[4], wn[8];
-      load_words<P>(d.st + 4 * (sb + static_cast<long long>(j) * kSlice), 0, 4, e4);
-      const int e = index_of(e4[3]);
-      if (e >= 0) {
-        load_words<P>(d.rec + static_cast<long long>(e) * kRec, 0, 8, wn);
-      } else {
-        load_words<P>(d.prim_b + static_cast<long long>(-e - 1) * kPrimB, 0, 8, wn);
-      }
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) E[(j * 8 + k) * 32 + lane] = wn[k];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) E[(j * 8 + 5 + a) * 32 + lane] = e4[a];
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
     }
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < 25 * 32; t += blockDim.x) {
-    const int q = t >> 5, l = t & 31;
-    const int cc = slice * 32 + l;
-    if (cc >= d.n) continue;
-    const int ln = __ldg(d.st_len + cc);
-    if (q < 15) {
-      const int i = q / 3, a = q % 3;
-      const C wci = cell[i * 32 + l];
-      double acc = 0.0;
-      for (int j = 0; j < ln; ++j) {
-        const C dw = E[(j * 8 + i) * 32 + l] - wci;
-        acc += static_cast<double>(dw * E[(j * 8 + 5 + a) * 32 + l]);
-      }
-      cell[(5 + q) * 32 + l] = static_cast<C>(acc);  // include_own_value (:517-521)
-    } else if (q < 20) {
-      const int i = q - 15;
-      C lo = C(INFINITY);
-      for (int j = 0; j < ln; ++j) {
-        const C v = E[(j * 8 + i) * 32 + l];
-        if (v < lo) lo = v;
-      }
-      cell[(20 + i) * 32 + l] = minv(lo, cell[i * 32 + l]);
-    } else {
-      const int i = q - 20;
-      C hi = -C(INFINITY);
-      for (int j = 0; j < ln; ++j) {
-        const C v = E[(j * 8 + i) * 32 + l];
-        if (v > hi) hi = v;
-      }
-      cell[(25 + i) * 32 + l] = maxv(hi, cell[i * 32 + l]);
-    }
-  }
-  __syncthreads();
-  if constexpr (LIMIT || DT) {
-    const int ib = __ldg(d.inc_start + slice) + lane;
-    const C vol = live ? static_cast<C>(__ldg(d.volume + c)) : C(0);
-    for (int j = warp; j < i_max; j += nw) {
-      if (j < il) {
-        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
-        C fr[kFace];
-        const C* r;
-        if (code >= 0) {
-          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
-          r = (code & 1) ? fr + 8 : fr + 4;
-        } else {
-          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 0, 8, fr);
-          r = fr + 4;
+    const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
+    const int len = __ldg(d.st_len + c);
+    for (int j0 = 0; j0 < len; j0 += CHUNK) {
+      C e4[CHUNK][4], wn[CHUNK][5];
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q)
+        if (j0 + q < len)
+          load_words<P>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice), 0, 4, e4[q]);
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q) {
+        if (j0 + q < len) {
+          const int e = index_of(e4[q][3]);
+          load5<P>(e >= 0 ? d.rec + static_cast<long long>(e) * kRec
+                          : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
+                   wn[q]);
         }
-        if constexpr (LIMIT) {
+      }
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q) {
+        if (j0 + q < len) {
 #pragma unroll
           for (int i = 0; i < 5; ++i) {
-            const C* g = cell + (5 + 3 * i) * 32 + lane;
-            const C dd = g[0] * r[0] + g[32] * r[1] + g[64] * r[2];
-            const C wci = cell[i * 32 + lane];
-            V[(j * 5 + i) * 32 + lane] = venkat(dd, cell[(25 + i) * 32 + lane] - wci,
-                                                cell[(20 + i) * 32 + lane] - wci, d.p.scale[i] * vol);
-          }
-        }
-        if constexpr (DT) {
-          C wn[8], wc[5];
-          if (code >= 0) {
-            const int o = (code & 1) ? index_of(fr[7]) : index_of(fr[11]);
-            load_words<P>(d.rec + static_cast<long long>(o) * kRec, 0, 8, wn);
-          } else {
-            load_words<P>(d.prim_b + static_cast<long long>(-code - 1) * kPrimB, 0, 8, wn);
+            const C dw = wn[q][i] - wc[i];
+            acc[3 * i] += static_cast<double>(dw * e4[q][0]);
+            acc[3 * i + 1] += static_cast<double>(dw * e4[q][1]);
+            acc[3 * i + 2] += static_cast<double>(dw * e4[q][2]);
           }
 #pragma unroll
-          for (int k = 0; k < 5; ++k) wc[k] = cell[k * 32 + lane];
-          W[j * 32 + lane] = static_cast<double>(wave_speed(wc, wn, fr, fr[3], d.p.g, d.p.pref));
+          for (int i = 0; i < 5; ++i) {
+            if (wn[q][i] < lo[i]) lo[i] = wn[q][i];
+            if (wn[q][i] > hi[i]) hi[i] = wn[q][i];
+          }
         }
       }
     }
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < 6 * 32; t += blockDim.x) {
-    const int q = t >> 5, l = t & 31;
-    const int cc = slice * 32 + l;
-    if (cc >= d.n) continue;
-    const int iln = __ldg(d.inc_len + cc);
-    if (q < 5) {
-      C phi = C(1.0);  // second order without limiter: phi = 1 (physics/src/euler.cpp:195)
-      if constexpr (LIMIT) {
-        phi = C(INFINITY);
-        for (int j = 0; j < iln; ++j) {
-          const C v = V[(j * 5 + q) * 32 + l];
-          if (v < phi) phi = v;
+    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
+    C out[20];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
+    const C* g = out + 5;
+    if constexpr (LIMIT) {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        lo[i] = minv(lo[i], wc[i]);
+        hi[i] = maxv(hi[i], wc[i]);
+      }
+      const C vol = static_cast<C>(__ldg(d.volume + c));
+      C phi[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
+      const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+      const int il = __ldg(d.inc_len + c);
+      for (int j = 0; j < il; ++j) {
+        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+        C r[4];
+        if (code >= 0) {
+          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, (code & 1) ? 8 : 4, 4, r);
+        } else {
+          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 4, 4, r);
         }
-        phi = minv(phi, C(1.0));  // at_most_one (:591-593)
-      }
-      cell[(30 + q) * 32 + l] = phi;
-    } else if constexpr (DT) {
-      double acc = 0.0;
-      for (int j = 0; j < iln; ++j) acc += W[j * 32 + l];
-      const double lam = static_cast<double>(static_cast<C>(acc));
-      const double dt = cfl * d.volume[cc] / lam;
-      if (local) d.dt_local[cc] = dt;
-      dts[l] = dt;
-    }
-  }
-  __syncthreads();
-  // Words 8-27 of the records: phi (8-12), then grad (13-27), as 16-byte vectors.
-  constexpr int nvec = 20 / P::kVec;
-  for (int t = threadIdx.x; t < nvec * 32; t += blockDim.x) {
-    const int v = t >> 5, l = t & 31;
-    const int cc = slice * 32 + l;
-    if (cc >= d.n) continue;
-    C x[P::kVec];
 #pragma unroll
-    for (int u = 0; u < P::kVec; ++u) {
-      const int w = 8 + v * P::kVec + u;
-      x[u] = w < kGrad ? cell[(30 + (w - kPhi)) * 32 + l] : cell[(5 + (w - kGrad)) * 32 + l];
-    }
-    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(cc) * kRec, 8 + v * P::kVec,
-                   P::kVec, x);
-  }
-  if constexpr (DT) {
-    if (warp == 0) {
-      unsigned long long b = ~0ULL;
-      if (live && dts[lane] > 0.0) b = static_cast<unsigned long long>(__double_as_longlong(dts[lane]));
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(0xffffffffu, b, off);
-        b = o < b ? o : b;
+        for (int i = 0; i < 5; ++i) {
+          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+          if (v < phi[i]) phi[i] = v;
+        }
       }
-      if (lane == 0 && b != ~0ULL) atomicMin(&d.ctl->dt_bits, b);
+      // at_most_one (:591-593)
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
+    } else {
+      // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = C(1.0);
+    }
+    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+    if constexpr (DT) {
+      dt = cell_time_step(d, c, wc, cfl);
+      if (local) d.dt_local[c] = dt;
     }
   }
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
 // The CFL step alone (first-order schemes), with the block minimum; `dt_out` for the host.
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int local,
-                                                     double* dt_out) {
+__global__ void __launch_bounds__(256) k_spectral(Dev<P> d, double cfl, int local,
+                                                  double* dt_out) {
   using C = typename P::C;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < d.n;
@@ -494,211 +437,309 @@ __global__ void __launch_bounds__(kBlock) k_spectral(Dev<P> d, double cfl, int l
 
 enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
 
-template <class P>
-size_t faces_smem(int i_max) {
-  return static_cast<size_t>(i_max) * 5 * 32 * sizeof(typename P::C) + 5 * 32 * sizeof(double) +
-         static_cast<size_t>(i_max) * 32;
+// The reconstruction data of a cell: primitives, limiter and gradient (zero gradient and limiter
+// for the first-order scheme).
+template <class P, bool SECOND>
+__device__ __forceinline__ void cell_recon(const Dev<P>& d, int c, typename P::C* w,
+                                           typename P::C* phi, typename P::C* g) {
+  using C = typename P::C;
+  if constexpr (SECOND) {
+    load_recon<P>(d.rec, c, w, phi, g);
+  } else {
+    load5<P>(d.rec + static_cast<long long>(c) * kRec, w);
+#pragma unroll
+    for (int k = 0; k < 15; ++k) g[k] = C(0.0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) phi[k] = C(0.0);
+  }
 }
 
-// The faces of the 32 cells of one slice per block (roe/hllc/ausm _faces and _boundaries,
-// kernels/euler.py:687-1049), face-parallel and gathered: warp j recomputes the flux of face j of
-// every cell (no float atomics, no face scratch in HBM); one thread per (cell, component) then
-// adds them in increasing face index from the source term -V s, the order in which the
-// reference's scatter adds them (emit_cpu.py emit_loop), and in the RK modes updates that
-// component in FP64; one thread per cell finally writes the next stage's primitives.
-template <class P, int FLUX, bool PLANAR, bool SECOND>
-__global__ void __launch_bounds__(256) k_faces(Dev<P> d, int mode, int stage, double wa,
-                                               double wb, int local, int last, int i_max) {
+// The flux of interior face f in its orientation (roe_face / hllc_face / ausm_face,
+// kernels/euler.py:687-753, planar forms :783-844): both sides reconstructed, the numerical flux
+// times the area, plus the warped-face term.
+template <class P, int FLUX, bool PLANAR>
+__device__ __forceinline__ void interior_flux(const Dev<P>& d, int f, const typename P::C* fr,
+                                              const typename P::C* wl, const typename P::C* gl,
+                                              const typename P::C* pl, const typename P::C* wr,
+                                              const typename P::C* gr, const typename P::C* pr,
+                                              typename P::C* out) {
   using C = typename P::C;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* F = reinterpret_cast<C*>(smem_raw);
-  double* NU = reinterpret_cast<double*>(F + static_cast<size_t>(i_max) * 5 * 32);
-  signed char* side = reinterpret_cast<signed char*>(NU + 5 * 32);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int slice = blockIdx.x;
-  const int c = slice * 32 + lane;
-  const bool live = c < d.n;
-  const int il = live ? __ldg(d.inc_len + c) : 0;
-  const int ib = __ldg(d.inc_start + slice) + lane;
-  for (int j = warp; j < i_max; j += nw) {
-    if (j >= il) continue;
-    C wc[5], gc[15], pc[5];
-    if constexpr (SECOND) {
-      load_recon<P>(d.rec, c, wc, pc, gc);
-    } else {
-      load_prim<P>(d.rec, c, wc);
+  const C* n = fr;
+  const C area = fr[3];
+  C fl[5], frr[5], fx[5];
+  reconstruct(wl, gl, pl, fr + 4, d.p.pref, fl);
+  reconstruct(wr, gr, pr, fr + 8, d.p.pref, frr);
+  numerical_flux<FLUX>(fl, frr, n, d.p, fx);
+  if constexpr (PLANAR) {
 #pragma unroll
-      for (int k = 0; k < 15; ++k) gc[k] = C(0.0);
+    for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
+  } else {
+    C m[9], avg[5], wt[5];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) pc[k] = C(0.0);
-    }
-    const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
-    C out[5];
-    signed char sgn = 1;
-    if (code >= 0) {
-      const int f = code >> 1;
-      const bool left = (code & 1) == 0;
-      sgn = left ? 1 : -1;
-      C fr_[kFace];
-      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr_);
-      const int o = left ? index_of(fr_[11]) : index_of(fr_[7]);
-      C wo[5], go[15], po[5];
-      if constexpr (SECOND) {
-        load_recon<P>(d.rec, o, wo, po, go);
-      } else {
-        load_prim<P>(d.rec, o, wo);
+    for (int q = 0; q < 9; ++q) m[q] = __ldg(d.f_m + static_cast<long long>(q) * d.n_if + f);
 #pragma unroll
-        for (int k = 0; k < 15; ++k) go[k] = C(0.0);
+    for (int k = 0; k < 5; ++k) avg[k] = C(0.5) * (fl[k] + frr[k]);
+    warp_term(avg, gl, pl, gr, pr, m, d.p.g, d.p.pref, wt);
 #pragma unroll
-        for (int k = 0; k < 5; ++k) po[k] = C(0.0);
-      }
-      const C* n = fr_;
-      const C area = fr_[3];
-      const C* wl = left ? wc : wo;
-      const C* gl = left ? gc : go;
-      const C* pl = left ? pc : po;
-      const C* wr = left ? wo : wc;
-      const C* gr = left ? go : gc;
-      const C* pr = left ? po : pc;
-      C fl[5], frr[5], fx[5];
-      reconstruct(wl, gl, pl, fr_ + 4, d.p.pref, fl);
-      reconstruct(wr, gr, pr, fr_ + 8, d.p.pref, frr);
-      numerical_flux<FLUX>(fl, frr, n, d.p, fx);
-      if constexpr (PLANAR) {
-#pragma unroll
-        for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
-      } else {
-        C m[9], avg[5], wt[5];
-#pragma unroll
-        for (int q = 0; q < 9; ++q) m[q] = __ldg(d.f_m + static_cast<long long>(q) * d.n_if + f);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) avg[k] = C(0.5) * (fl[k] + frr[k]);
-        warp_term(avg, gl, pl, gr, pr, m, d.p.g, d.p.pref, wt);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) out[k] = area * fx[k] + wt[k];
-      }
-    } else {
-      const int b = -code - 1;
-      C br[kBface], wf[5], wbv[5];
-      load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
-      const C* n = br;
-      const C area = br[3];
-      const C kind = br[7];
-      reconstruct(wc, gc, pc, br + 4, d.p.pref, wf);
-      const bool slip = (kind > C(1.5)) & (kind < C(2.5));
-      const bool wall = PLANAR ? slip : (slip | (kind > C(4.5)));
-      if (wall) {
-        const C wfl[5] = {C(0.0), wf[4] * n[0], wf[4] * n[1], wf[4] * n[2], C(0.0)};
-        if constexpr (PLANAR) {
-#pragma unroll
-          for (int k = 0; k < 5; ++k) out[k] = area * wfl[k];
-        } else {
-          C m[9];
-#pragma unroll
-          for (int q = 0; q < 9; ++q) m[q] = __ldg(d.b_m + static_cast<long long>(q) * d.nb + b);
-          // wall_warp (:678-681): p_l M^T grad p.
-          C ww[5] = {C(0.0), C(0.0), C(0.0), C(0.0), C(0.0)};
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-            ww[1 + i] = pc[4] * (m[i] * gc[12] + m[3 + i] * gc[13] + m[6 + i] * gc[14]);
-#pragma unroll
-          for (int k = 0; k < 5; ++k) out[k] = area * wfl[k] + ww[k];
-        }
-      } else {
-        boundary_value(wf, kind, br + 8, n, d.p, wbv);
-        C fx[5];
-        numerical_flux<FLUX>(wf, wbv, n, d.p, fx);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) F[(j * 5 + k) * 32 + lane] = out[k];
-    side[j * 32 + lane] = sgn;
+    for (int k = 0; k < 5; ++k) out[k] = area * fx[k] + wt[k];
   }
-  __syncthreads();
-  for (int t = threadIdx.x; t < 5 * 32; t += blockDim.x) {
-    const int k = t >> 5, l = t & 31;
-    const int cc = slice * 32 + l;
-    if (cc >= d.n) continue;
-    const int iln = __ldg(d.inc_len + cc);
-    const double vol = __ldg(d.volume + cc);
-    const long long i = static_cast<long long>(k) * d.n + cc;
-    // sources (:611-616): res = -V s, in the compute type, stored in FP64.
-    const C s = d.source != nullptr ? __ldg(d.source + i) : C(0.0);
-    double res = static_cast<double>(-static_cast<C>(vol) * s);
-    for (int j = 0; j < iln; ++j) {
-      const double o = static_cast<double>(F[(j * 5 + k) * 32 + l]);
-      if (side[j * 32 + l] > 0) {
-        res += o;
+}
+
+// The flux of boundary face b (roe_boundary ..., kernels/euler.py:868-941, planar :967-1037):
+// slip walls (and no-slip walls in the full loops) carry the pressure only.
+template <class P, int FLUX, bool PLANAR>
+__device__ __forceinline__ void boundary_flux(const Dev<P>& d, int b, const typename P::C* br,
+                                              const typename P::C* wc, const typename P::C* gc,
+                                              const typename P::C* pc, typename P::C* out) {
+  using C = typename P::C;
+  const C* n = br;
+  const C area = br[3];
+  const C kind = br[7];
+  C wf[5];
+  reconstruct(wc, gc, pc, br + 4, d.p.pref, wf);
+  const bool slip = (kind > C(1.5)) & (kind < C(2.5));
+  const bool wall = PLANAR ? slip : (slip | (kind > C(4.5)));
+  if (wall) {
+    const C wfl[5] = {C(0.0), wf[4] * n[0], wf[4] * n[1], wf[4] * n[2], C(0.0)};
+    if constexpr (PLANAR) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) out[k] = area * wfl[k];
+    } else {
+      C m[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) m[q] = __ldg(d.b_m + static_cast<long long>(q) * d.nb + b);
+      // wall_warp (:678-681): p_l M^T grad p.
+      C ww[5] = {C(0.0), C(0.0), C(0.0), C(0.0), C(0.0)};
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        ww[1 + i] = pc[4] * (m[i] * gc[12] + m[3 + i] * gc[13] + m[6 + i] * gc[14]);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) out[k] = area * wfl[k] + ww[k];
+    }
+  } else {
+    C wbv[5], fx[5];
+    boundary_value(wf, kind, br + 8, n, d.p, wbv);
+    numerical_flux<FLUX>(wf, wbv, n, d.p, fx);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
+  }
+}
+
+// After a cell's residual: the residual output, the RK stage update of the FP64 state, the next
+// stage's primitives and, after the last stage, the validity checks.
+template <class P>
+__device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double* res,
+                                            double vol, int mode, int stage, double wa, double wb,
+                                            int local, int last) {
+  using C = typename P::C;
+  if (mode == kResidual || stage == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
+  }
+  if (mode == kResidual) return;
+  const double h = local ? d.dt_local[c] : d.ctl->dt;
+  double nu[5];
+  if (mode == kRk3) {
+    // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const long long i = static_cast<long long>(k) * d.n + c;
+      const double uk = d.u[i];
+      const double sk = stage == 0 ? uk : d.stage[i];
+      const double next = sk - h / vol * res[k];
+      nu[k] = wa * uk + wb * next;
+      if (last) {
+        d.u[i] = nu[k];
       } else {
-        res -= o;
+        d.stage[i] = nu[k];
       }
     }
-    if (mode == kResidual || stage == 0) d.res[i] = res;
-    if (mode == kResidual) continue;
-    const double h = local ? d.dt_local[cc] : d.ctl->dt;
-    const double uk = d.u[i];
-    double nu;
-    if (mode == kRk3) {
-      // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
-      const double sk = stage == 0 ? uk : d.stage[i];
-      const double next = sk - h / vol * res;
-      nu = wa * uk + wb * next;
-      if (!last) d.stage[i] = nu;
-    } else {
-      // Classical RK4: stage_s = u - ((c_s h) / V) R_s; u = u - ((h / 6) / V) (R_0 + 2 R_1 +
-      // 2 R_2 + R_3).
+  } else {
+    // Classical RK4: stage_s = u - ((c_s h) / V) R_s; u = u - ((h / 6) / V) (R_0 + 2 R_1 +
+    // 2 R_2 + R_3).
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const long long i = static_cast<long long>(k) * d.n + c;
+      const double uk = d.u[i];
       double a;
       if (stage == 0) {
-        a = res;
+        a = res[k];
       } else if (stage < 3) {
-        a = d.racc[i] + 2.0 * res;
+        a = d.racc[i] + 2.0 * res[k];
       } else {
-        a = d.racc[i] + res;
+        a = d.racc[i] + res[k];
       }
       if (stage < 3) {
         d.racc[i] = a;
-        nu = uk - wa * h / vol * res;
+        nu[k] = uk - wa * h / vol * res[k];
       } else {
-        nu = uk - h / 6.0 / vol * a;
+        nu[k] = uk - h / 6.0 / vol * a;
+        d.u[i] = nu[k];
       }
     }
-    if (last) {
-      d.u[i] = nu;
-      if (!isfinite(res)) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(cc));
-    }
-    NU[k * 32 + l] = nu;
   }
-  if (mode == kResidual) return;
-  __syncthreads();
-  if (warp == 0 && live) {
-    double nu[5];
+  C w[5], dq[5];
+  prim_of_state(d, nu, w, dq);
+  store_prim<P>(d.rec_next, c, w);
+  if (last) {
+    // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
+    // it, in the compute type, then this stage's residual.
+    const C g = d.p.g;
+    const C r0 = static_cast<C>(d.ref[0]);
+    const C rho = r0 + dq[0];
+    C dm_m = C(0), mr_mr = C(0);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) nu[k] = NU[k * 32 + lane];
-    C w[5], dq[5];
-    prim_of_state(d, nu, w, dq);
-    store_prim<P>(d.rec_next, c, w);
-    if (last) {
-      // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will
-      // read it, in the compute type.
-      const C g = d.p.g;
-      const C r0 = static_cast<C>(d.ref[0]);
-      const C rho = r0 + dq[0];
-      C dm_m = C(0), mr_mr = C(0);
+    for (int k = 0; k < 3; ++k) {
+      const C mr = static_cast<C>(d.ref[k + 1]);
+      dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
+      mr_mr = mr_mr + mr * mr;
+    }
+    const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
+    const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
+    const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
+                     !(rho > C(0)) || !(pr > C(0));
+    if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
+    bool badr = false;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const C mr = static_cast<C>(d.ref[k + 1]);
-        dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
-        mr_mr = mr_mr + mr * mr;
+    for (int k = 0; k < 5; ++k) badr = badr || !isfinite(res[k]);
+    if (badr) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(c));
+  }
+}
+
+// Gather-recompute: the faces of one owned cell (roe/hllc/ausm _faces and _boundaries), every
+// face flux of the cell recomputed here and added in increasing face index from the source term
+// -V s, the order in which the reference's scatter adds them (emit_cpu.py emit_loop); then
+// finish_cell.
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stage, double wa,
+                                                    double wb, int local, int last) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  C wc[5], gc[15], pc[5];
+  cell_recon<P, SECOND>(d, c, wc, pc, gc);
+  const double vol = __ldg(d.volume + c);
+  double res[5];
+  {
+    const C nv = -static_cast<C>(vol);  // sources (:611-616): res = -V s
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const C s = d.source != nullptr ? __ldg(d.source + static_cast<long long>(k) * d.n + c) : C(0.0);
+      res[k] = static_cast<double>(nv * s);
+    }
+  }
+  const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+  const int il = __ldg(d.inc_len + c);
+  for (int j = 0; j < il; ++j) {
+    const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+    C out[5];
+    if (code >= 0) {
+      const int f = code >> 1;
+      const bool left = (code & 1) == 0;
+      C fr[kFace], wo[5], go[15], po[5];
+      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
+      cell_recon<P, SECOND>(d, left ? index_of(fr[11]) : index_of(fr[7]), wo, po, go);
+      if (left) {
+        interior_flux<P, FLUX, PLANAR>(d, f, fr, wc, gc, pc, wo, go, po, out);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
+      } else {
+        interior_flux<P, FLUX, PLANAR>(d, f, fr, wo, go, po, wc, gc, pc, out);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) res[k] -= static_cast<double>(out[k]);
       }
-      const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
-      const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
-      const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
-                       !(rho > C(0)) || !(pr > C(0));
-      if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
+    } else {
+      const int b = -code - 1;
+      C br[kBface];
+      load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+      boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
     }
   }
+  finish_cell(d, c, res, vol, mode, stage, wa, wb, local, last);
+}
+
+constexpr int kFlux = 8;  // flux record width (5 used): one 32-byte sector in fp32+acc64
+
+// Store-gather, first half (the reference's store strategy, emit_gpu.py): the flux of every owned
+// interior face, once, in its orientation, into the face scratch.
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux) {
+  using C = typename P::C;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.n_if) return;
+  C fr[kFace], wl[5], gl[15], pl[5], wr[5], gr[15], pr[5], out[8];
+  load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
+  cell_recon<P, SECOND>(d, index_of(fr[7]), wl, pl, gl);
+  cell_recon<P, SECOND>(d, index_of(fr[11]), wr, pr, gr);
+  interior_flux<P, FLUX, PLANAR>(d, f, fr, wl, gl, pl, wr, gr, pr, out);
+  out[5] = out[6] = out[7] = C(0);
+  store_words<P>(flux + static_cast<long long>(f) * kFlux, 0, kFlux, out);
+}
+
+// ... and of every boundary face of an owned cell (the first n_owned_faces - n_interior_faces).
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flux, int nbo) {
+  using C = typename P::C;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbo) return;
+  C br[kBface], wc[5], gc[15], pc[5], out[8];
+  load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+  cell_recon<P, SECOND>(d, index_of(br[13]), wc, pc, gc);
+  boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
+  out[5] = out[6] = out[7] = C(0);
+  store_words<P>(flux + static_cast<long long>(b) * kFlux, 0, kFlux, out);
+}
+
+// Store-gather, second half: each owned cell adds its faces' fluxes in increasing face index
+// from the source term (loads of four faces in flight at a time), then finish_cell.
+template <class P>
+__global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* flux,
+                                                const typename P::C* bflux, int mode, int stage,
+                                                double wa, double wb, int local, int last) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  const double vol = __ldg(d.volume + c);
+  double res[5];
+  {
+    const C nv = -static_cast<C>(vol);  // sources (:611-616): res = -V s
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const C s = d.source != nullptr ? __ldg(d.source + static_cast<long long>(k) * d.n + c) : C(0.0);
+      res[k] = static_cast<double>(nv * s);
+    }
+  }
+  const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+  const int il = __ldg(d.inc_len + c);
+  constexpr int kChunk = 4;
+  for (int j0 = 0; j0 < il; j0 += kChunk) {
+    int code[kChunk];
+    C fv[kChunk][5];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q)
+      code[q] = j0 + q < il ? __ldg(d.inc_code + ib + static_cast<long long>(j0 + q) * kSlice) : 0;
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q)
+      if (j0 + q < il)
+        load5<P>(code[q] >= 0 ? flux + static_cast<long long>(code[q] >> 1) * kFlux
+                              : bflux + static_cast<long long>(-code[q] - 1) * kFlux,
+                 fv[q]);
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+      if (j0 + q < il) {
+        if (code[q] >= 0 && (code[q] & 1)) {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) res[k] -= static_cast<double>(fv[q][k]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(fv[q][k]);
+        }
+      }
+    }
+  }
+  finish_cell(d, c, res, vol, mode, stage, wa, wb, local, last);
 }
 
 // The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176).
@@ -876,6 +917,43 @@ struct Counters {
   long long launches = 0, steps = 0, residuals = 0;
 };
 
+// Launch choices of the hot kernels; every choice computes the same bits (the summation order of
+// each cell is fixed), so the autotuner picks by time alone.
+struct Tuning {
+  int grad_chunk = 4;    // stencil entries loaded together by the gradient kernel: 1, 2 or 4
+  int grad_block = 128;  // its threads per block
+  int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather
+  int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
+  int gather_block = 256;  // threads per block of the store-gather sum
+  static constexpr int kCount = 5;
+  void to(int32_t* p) const {
+    p[0] = grad_chunk;
+    p[1] = grad_block;
+    p[2] = face_mode;
+    p[3] = face_block;
+    p[4] = gather_block;
+  }
+  static Tuning from(const int32_t* p) {
+    Tuning t;
+    t.grad_chunk = p[0];
+    t.grad_block = p[1];
+    t.face_mode = p[2];
+    t.face_block = p[3];
+    t.gather_block = p[4];
+    t.validate();
+    return t;
+  }
+  void validate() const;
+};
+
+void Tuning::validate() const {
+  auto block_ok = [](int b) { return b >= 32 && b <= 256 && b % 32 == 0; };
+  if (grad_chunk != 1 && grad_chunk != 2 && grad_chunk != 4) fail("E1101: grad_chunk is 1, 2 or 4");
+  if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
+  if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
+    fail("E1101: block sizes are multiples of 32 in [32, 256]");
+}
+
 class Stepper {
  public:
   virtual ~Stepper() = default;
@@ -895,6 +973,9 @@ class Stepper {
   virtual long long device_bytes() const = 0;
   virtual void kernel_times(double cfl, double dt, bool local, int rk, long long n, double* ms,
                             long long* launches) = 0;
+  virtual void set_tuning(const Tuning& t) = 0;
+  virtual Tuning tuning() const = 0;
+  virtual double autotune(double cfl, double dt, bool local, int rk, int trial_steps) = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
@@ -1043,14 +1124,7 @@ class Impl final : public Stepper {
       }
     }
     std::vector<double> vol(m.cell_volume, m.cell_volume + n_);
-    for (int c = 0; c < n_; ++c) {
-      s_max_ = std::max(s_max_, st_.len[c]);
-      i_max_ = std::max(i_max_, inc_.len[c]);
-    }
-    grad_warps_ = std::min(16, std::max(8, (s_max_ + 1) / 2));
-    face_warps_ = std::min(8, std::max(i_max_, 5));
-    if (gradient_smem<P>(s_max_, i_max_) > 200 * 1024)
-      fail("E1101: a stencil row is too long for the gradient kernel's shared memory");
+    nbo_ = m.n_owned_faces - m.n_interior_faces;
     // Device arrays.
     const size_t n5 = 5ULL * n_;
     for (auto& b : rec_) b.alloc(static_cast<size_t>(kRec) * n_ * sizeof(C));
@@ -1110,7 +1184,7 @@ class Impl final : public Stepper {
     long long t = 0;
     for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
                             &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
-                            &face_, &f_m_, &bface_, &b_m_, &source_})
+                            &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_})
       t += static_cast<long long>(b->bytes());
     for (const auto& b : rec_) t += static_cast<long long>(b.bytes());
     return t;
@@ -1310,6 +1384,81 @@ class Impl final : public Stepper {
     counters.steps += n;
   }
 
+  void set_tuning(const Tuning& t) override {
+    t.validate();
+    tuning_ = t;
+    drop_graph();
+  }
+
+  Tuning tuning() const override { return tuning_; }
+
+  // The autotuner: each candidate launch configuration steps the device state `trial_steps` times
+  // (after one untimed step) with event timing; the gradient choices are picked by the gradient
+  // kernel's time, then the face choices by the face kernels' time. The state is restored after
+  // every trial, so tuning leaves the solution unchanged. Returns the tuned ms per step.
+  double autotune(double cfl, double dt, bool local, int rk, int trial_steps) override {
+    if (trial_steps < 1) fail("E1101: trial_steps must be positive");
+    Buffer saved(5ULL * n_ * sizeof(double));
+    check(cudaMemcpyAsync(saved.ptr(), u_.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),
+          "save state");
+    auto restore = [&]() {
+      check(cudaMemcpyAsync(u_.ptr(), saved.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),
+            "restore state");
+      launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
+             rec_[0].as<C>());
+      check(cudaStreamSynchronize(stream), "restore state");
+    };
+    auto measure = [&](const Tuning& t, int kind) {
+      tuning_ = t;
+      double ms[6];
+      long long l[6];
+      kernel_times(cfl, dt, local, rk, 1, ms, l);
+      kernel_times(cfl, dt, local, rk, trial_steps, ms, l);
+      restore();
+      double total = 0.0;
+      for (int k = 0; k < 6; ++k) total += ms[k];
+      return (kind < 0 ? total : ms[kind]) / trial_steps;
+    };
+    Tuning best = tuning_;
+    if (second_) {
+      double best_ms = 1e300;
+      Tuning keep = best;
+      for (int chunk : {1, 2, 4})
+        for (int block : {64, 128, 256}) {
+          Tuning t = keep;
+          t.grad_chunk = chunk;
+          t.grad_block = block;
+          const double ms = measure(t, kGradients);
+          if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+          }
+        }
+    }
+    {
+      double best_ms = 1e300;
+      Tuning keep = best;
+      for (int mode : {0, 1})
+        for (int block : {64, 128, 256})
+          for (int gather : {128, 256}) {
+            if (mode == 0 && gather != 256) continue;
+            Tuning t = keep;
+            t.face_mode = mode;
+            t.face_block = block;
+            t.gather_block = gather;
+            const double ms = measure(t, kFaces);
+            if (ms < best_ms) {
+              best_ms = ms;
+              best = t;
+            }
+          }
+    }
+    const double total = measure(best, -1);
+    tuning_ = best;
+    drop_graph();
+    return total;
+  }
+
   std::vector<int> ghost_owner_;
 
  private:
@@ -1350,8 +1499,8 @@ class Impl final : public Stepper {
 
   int slices() const { return std::max(1, (n_ + kSlice - 1) / kSlice); }
 
-  static int blocks(long long n) {
-    return static_cast<int>(std::max<long long>(1, (n + kBlock - 1) / kBlock));
+  static int blocks(long long n, int block = kBlock) {
+    return static_cast<int>(std::max<long long>(1, (n + block - 1) / block));
   }
   int norm_blocks() const { return std::min(blocks(n_), 148 * 8); }
 
@@ -1394,33 +1543,57 @@ class Impl final : public Stepper {
 
   void launch_faces(const Dev<P>& d, int mode, int stage, double wa, double wb, int local,
                     int last) {
-    const int g = slices();
-    const size_t smem = faces_smem<P>(i_max_);
-    auto go = [&](auto kernel) {
-      launch_smem(kFaces, kernel, g, 32 * face_warps_, smem, d, mode, stage, wa, wb, local, last,
-                  i_max_);
+    if (tuning_.face_mode == 0) {
+      dispatch_faces([&](auto flux, auto planar, auto second) {
+        constexpr int F = decltype(flux)::value;
+        constexpr bool PL = decltype(planar)::value, SE = decltype(second)::value;
+        const int bs = tuning_.face_block;
+        launch_as(kFaces, k_faces_cell<P, F, PL, SE>, blocks(n_, bs), bs, d, mode, stage, wa, wb,
+                  local, last);
+      });
+      return;
+    }
+    ensure_flux_scratch();
+    C* fl = flux_.as<C>();
+    C* bfl = bflux_.as<C>();
+    dispatch_faces([&](auto flux, auto planar, auto second) {
+      constexpr int F = decltype(flux)::value;
+      constexpr bool PL = decltype(planar)::value, SE = decltype(second)::value;
+      const int bs = tuning_.face_block;
+      launch_as(kFaces, k_face_flux<P, F, PL, SE>, blocks(nif_, bs), bs, d, fl);
+      if (nbo_ > 0) launch_as(kFaces, k_bface_flux<P, F, PL, SE>, blocks(nbo_, bs), bs, d, bfl, nbo_);
+    });
+    const int gb = tuning_.gather_block;
+    launch_as(kFaces, k_gather<P>, blocks(n_, gb), gb, d, static_cast<const C*>(fl),
+              static_cast<const C*>(bfl), mode, stage, wa, wb, local, last);
+  }
+
+  // Calls body(flux, planar, second) with the scheme's compile-time choices.
+  template <class B>
+  void dispatch_faces(B&& body) {
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using I2 = std::integral_constant<int, 2>;
+    using T = std::true_type;
+    using Fa = std::false_type;
+    auto by_flux = [&](auto pl, auto se) {
+      if (scheme_.flux == 0) body(I0{}, pl, se);
+      else if (scheme_.flux == 1) body(I1{}, pl, se);
+      else body(I2{}, pl, se);
     };
-    const int f = scheme_.flux;
     if (planar_) {
-      if (second_) {
-        if (f == 0) go(k_faces<P, 0, true, true>);
-        else if (f == 1) go(k_faces<P, 1, true, true>);
-        else go(k_faces<P, 2, true, true>);
-      } else {
-        if (f == 0) go(k_faces<P, 0, true, false>);
-        else if (f == 1) go(k_faces<P, 1, true, false>);
-        else go(k_faces<P, 2, true, false>);
-      }
+      if (second_) by_flux(T{}, T{});
+      else by_flux(T{}, Fa{});
     } else {
-      if (second_) {
-        if (f == 0) go(k_faces<P, 0, false, true>);
-        else if (f == 1) go(k_faces<P, 1, false, true>);
-        else go(k_faces<P, 2, false, true>);
-      } else {
-        if (f == 0) go(k_faces<P, 0, false, false>);
-        else if (f == 1) go(k_faces<P, 1, false, false>);
-        else go(k_faces<P, 2, false, false>);
-      }
+      if (second_) by_flux(Fa{}, T{});
+      else by_flux(Fa{}, Fa{});
+    }
+  }
+
+  void ensure_flux_scratch() {
+    if (flux_.bytes() == 0) {
+      flux_.alloc(static_cast<size_t>(kFlux) * std::max(nif_, 1) * sizeof(C));
+      bflux_.alloc(static_cast<size_t>(kFlux) * std::max(nbo_, 1) * sizeof(C));
     }
   }
 
@@ -1432,14 +1605,23 @@ class Impl final : public Stepper {
     const int g = blocks(n_);
     const int loc = local ? 1 : 0;
     if (second_) {
-      const int gs = slices(), bs = 32 * grad_warps_;
-      const size_t smem = gradient_smem<P>(s_max_, i_max_);
+      const int bs = tuning_.grad_block;
+      const int gs = blocks(n_, bs);
+      auto go = [&](auto lim, auto with_dt) {
+        constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
+        if (tuning_.grad_chunk == 1)
+          launch_as(kGradients, k_gradients<P, L, D, 1>, gs, bs, d, cfl, loc);
+        else if (tuning_.grad_chunk == 2)
+          launch_as(kGradients, k_gradients<P, L, D, 2>, gs, bs, d, cfl, loc);
+        else
+          launch_as(kGradients, k_gradients<P, L, D, 4>, gs, bs, d, cfl, loc);
+      };
       if (limiter_) {
-        if (dt) launch_smem(kGradients, k_gradients<P, true, true>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
-        else launch_smem(kGradients, k_gradients<P, true, false>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
+        if (dt) go(std::true_type{}, std::true_type{});
+        else go(std::true_type{}, std::false_type{});
       } else {
-        if (dt) launch_smem(kGradients, k_gradients<P, false, true>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
-        else launch_smem(kGradients, k_gradients<P, false, false>, gs, bs, smem, d, cfl, loc, s_max_, i_max_);
+        if (dt) go(std::false_type{}, std::true_type{});
+        else go(std::false_type{}, std::false_type{});
       }
     } else if (dt) {
       launch_as(kSpectral, k_spectral<P>, g, kBlock, d, cfl, loc, static_cast<double*>(nullptr));
@@ -1549,8 +1731,9 @@ class Impl final : public Stepper {
   long long graph_nodes_ = 0;
   StepKey graph_key_{0.0, 0.0, false, 0};
   int last_rec_ = 0;
-  int s_max_ = 1, i_max_ = 1;        // longest stencil and incidence rows
-  int grad_warps_ = 8, face_warps_ = 4;  // warps per block of the slice-parallel kernels
+  int nbo_ = 0;  // boundary faces of owned cells
+  Tuning tuning_;
+  Buffer flux_, bflux_;  // face scratch of the store-gather strategy
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {
     int kind;
@@ -1757,6 +1940,33 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
     long long l[6];
     h->kernel_times(cfl, dt, local != 0, rk, n_steps, ms, l);
     for (int k = 0; k < 6; ++k) launches[k] = l[k];
+  });
+}
+
+int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
+                                  size_t err_len) {
+  AUTAN_CALL({
+    if (params == nullptr || count < Tuning::kCount) fail("E1101: 5 tuning parameters expected");
+    h->set_tuning(Tuning::from(params));
+  });
+}
+
+int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, char* err,
+                                  size_t err_len) {
+  AUTAN_CALL({
+    if (params == nullptr || count < Tuning::kCount) fail("E1101: room for 5 parameters expected");
+    h->tuning().to(params);
+  });
+}
+
+int autan_euler_device_autotune(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                                int32_t trial_steps, int32_t* params, double* ms_per_step,
+                                char* err, size_t err_len) {
+  AUTAN_CALL({
+    if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
+    const double ms = h->autotune(cfl, dt, local != 0, rk, trial_steps);
+    if (params != nullptr) h->tuning().to(params);
+    if (ms_per_step != nullptr) *ms_per_step = ms;
   });
 }
 

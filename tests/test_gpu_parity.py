@@ -188,3 +188,34 @@ def test_conservation_full_size():
     assert r.invalid_cell is None
     for k in (0, 1, 2, 4):
         assert abs(after[k] - before[k]) <= 1e-12 * abs(before[k]), (k, after[k] - before[k])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
+def test_tuning_variants_are_bit_identical(precision):
+    """Every launch choice of the autotuner's space (gradient chunking and blocks, gather-recompute
+    or store-gather faces) gives the same bits, and equals the oracle."""
+    case = cases.vortex_tets(16, 16, 6, steps=3, precision=precision)
+    u_o, *_ = run_oracle(case, case.steps)
+    no = case.mesh.n_owned_cells
+    for chunk in (1, 2, 4):
+        for mode in (0, 1):
+            for block in (64, 256):
+                with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+                    dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=mode,
+                                   face_block=block, gather_block=256 if block == 64 else 128)
+                    dev.upload(case.u0)
+                    dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
+                    u = dev.download()
+                assert bits_equal(u[:, :no], u_o[:, :no]), (chunk, mode, block)
+
+
+def test_autotune_leaves_the_solution_unchanged():
+    case = cases.vortex_tets(20, 20, 6, steps=3, precision="fp32+acc64")
+    a, *_ = run_device(case, case.steps)
+    with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+        dev.upload(case.u0)
+        tuned, ms = dev.autotune(cfl=case.cfl, rk=3, trial_steps=1)
+        assert ms > 0 and dev.tuning() == tuned
+        dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
+        b = dev.download()
+    assert bits_equal(a, b)
