@@ -1172,6 +1172,7 @@ class Impl final : public Stepper {
     d_.b_m = b_m_.as<C>();
     d_.ctl = ctl_.as<Control>();
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
+    if (tuning_.face_mode == 1) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
   }
 
@@ -1387,6 +1388,7 @@ class Impl final : public Stepper {
   void set_tuning(const Tuning& t) override {
     t.validate();
     tuning_ = t;
+    if (t.face_mode == 1) ensure_flux_scratch();  // never inside a graph capture
     drop_graph();
   }
 
@@ -1408,6 +1410,7 @@ class Impl final : public Stepper {
              rec_[0].as<C>());
       check(cudaStreamSynchronize(stream), "restore state");
     };
+    ensure_flux_scratch();
     auto measure = [&](const Tuning& t, int kind) {
       tuning_ = t;
       double ms[6];
@@ -1553,7 +1556,7 @@ class Impl final : public Stepper {
       });
       return;
     }
-    ensure_flux_scratch();
+    if (flux_.bytes() == 0) fail("E1200: face scratch missing");
     C* fl = flux_.as<C>();
     C* bfl = bflux_.as<C>();
     dispatch_faces([&](auto flux, auto planar, auto second) {

@@ -280,8 +280,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
     dev.upload(case.u0)
     stream = torch.cuda.ExternalStream(dev.stream)
-    # The autotuner picks the launch choices on this case (the state is restored after it).
-    tuned, tuned_ms = dev.autotune(cfl=case.cfl, rk=case.rk, trial_steps=2)
+    if args.tuning:
+        dev.set_tuning(**dict(zip(dev.TUNING_KEYS, (int(v) for v in args.tuning.split(",")))))
+        tuned = dev.tuning()
+    else:
+        # The autotuner picks the launch choices on this case (the state is restored after it).
+        tuned, _ = dev.autotune(cfl=case.cfl, rk=case.rk, trial_steps=2)
     # Warm-up (and graph capture).
     dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.warmup, graph=True)
     if args.profile:
@@ -420,6 +424,8 @@ def main() -> None:
     ap.add_argument("--workload", choices=["tets", "hex"], default="tets")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")
+    ap.add_argument("--tuning", default="", help="launch choices instead of the autotuner: "
+                    "grad_chunk,grad_block,face_mode,face_block,gather_block")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()
