@@ -80,10 +80,11 @@ def vortex_hex(nx=64, ny=64, nz=2, steps=200, precision="fp64") -> Case:
                 isentropic_vortex(mesh), rk=4, cfl=0.5, steps=steps)  # fmt: skip
 
 
-def vortex_tets(nx=240, ny=240, nz=6, steps=100, precision="fp32+acc64", rcm=True,
+def vortex_tets(nx=240, ny=240, nz=6, steps=100, precision="fp32+acc64", rcm="morton",
                 extent=None) -> Case:  # fmt: skip
     """The jittered-tetrahedra vortex; smaller lattices keep the cell size (h = 10 / 240) unless
-    `extent` is given, so that parity cases are the same problem on a smaller periodic box."""
+    `extent` is given, so that parity cases are the same problem on a smaller periodic box. Cells
+    in Morton order of their centres by default (`rcm`: see mesh.lattice)."""
     if extent is None:
         h = 10.0 / 240
         extent = (nx * h, ny * h, nz * h)

@@ -145,7 +145,7 @@ struct Instance {
 // within two face layers of them; faces that touch an owned cell or a first-layer ghost are kept.
 // Interior faces sorted by (owner, neighbour); boundary faces of owned cells, then of ghosts,
 // each by (zone, owner); each cell's faces in increasing index.
-Mesh assemble(const Cellwise& in, bool use_rcm) {
+Mesh assemble(const Cellwise& in, int order) {
   const i32 ncw = in.n_cells();
   const i64 ncf = static_cast<i64>(in.face_node_offsets.size()) - 1;
   std::vector<i32> face_cell(static_cast<std::size_t>(ncf));
@@ -233,7 +233,55 @@ Mesh assemble(const Cellwise& in, bool use_rcm) {
   const i32 n_owned = static_cast<i32>(owned_cw.size());
   std::vector<i32> owned_index(static_cast<std::size_t>(ncw), -1);
   for (i32 i = 0; i < n_owned; ++i) owned_index[owned_cw[i]] = i;
-  if (use_rcm) {
+  if (order == 2) {
+    // Morton (Z-order) of the cells' node means, quantised to 21 bits per axis over the owned
+    // cells' bounding box: a warp's 32 consecutive cells form a compact blob whose stencils
+    // overlap, so neighbours' records are shared within the warp and stay in cache.
+    std::vector<std::array<double, 3>> centre(static_cast<std::size_t>(n_owned));
+    std::array<double, 3> lo{1e300, 1e300, 1e300}, hi{-1e300, -1e300, -1e300};
+    for (i32 i = 0; i < n_owned; ++i) {
+      const i32 c = owned_cw[i];
+      std::array<double, 3> m{0.0, 0.0, 0.0};
+      i64 count = 0;
+      for (i64 f = in.cell_face_offsets[c]; f < in.cell_face_offsets[c + 1]; ++f)
+        for (i64 k = in.face_node_offsets[f]; k < in.face_node_offsets[f + 1]; ++k) {
+          const i32 p = in.face_nodes[k];
+          m[0] += in.x[p];
+          m[1] += in.y[p];
+          m[2] += in.z[p];
+          ++count;
+        }
+      for (int a = 0; a < 3; ++a) {
+        m[a] /= static_cast<double>(count);
+        lo[a] = std::min(lo[a], m[a]);
+        hi[a] = std::max(hi[a], m[a]);
+      }
+      centre[i] = m;
+    }
+    auto spread = [](std::uint64_t v) {
+      v &= 0x1fffffULL;
+      v = (v | v << 32) & 0x1f00000000ffffULL;
+      v = (v | v << 16) & 0x1f0000ff0000ffULL;
+      v = (v | v << 8) & 0x100f00f00f00f00fULL;
+      v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+      v = (v | v << 2) & 0x1249249249249249ULL;
+      return v;
+    };
+    std::vector<std::pair<std::uint64_t, i32>> key(static_cast<std::size_t>(n_owned));
+    // One scale for the three axes, so that the curve's boxes stay cubes on a flat domain.
+    double span = 0.0;
+    for (int a = 0; a < 3; ++a) span = std::max(span, hi[a] - lo[a]);
+    if (!(span > 0.0)) span = 1.0;
+    for (i32 i = 0; i < n_owned; ++i) {
+      std::uint64_t q[3];
+      for (int a = 0; a < 3; ++a)
+        q[a] = static_cast<std::uint64_t>((centre[i][a] - lo[a]) / span * 2097151.0);
+      key[i] = {spread(q[0]) | spread(q[1]) << 1 | spread(q[2]) << 2, owned_cw[i]};
+    }
+    std::stable_sort(key.begin(), key.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (i32 i = 0; i < n_owned; ++i) owned_cw[i] = key[i].second;
+  } else if (order == 1) {
     std::vector<i64> off(static_cast<std::size_t>(n_owned) + 1, 0);
     std::vector<i32> adj;
     for (i32 i = 0; i < n_owned; ++i) {
@@ -717,7 +765,7 @@ Mesh lattice(const autan_lattice& s) {
       cw.cell_face_offsets.push_back(static_cast<i64>(cw.face_node_offsets.size()) - 1);
     }
   }
-  Mesh m = assemble(cw, s.rcm != 0);
+  Mesh m = assemble(cw, s.rcm);
   finish(m);
   return m;
 }
@@ -838,7 +886,7 @@ int autan_mesh_build_cells(int64_t n_points, const double* points, int64_t n_cel
       if (p < 0 || p >= n_points) fail("E1101", "a face node is out of range");
     cw.image.assign(static_cast<std::size_t>(n_cells), -1);
     cw.shift.assign(3 * static_cast<std::size_t>(n_cells), 0.0);
-    Mesh m = assemble(cw, rcm_flag != 0);
+    Mesh m = assemble(cw, rcm_flag);
     finish(m);
     *mesh = new Mesh(std::move(m));
   });

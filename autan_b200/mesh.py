@@ -21,6 +21,7 @@ from autan_b200 import _native as N
 
 # Boundary condition codes (kernels/euler.py:55-60, physics/include/autan/physics/euler.hpp:31-38).
 BC_STATE, BC_FARFIELD, BC_SLIP, BC_INLET, BC_OUTLET, BC_WALL = range(6)
+ORDERS = {"none": 0, "rcm": 1, "morton": 2}
 
 _DTYPES = {("int32", 4): np.int32, ("int64", 8): np.int64, ("float64", 8): np.float64}
 _INT32 = {"owner", "neighbour", "cell_faces", "face_zone", "stencil", "ghost_owner", "face_nodes",
@@ -140,11 +141,13 @@ def lattice(
     periodic=(False, False, False),
     zones=(0, 1, 2, 3, 4, 5),
     displacement: np.ndarray | None = None,
-    rcm: bool = False,
+    rcm: bool | int = False,
 ) -> Mesh:
     """A lattice mesh of hexahedra (`fill="hexa"`) or Kuhn tetrahedra (`fill="tetra"`).
     `zones`: boundary zone of the sides x-, x+, y-, y+, z-, z+ (ignored on periodic axes).
-    `displacement`: 3 x (nx+1)(ny+1)(nz+1) node moves, node (i, j, k) at i + (nx+1)(j + (ny+1) k)."""
+    `displacement`: 3 x (nx+1)(ny+1)(nz+1) node moves, node (i, j, k) at i + (nx+1)(j + (ny+1) k).
+    `rcm`: owned cell order, False/0 the generator's, True/1 reverse Cuthill-McKee, 2 or "morton"
+    the Z-order of the cell centres."""
     spec = N.Lattice()
     spec.fill = {"hexa": 0, "tetra": 1}[fill]
     spec.nx, spec.ny, spec.nz = n
@@ -158,7 +161,7 @@ def lattice(
         if disp.size != 3 * (n[0] + 1) * (n[1] + 1) * (n[2] + 1):
             raise ValueError("displacement must hold 3 values per lattice node")
         spec.displacement = N.ptr(disp, C.c_double)
-    spec.rcm = int(rcm)
+    spec.rcm = ORDERS.get(rcm, rcm) if isinstance(rcm, str) else int(rcm)
     handle = C.c_void_p()
     err = N.errbuf()
     N.check(N.lib().autan_mesh_build_lattice(C.byref(spec), C.byref(handle), err, len(err)), err)
@@ -177,7 +180,8 @@ def from_cells(points, cell_face_offsets, face_node_offsets, face_nodes, face_zo
     N.check(
         N.lib().autan_mesh_build_cells(
             pts.shape[-1], N.ptr(pts, C.c_double), cfo.size - 1, N.ptr(cfo, C.c_int64),
-            N.ptr(fno, C.c_int64), N.ptr(fn, C.c_int32), N.ptr(fz, C.c_int32), int(rcm),
+            N.ptr(fno, C.c_int64), N.ptr(fn, C.c_int32), N.ptr(fz, C.c_int32),
+        ORDERS.get(rcm, 0) if isinstance(rcm, str) else int(rcm),
             C.byref(handle), err, len(err),
         ),
         err,
@@ -210,7 +214,7 @@ def vortex_jitter(n: tuple[int, int, int], extent, amplitude=0.2, seed=0) -> np.
 
 
 def jittered_tets(nx=240, ny=240, nz=6, extent=(10.0, 10.0, 0.25), amplitude=0.2, seed=0,
-                  rcm=True) -> Mesh:  # fmt: skip
+                  rcm="morton") -> Mesh:  # fmt: skip
     """Kuhn tetrahedra of a jittered lattice, periodic in x and y, zones 4 (z-) and 5 (z+)."""
     disp = vortex_jitter((nx, ny, nz), extent, amplitude, seed)
     return lattice("tetra", (nx, ny, nz), (0.0, 0.0, 0.0), extent, (True, True, False),

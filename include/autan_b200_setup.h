@@ -4,7 +4,8 @@
  * These entry points replace, for callers that have no Autan mesh of their own (tests, the
  * benchmark), the reference's set-up chain:
  *   core/src/cellwise.cpp  to_face_based + core/src/mesh.cpp assemble  -> autan_mesh_build_*
- *   core/src/renumber.cpp:109 rcm_order                                  -> spec.rcm
+ *   core/src/renumber.cpp:109 rcm_order                                  -> spec.rcm = 1
+ *   (a Morton order of the cell centres, spec.rcm = 2, has no counterpart in the reference)
  *   core/src/geometry.cpp:120 compute_geometry                           -> built with the mesh
  *   codegen/cpp/geometry.cpp:166 pack_geometry (normals, moments)        -> built with the mesh
  *   codegen/cpp/geometry.cpp:432 cell_stencil (face2)                    -> built with the mesh
@@ -46,7 +47,7 @@ struct autan_lattice {
   int32_t periodic[3];
   int32_t zone[6];
   const double* displacement;
-  int32_t rcm; /* renumber the owned cells in reverse Cuthill-McKee order */
+  int32_t rcm; /* owned cell order: 0 generator's, 1 reverse Cuthill-McKee, 2 Morton (Z-order) */
 };
 
 /* Builds an assembled mesh with its geometry and face2 stencil. */
@@ -61,7 +62,7 @@ int autan_mesh_build_lattice(const struct autan_lattice* spec, void** mesh, char
  * No ghost cells (no periodic axis). */
 int autan_mesh_build_cells(int64_t n_points, const double* points, int64_t n_cells,
                            const int64_t* cell_face_offsets, const int64_t* face_node_offsets,
-                           const int32_t* face_nodes, const int32_t* face_zone, int32_t rcm,
+                           const int32_t* face_nodes, const int32_t* face_zone, int32_t order,
                            void** mesh, char* err, size_t err_len);
 
 void autan_mesh_free(void* mesh);
