@@ -76,6 +76,7 @@ struct Control {
   unsigned long long bad_res;    // least cell with a non-finite residual
   long long step;                // steps taken since the last reset
   double dt;                     // the global step of the current step
+  unsigned long long fault;      // a bounded device wait timed out
   double rms[5];
   unsigned long long words[5][kWords];
   double hist_rms[kHistory][5];
@@ -108,6 +109,8 @@ struct Dev {
   const int* inc_start;
   const int* inc_len;
   const int* inc_code;
+  const C* inc_rec;  // 4 per incidence, sliced: rel(x_f, x_c) of the cell's side, code
+  int n_slices;
   const C* face;    // kFace per owned interior face
   const C* bface;   // kBface per boundary face
   const C* f_m;     // 9 x n_if, warped meshes only
@@ -411,6 +414,191 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
     store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
     if constexpr (DT) {
       dt = cell_time_step(d, c, wc, cfl);
+      if (local) d.dt_local[c] = dt;
+    }
+  }
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+// ---------------------------------------------------------------- TMA bulk staging
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// One 1-D bulk copy global -> shared (TMA, no tensor map, no multicast), completing on `bar`.
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, unsigned bytes,
+                                               unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, "
+      "p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr int kWaitLimit = 1 << 20;  // polls of an mbarrier before a kernel gives up
+
+// Waits for phase 0 of `bar` with an iteration limit. On a timeout it marks the control's fault
+// word and waits once more, again bounded, so that no copy into this block's shared memory is
+// left in flight when the block exits.
+__device__ __forceinline__ bool bounded_wait(unsigned long long* bar, Control* ctl) {
+  for (int it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, 0)) return true;
+  if (threadIdx.x == 0 && ctl != nullptr) atomicExch(&ctl->fault, 1ULL);
+  for (int it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, 0)) break;
+  return false;
+}
+
+// gradients + limiter (as k_gradients) for the cells of blockDim.x / 32 consecutive slices, their
+// stencil rows and per-incidence limiter records staged into shared memory by one TMA bulk copy
+// each (the slices' rows are contiguous in the sliced layout): the block's whole streaming input
+// is in flight at once, and the threads then only gather their neighbours' primitives (L2).
+template <class P, bool LIMIT, bool DT>
+__global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
+  using C = typename P::C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long bar;
+  const int per_block = blockDim.x / 32;
+  const int s0 = blockIdx.x * per_block;
+  const int s1 = min(s0 + per_block, d.n_slices);
+  const long long e0 = __ldg(d.st_start + s0), e1 = __ldg(d.st_start + s1);
+  const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s1);
+  C* ent = reinterpret_cast<C*>(smem_raw);
+  C* inc = ent + 4 * (e1 - e0);
+  const unsigned eb = static_cast<unsigned>((e1 - e0) * 4 * sizeof(C));
+  const unsigned ib = (LIMIT || DT) ? static_cast<unsigned>((i1 - i0) * 4 * sizeof(C)) : 0u;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, eb + ib);
+    if (eb > 0) bulk_to_shared(ent, d.st + 4 * e0, eb, &bar);
+    if (ib > 0) bulk_to_shared(inc, d.inc_rec + 4 * i0, ib, &bar);
+  }
+  if (!bounded_wait(&bar, d.ctl)) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n;
+  double dt = 0.0;
+  if (live) {
+    C wc[5];
+    load5<P>(d.rec + static_cast<long long>(c) * kRec, wc);
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
+    }
+    const C* row = ent + 4 * (__ldg(d.st_start + (c >> 5)) - e0 + (c & 31));
+    const int len = __ldg(d.st_len + c);
+    constexpr int kChunk = 4;
+    for (int j0 = 0; j0 < len; j0 += kChunk) {
+      C wn[kChunk][5];
+#pragma unroll
+      for (int q = 0; q < kChunk; ++q) {
+        if (j0 + q < len) {
+          const int e = index_of(row[4 * kSlice * (j0 + q) + 3]);
+          load5<P>(e >= 0 ? d.rec + static_cast<long long>(e) * kRec
+                          : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
+                   wn[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kChunk; ++q) {
+        if (j0 + q < len) {
+          const C* w = row + 4 * kSlice * (j0 + q);
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            const C dw = wn[q][i] - wc[i];
+            acc[3 * i] += static_cast<double>(dw * w[0]);
+            acc[3 * i + 1] += static_cast<double>(dw * w[1]);
+            acc[3 * i + 2] += static_cast<double>(dw * w[2]);
+          }
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            if (wn[q][i] < lo[i]) lo[i] = wn[q][i];
+            if (wn[q][i] > hi[i]) hi[i] = wn[q][i];
+          }
+        }
+      }
+    }
+    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
+    C out[20];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
+    const C* g = out + 5;
+    const C* irow = inc + 4 * (__ldg(d.inc_start + (c >> 5)) - i0 + (c & 31));
+    const int il = __ldg(d.inc_len + c);
+    if constexpr (LIMIT) {
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        lo[i] = minv(lo[i], wc[i]);
+        hi[i] = maxv(hi[i], wc[i]);
+      }
+      const C vol = static_cast<C>(__ldg(d.volume + c));
+      C phi[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
+      for (int j = 0; j < il; ++j) {
+        const C* r = irow + 4 * kSlice * j;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+          if (v < phi[i]) phi[i] = v;
+        }
+      }
+      // at_most_one (:591-593)
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
+    } else {
+      // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
+#pragma unroll
+      for (int i = 0; i < 5; ++i) out[i] = C(1.0);
+    }
+    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+    if constexpr (DT) {
+      // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89).
+      double lam = 0.0;
+      for (int j = 0; j < il; ++j) {
+        const int code = index_of(irow[4 * kSlice * j + 3]);
+        C wn[5], fr[kFace];
+        if (code >= 0) {
+          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
+          load5<P>(d.rec + static_cast<long long>((code & 1) ? index_of(fr[7]) : index_of(fr[11])) * kRec,
+                   wn);
+        } else {
+          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 0, 4, fr);
+          load5<P>(d.prim_b + static_cast<long long>(-code - 1) * kPrimB, wn);
+        }
+        lam += static_cast<double>(wave_speed(wc, wn, fr, fr[3], d.p.g, d.p.pref));
+      }
+      dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
     }
   }
@@ -925,13 +1113,15 @@ struct Tuning {
   int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather
   int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
   int gather_block = 256;  // threads per block of the store-gather sum
-  static constexpr int kCount = 5;
+  int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies
+  static constexpr int kCount = 6;
   void to(int32_t* p) const {
     p[0] = grad_chunk;
     p[1] = grad_block;
     p[2] = face_mode;
     p[3] = face_block;
     p[4] = gather_block;
+    p[5] = grad_mode;
   }
   static Tuning from(const int32_t* p) {
     Tuning t;
@@ -940,6 +1130,7 @@ struct Tuning {
     t.face_mode = p[2];
     t.face_block = p[3];
     t.gather_block = p[4];
+    t.grad_mode = p[5];
     t.validate();
     return t;
   }
@@ -950,6 +1141,8 @@ void Tuning::validate() const {
   auto block_ok = [](int b) { return b >= 32 && b <= 256 && b % 32 == 0; };
   if (grad_chunk != 1 && grad_chunk != 2 && grad_chunk != 4) fail("E1101: grad_chunk is 1, 2 or 4");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
+  if (grad_mode != 0 && grad_mode != 1) fail("E1101: grad_mode is 0 or 1");
+  if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
   if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
     fail("E1101: block sizes are multiples of 32 in [32, 256]");
 }
@@ -1073,6 +1266,7 @@ class Impl final : public Stepper {
     for (int c = 0; c <= n_; ++c) ioff[c] = m.cell_face_offsets[c];
     inc_ = slice_rows(ioff);
     std::vector<int> code(std::max<long long>(inc_.total, 1), 0);
+    std::vector<C> irec(4 * std::max<long long>(inc_.total, 1), C(0));
     for (int c = 0; c < n_; ++c) {
       int prev = -1;
       for (long long k = ioff[c]; k < ioff[c + 1]; ++k) {
@@ -1094,7 +1288,13 @@ class Impl final : public Stepper {
           if (m.owner[f] != c) fail("E1101: cell_faces lists a boundary face of another cell");
           v = -(f - ni_ + 1);
         }
-        code[inc_.at(c, static_cast<int>(k - ioff[c]))] = v;
+        const long long at = inc_.at(c, static_cast<int>(k - ioff[c]));
+        code[at] = v;
+        // The limiter's offset rel(x_f, x_c), as the face record holds it for this side.
+        const C* rel = v >= 0 ? face.data() + static_cast<long long>(f) * kFace + ((v & 1) ? 8 : 4)
+                              : bface_host_.data() + static_cast<long long>(f - ni_) * kBface + 4;
+        for (int a = 0; a < 3; ++a) irec[4 * at + a] = rel[a];
+        irec[4 * at + 3] = index_bits<C>(v);
       }
     }
     // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, value index or -(b + 1)}.
@@ -1142,6 +1342,7 @@ class Impl final : public Stepper {
     inc_start_ = upload(inc_.start, stream);
     inc_len_ = upload(inc_.len, stream);
     inc_code_ = upload(code, stream);
+    inc_rec_ = upload(irec, stream);
     face_ = upload(face, stream);
     f_m_ = upload(fm, stream);
     bface_ = upload(bface_host_, stream);
@@ -1166,6 +1367,8 @@ class Impl final : public Stepper {
     d_.inc_start = inc_start_.as<int>();
     d_.inc_len = inc_len_.as<int>();
     d_.inc_code = inc_code_.as<int>();
+    d_.inc_rec = inc_rec_.as<C>();
+    d_.n_slices = slices();
     d_.face = face_.as<C>();
     d_.bface = bface_.as<C>();
     d_.f_m = f_m_.as<C>();
@@ -1185,7 +1388,8 @@ class Impl final : public Stepper {
     long long t = 0;
     for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
                             &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
-                            &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_})
+                            &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_,
+                            &inc_rec_})
       t += static_cast<long long>(b->bytes());
     for (const auto& b : rec_) t += static_cast<long long>(b.bytes());
     return t;
@@ -1297,8 +1501,9 @@ class Impl final : public Stepper {
     if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
     if (n < 1) fail("E1101: n_steps must be positive");
     if (!(dt > 0.0) && !(cfl > 0.0)) fail("E1101: a positive dt or CFL is needed");
-    // Reset the step count so that the history holds this call's steps.
+    // Reset the step count so that the history holds this call's steps, and the fault word.
     check(cudaMemsetAsync(&d_.ctl->step, 0, sizeof(long long), stream), "reset");
+    check(cudaMemsetAsync(&d_.ctl->fault, 0, sizeof(unsigned long long), stream), "reset");
     const StepKey key{cfl, dt, local, rk};
     if (graph) {
       if (graph_exec_ == nullptr || !(key == graph_key_)) capture(key);
@@ -1314,6 +1519,7 @@ class Impl final : public Stepper {
     // The result: the control's head (the last step's sums, step and marks) only.
     check(cudaMemcpyAsync(head_, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
     check(cudaStreamSynchronize(stream), "control");
+    if (head_->fault != 0) fail("E1201: a bounded device wait timed out; results of this call are invalid");
     for (int k = 0; k < 5; ++k) out->residuals[k] = head_->rms[k];
     out->time_step = head_->dt;
     out->steps = head_->step;
@@ -1426,9 +1632,12 @@ class Impl final : public Stepper {
     if (second_) {
       double best_ms = 1e300;
       Tuning keep = best;
+      for (int mode : {0, 1})
       for (int chunk : {1, 2, 4})
         for (int block : {64, 128, 256}) {
+          if (mode == 1 && (chunk != 4 || block > 128)) continue;
           Tuning t = keep;
+          t.grad_mode = mode;
           t.grad_chunk = chunk;
           t.grad_block = block;
           const double ms = measure(t, kGradients);
@@ -1501,6 +1710,25 @@ class Impl final : public Stepper {
   }
 
   int slices() const { return std::max(1, (n_ + kSlice - 1) / kSlice); }
+
+  // Shared memory of the staged gradient kernel at `block` threads: the largest of its blocks'
+  // stencil rows and incidence records.
+  size_t staged_smem(int block) {
+    const int per = block / kSlice;
+    auto& cached = staged_smem_[per];
+    if (cached == 0) {
+      long long most = 0;
+      const int ns = slices();
+      for (int s0 = 0; s0 < ns; s0 += per) {
+        const int s1 = std::min(s0 + per, ns);
+        most = std::max<long long>(
+            most, static_cast<long long>(st_.start[s1] - st_.start[s0]) + (inc_.start[s1] - inc_.start[s0]));
+      }
+      cached = static_cast<size_t>(most) * 4 * sizeof(C) + 16;
+      if (cached > 220 * 1024) fail("E1101: stencil rows too long for the staged gradient kernel");
+    }
+    return cached;
+  }
 
   static int blocks(long long n, int block = kBlock) {
     return static_cast<int>(std::max<long long>(1, (n + block - 1) / block));
@@ -1612,6 +1840,11 @@ class Impl final : public Stepper {
       const int gs = blocks(n_, bs);
       auto go = [&](auto lim, auto with_dt) {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
+        if (tuning_.grad_mode == 1) {
+          launch_smem(kGradients, k_gradients_tma<P, L, D>, blocks(n_, bs), bs, staged_smem(bs),
+                      d, cfl, loc);
+          return;
+        }
         if (tuning_.grad_chunk == 1)
           launch_as(kGradients, k_gradients<P, L, D, 1>, gs, bs, d, cfl, loc);
         else if (tuning_.grad_chunk == 2)
@@ -1726,7 +1959,7 @@ class Impl final : public Stepper {
   Dev<P> d_{};
   Buffer rec_[3];
   Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
-  Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_;
+  Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_;
   Buffer face_, f_m_, bface_, b_m_, source_;
   std::vector<C> bface_host_;
   cudaGraph_t graph_ = nullptr;
@@ -1736,6 +1969,7 @@ class Impl final : public Stepper {
   int last_rec_ = 0;
   int nbo_ = 0;  // boundary faces of owned cells
   Tuning tuning_;
+  size_t staged_smem_[5] = {0, 0, 0, 0, 0};
   Buffer flux_, bflux_;  // face scratch of the store-gather strategy
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {
@@ -1949,7 +2183,7 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
                                   size_t err_len) {
   AUTAN_CALL({
-    if (params == nullptr || count < Tuning::kCount) fail("E1101: 5 tuning parameters expected");
+    if (params == nullptr || count < Tuning::kCount) fail("E1101: 6 tuning parameters expected");
     h->set_tuning(Tuning::from(params));
   });
 }
@@ -1957,7 +2191,7 @@ int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t c
 int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, char* err,
                                   size_t err_len) {
   AUTAN_CALL({
-    if (params == nullptr || count < Tuning::kCount) fail("E1101: room for 5 parameters expected");
+    if (params == nullptr || count < Tuning::kCount) fail("E1101: room for 6 parameters expected");
     h->tuning().to(params);
   });
 }

@@ -162,10 +162,12 @@ int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* er
 int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                     int64_t n_steps, double* ms, int64_t* launches, char* err,
                                     size_t err_len);
-/* Launch choices of the hot kernels (5 values): [0] stencil entries the gradient kernel loads
+/* Launch choices of the hot kernels (6 values): [0] stencil entries the gradient kernel loads
  * together (1, 2 or 4), [1] its threads per block, [2] face strategy (0 gather-recompute: each
  * cell recomputes its faces' fluxes; 1 store-gather: each face's flux once into a face scratch,
- * then summed per cell), [3] threads per block of the face kernel, [4] of the store-gather sum.
+ * then summed per cell), [3] threads per block of the face kernel, [4] of the store-gather sum,
+ * [5] gradient staging (0: each thread loads its stencil rows; 1: each block's rows staged into
+ * shared memory by TMA bulk copies, at most 128 threads per block).
  * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
  * (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
@@ -174,7 +176,7 @@ int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, 
                                   size_t err_len);
 /* The autotuner: times candidate launch choices on `trial_steps` steps each of this handle's own
  * case (the device state is restored after every trial), keeps the fastest and returns it in
- * params (5 values) with its ms per step. */
+ * params (6 values) with its ms per step. */
 int autan_euler_device_autotune(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                 int32_t trial_steps, int32_t* params, double* ms_per_step,
                                 char* err, size_t err_len);

@@ -197,16 +197,17 @@ def test_tuning_variants_are_bit_identical(precision):
     case = cases.vortex_tets(16, 16, 6, steps=3, precision=precision)
     u_o, *_ = run_oracle(case, case.steps)
     no = case.mesh.n_owned_cells
-    for chunk in (1, 2, 4):
+    for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 4)):
         for mode in (0, 1):
-            for block in (64, 256):
+            for block in (64, 128) if gmode else (64, 256):
                 with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
                     dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=mode,
-                                   face_block=block, gather_block=256 if block == 64 else 128)
+                                   face_block=block, gather_block=256 if block == 64 else 128,
+                                   grad_mode=gmode)
                     dev.upload(case.u0)
                     dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
                     u = dev.download()
-                assert bits_equal(u[:, :no], u_o[:, :no]), (chunk, mode, block)
+                assert bits_equal(u[:, :no], u_o[:, :no]), (gmode, chunk, mode, block)
 
 
 def test_autotune_leaves_the_solution_unchanged():
