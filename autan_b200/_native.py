@@ -132,6 +132,8 @@ def _bind(lib: C.CDLL) -> None:
            C.c_char_p, sz)  # fmt: skip
         fn("autan_euler_device_kernel_times", C.c_int, vp, f64, f64, i32, i32, i64, P(f64), P(i64),
            C.c_char_p, sz)  # fmt: skip
+    if hasattr(lib, "autan_exact_rms_static"):
+        fn("autan_exact_rms_static", C.c_int, vp, i64, i64, i32, vp, vp, C.c_char_p, sz)
 
 
 def lib() -> C.CDLL:

@@ -188,6 +188,22 @@ void* autan_euler_device_stream(void* handle);
  * [2] residual evaluations, [3] device bytes held. */
 int autan_euler_device_counters(void* handle, int64_t* counters, char* err, size_t err_len);
 
+/* Exact-sum RMS of device arrays that allocates no device memory: rms[k] = sqrt(sum_i
+ * values[k * stride + i]^2 / n) for k < components, each sum exact and rounded once (the norms of
+ * autan_euler_device_evaluate, bit for bit on the same residual). No counterpart in the reference.
+ *   values: device pointer; rms: device pointer to `components` doubles, written on `stream`
+ *   (a cudaStream_t, NULL for the default stream) of the calling thread's current device.
+ * Limits: components 1 to 8, n 1 to 2^30 (a sum's words cannot overflow), device index < 64;
+ * anything beyond is refused with E1101 before any device work.
+ * Scratch: 4544 bytes of module-level device memory per device, found with cudaGetSymbolAddress
+ * on the first call for each device (make that first call before any stream capture); each call
+ * clears the words it uses on `stream` first. Calls that overlap in time on one device share the
+ * scratch and race: order them on one stream or wait between them. For callers that cannot
+ * allocate at the point of the call (a pool allocator holding all device memory, a path where
+ * cudaFree's device-wide wait is not acceptable). */
+int autan_exact_rms_static(const double* values, int64_t n, int64_t stride, int32_t components,
+                           double* rms, void* stream, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
