@@ -123,11 +123,49 @@ __device__ __forceinline__ int index_of(double x) {
   return static_cast<int>(__double_as_longlong(x));
 }
 
-// 16-byte vector loads of a record's words [w, w + count), count a multiple of the vector width.
+// Interior face records start on 32-byte boundaries in FP64 (96 bytes) but not in fp32 (48).
 template <class P>
+constexpr bool kFaceA32 = (kFace * sizeof(typename P::C)) % 32 == 0;
+
+// 32-byte vector loads and stores (the 256-bit ld / st of sm_100): one L1 wavefront per lane
+// where two 16-byte vectors take two. The address must be 32-byte aligned.
+__device__ __forceinline__ void ld32(const float* p, float* o) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]), "=f"(o[6]),
+        "=f"(o[7])
+      : "l"(p));
+}
+__device__ __forceinline__ void ld32(const double* p, double* o) {
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3])
+      : "l"(p));
+}
+__device__ __forceinline__ void st32(float* p, const float* v) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]), "f"(v[1]),
+               "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void st32(double* p, const double* v) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]),
+               "d"(v[3])
+               : "memory");
+}
+
+// Vector loads of a record's words [w, w + count), count a multiple of the 16-byte vector width:
+// with A32 (base + w 32-byte aligned) 32-byte vectors first, then 16-byte ones.
+template <class P, bool A32 = false>
 __device__ __forceinline__ void load_words(const typename P::C* base, int w, int count,
                                            typename P::C* out) {
   using V = typename P::V;
+  constexpr int kW32 = 32 / static_cast<int>(sizeof(typename P::C));
+  if constexpr (A32) {
+#pragma unroll
+    for (int q = 0; q < count / kW32; ++q) ld32(base + w + kW32 * q, out + kW32 * q);
+    const int done = (count / kW32) * kW32;
+    base += done;
+    out += done;
+    count -= done;
+  }
   const V* v = reinterpret_cast<const V*>(base + w);
 #pragma unroll
   for (int q = 0; q < count / P::kVec; ++q) {
@@ -144,10 +182,19 @@ __device__ __forceinline__ void load_words(const typename P::C* base, int w, int
   }
 }
 
-template <class P>
+template <class P, bool A32 = false>
 __device__ __forceinline__ void store_words(typename P::C* base, int w, int count,
                                             const typename P::C* in) {
   using V = typename P::V;
+  constexpr int kW32 = 32 / static_cast<int>(sizeof(typename P::C));
+  if constexpr (A32) {
+#pragma unroll
+    for (int q = 0; q < count / kW32; ++q) st32(base + w + kW32 * q, in + kW32 * q);
+    const int done = (count / kW32) * kW32;
+    base += done;
+    in += done;
+    count -= done;
+  }
   V* v = reinterpret_cast<V*>(base + w);
 #pragma unroll
   for (int q = 0; q < count / P::kVec; ++q) {
@@ -169,7 +216,7 @@ __device__ __forceinline__ void store_words(typename P::C* base, int w, int coun
 template <class P>
 __device__ __forceinline__ void load_prim(const typename P::C* rec, int c, typename P::C* w) {
   typename P::C t[8];
-  load_words<P>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+  load_words<P, true>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
 #pragma unroll
   for (int k = 0; k < 5; ++k) w[k] = t[k];
 }
@@ -180,8 +227,8 @@ __device__ __forceinline__ void load_recon(const typename P::C* rec, int c, type
                                            typename P::C* phi, typename P::C* g) {
   typename P::C t[28];
   const typename P::C* base = rec + static_cast<long long>(c) * kRec;
-  load_words<P>(base, 0, 8, t);
-  load_words<P>(base, 8, 20, t + 8);
+  load_words<P, true>(base, 0, 8, t);
+  load_words<P, true>(base, 8, 20, t + 8);
 #pragma unroll
   for (int k = 0; k < 5; ++k) w[k] = t[k];
 #pragma unroll
@@ -195,7 +242,7 @@ template <class P>
 __device__ __forceinline__ void store_prim(typename P::C* rec, int c, const typename P::C* w) {
   using C = typename P::C;
   const C t[8] = {w[0], w[1], w[2], w[3], w[4], C(0), C(0), C(0)};
-  store_words<P>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+  store_words<P, true>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
 }
 
 // Euler<P>::state then to_primitive: W of the stored state S(u - U_ref) (euler.cpp:925-932,
@@ -231,11 +278,11 @@ __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   C r[kBface], w[5], out[8];
-  load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
+  load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
   load_prim<P>(d.rec, index_of(r[13]), w);
   boundary_value(w, r[7], r + 8, r, d.p, out);
   out[5] = out[6] = out[7] = C(0);
-  store_words<P>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
+  store_words<P, true>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
 }
 
 // The minimum over a block of positive doubles' bits, then one atomicMin. Every thread of the
@@ -273,14 +320,14 @@ __device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const t
     C wn[5], rec[kFace];
     if (code >= 0) {
       const int f = code >> 1;
-      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, rec);
+      load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, rec);
       const int o = (code & 1) ? index_of(rec[7]) : index_of(rec[11]);
       load_prim<P>(d.rec, o, wn);
     } else {
       const int b = -code - 1;
       load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, 4, rec);
       C t[8];
-      load_words<P>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, t);
+      load_words<P, true>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, t);
 #pragma unroll
       for (int k = 0; k < 5; ++k) wn[k] = t[k];
     }
@@ -290,27 +337,22 @@ __device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const t
   return cfl * d.volume[c] / lam;
 }
 
-// The primitives of a cell (words 0-4) or of a boundary face's state, five values only.
+// The primitives of a cell (words 0-4), of a boundary face's state or of a face's flux, five
+// values only; src is 32-byte aligned (record, prim_b and flux strides are multiples of 32 bytes).
 template <class P>
 __device__ __forceinline__ void load5(const typename P::C* src, typename P::C* w) {
-  using C = typename P::C;
   if constexpr (P::kVec == 4) {
-    const float4 a = __ldg(reinterpret_cast<const float4*>(src));
-    w[0] = a.x;
-    w[1] = a.y;
-    w[2] = a.z;
-    w[3] = a.w;
-    w[4] = __ldg(src + 4);
+    float t[8];
+    ld32(src, t);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) w[k] = t[k];
   } else {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(src));
-    const double2 b = __ldg(reinterpret_cast<const double2*>(src) + 1);
-    w[0] = a.x;
-    w[1] = a.y;
-    w[2] = b.x;
-    w[3] = b.y;
+    double t[4];
+    ld32(src, t);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) w[k] = t[k];
     w[4] = __ldg(src + 4);
   }
-  (void)sizeof(C);
 }
 
 // gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the LSQ
@@ -343,7 +385,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
 #pragma unroll
       for (int q = 0; q < CHUNK; ++q)
         if (j0 + q < len)
-          load_words<P>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice), 0, 4, e4[q]);
+          load_words<P, sizeof(C) == 8>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice), 0, 4, e4[q]);
 #pragma unroll
       for (int q = 0; q < CHUNK; ++q) {
         if (j0 + q < len) {
@@ -411,7 +453,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = C(1.0);
     }
-    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+    store_words<P, true>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
     if constexpr (DT) {
       dt = cell_time_step(d, c, wc, cfl);
       if (local) d.dt_local[c] = dt;
@@ -581,7 +623,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = C(1.0);
     }
-    store_words<P>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+    store_words<P, true>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
     if constexpr (DT) {
       // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89).
       double lam = 0.0;
@@ -589,7 +631,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
         const int code = index_of(irow[4 * kSlice * j + 3]);
         C wn[5], fr[kFace];
         if (code >= 0) {
-          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
+          load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
           load5<P>(d.rec + static_cast<long long>((code & 1) ? index_of(fr[7]) : index_of(fr[11])) * kRec,
                    wn);
         } else {
@@ -825,7 +867,7 @@ __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stag
       const int f = code >> 1;
       const bool left = (code & 1) == 0;
       C fr[kFace], wo[5], go[15], po[5];
-      load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
+      load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
       cell_recon<P, SECOND>(d, left ? index_of(fr[11]) : index_of(fr[7]), wo, po, go);
       if (left) {
         interior_flux<P, FLUX, PLANAR>(d, f, fr, wc, gc, pc, wo, go, po, out);
@@ -839,7 +881,7 @@ __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stag
     } else {
       const int b = -code - 1;
       C br[kBface];
-      load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+      load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
       boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
 #pragma unroll
       for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
@@ -858,12 +900,12 @@ __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.n_if) return;
   C fr[kFace], wl[5], gl[15], pl[5], wr[5], gr[15], pr[5], out[8];
-  load_words<P>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
+  load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
   cell_recon<P, SECOND>(d, index_of(fr[7]), wl, pl, gl);
   cell_recon<P, SECOND>(d, index_of(fr[11]), wr, pr, gr);
   interior_flux<P, FLUX, PLANAR>(d, f, fr, wl, gl, pl, wr, gr, pr, out);
   out[5] = out[6] = out[7] = C(0);
-  store_words<P>(flux + static_cast<long long>(f) * kFlux, 0, kFlux, out);
+  store_words<P, true>(flux + static_cast<long long>(f) * kFlux, 0, kFlux, out);
 }
 
 // ... and of every boundary face of an owned cell (the first n_owned_faces - n_interior_faces).
@@ -873,11 +915,11 @@ __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flu
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbo) return;
   C br[kBface], wc[5], gc[15], pc[5], out[8];
-  load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+  load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
   cell_recon<P, SECOND>(d, index_of(br[13]), wc, pc, gc);
   boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
   out[5] = out[6] = out[7] = C(0);
-  store_words<P>(flux + static_cast<long long>(b) * kFlux, 0, kFlux, out);
+  store_words<P, true>(flux + static_cast<long long>(b) * kFlux, 0, kFlux, out);
 }
 
 // Store-gather, second half: each owned cell adds its faces' fluxes in increasing face index
