@@ -62,9 +62,9 @@ struct Fp32Acc64 {
 constexpr int kSlice = 32;
 constexpr int kHistory = 4096;
 constexpr int kBlock = 256;
-constexpr int kRec = 32;    // record width, elements
-constexpr int kPhi = 8;     // phi at words 8-12
-constexpr int kGrad = 13;   // grad at words 13-27
+constexpr int kPrimW = 8;   // primitive record width: rho, u, v, w, p, then padding
+constexpr int kGroup = 8;   // words per cell in each group of the reconstruction array
+constexpr int kRecon = 24;  // reconstruction words per cell: phi 0-4, grad 5-19, padding 20-23
 constexpr int kFace = 12;   // interior face record width
 constexpr int kBface = 16;  // boundary face record width
 constexpr int kPrimB = 8;   // boundary state record width
@@ -93,8 +93,10 @@ struct Dev {
   int n_if;  // owned interior faces
   Params<C> p;
   double ref[5];
-  const C* rec;    // records read this stage
-  C* rec_next;     // records whose primitives this stage writes
+  const C* prim;      // kPrimW x n: the primitives this stage reads
+  C* prim_next;       // the primitives this stage writes
+  C* recon;           // phi and grad of this stage: kRecon / kGroup groups of kGroup x n words
+  long long rstride;  // words from one group to the next (kGroup x n)
   C* prim_b;       // kPrimB x nb
   double* u;
   double* stage;
@@ -212,37 +214,50 @@ __device__ __forceinline__ void store_words(typename P::C* base, int w, int coun
   }
 }
 
-// The primitives of cell c (words 0-4 of its record).
+// The primitives of cell c (words 0-4 of its primitive record).
 template <class P>
-__device__ __forceinline__ void load_prim(const typename P::C* rec, int c, typename P::C* w) {
+__device__ __forceinline__ void load_prim(const typename P::C* prim, int c, typename P::C* w) {
   typename P::C t[8];
-  load_words<P, true>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+  load_words<P, true>(prim + static_cast<long long>(c) * kPrimW, 0, 8, t);
 #pragma unroll
   for (int k = 0; k < 5; ++k) w[k] = t[k];
 }
 
-// Primitives, limiter and gradient of cell c.
+// Primitives, limiter and gradient of cell c: its primitive record and its word group of each of
+// the reconstruction array's groups (cell-contiguous within a group, so that the records of
+// consecutive cells share cache lines).
 template <class P>
-__device__ __forceinline__ void load_recon(const typename P::C* rec, int c, typename P::C* w,
+__device__ __forceinline__ void load_recon(const Dev<P>& d, int c, typename P::C* w,
                                            typename P::C* phi, typename P::C* g) {
-  typename P::C t[28];
-  const typename P::C* base = rec + static_cast<long long>(c) * kRec;
-  load_words<P, true>(base, 0, 8, t);
-  load_words<P, true>(base, 8, 20, t + 8);
+  typename P::C t[kRecon], q[8];
+  load_words<P, true>(d.prim + static_cast<long long>(c) * kPrimW, 0, 8, q);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) w[k] = t[k];
+  for (int k = 0; k < kRecon / kGroup; ++k)
+    load_words<P, true>(d.recon + k * d.rstride + static_cast<long long>(c) * kGroup, 0, kGroup,
+                        t + kGroup * k);
 #pragma unroll
-  for (int k = 0; k < 5; ++k) phi[k] = t[kPhi + k];
+  for (int k = 0; k < 5; ++k) w[k] = q[k];
 #pragma unroll
-  for (int k = 0; k < 15; ++k) g[k] = t[kGrad + k];
+  for (int k = 0; k < 5; ++k) phi[k] = t[k];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) g[k] = t[5 + k];
+}
+
+// Writes phi (out[0-4]) and grad (out[5-19]) of cell c; out[20-23] are the padding.
+template <class P>
+__device__ __forceinline__ void store_recon(const Dev<P>& d, int c, const typename P::C* out) {
+#pragma unroll
+  for (int k = 0; k < kRecon / kGroup; ++k)
+    store_words<P, true>(d.recon + k * d.rstride + static_cast<long long>(c) * kGroup, 0, kGroup,
+                         out + kGroup * k);
 }
 
 // Writes the primitives of cell c (words 0-7, the padding 5-7 zero).
 template <class P>
-__device__ __forceinline__ void store_prim(typename P::C* rec, int c, const typename P::C* w) {
+__device__ __forceinline__ void store_prim(typename P::C* prim, int c, const typename P::C* w) {
   using C = typename P::C;
   const C t[8] = {w[0], w[1], w[2], w[3], w[4], C(0), C(0), C(0)};
-  store_words<P, true>(rec + static_cast<long long>(c) * kRec, 0, 8, t);
+  store_words<P, true>(prim + static_cast<long long>(c) * kPrimW, 0, 8, t);
 }
 
 // Euler<P>::state then to_primitive: W of the stored state S(u - U_ref) (euler.cpp:925-932,
@@ -279,7 +294,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   if (b >= d.nb) return;
   C r[kBface], w[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
-  load_prim<P>(d.rec, index_of(r[13]), w);
+  load_prim<P>(d.prim, index_of(r[13]), w);
   boundary_value(w, r[7], r + 8, r, d.p, out);
   out[5] = out[6] = out[7] = C(0);
   store_words<P, true>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
@@ -322,7 +337,7 @@ __device__ __forceinline__ double cell_time_step(const Dev<P>& d, int c, const t
       const int f = code >> 1;
       load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, rec);
       const int o = (code & 1) ? index_of(rec[7]) : index_of(rec[11]);
-      load_prim<P>(d.rec, o, wn);
+      load_prim<P>(d.prim, o, wn);
     } else {
       const int b = -code - 1;
       load_words<P>(d.bface + static_cast<long long>(b) * kBface, 0, 4, rec);
@@ -368,7 +383,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
   double dt = 0.0;
   if (live) {
     C wc[5];
-    load5<P>(d.rec + static_cast<long long>(c) * kRec, wc);
+    load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
     double acc[15];
 #pragma unroll
     for (int k = 0; k < 15; ++k) acc[k] = 0.0;
@@ -390,7 +405,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
       for (int q = 0; q < CHUNK; ++q) {
         if (j0 + q < len) {
           const int e = index_of(e4[q][3]);
-          load5<P>(e >= 0 ? d.rec + static_cast<long long>(e) * kRec
+          load5<P>(e >= 0 ? d.prim + static_cast<long long>(e) * kPrimW
                           : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
                    wn[q]);
         }
@@ -413,8 +428,8 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
         }
       }
     }
-    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
-    C out[20];
+    // include_own_value (:517-521); out: phi, then grad, then padding.
+    C out[kRecon];
 #pragma unroll
     for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
     const C* g = out + 5;
@@ -453,7 +468,9 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = C(1.0);
     }
-    store_words<P, true>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+#pragma unroll
+    for (int k = 20; k < kRecon; ++k) out[k] = C(0);
+    store_recon<P>(d, c, out);
     if constexpr (DT) {
       dt = cell_time_step(d, c, wc, cfl);
       if (local) d.dt_local[c] = dt;
@@ -546,7 +563,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
   double dt = 0.0;
   if (live) {
     C wc[5];
-    load5<P>(d.rec + static_cast<long long>(c) * kRec, wc);
+    load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
     double acc[15];
 #pragma unroll
     for (int k = 0; k < 15; ++k) acc[k] = 0.0;
@@ -565,7 +582,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
       for (int q = 0; q < kChunk; ++q) {
         if (j0 + q < len) {
           const int e = index_of(row[4 * kSlice * (j0 + q) + 3]);
-          load5<P>(e >= 0 ? d.rec + static_cast<long long>(e) * kRec
+          load5<P>(e >= 0 ? d.prim + static_cast<long long>(e) * kPrimW
                           : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
                    wn[q]);
         }
@@ -589,8 +606,8 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
         }
       }
     }
-    // include_own_value (:517-521); words 8-27 of the record: phi, then grad.
-    C out[20];
+    // include_own_value (:517-521); out: phi, then grad, then padding.
+    C out[kRecon];
 #pragma unroll
     for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
     const C* g = out + 5;
@@ -623,7 +640,9 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = C(1.0);
     }
-    store_words<P, true>(const_cast<C*>(d.rec) + static_cast<long long>(c) * kRec, 8, 20, out);
+#pragma unroll
+    for (int k = 20; k < kRecon; ++k) out[k] = C(0);
+    store_recon<P>(d, c, out);
     if constexpr (DT) {
       // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89).
       double lam = 0.0;
@@ -632,7 +651,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
         C wn[5], fr[kFace];
         if (code >= 0) {
           load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
-          load5<P>(d.rec + static_cast<long long>((code & 1) ? index_of(fr[7]) : index_of(fr[11])) * kRec,
+          load5<P>(d.prim + static_cast<long long>((code & 1) ? index_of(fr[7]) : index_of(fr[11])) * kPrimW,
                    wn);
         } else {
           load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 0, 4, fr);
@@ -657,7 +676,7 @@ __global__ void __launch_bounds__(256) k_spectral(Dev<P> d, double cfl, int loca
   double dt = 0.0;
   if (live) {
     C wc[5];
-    load_prim<P>(d.rec, c, wc);
+    load_prim<P>(d.prim, c, wc);
     dt = cell_time_step(d, c, wc, cfl);
     if (local && d.dt_local != nullptr) d.dt_local[c] = dt;
     if (dt_out != nullptr) dt_out[c] = dt;
@@ -674,9 +693,9 @@ __device__ __forceinline__ void cell_recon(const Dev<P>& d, int c, typename P::C
                                            typename P::C* phi, typename P::C* g) {
   using C = typename P::C;
   if constexpr (SECOND) {
-    load_recon<P>(d.rec, c, w, phi, g);
+    load_recon<P>(d, c, w, phi, g);
   } else {
-    load5<P>(d.rec + static_cast<long long>(c) * kRec, w);
+    load5<P>(d.prim + static_cast<long long>(c) * kPrimW, w);
 #pragma unroll
     for (int k = 0; k < 15; ++k) g[k] = C(0.0);
 #pragma unroll
@@ -810,7 +829,7 @@ __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double
   }
   C w[5], dq[5];
   prim_of_state(d, nu, w, dq);
-  store_prim<P>(d.rec_next, c, w);
+  store_prim<P>(d.prim_next, c, w);
   if (last) {
     // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
     // it, in the compute type, then this stage's residual.
@@ -1031,14 +1050,17 @@ __global__ void k_end_step(Control* ctl) {
   if (threadIdx.x == 0) ctl->step += 1;
 }
 
-// Gradients and limiter of the records, as FP64 SoA (15 x n, 5 x n).
+// Gradients and limiter of the reconstruction array, as FP64 SoA (15 x n, 5 x n).
 template <class P>
-__global__ void k_unpack(const typename P::C* rec, int n, double* grad, double* phi) {
+__global__ void k_unpack(const typename P::C* recon, int n, double* grad, double* phi) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  const typename P::C* r = rec + static_cast<long long>(c) * kRec;
-  for (int k = 0; k < 15; ++k) grad[static_cast<long long>(k) * n + c] = static_cast<double>(r[kGrad + k]);
-  for (int k = 0; k < 5; ++k) phi[static_cast<long long>(k) * n + c] = static_cast<double>(r[kPhi + k]);
+  auto word = [&](int w) {
+    return static_cast<double>(recon[(w / kGroup) * static_cast<long long>(kGroup) * n +
+                                     static_cast<long long>(c) * kGroup + w % kGroup]);
+  };
+  for (int k = 0; k < 15; ++k) grad[static_cast<long long>(k) * n + c] = word(5 + k);
+  for (int k = 0; k < 5; ++k) phi[static_cast<long long>(k) * n + c] = word(k);
 }
 
 // ---------------------------------------------------------------- host side
@@ -1369,7 +1391,8 @@ class Impl final : public Stepper {
     nbo_ = m.n_owned_faces - m.n_interior_faces;
     // Device arrays.
     const size_t n5 = 5ULL * n_;
-    for (auto& b : rec_) b.alloc(static_cast<size_t>(kRec) * n_ * sizeof(C));
+    for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * n_ * sizeof(C));
+    recon_.alloc(static_cast<size_t>(kRecon) * n_ * sizeof(C));
     prim_b_.alloc(static_cast<size_t>(kPrimB) * std::max(nb_, 1) * sizeof(C));
     u_.alloc(n5 * sizeof(double));
     stage_.alloc(n5 * sizeof(double));
@@ -1391,11 +1414,14 @@ class Impl final : public Stepper {
     b_m_ = upload(bm, stream);
     for (Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
       check(cudaMemsetAsync(b->ptr(), 0, b->bytes(), stream), "memset");
-    for (auto& b : rec_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
+    for (auto& b : prim_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
+    check(cudaMemsetAsync(recon_.ptr(), 0, recon_.bytes(), stream), "memset");
     d_.n = n_;
     d_.nb = nb_;
     d_.n_if = nif_;
     d_.prim_b = prim_b_.as<C>();
+    d_.recon = recon_.as<C>();
+    d_.rstride = static_cast<long long>(kGroup) * n_;
     d_.u = u_.as<double>();
     d_.stage = stage_.as<double>();
     d_.racc = racc_.as<double>();
@@ -1433,7 +1459,8 @@ class Impl final : public Stepper {
                             &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_,
                             &inc_rec_})
       t += static_cast<long long>(b->bytes());
-    for (const auto& b : rec_) t += static_cast<long long>(b.bytes());
+    for (const auto& b : prim_) t += static_cast<long long>(b.bytes());
+    t += static_cast<long long>(recon_.bytes());
     return t;
   }
 
@@ -1504,7 +1531,7 @@ class Impl final : public Stepper {
   void upload_state(const double* u) override {
     copy_in(u, u_.as<double>());
     launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
-           rec_[0].as<C>());
+           prim_[0].as<C>());
     check(cudaStreamSynchronize(stream), "upload");
   }
 
@@ -1513,7 +1540,7 @@ class Impl final : public Stepper {
   void residual(const double* u, double* res) override {
     copy_in(u, stage_.as<double>());
     launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(stage_.as<double>()),
-           rec_[1].as<C>());
+           prim_[1].as<C>());
     enqueue_residual(1);
     copy_out(res_.as<double>(), res);
     for (int k = 0; k < 5; ++k)
@@ -1584,7 +1611,7 @@ class Impl final : public Stepper {
 
   void gradients(double* grad, double* phi) override {
     Buffer g(15ULL * n_ * sizeof(double)), f(5ULL * n_ * sizeof(double));
-    launch(k_unpack<P>, blocks(n_), kBlock, static_cast<const C*>(rec_[last_rec_].as<C>()), n_,
+    launch(k_unpack<P>, blocks(n_), kBlock, static_cast<const C*>(recon_.as<C>()), n_,
            g.as<double>(), f.as<double>());
     if (grad != nullptr)
       check(cudaMemcpyAsync(grad, g.ptr(), 15ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "grad");
@@ -1655,7 +1682,7 @@ class Impl final : public Stepper {
       check(cudaMemcpyAsync(u_.ptr(), saved.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),
             "restore state");
       launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
-             rec_[0].as<C>());
+             prim_[0].as<C>());
       check(cudaStreamSynchronize(stream), "restore state");
     };
     ensure_flux_scratch();
@@ -1809,8 +1836,8 @@ class Impl final : public Stepper {
 
   Dev<P> with_rec(int in, int out) const {
     Dev<P> d = d_;
-    d.rec = rec_[in].as<C>();
-    d.rec_next = rec_[out].as<C>();
+    d.prim = prim_[in].as<C>();
+    d.prim_next = prim_[out].as<C>();
     return d;
   }
 
@@ -1999,7 +2026,8 @@ class Impl final : public Stepper {
   int nc_ = 0, n_ = 0, nf_ = 0, ni_ = 0, nif_ = 0, nb_ = 0;
   Sliced st_, inc_;
   Dev<P> d_{};
-  Buffer rec_[3];
+  Buffer prim_[3];  // primitive records, rotated through the stages
+  Buffer recon_;    // phi and grad of the current stage
   Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_;
   Buffer face_, f_m_, bface_, b_m_, source_;
