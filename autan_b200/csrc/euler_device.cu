@@ -111,7 +111,9 @@ struct Dev {
   const int* inc_start;
   const int* inc_len;
   const int* inc_code;
-  const C* inc_rec;  // 4 per incidence, sliced: rel(x_f, x_c) of the cell's side, code
+  const C* inc_rec;  // 4 per incidence, sliced: rel(x_f, x_c) of the cell's side, the other side
+                     // (its cell's value index, or -(b + 1) for boundary face b)
+  const C* inc_dt;   // 4 per incidence, sliced: the face's unit normal and area
   int n_slices;
   const C* face;    // kFace per owned interior face
   const C* bface;   // kBface per boundary face
@@ -536,7 +538,7 @@ __device__ __forceinline__ bool bounded_wait(unsigned long long* bar, Control* c
 // stencil rows and per-incidence limiter records staged into shared memory by one TMA bulk copy
 // each (the slices' rows are contiguous in the sliced layout): the block's whole streaming input
 // is in flight at once, and the threads then only gather their neighbours' primitives (L2).
-template <class P, bool LIMIT, bool DT>
+template <class P, bool LIMIT, bool DT, int CHUNK>
 __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -548,14 +550,17 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
   const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s1);
   C* ent = reinterpret_cast<C*>(smem_raw);
   C* inc = ent + 4 * (e1 - e0);
+  C* ndt = inc + 4 * (i1 - i0);
   const unsigned eb = static_cast<unsigned>((e1 - e0) * 4 * sizeof(C));
   const unsigned ib = (LIMIT || DT) ? static_cast<unsigned>((i1 - i0) * 4 * sizeof(C)) : 0u;
+  const unsigned db = DT ? static_cast<unsigned>((i1 - i0) * 4 * sizeof(C)) : 0u;
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
   if (threadIdx.x == 0) {
-    mbar_expect_tx(&bar, eb + ib);
+    mbar_expect_tx(&bar, eb + ib + db);
     if (eb > 0) bulk_to_shared(ent, d.st + 4 * e0, eb, &bar);
     if (ib > 0) bulk_to_shared(inc, d.inc_rec + 4 * i0, ib, &bar);
+    if (db > 0) bulk_to_shared(ndt, d.inc_dt + 4 * i0, db, &bar);
   }
   if (!bounded_wait(&bar, d.ctl)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -575,7 +580,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
     }
     const C* row = ent + 4 * (__ldg(d.st_start + (c >> 5)) - e0 + (c & 31));
     const int len = __ldg(d.st_len + c);
-    constexpr int kChunk = 4;
+    constexpr int kChunk = CHUNK;
     for (int j0 = 0; j0 < len; j0 += kChunk) {
       C wn[kChunk][5];
 #pragma unroll
@@ -645,19 +650,17 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
     store_recon<P>(d, c, out);
     if constexpr (DT) {
       // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89).
+      // Each incidence's other side from the limiter record, its normal and area staged.
+      const C* drow = ndt + (irow - inc);
       double lam = 0.0;
       for (int j = 0; j < il; ++j) {
-        const int code = index_of(irow[4 * kSlice * j + 3]);
-        C wn[5], fr[kFace];
-        if (code >= 0) {
-          load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(code >> 1) * kFace, 0, kFace, fr);
-          load5<P>(d.prim + static_cast<long long>((code & 1) ? index_of(fr[7]) : index_of(fr[11])) * kPrimW,
-                   wn);
-        } else {
-          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 0, 4, fr);
-          load5<P>(d.prim_b + static_cast<long long>(-code - 1) * kPrimB, wn);
-        }
-        lam += static_cast<double>(wave_speed(wc, wn, fr, fr[3], d.p.g, d.p.pref));
+        const int o = index_of(irow[4 * kSlice * j + 3]);
+        const C* nd = drow + 4 * kSlice * j;
+        C wn[5];
+        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
+                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
+                 wn);
+        lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
       }
       dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
@@ -776,25 +779,49 @@ __device__ __forceinline__ void boundary_flux(const Dev<P>& d, int b, const type
 
 // After a cell's residual: the residual output, the RK stage update of the FP64 state, the next
 // stage's primitives and, after the last stage, the validity checks.
+// The FP64 words of a cell that its update reads: u, the stage state (SSP-RK3) or the RK4
+// accumulator (stages > 0), and the step h. The kernels load them before their flux sums, so that
+// these loads are in flight together with the flux loads.
+struct CellIn {
+  double u[5], x[5], h;
+};
+
+template <class P>
+__device__ __forceinline__ void load_cell_in(const Dev<P>& d, int c, int mode, int stage, int local,
+                                             CellIn& in) {
+  if (mode == kResidual) return;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) in.u[k] = d.u[static_cast<long long>(k) * d.n + c];
+  if (stage > 0) {
+    const double* src = mode == kRk3 ? d.stage : d.racc;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) in.x[k] = src[static_cast<long long>(k) * d.n + c];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) in.x[k] = 0.0;
+  }
+  in.h = local ? d.dt_local[c] : d.ctl->dt;
+}
+
 template <class P>
 __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double* res,
                                             double vol, int mode, int stage, double wa, double wb,
-                                            int local, int last) {
+                                            int last, const CellIn& in) {
   using C = typename P::C;
   if (mode == kResidual || stage == 0) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
   }
   if (mode == kResidual) return;
-  const double h = local ? d.dt_local[c] : d.ctl->dt;
+  const double h = in.h;
   double nu[5];
   if (mode == kRk3) {
     // rk_stage (device_stepper.cuh:93-104): next = stage - (h / V) R; stage = a u + b next.
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       const long long i = static_cast<long long>(k) * d.n + c;
-      const double uk = d.u[i];
-      const double sk = stage == 0 ? uk : d.stage[i];
+      const double uk = in.u[k];
+      const double sk = stage == 0 ? uk : in.x[k];
       const double next = sk - h / vol * res[k];
       nu[k] = wa * uk + wb * next;
       if (last) {
@@ -809,14 +836,14 @@ __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       const long long i = static_cast<long long>(k) * d.n + c;
-      const double uk = d.u[i];
+      const double uk = in.u[k];
       double a;
       if (stage == 0) {
         a = res[k];
       } else if (stage < 3) {
-        a = d.racc[i] + 2.0 * res[k];
+        a = in.x[k] + 2.0 * res[k];
       } else {
-        a = d.racc[i] + res[k];
+        a = in.x[k] + res[k];
       }
       if (stage < 3) {
         d.racc[i] = a;
@@ -906,7 +933,9 @@ __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stag
       for (int k = 0; k < 5; ++k) res[k] += static_cast<double>(out[k]);
     }
   }
-  finish_cell(d, c, res, vol, mode, stage, wa, wb, local, last);
+  CellIn in;
+  load_cell_in(d, c, mode, stage, local, in);
+  finish_cell(d, c, res, vol, mode, stage, wa, wb, last, in);
 }
 
 constexpr int kFlux = 8;  // flux record width (5 used): one 32-byte sector in fp32+acc64
@@ -951,6 +980,8 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.n) return;
   const double vol = __ldg(d.volume + c);
+  CellIn in;
+  load_cell_in(d, c, mode, stage, local, in);
   double res[5];
   {
     const C nv = -static_cast<C>(vol);  // sources (:611-616): res = -V s
@@ -988,26 +1019,32 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
       }
     }
   }
-  finish_cell(d, c, res, vol, mode, stage, wa, wb, local, last);
+  finish_cell(d, c, res, vol, mode, stage, wa, wb, last, in);
 }
 
-// The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176).
+// The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176): each
+// warp adds into words of its own in shared memory, the block then sums its warps' words and adds
+// the non-zero ones to the global words.
 __global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, Control* ctl) {
-  __shared__ unsigned long long sh[5 * kWords];
-  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
+  constexpr int kWarps = kBlock / 32;
+  __shared__ unsigned long long sh[kWarps][5 * kWords];
+  for (int i = threadIdx.x; i < kWarps * 5 * kWords; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
+  unsigned long long* mine = sh[threadIdx.x >> 5];
   const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
   for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < n; base += stride) {
     const long long c = base + threadIdx.x;
+    double r[5];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
-      warp_exact_add(sh + k * kWords, r * r);
-    }
+    for (int k = 0; k < 5; ++k) r[k] = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) warp_exact_add_nonneg<true>(mine + k * kWords, r[k] * r[k]);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
-    const unsigned long long v = sh[i];
+    unsigned long long v = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) v += sh[w][i];
     if (v != 0) atomicAdd(&ctl->words[i / kWords][i % kWords], v);
   }
 }
@@ -1172,7 +1209,7 @@ struct Counters {
 // Launch choices of the hot kernels; every choice computes the same bits (the summation order of
 // each cell is fixed), so the autotuner picks by time alone.
 struct Tuning {
-  int grad_chunk = 4;    // stencil entries loaded together by the gradient kernel: 1, 2 or 4
+  int grad_chunk = 4;    // stencil entries loaded together by the gradient kernel: 1, 2, 4 (8 staged)
   int grad_block = 128;  // its threads per block
   int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather
   int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
@@ -1203,7 +1240,10 @@ struct Tuning {
 
 void Tuning::validate() const {
   auto block_ok = [](int b) { return b >= 32 && b <= 256 && b % 32 == 0; };
-  if (grad_chunk != 1 && grad_chunk != 2 && grad_chunk != 4) fail("E1101: grad_chunk is 1, 2 or 4");
+  if (grad_mode == 0 && grad_chunk != 1 && grad_chunk != 2 && grad_chunk != 4)
+    fail("E1101: grad_chunk is 1, 2 or 4");
+  if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
+    fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
   if (grad_mode != 0 && grad_mode != 1) fail("E1101: grad_mode is 0 or 1");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
@@ -1331,6 +1371,7 @@ class Impl final : public Stepper {
     inc_ = slice_rows(ioff);
     std::vector<int> code(std::max<long long>(inc_.total, 1), 0);
     std::vector<C> irec(4 * std::max<long long>(inc_.total, 1), C(0));
+    std::vector<C> idt(4 * std::max<long long>(inc_.total, 1), C(0));
     for (int c = 0; c < n_; ++c) {
       int prev = -1;
       for (long long k = ioff[c]; k < ioff[c + 1]; ++k) {
@@ -1358,7 +1399,11 @@ class Impl final : public Stepper {
         const C* rel = v >= 0 ? face.data() + static_cast<long long>(f) * kFace + ((v & 1) ? 8 : 4)
                               : bface_host_.data() + static_cast<long long>(f - ni_) * kBface + 4;
         for (int a = 0; a < 3; ++a) irec[4 * at + a] = rel[a];
-        irec[4 * at + 3] = index_bits<C>(v);
+        // The other side: the owner for the neighbour's incidence and the reverse, or the face.
+        const C* q = v >= 0 ? face.data() + static_cast<long long>(f) * kFace
+                            : bface_host_.data() + static_cast<long long>(f - ni_) * kBface;
+        irec[4 * at + 3] = v >= 0 ? ((v & 1) ? q[7] : q[11]) : index_bits<C>(v);
+        for (int a = 0; a < 4; ++a) idt[4 * at + a] = q[a];
       }
     }
     // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, value index or -(b + 1)}.
@@ -1408,6 +1453,7 @@ class Impl final : public Stepper {
     inc_len_ = upload(inc_.len, stream);
     inc_code_ = upload(code, stream);
     inc_rec_ = upload(irec, stream);
+    inc_dt_ = upload(idt, stream);
     face_ = upload(face, stream);
     f_m_ = upload(fm, stream);
     bface_ = upload(bface_host_, stream);
@@ -1436,6 +1482,7 @@ class Impl final : public Stepper {
     d_.inc_len = inc_len_.as<int>();
     d_.inc_code = inc_code_.as<int>();
     d_.inc_rec = inc_rec_.as<C>();
+    d_.inc_dt = inc_dt_.as<C>();
     d_.n_slices = slices();
     d_.face = face_.as<C>();
     d_.bface = bface_.as<C>();
@@ -1457,7 +1504,7 @@ class Impl final : public Stepper {
     for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
                             &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
                             &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_,
-                            &inc_rec_})
+                            &inc_rec_, &inc_dt_})
       t += static_cast<long long>(b->bytes());
     for (const auto& b : prim_) t += static_cast<long long>(b.bytes());
     t += static_cast<long long>(recon_.bytes());
@@ -1702,9 +1749,10 @@ class Impl final : public Stepper {
       double best_ms = 1e300;
       Tuning keep = best;
       for (int mode : {0, 1})
-      for (int chunk : {1, 2, 4})
+      for (int chunk : {1, 2, 4, 8})
         for (int block : {64, 128, 256}) {
-          if (mode == 1 && (chunk != 4 || block > 128)) continue;
+          if (mode == 0 && chunk == 8) continue;
+          if (mode == 1 && (chunk == 1 || block > 128)) continue;
           Tuning t = keep;
           t.grad_mode = mode;
           t.grad_chunk = chunk;
@@ -1781,17 +1829,19 @@ class Impl final : public Stepper {
   int slices() const { return std::max(1, (n_ + kSlice - 1) / kSlice); }
 
   // Shared memory of the staged gradient kernel at `block` threads: the largest of its blocks'
-  // stencil rows and incidence records.
-  size_t staged_smem(int block) {
+  // stencil rows and incidence records (twice the incidences when it also stages their normals
+  // and areas for the time step).
+  size_t staged_smem(int block, bool dt) {
     const int per = block / kSlice;
-    auto& cached = staged_smem_[per];
+    auto& cached = staged_smem_[dt ? 1 : 0][per];
     if (cached == 0) {
       long long most = 0;
       const int ns = slices();
+      const int rows = dt ? 2 : 1;
       for (int s0 = 0; s0 < ns; s0 += per) {
         const int s1 = std::min(s0 + per, ns);
-        most = std::max<long long>(
-            most, static_cast<long long>(st_.start[s1] - st_.start[s0]) + (inc_.start[s1] - inc_.start[s0]));
+        most = std::max<long long>(most, static_cast<long long>(st_.start[s1] - st_.start[s0]) +
+                                             rows * (inc_.start[s1] - inc_.start[s0]));
       }
       cached = static_cast<size_t>(most) * 4 * sizeof(C) + 16;
       if (cached > 220 * 1024) fail("E1101: stencil rows too long for the staged gradient kernel");
@@ -1910,8 +1960,13 @@ class Impl final : public Stepper {
       auto go = [&](auto lim, auto with_dt) {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
         if (tuning_.grad_mode == 1) {
-          launch_smem(kGradients, k_gradients_tma<P, L, D>, blocks(n_, bs), bs, staged_smem(bs),
-                      d, cfl, loc);
+          const int sm = static_cast<int>(staged_smem(bs, D));
+          if (tuning_.grad_chunk == 2)
+            launch_smem(kGradients, k_gradients_tma<P, L, D, 2>, blocks(n_, bs), bs, sm, d, cfl, loc);
+          else if (tuning_.grad_chunk == 8)
+            launch_smem(kGradients, k_gradients_tma<P, L, D, 8>, blocks(n_, bs), bs, sm, d, cfl, loc);
+          else
+            launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, blocks(n_, bs), bs, sm, d, cfl, loc);
           return;
         }
         if (tuning_.grad_chunk == 1)
@@ -2029,7 +2084,7 @@ class Impl final : public Stepper {
   Buffer prim_[3];  // primitive records, rotated through the stages
   Buffer recon_;    // phi and grad of the current stage
   Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
-  Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_;
+  Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
   Buffer face_, f_m_, bface_, b_m_, source_;
   std::vector<C> bface_host_;
   cudaGraph_t graph_ = nullptr;
@@ -2039,7 +2094,7 @@ class Impl final : public Stepper {
   int last_rec_ = 0;
   int nbo_ = 0;  // boundary faces of owned cells
   Tuning tuning_;
-  size_t staged_smem_[5] = {0, 0, 0, 0, 0};
+  size_t staged_smem_[2][5] = {};  // [time step staged][slices per block]
   Buffer flux_, bflux_;  // face scratch of the store-gather strategy
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {

@@ -68,6 +68,63 @@ __device__ __forceinline__ void warp_exact_add(unsigned long long* words, double
   }
 }
 
+// warp_exact_add for terms that are never negative (squares): +0, positive, +inf or NaN. The
+// shifted mantissa m << s (below 2^84) is cut into six 16-bit chunks; the lanes of one limb group
+// sum each chunk with one redux.sync (32 terms below 2^16 sum below 2^21, exactly), and the leader
+// adds chunk pairs to the group's three words: each addend is below 2^38, as in warp_exact_add.
+// PRIVATE: `words` belong to this warp alone, so the leader's adds need no atomics.
+template <bool PRIVATE = false>
+__device__ __forceinline__ void warp_exact_add_nonneg(unsigned long long* words, double t) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(t));
+  const int biased = static_cast<int>((bits >> 52) & 0x7ff);
+  const unsigned long long fraction = bits & ((1ULL << 52) - 1);
+  if (biased == 0x7ff) atomicAdd(&words[fraction != 0 ? kLimbs + 2 : kLimbs], 1ULL);
+  const bool has = biased != 0x7ff && !(biased == 0 && fraction == 0);
+  int limb = 0;
+  unsigned long long lo = 0, hi = 0;
+  if (has) {
+    const unsigned long long m = biased == 0 ? fraction : (fraction | (1ULL << 52));
+    const int e = biased == 0 ? -1074 : biased - 1075;
+    const int p = e + kOffset;
+    limb = p >> 5;
+    const int s = p & 31;
+    lo = m << s;
+    hi = s == 0 ? 0ULL : m >> (64 - s);
+  }
+  unsigned todo = __ballot_sync(full, has);
+  while (todo != 0) {
+    const int leader = __ffs(todo) - 1;
+    const int li = __shfl_sync(full, limb, leader);
+    const bool mine = has && limb == li;
+    const unsigned group = __ballot_sync(full, mine);
+    const unsigned long long a = mine ? lo : 0ULL, b = mine ? hi : 0ULL;
+    const unsigned s0 = __reduce_add_sync(full, static_cast<unsigned>(a & 0xffff));
+    const unsigned s1 = __reduce_add_sync(full, static_cast<unsigned>((a >> 16) & 0xffff));
+    const unsigned s2 = __reduce_add_sync(full, static_cast<unsigned>((a >> 32) & 0xffff));
+    const unsigned s3 = __reduce_add_sync(full, static_cast<unsigned>(a >> 48));
+    const unsigned s4 = __reduce_add_sync(full, static_cast<unsigned>(b & 0xffff));
+    const unsigned s5 = __reduce_add_sync(full, static_cast<unsigned>(b >> 16));
+    if (lane == leader) {
+      const unsigned long long w0 = static_cast<unsigned long long>(s0) + (static_cast<unsigned long long>(s1) << 16);
+      const unsigned long long w1 = static_cast<unsigned long long>(s2) + (static_cast<unsigned long long>(s3) << 16);
+      const unsigned long long w2 = static_cast<unsigned long long>(s4) + (static_cast<unsigned long long>(s5) << 16);
+      if constexpr (PRIVATE) {
+        words[li] += w0;
+        words[li + 1] += w1;
+        words[li + 2] += w2;
+      } else {
+        atomicAdd(&words[li], w0);
+        atomicAdd(&words[li + 1], w1);
+        atomicAdd(&words[li + 2], w2);
+      }
+    }
+    __syncwarp();
+    todo &= ~group;
+  }
+}
+
 // The rounded value of a word array (ExactSum::value, runtime/src/exact_sum.cpp:99-140).
 __device__ inline double exact_value(const unsigned long long* in) {
   long long w[kWords];

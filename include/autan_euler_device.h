@@ -163,7 +163,7 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
                                     int64_t n_steps, double* ms, int64_t* launches, char* err,
                                     size_t err_len);
 /* Launch choices of the hot kernels (6 values): [0] stencil entries the gradient kernel loads
- * together (1, 2 or 4), [1] its threads per block, [2] face strategy (0 gather-recompute: each
+ * together (1, 2 or 4; 2, 4 or 8 when staged), [1] its threads per block, [2] face strategy (0 gather-recompute: each
  * cell recomputes its faces' fluxes; 1 store-gather: each face's flux once into a face scratch,
  * then summed per cell), [3] threads per block of the face kernel, [4] of the store-gather sum,
  * [5] gradient staging (0: each thread loads its stencil rows; 1: each block's rows staged into
