@@ -170,14 +170,16 @@ def gpu_uuid(device: int) -> str:
 # ------------------------------------------------------------------ CPU (oracle) throughput
 
 
-def cpu_throughput(steps: int, warmup: int, threads: int) -> tuple[float, str, int]:
+def cpu_throughput(steps: int, warmup: int, threads: int,
+                   slab: tuple[int, int, int] = (240, 24, 6)) -> tuple[float, str, int]:  # fmt: skip
     """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
-    240 x 24 x 6 slab of the benchmark lattice (SSP-RK3, fp32+acc64); the rate of the whole host."""
+    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64); the rate of the
+    whole host."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle as O
     from autan_b200 import cases
 
-    case = cases.vortex_tets(240, 24, 6, steps=1, precision="fp32+acc64")
+    case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
     md = cases.oracle_mesh_dict(case)
     sch = case.scheme.as_dict()
     oracles = [O.Oracle(md, sch, case.bc_kind, case.bc_data) for _ in range(threads)]
@@ -201,7 +203,7 @@ def cpu_throughput(steps: int, warmup: int, threads: int) -> tuple[float, str, i
     elapsed = time.perf_counter() - t0
     cells = case.mesh.n_owned_cells
     rate = cells * threads * steps / elapsed
-    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a 240x24x6 slab "
+    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a {slab[0]}x{slab[1]}x{slab[2]} slab "
               f"({cells} cells) of the benchmark lattice, CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
     return rate, sample, threads
 
@@ -213,14 +215,40 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+# ------------------------------------------------------------------ ranks
+
+
+def reduce_max(x: float, dist=None, device: str = "cpu") -> float:
+    """The maximum of x over the ranks of the default process group (x itself without one)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, cells: int, steps: int, seconds: float) -> float:
+    """Cell-iterations per second of the whole job: every rank steps its own replica of `cells`
+    cells `steps` times, and the job takes the slowest rank's time."""
+    return world * cells * steps / seconds
+
+
+def parse_triple(text: str) -> tuple[int, int, int]:
+    a, b, c = (int(v) for v in text.split(","))
+    return a, b, c
+
+
 # ------------------------------------------------------------------ arms
 
 
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
-    threads = host_threads()
-    rate, sample, cores = cpu_throughput(args.steps, max(1, min(args.warmup, 1)), threads)
+    threads = args.cpu_threads or host_threads()
+    rate, sample, cores = cpu_throughput(args.steps, max(1, min(args.warmup, 1)), threads,
+                                         parse_triple(args.cpu_slab))  # fmt: skip
     line = {
         "impl": "reference",
         "metric": "cell-iterations/s",
@@ -304,11 +332,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     # -- device-timed steps, state resident in HBM
     launches0 = dev.counters()["launches"]
@@ -322,7 +346,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     barrier()
     launches = dev.counters()["launches"] - launches0
     ms = max_over_ranks(start.elapsed_time(end))
-    value = world * n * args.steps / (ms * 1e-3)
+    value = whole_job_rate(world, n, args.steps, ms * 1e-3)
     if r.invalid_cell is not None:
         raise RuntimeError(f"invalid state at cell {r.invalid_cell}")
 
@@ -338,7 +362,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dev.download(out=u_host)
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(t1 - t0)
-    e2e = world * n * e2e_steps / e2e_s
+    e2e = whole_job_rate(world, n, e2e_steps, e2e_s)
 
     # -- per-kernel times (CUDA events around every launch on the stepper's stream)
     kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, n_steps=3)
@@ -396,7 +420,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         dist.destroy_process_group()
     if rank == 0:
         if world == 1 and not args.no_cpu:
-            rate, sample, cores = cpu_throughput(2, 1, host_threads())
+            rate, sample, cores = cpu_throughput(2, 1, args.cpu_threads or host_threads(),
+                                                 parse_triple(args.cpu_slab))  # fmt: skip
             line["cpu_baseline"] = {"value": rate, "unit": "cell-iterations/s", "cores": cores,
                                     "kind": "port", "sample": sample}  # fmt: skip
         print(json.dumps(line), flush=True)
@@ -423,6 +448,10 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["tets", "hex"], default="tets")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-slab", default="240,24,6",
+                    help="lattice NX,NY,NZ each CPU thread steps for the CPU baseline")
+    ap.add_argument("--cpu-threads", type=int, default=0,
+                    help="threads of the CPU baseline (0: every core this process may use)")
     ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")
     ap.add_argument("--tuning", default="", help="launch choices instead of the autotuner: "
                     "grad_chunk,grad_block,face_mode,face_block,gather_block")
