@@ -7,9 +7,12 @@ by accident. Build it with `python -m autan_b200.build`.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libautan_b200.so"
+# The in-tree build, or another build of the same sources named by AUTAN_B200_LIB.
+LIB_PATH = Path(os.environ.get("AUTAN_B200_LIB") or
+                Path(__file__).resolve().parent / "_lib" / "libautan_b200.so")
 
 _lib: C.CDLL | None = None
 
@@ -132,6 +135,10 @@ def _bind(lib: C.CDLL) -> None:
            C.c_char_p, sz)  # fmt: skip
         fn("autan_euler_device_kernel_times", C.c_int, vp, f64, f64, i32, i32, i64, P(f64), P(i64),
            C.c_char_p, sz)  # fmt: skip
+        fn("autan_euler_device_face_parts", C.c_int, vp, P(f64), P(f64), P(f64), C.c_char_p, sz)
+        fn("autan_euler_device_boundary_pressure", C.c_int, vp, P(f64), P(f64), P(f64), C.c_char_p,
+           sz)  # fmt: skip
+        fn("autan_euler_device_conservation", C.c_int, vp, P(f64), P(i32), C.c_char_p, sz)
     if hasattr(lib, "autan_exact_rms_static"):
         fn("autan_exact_rms_static", C.c_int, vp, i64, i64, i32, vp, vp, C.c_char_p, sz)
 

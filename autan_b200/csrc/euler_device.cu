@@ -687,7 +687,8 @@ __global__ void __launch_bounds__(256) k_spectral(Dev<P> d, double cfl, int loca
   if (d.ctl != nullptr) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
-enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2 };
+// kFaceParts: the residual's face part alone (no sources, from zero), Euler<P>::face_parts.
+enum Mode : int { kResidual = 0, kRk3 = 1, kRk4 = 2, kFaceParts = 3 };
 
 // The reconstruction data of a cell: primitives, limiter and gradient (zero gradient and limiter
 // for the first-order scheme).
@@ -789,7 +790,7 @@ struct CellIn {
 template <class P>
 __device__ __forceinline__ void load_cell_in(const Dev<P>& d, int c, int mode, int stage, int local,
                                              CellIn& in) {
-  if (mode == kResidual) return;
+  if (mode == kResidual || mode == kFaceParts) return;
 #pragma unroll
   for (int k = 0; k < 5; ++k) in.u[k] = d.u[static_cast<long long>(k) * d.n + c];
   if (stage > 0) {
@@ -808,11 +809,12 @@ __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double
                                             double vol, int mode, int stage, double wa, double wb,
                                             int last, const CellIn& in) {
   using C = typename P::C;
-  if (mode == kResidual || stage == 0) {
+  const bool residual_only = mode == kResidual || mode == kFaceParts;
+  if (residual_only || stage == 0) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
   }
-  if (mode == kResidual) return;
+  if (residual_only) return;
   const double h = in.h;
   double nu[5];
   if (mode == kRk3) {
@@ -988,7 +990,7 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       const C s = d.source != nullptr ? __ldg(d.source + static_cast<long long>(k) * d.n + c) : C(0.0);
-      res[k] = static_cast<double>(nv * s);
+      res[k] = mode == kFaceParts ? 0.0 : static_cast<double>(nv * s);  // face_parts: from zero
     }
   }
   const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
@@ -1098,6 +1100,119 @@ __global__ void k_unpack(const typename P::C* recon, int n, double* grad, double
   };
   for (int k = 0; k < 15; ++k) grad[static_cast<long long>(k) * n + c] = word(5 + k);
   for (int k = 0; k < 5; ++k) phi[static_cast<long long>(k) * n + c] = word(k);
+}
+
+// The face scratch as FP64 face fluxes, 5 x nf (owned interior faces, then owned boundary faces
+// at ni + b): the write-only loops' face_flux (kernels/euler.py:1059-1085).
+template <class P>
+__global__ void k_unpack_flux(const typename P::C* flux, const typename P::C* bflux, int nif,
+                              int nbo, int ni, int nf, double* out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < nif) {
+    for (int k = 0; k < 5; ++k)
+      out[static_cast<long long>(k) * nf + i] = static_cast<double>(flux[i * kFlux + k]);
+  } else if (i < static_cast<long long>(nif) + nbo) {
+    const long long b = i - nif;
+    for (int k = 0; k < 5; ++k)
+      out[static_cast<long long>(k) * nf + ni + b] = static_cast<double>(bflux[b * kFlux + k]);
+  }
+}
+
+// Euler<P>::boundary_pressure (physics/src/euler.cpp:1182-1223) for every boundary face, in FP64
+// from the stored primitives, gradient and limiter of its owner: the face pressure
+// p_f = p_c + phi_p (grad p . (x_f - x_c)), p_c when rho_f or p_f is not positive, and the force
+// p_f S + phi_p M^T grad p. r64: the FP64 offsets x_f - x_c, 3 x nb; pref: p_ref in FP64.
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_boundary_pressure(Dev<P> d, const double* r64,
+                                                              int second, double pref, double* p,
+                                                              double* force) {
+  using C = typename P::C;
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const long long nb = d.nb;
+  const C* br = d.bface + static_cast<long long>(b) * kBface;
+  const int o = index_of(br[13]);
+  C w[5], phi[5], g[15];
+  if (second) {
+    load_recon<P>(d, o, w, phi, g);
+  } else {
+    // set_second_order(false) zeroes grad and phi (physics/src/euler.cpp:903-912).
+    load_prim<P>(d.prim, o, w);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) phi[k] = C(0);
+#pragma unroll
+    for (int k = 0; k < 15; ++k) g[k] = C(0);
+  }
+  double drho = 0.0, dp = 0.0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double r = r64[j * nb + b];
+    drho += static_cast<double>(g[j]) * r;
+    dp += static_cast<double>(g[12 + j]) * r;
+  }
+  const double rho_c = static_cast<double>(w[0]);
+  const double p_c = pref + static_cast<double>(w[4]);
+  const double rho_f = rho_c + static_cast<double>(phi[0]) * drho;
+  double p_f = p_c + static_cast<double>(phi[4]) * dp;
+  if (!(rho_f > 0.0 && p_f > 0.0)) p_f = p_c;
+  p[b] = p_f;
+  if (force == nullptr) return;
+  const double phi_p = static_cast<double>(phi[4]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double warp = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const C m = d.b_m != nullptr ? d.b_m[(3 * j + k) * nb + b] : C(0);
+      warp += static_cast<double>(m) * static_cast<double>(g[12 + j]);
+    }
+    const double area_k = static_cast<double>(br[k]) * static_cast<double>(br[3]);
+    force[k * nb + b] = p_f * area_k + phi_p * warp;
+  }
+}
+
+// The sums of EulerPhysics::check_conservation (physics/src/euler_physics.cpp:1747-1779) on one
+// rank, each exact: words of E_k (R^F and minus the boundary fluxes), D_k (|flux| per incidence of
+// an owned cell: `mult` incidences of each owned interior face, one of each owned boundary face),
+// boundary_k and faces_k, 20 x kWords in that order. res: the face parts of the owned cells.
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_conservation(Dev<P> d, const typename P::C* flux,
+                                                         const typename P::C* bflux,
+                                                         const unsigned char* mult, int nbo,
+                                                         unsigned long long* words) {
+  __shared__ unsigned long long sh[20 * kWords];
+  for (int i = threadIdx.x; i < 20 * kWords; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const long long total = max(max(static_cast<long long>(d.n), static_cast<long long>(d.n_if)),
+                              static_cast<long long>(nbo));
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < total;
+       base += stride) {
+    const long long i = base + threadIdx.x;
+    const int mu = i < d.n_if ? mult[i] : 0;
+    for (int k = 0; k < 5; ++k) {
+      const double r = i < d.n ? d.res[k * static_cast<long long>(d.n) + i] : 0.0;
+      const double fb = i < nbo ? static_cast<double>(bflux[i * kFlux + k]) : 0.0;
+      const double fi = i < d.n_if ? static_cast<double>(flux[i * kFlux + k]) : 0.0;
+      warp_exact_add(sh + k * kWords, r);
+      warp_exact_add(sh + k * kWords, -fb);
+      warp_exact_add(sh + (5 + k) * kWords, fabs(fb));
+      warp_exact_add(sh + (5 + k) * kWords, mu >= 1 ? fabs(fi) : 0.0);
+      warp_exact_add(sh + (5 + k) * kWords, mu >= 2 ? fabs(fi) : 0.0);
+      warp_exact_add(sh + (10 + k) * kWords, fb);
+      warp_exact_add(sh + (15 + k) * kWords, r);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 20 * kWords; i += blockDim.x) {
+    const unsigned long long v = sh[i];
+    if (v != 0) atomicAdd(&words[i], v);
+  }
+}
+
+__global__ void k_conservation_finish(const unsigned long long* words, double* out) {
+  const int q = threadIdx.x;
+  if (q < 20) out[q] = exact_value(words + q * kWords);
 }
 
 // ---------------------------------------------------------------- host side
@@ -1273,6 +1388,9 @@ class Stepper {
   virtual void set_tuning(const Tuning& t) = 0;
   virtual Tuning tuning() const = 0;
   virtual double autotune(double cfl, double dt, bool local, int rk, int trial_steps) = 0;
+  virtual void face_parts(const double* u, double* res_faces, double* face_flux) = 0;
+  virtual void boundary_pressure(const double* u, double* p, double* force) = 0;
+  virtual int conservation(double* sums) = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
@@ -1314,6 +1432,7 @@ class Impl final : public Stepper {
     p.g = static_cast<C>(sc.gamma);
     p.rgas = static_cast<C>(sc.gas_constant);
     p.pref = static_cast<C>(p_ref);
+    pref64_ = p_ref;
     p.minf = static_cast<C>(sc.mach_ref);
     for (int k = 0; k < 5; ++k) {
       p.ur[k] = static_cast<C>(r[k]);
@@ -1434,6 +1553,20 @@ class Impl final : public Stepper {
     }
     std::vector<double> vol(m.cell_volume, m.cell_volume + n_);
     nbo_ = m.n_owned_faces - m.n_interior_faces;
+    // Boundary pressure and conservation data: the FP64 offsets x_f - x_o of every boundary face
+    // (3 x nb), the owned cells of each owned interior face (1 or 2: an image counts as not
+    // owned) and the most faces of an owned cell.
+    std::vector<double> r64(3ULL * std::max(nb_, 1), 0.0);
+    for (int b = 0; b < nb_; ++b) {
+      const int f = ni_ + b, o = m.owner[f];
+      for (int a = 0; a < 3; ++a)
+        r64[a * static_cast<long long>(nb_) + b] = m.face_centroid[a * NF + f] - m.cell_centroid[a * NC + o];
+    }
+    std::vector<unsigned char> mult(std::max(nif_, 1), 0);
+    for (int f = 0; f < nif_; ++f)
+      mult[f] = static_cast<unsigned char>((m.owner[f] < n_ ? 1 : 0) + (m.neighbour[f] < n_ ? 1 : 0));
+    for (int c = 0; c < n_; ++c)
+      max_faces_ = std::max<int>(max_faces_, static_cast<int>(m.cell_face_offsets[c + 1] - m.cell_face_offsets[c]));
     // Device arrays.
     const size_t n5 = 5ULL * n_;
     for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * n_ * sizeof(C));
@@ -1453,6 +1586,9 @@ class Impl final : public Stepper {
     inc_len_ = upload(inc_.len, stream);
     inc_code_ = upload(code, stream);
     inc_rec_ = upload(irec, stream);
+    bface_r64_ = upload(r64, stream);
+    face_mult_ = upload(mult, stream);
+    cons_words_.alloc(20ULL * kWords * sizeof(unsigned long long));
     inc_dt_ = upload(idt, stream);
     face_ = upload(face, stream);
     f_m_ = upload(fm, stream);
@@ -1504,7 +1640,7 @@ class Impl final : public Stepper {
     for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
                             &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
                             &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_,
-                            &inc_rec_, &inc_dt_})
+                            &inc_rec_, &inc_dt_, &bface_r64_, &face_mult_, &cons_words_})
       t += static_cast<long long>(b->bytes());
     for (const auto& b : prim_) t += static_cast<long long>(b.bytes());
     t += static_cast<long long>(recon_.bytes());
@@ -1903,6 +2039,16 @@ class Impl final : public Stepper {
       });
       return;
     }
+    launch_flux(d);
+    C* fl = flux_.as<C>();
+    C* bfl = bflux_.as<C>();
+    const int gb = tuning_.gather_block;
+    launch_as(kFaces, k_gather<P>, blocks(n_, gb), gb, d, static_cast<const C*>(fl),
+              static_cast<const C*>(bfl), mode, stage, wa, wb, local, last);
+  }
+
+  // Every owned face's flux, once, into the face scratch (the store-gather strategy's first half).
+  void launch_flux(const Dev<P>& d) {
     if (flux_.bytes() == 0) fail("E1200: face scratch missing");
     C* fl = flux_.as<C>();
     C* bfl = bflux_.as<C>();
@@ -1913,9 +2059,82 @@ class Impl final : public Stepper {
       launch_as(kFaces, k_face_flux<P, F, PL, SE>, blocks(nif_, bs), bs, d, fl);
       if (nbo_ > 0) launch_as(kFaces, k_bface_flux<P, F, PL, SE>, blocks(nbo_, bs), bs, d, bfl, nbo_);
     });
-    const int gb = tuning_.gather_block;
-    launch_as(kFaces, k_gather<P>, blocks(n_, gb), gb, d, static_cast<const C*>(fl),
-              static_cast<const C*>(bfl), mode, stage, wa, wb, local, last);
+  }
+
+  // The primitives (in prim_[1]), boundary states, gradients and limiter of the host state u
+  // (5 x n_cells) or, with u == nullptr, of the device state.
+  void prepare(const double* u) {
+    const double* src = u_.as<double>();
+    if (u != nullptr) {
+      copy_in(u, stage_.as<double>());
+      src = stage_.as<double>();
+    }
+    launch(k_store<P>, blocks(n_), kBlock, d_, src, prim_[1].as<C>());
+    enqueue_cells(1, false, 0.0, false);
+  }
+
+  // After prepare: each owned face's flux into the face scratch and the face parts R^F of the
+  // owned cells into res_ (Euler<P>::face_parts, physics/src/euler.cpp:944-965).
+  void enqueue_face_parts() {
+    ensure_flux_scratch();
+    const Dev<P> d = with_rec(1, 1);
+    launch_flux(d);
+    launch(k_gather<P>, blocks(n_), kBlock, d, static_cast<const C*>(flux_.as<C>()),
+           static_cast<const C*>(bflux_.as<C>()), static_cast<int>(kFaceParts), 0, 0.0, 0.0, 0, 0);
+  }
+
+  void face_parts(const double* u, double* res_faces, double* face_flux) override {
+    prepare(u);
+    enqueue_face_parts();
+    if (res_faces != nullptr) {
+      copy_out(res_.as<double>(), res_faces);
+      for (int k = 0; k < 5; ++k)
+        for (int g = n_; g < nc_; ++g) res_faces[k * static_cast<long long>(nc_) + g] = 0.0;
+    }
+    if (face_flux != nullptr) {
+      Buffer out(5ULL * nf_ * sizeof(double));
+      check(cudaMemsetAsync(out.ptr(), 0, out.bytes(), stream), "face_flux");
+      launch(k_unpack_flux<P>, blocks(static_cast<long long>(nif_) + nbo_), kBlock,
+             static_cast<const C*>(flux_.as<C>()), static_cast<const C*>(bflux_.as<C>()), nif_, nbo_,
+             ni_, nf_, out.as<double>());
+      check(cudaMemcpyAsync(face_flux, out.ptr(), out.bytes(), cudaMemcpyDeviceToHost, stream),
+            "face_flux");
+    }
+    check(cudaStreamSynchronize(stream), "face_parts");
+  }
+
+  void boundary_pressure(const double* u, double* p, double* force) override {
+    prepare(u);
+    Buffer pb(std::max<size_t>(1, static_cast<size_t>(nb_)) * sizeof(double));
+    Buffer fb(force != nullptr ? 3ULL * std::max(nb_, 1) * sizeof(double) : 0);
+    launch(k_boundary_pressure<P>, blocks(nb_), kBlock, with_rec(1, 1),
+           static_cast<const double*>(bface_r64_.as<double>()), second_ ? 1 : 0, pref64_,
+           pb.as<double>(), force != nullptr ? fb.as<double>() : static_cast<double*>(nullptr));
+    if (p != nullptr && nb_ > 0)
+      check(cudaMemcpyAsync(p, pb.ptr(), nb_ * sizeof(double), cudaMemcpyDeviceToHost, stream), "p");
+    if (force != nullptr && nb_ > 0)
+      check(cudaMemcpyAsync(force, fb.ptr(), 3ULL * nb_ * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream), "force");
+    check(cudaStreamSynchronize(stream), "boundary_pressure");
+  }
+
+  int conservation(double* sums) override {
+    prepare(nullptr);
+    enqueue_face_parts();
+    check(cudaMemsetAsync(cons_words_.ptr(), 0, cons_words_.bytes(), stream), "conservation");
+    const long long total = std::max<long long>({n_, nif_, nbo_});
+    launch(k_conservation<P>, std::min(blocks(total), 148 * 4), kBlock, with_rec(1, 1),
+           static_cast<const C*>(flux_.as<C>()), static_cast<const C*>(bflux_.as<C>()),
+           static_cast<const unsigned char*>(face_mult_.as<unsigned char>()), nbo_,
+           cons_words_.as<unsigned long long>());
+    Buffer out(20 * sizeof(double));
+    launch(k_conservation_finish, 1, 32, static_cast<const unsigned long long*>(
+                                             cons_words_.as<unsigned long long>()),
+           out.as<double>());
+    check(cudaMemcpyAsync(sums, out.ptr(), 20 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+          "conservation");
+    check(cudaStreamSynchronize(stream), "conservation");
+    return max_faces_;
   }
 
   // Calls body(flux, planar, second) with the scheme's compile-time choices.
@@ -2085,6 +2304,9 @@ class Impl final : public Stepper {
   Buffer recon_;    // phi and grad of the current stage
   Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
+  Buffer bface_r64_, face_mult_, cons_words_;  // boundary pressure and conservation
+  double pref64_ = 0.0;
+  int max_faces_ = 0;
   Buffer face_, f_m_, bface_, b_m_, source_;
   std::vector<C> bface_host_;
   cudaGraph_t graph_ = nullptr;
@@ -2329,6 +2551,28 @@ int autan_euler_device_autotune(void* handle, double cfl, double dt, int32_t loc
     const double ms = h->autotune(cfl, dt, local != 0, rk, trial_steps);
     if (params != nullptr) h->tuning().to(params);
     if (ms_per_step != nullptr) *ms_per_step = ms;
+  });
+}
+
+int autan_euler_device_face_parts(void* handle, const double* u, double* res_faces,
+                                  double* face_flux, char* err, size_t err_len) {
+  AUTAN_CALL(h->face_parts(u, res_faces, face_flux));
+}
+
+int autan_euler_device_boundary_pressure(void* handle, const double* u, double* p, double* force,
+                                         char* err, size_t err_len) {
+  AUTAN_CALL({
+    if (p == nullptr) fail("E1101: null pressure output");
+    h->boundary_pressure(u, p, force);
+  });
+}
+
+int autan_euler_device_conservation(void* handle, double* sums, int32_t* max_faces, char* err,
+                                    size_t err_len) {
+  AUTAN_CALL({
+    if (sums == nullptr) fail("E1101: null output");
+    const int d = h->conservation(sums);
+    if (max_faces != nullptr) *max_faces = d;
   });
 }
 

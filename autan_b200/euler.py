@@ -133,6 +133,7 @@ class EulerDevice:
         get = (lambda k: mesh[k]) if isinstance(mesh, dict) else (lambda k: getattr(mesh, k))
         self.n_cells = int(get("n_cells"))
         self.n_owned_cells = int(get("n_owned_cells"))
+        self.n_faces = int(get("n_faces"))
         self.n_boundary = int(get("n_faces")) - int(get("n_interior_faces"))
         self.scheme = scheme
         if bc_kind is None:
@@ -206,6 +207,38 @@ class EulerDevice:
         out = N.StepResult()
         self._call("autan_euler_device_evaluate", C.byref(out))
         return _result(out)
+
+    def face_parts(self, u=None) -> tuple[np.ndarray, np.ndarray]:
+        """Euler<P>::face_parts of the host state u (or of the device state): the residual's face
+        part (5 x n_cells) and every owned face's flux (5 x n_faces)."""
+        rf = np.zeros((5, self.n_cells))
+        ff = np.zeros((5, self.n_faces))
+        self._call("autan_euler_device_face_parts", self._state_ptr(u), N.ptr(rf, C.c_double),
+                   N.ptr(ff, C.c_double))  # fmt: skip
+        return rf, ff
+
+    def boundary_pressure(self, u=None) -> tuple[np.ndarray, np.ndarray]:
+        """Euler<P>::boundary_pressure after evaluating u (or the device state): the face pressure
+        of every boundary face and its force p_f S + phi_p M^T grad p (3 x n_boundary)."""
+        p = np.zeros(self.n_boundary)
+        force = np.zeros((3, self.n_boundary))
+        self._call("autan_euler_device_boundary_pressure", self._state_ptr(u),
+                   N.ptr(p, C.c_double), N.ptr(force, C.c_double))  # fmt: skip
+        return p, force
+
+    def conservation(self) -> tuple[np.ndarray, int]:
+        """check_conservation's exact sums on the device state: rows E, D, boundary, faces (one
+        column per equation), and the most faces of a cell."""
+        sums = np.zeros((4, 5))
+        d = C.c_int32()
+        self._call("autan_euler_device_conservation", N.ptr(sums, C.c_double), C.byref(d))
+        return sums, int(d.value)
+
+    def _state_ptr(self, u):
+        if u is None:
+            return None
+        self._u_keep = np.ascontiguousarray(u, dtype=np.float64).reshape(5, self.n_cells)
+        return N.ptr(self._u_keep, C.c_double)
 
     def history(self, count: int) -> tuple[np.ndarray, np.ndarray]:
         rms = np.zeros((count, 5))

@@ -180,6 +180,26 @@ int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, 
 int autan_euler_device_autotune(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                 int32_t trial_steps, int32_t* params, double* ms_per_step,
                                 char* err, size_t err_len);
+/* Euler<P>::face_parts (physics/src/euler.cpp:944-965) of the host state u (5 x n_cells) or, with
+ * u NULL, of the device state: res_faces (5 x n_cells) the residual's face part R^F, no sources,
+ * summed from zero in each cell's face order (ghost entries 0); face_flux (5 x n_faces) the flux of
+ * every owned interior and owned boundary face as the write-only loops give it
+ * (kernels/euler.py:1059-1085), other entries 0. Either output may be NULL. */
+int autan_euler_device_face_parts(void* handle, const double* u, double* res_faces,
+                                  double* face_flux, char* err, size_t err_len);
+/* Euler<P>::boundary_pressure (physics/src/euler.cpp:1182-1223) after evaluating the host state u
+ * or, with u NULL, the device state (EulerPhysics::face_pressure, euler_physics.cpp:1478-1492): p
+ * (n_faces - n_interior_faces) the reconstructed face pressure of every boundary face, force
+ * (3 x that, or NULL) p_f S + phi_p M^T grad p. */
+int autan_euler_device_boundary_pressure(void* handle, const double* u, double* p, double* force,
+                                         char* err, size_t err_len);
+/* The sums of EulerPhysics::check_conservation (physics/src/euler_physics.cpp:1740-1779) on the
+ * device state, one rank: sums[20] = E[5], D[5], boundary[5], faces[5], each an exact sum over the
+ * owned cells and faces (E = sum R^F - sum boundary fluxes; D = sum |flux| per incidence of an
+ * owned cell); *max_faces (may be NULL) the most faces of an owned cell, the d of the bound
+ * tau = max(64 2^-52, 2 gamma_(d+2)) (docs/validation/acceptance.md, D2 gate 7). */
+int autan_euler_device_conservation(void* handle, double* sums, int32_t* max_faces, char* err,
+                                    size_t err_len);
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);
 /* The handle's cudaStream_t. */

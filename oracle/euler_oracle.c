@@ -221,11 +221,34 @@ void oracle_residual(oracle* o, const double* u, double* res) {
   if (o->precision == 0) {
     data_f64* d = (data_f64*)o->data;
     store_f64(d, u, o->s.reference);
-    residual_f64(d, res);
+    residual_f64(d, res, NULL);
   } else {
     data_f32* d = (data_f32*)o->data;
     store_f32(d, u, o->s.reference);
-    residual_f32(d, res);
+    residual_f32(d, res, NULL);
+  }
+}
+
+void oracle_face_parts(oracle* o, const double* u, double* res_faces, double* face_flux) {
+  const size_t n5 = 5 * (size_t)o->m.n_cells, nf5 = 5 * (size_t)o->m.n_faces;
+  memset(res_faces, 0, n5 * sizeof(double));
+  memset(face_flux, 0, nf5 * sizeof(double));
+  if (o->precision == 0) {
+    data_f64* d = (data_f64*)o->data;
+    store_f64(d, u, o->s.reference);
+    residual_f64(d, res_faces, face_flux);
+  } else {
+    data_f32* d = (data_f32*)o->data;
+    store_f32(d, u, o->s.reference);
+    residual_f32(d, res_faces, face_flux);
+  }
+}
+
+void oracle_boundary_pressure(const oracle* o, double* p, double* force) {
+  if (o->precision == 0) {
+    boundary_pressure_f64((const data_f64*)o->data, p, force);
+  } else {
+    boundary_pressure_f32((const data_f32*)o->data, p, force);
   }
 }
 

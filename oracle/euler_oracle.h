@@ -71,6 +71,13 @@ void oracle_spectral_radius(oracle* o, double* lambda);
  * step; *dt_out: the global step. Returns the least invalid cell after the step, or -1. */
 int64_t oracle_step(oracle* o, double* u, int32_t rk, double cfl, double dt, int32_t local,
                     double* norms, double* dt_out);
+/* Euler<P>::face_parts (physics/src/euler.cpp:944-965) of state(u): res_faces (5 x n_cells) the
+ * residual's face part (no sources, from zero), face_flux (5 x n_faces) each owned interior and
+ * owned boundary face's flux (kernels/euler.py:1059-1085); other entries zero. */
+void oracle_face_parts(oracle* o, const double* u, double* res_faces, double* face_flux);
+/* Euler<P>::boundary_pressure (physics/src/euler.cpp:1182-1223) of the last evaluation's arrays:
+ * p (n_faces - n_interior_faces), force (3 x that, or NULL). */
+void oracle_boundary_pressure(const oracle* o, double* p, double* force);
 /* RMS over the owned cells of each residual component, exact sums. */
 void oracle_norms(const double* res, int32_t n_owned, int32_t n_cells, double* rms);
 /* ExactSum (runtime/src/exact_sum.cpp) of n terms, rounded once to the nearest double. */

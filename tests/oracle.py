@@ -43,6 +43,8 @@ def lib():
         L.oracle_free.argtypes = [vp]
         L.oracle_set_second_order.argtypes = [vp, i32]
         L.oracle_residual.argtypes = [vp, P(f64), P(f64)]
+        L.oracle_face_parts.argtypes = [vp, P(f64), P(f64), P(f64)]
+        L.oracle_boundary_pressure.argtypes = [vp, P(f64), P(f64)]
         L.oracle_arrays.argtypes = [vp] + [P(f64)] * 6
         L.oracle_spectral_radius.argtypes = [vp, P(f64)]
         L.oracle_step.restype = i64
@@ -123,6 +125,22 @@ class Oracle:
         lib().oracle_residual(self.h, _p(u), _p(res))
         return res
 
+    def face_parts(self, u):
+        """Euler<P>::face_parts of state(u): (res_faces 5 x n_cells, face_flux 5 x n_faces)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        rf = np.zeros((5, self.n_cells))
+        ff = np.zeros((5, self.n_faces))
+        lib().oracle_face_parts(self.h, _p(u), _p(rf), _p(ff))
+        return rf, ff
+
+    def boundary_pressure(self):
+        """Euler<P>::boundary_pressure of the last evaluation: (p nb, force 3 x nb)."""
+        nb = self.n_faces - int(self.mesh.n_interior_faces)
+        p = np.zeros(nb)
+        force = np.zeros((3, nb))
+        lib().oracle_boundary_pressure(self.h, _p(p), _p(force))
+        return p, force
+
     def arrays(self):
         nc, nf = self.n_cells, self.n_faces
         out = dict(prim=np.zeros((5, nc)), grad=np.zeros((15, nc)), phi=np.zeros((5, nc)),
@@ -147,6 +165,27 @@ class Oracle:
     def first_invalid(self, u, res):
         return int(lib().oracle_first_invalid(self.h, _p(np.ascontiguousarray(u)),
                                               _p(np.ascontiguousarray(res))))  # fmt: skip
+
+
+def conservation_sums(mesh: dict, res_faces, face_flux) -> np.ndarray:
+    """The sums of EulerPhysics::check_conservation (physics/src/euler_physics.cpp:1747-1779) on
+    one rank, each an ExactSum: rows E, D, boundary, faces; one column per equation."""
+    n = int(mesh["n_owned_cells"])
+    ni, nof = int(mesh["n_interior_faces"]), int(mesh["n_owned_faces"])
+    noi = int(mesh["n_owned_interior_faces"])
+    owner, neighbour = mesh["owner"], mesh["neighbour"]
+    out = np.zeros((4, 5))
+    for k in range(5):
+        rf = res_faces[k, :n]
+        fb = face_flux[k, ni:nof]
+        fi = face_flux[k, :noi]
+        mult = (owner[:noi] < n).astype(np.int64) + (neighbour[:noi] < n).astype(np.int64)
+        d_terms = np.concatenate([np.abs(fb), np.repeat(np.abs(fi), mult)])
+        out[0, k] = exact_sum(np.concatenate([rf, -fb]))
+        out[1, k] = exact_sum(d_terms)
+        out[2, k] = exact_sum(fb)
+        out[3, k] = exact_sum(rf)
+    return out
 
 
 def exact_sum(terms) -> float:

@@ -220,3 +220,85 @@ def test_autotune_leaves_the_solution_unchanged():
         dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
         b = dev.download()
     assert bits_equal(a, b)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_golden_face_parts(case):
+    """Euler<P>::face_parts: the residual's face part and every owned face's flux."""
+    mesh, scheme, z = O.load_case(GOLDEN / f"{case}.npz")
+    o = O.Oracle(mesh, scheme, z["bc_kind"], z["bc"], z["source"])
+    rf0, ff0 = o.face_parts(z["u"])
+    with device_of(mesh, scheme, z["bc_kind"], z["bc"], z["source"]) as dev:
+        rf, ff = dev.face_parts(z["u"])
+    n = mesh["n_owned_cells"]
+    if case in EXP_LOG:
+        assert rel_err(rf[:, :n], rf0[:, :n]) <= 1e-12 and rel_err(ff, ff0) <= 1e-12
+    else:
+        assert bits_equal(rf[:, :n], rf0[:, :n]) and bits_equal(ff, ff0)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_golden_boundary_pressure(case):
+    """Euler<P>::boundary_pressure after a residual of the same state."""
+    mesh, scheme, z = O.load_case(GOLDEN / f"{case}.npz")
+    o = O.Oracle(mesh, scheme, z["bc_kind"], z["bc"], z["source"])
+    o.residual(z["u"])
+    p0, f0 = o.boundary_pressure()
+    with device_of(mesh, scheme, z["bc_kind"], z["bc"], z["source"]) as dev:
+        p, f = dev.boundary_pressure(z["u"])
+    if case in EXP_LOG:
+        assert rel_err(p, p0) <= 1e-12 and rel_err(f, f0) <= 1e-12
+    else:
+        assert bits_equal(p, p0) and bits_equal(f, f0)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_golden_conservation_sums(case):
+    """check_conservation's exact sums of the device state, against the oracle's face parts."""
+    mesh, scheme, z = O.load_case(GOLDEN / f"{case}.npz")
+    o = O.Oracle(mesh, scheme, z["bc_kind"], z["bc"], z["source"])
+    want = O.conservation_sums(mesh, *o.face_parts(z["u"]))
+    with device_of(mesh, scheme, z["bc_kind"], z["bc"], z["source"]) as dev:
+        dev.upload(z["u"])
+        sums, d = dev.conservation()
+    off = mesh["cell_face_offsets"]
+    assert d == int(np.diff(off[: mesh["n_owned_cells"] + 1]).max())
+    if case in EXP_LOG:
+        # E is a cancellation: compare it on the scale of D; the other rows relatively
+        assert np.all(np.abs(sums[0] - want[0]) <= 1e-12 * want[1])
+        assert np.allclose(sums[1:], want[1:], rtol=1e-12, atol=0.0)
+    else:
+        assert bits_equal(sums, want)
+
+
+def test_conservation_jittered_box_within_gate_bound():
+    """A non-periodic jittered tetrahedral box (38 400 cells, slip walls), second order, HLLC,
+    fp32+acc64: the device's E_k / D_k within tau = max(64 2^-52, 2 gamma_(d+2)), and its exact
+    sums equal to the oracle's."""
+    from autan_b200 import mesh as M
+
+    n = (40, 40, 4)
+    ext = (1.0, 1.0, 0.1)
+    disp = M.vortex_jitter(n, ext, 0.2, 0)
+    mesh = M.lattice("tetra", n, (0, 0, 0), ext, (False, False, False), displacement=disp,
+                     rcm="morton")  # fmt: skip
+    case = cases.vortex_tets(24, 24, 6)  # the scheme of the tetrahedral workload
+    kind = np.full(mesh.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
+    rng = np.random.default_rng(3)
+    x = mesh.cell_centroid
+    rho = 1.0 + 0.1 * np.sin(6 * x[0]) * np.cos(5 * x[1])
+    u = np.stack([rho, rho * (0.3 + 0.05 * x[1]), rho * 0.1 * x[0], 0.01 * rng.standard_normal(mesh.n_cells),
+                  2.5 + 0.1 * np.cos(4 * x[0])])  # fmt: skip
+    with EulerDevice(mesh, case.scheme, bc_kind=kind) as dev:
+        dev.upload(u)
+        sums, d = dev.conservation()
+    md = cases.oracle_mesh_dict(cases.Case("box", mesh, case.scheme, kind, np.zeros((5, mesh.n_boundary_faces)),
+                                           u, 3, 0.8, 1))  # fmt: skip
+    o = O.Oracle(md, case.scheme.as_dict(), kind, np.zeros((5, mesh.n_boundary_faces)), None)
+    want = O.conservation_sums(md, *o.face_parts(u))
+    assert bits_equal(sums, want)
+    m = d + 2
+    tau = max(64 * 2.0**-52, 2 * m * 2.0**-53 / (1 - m * 2.0**-53))
+    E, D = sums[0], sums[1]
+    assert np.all(D > 0)
+    assert np.all(np.abs(E) / D <= tau), np.abs(E) / D
