@@ -39,6 +39,24 @@ class Lattice(C.Structure):
     ]
 
 
+class BumpChannel(C.Structure):
+    """struct autan_bump_channel of include/autan_b200_setup.h."""
+
+    _fields_ = [
+        ("nx", i32),
+        ("ny", i32),
+        ("nz", i32),
+        ("extent", f64 * 3),
+        ("bump", f64),
+        ("ratio", f64),
+        ("stretched", i32),
+        ("prism_rows", i32 * 2),
+        ("brick_rows", i32 * 2),
+        ("brick_cols", i32 * 2),
+        ("order", i32),
+    ]
+
+
 class Scheme(C.Structure):
     """struct autan_euler_scheme of include/autan_euler_device.h."""
 
@@ -105,6 +123,7 @@ def _bind(lib: C.CDLL) -> None:
     fn("autan_mesh_build_lattice", C.c_int, P(Lattice), P(vp), C.c_char_p, sz)
     fn("autan_mesh_build_cells", C.c_int, i64, P(f64), i64, P(i64), P(i64), P(i32), P(i32), i32,
        P(vp), C.c_char_p, sz)  # fmt: skip
+    fn("autan_mesh_build_bump_channel", C.c_int, P(BumpChannel), P(vp), C.c_char_p, sz)
     fn("autan_mesh_free", None, vp)
     fn("autan_mesh_counts", None, vp, P(i64))
     fn("autan_mesh_array", C.c_int, vp, C.c_char_p, P(vp), P(i64), P(i32))

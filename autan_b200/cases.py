@@ -2,6 +2,10 @@
 
 - `vortex_hex`: 64 x 64 x 2 hexahedra on [0,10] x [0,10] x [0,0.3125] (8192 cells), periodic in x
   and y, symmetry (slip) in z; first-order Roe, classical RK4, CFL 0.5, FP64.
+- `bump_channel`: steady subsonic flow (inlet Mach 0.5) through the hybrid hexahedral / prismatic /
+  polyhedral channel over the bump 0.05 exp(-25 (x - 1.5)^2) on [0,3] x [0,1] x [0,0.5]; AUSM+-up
+  (M_co = 0.5), second order with the Venkatakrishnan limiter (K = 5), total-pressure inlet,
+  static-pressure outlet, slip walls, SSP-RK3 with local steps at CFL 1.5, fp32+acc64.
 - `vortex_tets`: Kuhn tetrahedra of a 240 x 240 x 6 lattice on [0,10]^2 x [0,0.25] (2 073 600
   cells) whose nodes move by U(-0.2, 0.2) h (seed 0); second-order LSQ face2 gradient with the
   Venkatakrishnan limiter (K = 5), HLLC, SSP-RK3, CFL 0.8; FP64 or fp32+acc64.
@@ -64,6 +68,7 @@ class Case:
     rk: int
     cfl: float
     steps: int
+    local: bool = False
 
     @property
     def n_cells(self) -> int:
@@ -111,3 +116,34 @@ def oracle_mesh_dict(case: Case) -> dict:
         d[k] = getattr(m, k)
     d["stencil_lsq_weight"] = m.gradient_weights(case.bc_kind)
     return d
+
+
+def bump_channel(nx=480, ny=150, nz=100, mach=0.5, precision="fp32+acc64", steps=100,
+                 order="morton") -> Case:  # fmt: skip
+    """The steady bump channel (480 x 150 x 100 boxes: 8.0 M cells by default). Freestream
+    rho = 1, p = 1 / gamma (unit sound speed), u = mach along x; gas constant 1 / gamma (T = 1).
+    Inlet: total pressure and temperature of the freestream; outlet: its static pressure; bump,
+    top and z sides slip. Starts from the uniform freestream."""
+    mesh = M.bump_channel(nx, ny, nz, order=order)
+    g = GAMMA
+    rho, p = 1.0, 1.0 / g
+    rgas = 1.0 / g
+    t = p / (rho * rgas)
+    fac = 1.0 + 0.5 * (g - 1.0) * mach * mach
+    p0, t0 = p * fac ** (g / (g - 1.0)), t * fac
+    kind = np.full(mesh.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
+    data = np.zeros((5, mesh.n_boundary_faces))
+    zone = mesh.boundary_zone
+    kind[zone == M.ZONE_INLET] = M.BC_INLET
+    data[0, zone == M.ZONE_INLET] = p0
+    data[1, zone == M.ZONE_INLET] = t0
+    kind[zone == M.ZONE_OUTLET] = M.BC_OUTLET
+    data[4, zone == M.ZONE_OUTLET] = p
+    free = conserved(np.array(rho), np.array(mach), np.array(0.0), np.array(0.0), np.array(p), g)
+    scheme = Scheme(flux="ausm", second_order=True, limiter=True, venkat_k=5.0, length=1.0,
+                    gamma=g, gas_constant=rgas, mach_ref=mach,
+                    scale=(rho, mach, mach, mach, p), reference=tuple(float(x) for x in free),
+                    precision=precision, planar=bool(mesh.all_planar))  # fmt: skip
+    u0 = np.ascontiguousarray(np.repeat(free[:, None], mesh.n_cells, axis=1))
+    return Case("bump-channel", mesh, scheme, kind, data, u0, rk=3, cfl=1.5, steps=steps,
+                local=True)  # fmt: skip

@@ -372,6 +372,18 @@ __device__ __forceinline__ void load5(const typename P::C* src, typename P::C* w
   }
 }
 
+// Fire-and-forget TMA prefetch of a contiguous range into L2 (cp.async.bulk.prefetch.L2, no shared
+// memory, no completion to wait for): ptr 16-byte aligned, bytes a multiple of 16, issued in
+// pieces of at most 32 KB.
+__device__ __forceinline__ void prefetch_l2(const void* ptr, long long bytes) {
+  const char* p = static_cast<const char*>(ptr);
+  for (long long off = 0; off < bytes; off += 32768) {
+    const long long left = bytes - off;
+    const unsigned n = static_cast<unsigned>(left < 32768 ? left : 32768);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + off), "r"(n) : "memory");
+  }
+}
+
 // gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the LSQ
 // gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell, then
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
@@ -383,6 +395,18 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < d.n;
   double dt = 0.0;
+  if (threadIdx.x == 0) {
+    // The block's stencil rows and incidence records (contiguous in the sliced layout) to L2.
+    const int s0 = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x) >> 5);
+    const int s1 = min(s0 + static_cast<int>(blockDim.x >> 5), d.n_slices);
+    if (s0 < s1) {
+      const long long e0 = __ldg(d.st_start + s0), e1 = __ldg(d.st_start + s1);
+      const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s1);
+      prefetch_l2(d.st + 4 * e0, (e1 - e0) * 4 * static_cast<long long>(sizeof(C)));
+      if (LIMIT || DT) prefetch_l2(d.inc_rec + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+      if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+    }
+  }
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -448,13 +472,9 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
       const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
       const int il = __ldg(d.inc_len + c);
       for (int j = 0; j < il; ++j) {
-        const int code = __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice);
+        // The limiter record of the incidence: rel(x_f, x_c) of this side.
         C r[4];
-        if (code >= 0) {
-          load_words<P>(d.face + static_cast<long long>(code >> 1) * kFace, (code & 1) ? 8 : 4, 4, r);
-        } else {
-          load_words<P>(d.bface + static_cast<long long>(-code - 1) * kBface, 4, 4, r);
-        }
+        load_words<P, sizeof(C) == 8>(d.inc_rec + 4 * (ib + static_cast<long long>(j) * kSlice), 0, 4, r);
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
           const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
@@ -474,7 +494,23 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
     for (int k = 20; k < kRecon; ++k) out[k] = C(0);
     store_recon<P>(d, c, out);
     if constexpr (DT) {
-      dt = cell_time_step(d, c, wc, cfl);
+      // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89) from the
+      // incidence records: the other side and the face's normal and area.
+      const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+      const int il = __ldg(d.inc_len + c);
+      double lam = 0.0;
+      for (int j = 0; j < il; ++j) {
+        const long long at = 4 * (ib + static_cast<long long>(j) * kSlice);
+        C rr[4], nd[4], wn[5];
+        load_words<P, sizeof(C) == 8>(d.inc_rec + at, 0, 4, rr);
+        load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
+        const int o = index_of(rr[3]);
+        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
+                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
+                 wn);
+        lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
+      }
+      dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
     }
   }

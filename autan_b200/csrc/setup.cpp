@@ -770,6 +770,172 @@ Mesh lattice(const autan_lattice& s) {
   return m;
 }
 
+// ------------------------------------------------------------------ bump channel generator
+
+// The hybrid channel over a Gaussian bump (a steady subsonic test case of the path): nodes on
+// x_i = L_x i / nx, z_k = L_z k / nz and, in each column, y from the wall
+// y_w(x) = h exp(-25 (x - 1.5)^2) to L_y with wall-normal spacings growing by `ratio` per layer up
+// to layer `stretched`, constant above. Rows of hexahedra, a band of triangular prisms (each hex
+// split along its x-y diagonal), and a block of polyhedra: 2 x 1 "bricks" staggered from row to
+// row, so that each brick meets two half-faces above and below and has hexagonal z faces. Every
+// face is an extrusion along z, hence planar. Zones: 0 inlet (x = 0), 1 outlet (x = L_x), 2 the
+// bump wall, 3 the top, 4 z = 0, 5 z = L_z.
+Mesh bump_channel(const autan_bump_channel& s) {
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  if (nx < 2 || ny < 2 || nz < 1) fail("E1101", "channel sizes too small");
+  if (!(s.extent[0] > 0.0 && s.extent[1] > 0.0 && s.extent[2] > 0.0))
+    fail("E1101", "channel extents must be positive");
+  if (!(s.ratio >= 1.0)) fail("E1101", "the stretching ratio must be at least 1");
+  if (s.prism_rows[0] < 0 || s.prism_rows[1] < s.prism_rows[0] || s.prism_rows[1] > ny)
+    fail("E1101", "prism rows out of range");
+  const int bi0 = s.brick_cols[0], bi1 = s.brick_cols[1], bj0 = s.brick_rows[0], bj1 = s.brick_rows[1];
+  if (bi0 < 0 || bi1 < bi0 || bi1 > nx || bj0 < 0 || bj1 < bj0 || bj1 > ny)
+    fail("E1101", "brick block out of range");
+  if (bj1 > bj0 && !(bj0 >= s.prism_rows[1] || bj1 <= s.prism_rows[0]))
+    fail("E1101", "the brick block overlaps the prism band");
+  // Wall-normal distribution on [0, 1].
+  std::vector<double> sy(static_cast<std::size_t>(ny) + 1, 0.0);
+  {
+    std::vector<double> d(static_cast<std::size_t>(ny));
+    double step = 1.0;
+    for (int j = 0; j < ny; ++j) {
+      d[j] = step;
+      if (j + 1 < s.stretched) step *= s.ratio;
+    }
+    double total = 0.0;
+    for (int j = 0; j < ny; ++j) total += d[j];
+    for (int j = 0; j < ny; ++j) sy[j + 1] = sy[j] + d[j] / total;
+    sy[ny] = 1.0;
+  }
+  Cellwise cw;
+  const std::size_t nn = static_cast<std::size_t>(nx + 1) * (ny + 1) * (nz + 1);
+  cw.x.resize(nn);
+  cw.y.resize(nn);
+  cw.z.resize(nn);
+  auto node = [&](int i, int j, int k) {
+    return static_cast<i32>(i + (nx + 1) * (j + (ny + 1) * static_cast<i64>(k)));
+  };
+  for (int k = 0; k <= nz; ++k)
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        const double x = s.extent[0] * i / nx;
+        const double xc = x - 1.5;
+        const double yw = s.bump * std::exp(-25.0 * xc * xc);
+        const i32 id = node(i, j, k);
+        cw.x[id] = x;
+        cw.y[id] = yw + (s.extent[1] - yw) * sy[j];
+        cw.z[id] = s.extent[2] * k / nz;
+      }
+  using Ijk = std::array<int, 3>;
+  auto zone_of = [&](const std::vector<Ijk>& loop) {
+    auto all = [&](int a, int v) {
+      for (const auto& p : loop)
+        if (p[a] != v) return false;
+      return true;
+    };
+    if (all(0, 0)) return 0;
+    if (all(0, nx)) return 1;
+    if (all(1, 0)) return 2;
+    if (all(1, ny)) return 3;
+    if (all(2, 0)) return 4;
+    if (all(2, nz)) return 5;
+    return -1;
+  };
+  auto pos = [&](const Ijk& p) {
+    const i32 id = node(p[0], p[1], p[2]);
+    return Vec{cw.x[id], cw.y[id], cw.z[id]};
+  };
+  // A cell from its face loops, each turned outward: its area vector (Newell's sum) points away
+  // from the cell's node mean.
+  auto add_cell = [&](std::vector<std::vector<Ijk>> faces) {
+    Vec mid{0.0, 0.0, 0.0};
+    int cnt = 0;
+    for (const auto& f : faces)
+      for (const auto& p : f) {
+        mid = add(mid, pos(p));
+        ++cnt;
+      }
+    mid = scale(1.0 / cnt, mid);
+    for (auto& f : faces) {
+      Vec area{0.0, 0.0, 0.0}, fc{0.0, 0.0, 0.0};
+      for (std::size_t a = 0; a < f.size(); ++a) {
+        const Vec p = pos(f[a]), q = pos(f[(a + 1) % f.size()]);
+        area = add(area, cross(p, q));
+        fc = add(fc, p);
+      }
+      fc = scale(1.0 / static_cast<double>(f.size()), fc);
+      if (dot(area, sub(fc, mid)) < 0.0) std::reverse(f.begin(), f.end());
+      for (const auto& p : f) cw.face_nodes.push_back(node(p[0], p[1], p[2]));
+      cw.face_node_offsets.push_back(static_cast<i64>(cw.face_nodes.size()));
+      cw.face_zone.push_back(zone_of(f));
+    }
+    cw.cell_face_offsets.push_back(static_cast<i64>(cw.face_node_offsets.size()) - 1);
+    cw.image.push_back(-1);
+    for (int a = 0; a < 3; ++a) cw.shift.push_back(0.0);
+  };
+  auto quad = [](Ijk a, Ijk b, Ijk c, Ijk d) { return std::vector<Ijk>{a, b, c, d}; };
+  auto hex = [&](int i, int j, int k) {
+    auto v = [&](int di, int dj, int dk) { return Ijk{i + di, j + dj, k + dk}; };
+    add_cell({quad(v(0, 0, 0), v(0, 1, 0), v(0, 1, 1), v(0, 0, 1)),
+              quad(v(1, 0, 0), v(1, 1, 0), v(1, 1, 1), v(1, 0, 1)),
+              quad(v(0, 0, 0), v(1, 0, 0), v(1, 0, 1), v(0, 0, 1)),
+              quad(v(0, 1, 0), v(1, 1, 0), v(1, 1, 1), v(0, 1, 1)),
+              quad(v(0, 0, 0), v(1, 0, 0), v(1, 1, 0), v(0, 1, 0)),
+              quad(v(0, 0, 1), v(1, 0, 1), v(1, 1, 1), v(0, 1, 1))});
+  };
+  // The two prisms of box (i, j, k) split along the diagonal (i, j) - (i + 1, j + 1).
+  auto prisms = [&](int i, int j, int k) {
+    auto v = [&](int di, int dj, int dk) { return Ijk{i + di, j + dj, k + dk}; };
+    add_cell({{v(0, 0, 0), v(1, 0, 0), v(1, 1, 0)}, {v(0, 0, 1), v(1, 0, 1), v(1, 1, 1)},
+              quad(v(0, 0, 0), v(1, 0, 0), v(1, 0, 1), v(0, 0, 1)),
+              quad(v(1, 0, 0), v(1, 1, 0), v(1, 1, 1), v(1, 0, 1)),
+              quad(v(0, 0, 0), v(1, 1, 0), v(1, 1, 1), v(0, 0, 1))});
+    add_cell({{v(0, 0, 0), v(1, 1, 0), v(0, 1, 0)}, {v(0, 0, 1), v(1, 1, 1), v(0, 1, 1)},
+              quad(v(0, 0, 0), v(1, 1, 0), v(1, 1, 1), v(0, 0, 1)),
+              quad(v(0, 1, 0), v(1, 1, 0), v(1, 1, 1), v(0, 1, 1)),
+              quad(v(0, 0, 0), v(0, 1, 0), v(0, 1, 1), v(0, 0, 1))});
+  };
+  // A brick over columns i and i + 1 of row j.
+  auto brick = [&](int i, int j, int k) {
+    auto v = [&](int di, int dj, int dk) { return Ijk{i + di, j + dj, k + dk}; };
+    add_cell({quad(v(0, 0, 0), v(0, 1, 0), v(0, 1, 1), v(0, 0, 1)),
+              quad(v(2, 0, 0), v(2, 1, 0), v(2, 1, 1), v(2, 0, 1)),
+              quad(v(0, 0, 0), v(1, 0, 0), v(1, 0, 1), v(0, 0, 1)),
+              quad(v(1, 0, 0), v(2, 0, 0), v(2, 0, 1), v(1, 0, 1)),
+              quad(v(0, 1, 0), v(1, 1, 0), v(1, 1, 1), v(0, 1, 1)),
+              quad(v(1, 1, 0), v(2, 1, 0), v(2, 1, 1), v(1, 1, 1)),
+              {v(0, 0, 0), v(1, 0, 0), v(2, 0, 0), v(2, 1, 0), v(1, 1, 0), v(0, 1, 0)},
+              {v(0, 0, 1), v(1, 0, 1), v(2, 0, 1), v(2, 1, 1), v(1, 1, 1), v(0, 1, 1)}});
+  };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j) {
+      const bool prism_row = j >= s.prism_rows[0] && j < s.prism_rows[1];
+      const bool brick_row = j >= bj0 && j < bj1;
+      for (int i = 0; i < nx;) {
+        if (prism_row) {
+          prisms(i, j, k);
+          ++i;
+        } else if (brick_row && i >= bi0 && i < bi1) {
+          // bricks start at bi0 on even rows of the block, at bi0 + 1 on odd ones
+          const int off = (i - bi0 - ((j - bj0) & 1)) & 1;
+          if (off == 0 && i + 1 < bi1 && !((j - bj0) & 1 && i == bi0)) {
+            brick(i, j, k);
+            i += 2;
+          } else {
+            hex(i, j, k);
+            ++i;
+          }
+        } else {
+          hex(i, j, k);
+          ++i;
+        }
+      }
+    }
+  Mesh m = assemble(cw, s.order);
+  finish(m);
+  return m;
+}
+
 // ------------------------------------------------------------------ gradient weights
 
 // Euler::Impl::compute_gradient_weights (physics/src/euler.cpp:340-416), for the owned cells.
@@ -889,6 +1055,14 @@ int autan_mesh_build_cells(int64_t n_points, const double* points, int64_t n_cel
     Mesh m = assemble(cw, rcm_flag);
     finish(m);
     *mesh = new Mesh(std::move(m));
+  });
+}
+
+int autan_mesh_build_bump_channel(const autan_bump_channel* spec, void** mesh, char* err,
+                                  size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (spec == nullptr || mesh == nullptr) fail("E1101", "null argument");
+    *mesh = new Mesh(bump_channel(*spec));
   });
 }
 

@@ -189,6 +189,34 @@ def from_cells(points, cell_face_offsets, face_node_offsets, face_nodes, face_zo
     return _from_handle(handle.value)
 
 
+# Boundary zones of the bump channel (autan_mesh_build_bump_channel).
+ZONE_INLET, ZONE_OUTLET, ZONE_BUMP, ZONE_TOP, ZONE_ZMIN, ZONE_ZMAX = range(6)
+
+
+def bump_channel(nx: int, ny: int, nz: int, extent=(3.0, 1.0, 0.5), bump=0.05, ratio=1.1,
+                 stretched=None, prism_rows=None, brick_rows=None, brick_cols=None,
+                 order="morton") -> Mesh:  # fmt: skip
+    """The hybrid hexahedral / prismatic / polyhedral channel over the bump
+    y_w = bump exp(-25 (x - 1.5)^2) (autan_mesh_build_bump_channel). Defaults: spacings grow by
+    `ratio` over the first ny / 4 layers; prisms in rows [ny / 3, ny / 2); polyhedral bricks in
+    rows [2 ny / 3, ny) over the middle third of the columns."""
+    spec = N.BumpChannel()
+    spec.nx, spec.ny, spec.nz = nx, ny, nz
+    spec.extent[:] = extent
+    spec.bump = bump
+    spec.ratio = ratio
+    spec.stretched = ny // 4 if stretched is None else stretched
+    spec.prism_rows[:] = (ny // 3, ny // 2) if prism_rows is None else prism_rows
+    spec.brick_rows[:] = (2 * ny // 3, ny) if brick_rows is None else brick_rows
+    spec.brick_cols[:] = (nx // 3, 2 * nx // 3) if brick_cols is None else brick_cols
+    spec.order = ORDERS.get(order, order) if isinstance(order, str) else int(order)
+    handle = C.c_void_p()
+    err = N.errbuf()
+    N.check(N.lib().autan_mesh_build_bump_channel(C.byref(spec), C.byref(handle), err, len(err)),
+            err)  # fmt: skip
+    return _from_handle(handle.value)
+
+
 def periodic_box_hex(nx=64, ny=64, nz=2, extent=(10.0, 10.0, 0.3125), origin=(0.0, 0.0, 0.0),
                      rcm=False) -> Mesh:  # fmt: skip
     """Hexahedral box periodic in x and y (image ghosts), zones 4 (z-) and 5 (z+) in z."""

@@ -171,22 +171,26 @@ def gpu_uuid(device: int) -> str:
 
 
 def cpu_throughput(steps: int, warmup: int, threads: int,
-                   slab: tuple[int, int, int] = (240, 24, 6)) -> tuple[float, str, int]:  # fmt: skip
+                   slab: tuple[int, int, int] = (240, 24, 6),
+                   workload: str = "tets") -> tuple[float, str, int]:  # fmt: skip
     """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
-    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64); the rate of the
-    whole host."""
+    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64), or for the
+    channel workload its own channel of `slab` boxes; the rate of the whole host."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle as O
     from autan_b200 import cases
 
-    case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
+    if workload == "channel":
+        case = cases.bump_channel(*slab, steps=1)
+    else:
+        case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
     md = cases.oracle_mesh_dict(case)
     sch = case.scheme.as_dict()
     oracles = [O.Oracle(md, sch, case.bc_kind, case.bc_data) for _ in range(threads)]
     states = [case.u0.copy() for _ in range(threads)]
 
     def one_step(i):
-        oracles[i].step(states[i], rk=3, cfl=case.cfl)
+        oracles[i].step(states[i], rk=3, cfl=case.cfl, local=case.local)
 
     def all_threads():
         ts = [threading.Thread(target=one_step, args=(i,)) for i in range(threads)]
@@ -203,8 +207,9 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
     elapsed = time.perf_counter() - t0
     cells = case.mesh.n_owned_cells
     rate = cells * threads * steps / elapsed
-    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a {slab[0]}x{slab[1]}x{slab[2]} slab "
-              f"({cells} cells) of the benchmark lattice, CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
+    what = "channel" if workload == "channel" else "slab of the benchmark lattice"
+    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a {slab[0]}x{slab[1]}x{slab[2]} {what} "
+              f"({cells} cells), CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
     return rate, sample, threads
 
 
@@ -235,6 +240,14 @@ def whole_job_rate(world: int, cells: int, steps: int, seconds: float) -> float:
     return world * cells * steps / seconds
 
 
+def cpu_slab(args) -> tuple[int, int, int]:
+    """Boxes each CPU-baseline thread steps: --cpu-slab, else 240 x 24 x 6 of the tetrahedral
+    lattice or a 60 x 20 x 10 channel."""
+    if args.cpu_slab:
+        return parse_triple(args.cpu_slab)
+    return (60, 20, 10) if args.workload == "channel" else (240, 24, 6)
+
+
 def parse_triple(text: str) -> tuple[int, int, int]:
     a, b, c = (int(v) for v in text.split(","))
     return a, b, c
@@ -248,7 +261,7 @@ def run_reference(args, rank: int, world: int) -> None:
         return
     threads = args.cpu_threads or host_threads()
     rate, sample, cores = cpu_throughput(args.steps, max(1, min(args.warmup, 1)), threads,
-                                         parse_triple(args.cpu_slab))  # fmt: skip
+                                         cpu_slab(args), args.workload)  # fmt: skip
     line = {
         "impl": "reference",
         "metric": "cell-iterations/s",
@@ -272,6 +285,15 @@ def run_reference(args, rank: int, world: int) -> None:
 
 
 def workload_config(args) -> dict:
+    if args.workload == "channel":
+        nx, ny, nz = (int(v) for v in args.channel.split(","))
+        return {"workload": f"steady subsonic bump channel, {nx}x{ny}x{nz} boxes as hybrid "
+                            "hexahedra/prisms/polyhedra (8.0 M cells at the default size), "
+                            "AUSM+-up, LSQ face2 + Venkatakrishnan K=5, total-pressure inlet "
+                            "M 0.5, static-pressure outlet, slip walls, SSP-RK3 with local "
+                            "steps at CFL 1.5, fp32+acc64",
+                "parallelism": f"replicas x{args.gpus}",
+                "l2": "working set of every step larger than the 126 MB L2"}  # fmt: skip
     if args.workload == "hex":
         return {"workload": "isentropic vortex, 64x64x2 periodic hexahedra (8192 cells), "
                             "first-order Roe, classical RK4, CFL 0.5, fp64",
@@ -301,6 +323,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     if args.workload == "hex":
         case = cases.vortex_hex()
+    elif args.workload == "channel":
+        case = cases.bump_channel(*(int(v) for v in args.channel.split(",")))
     else:
         nx, ny, nz = (int(v) for v in args.lattice.split(","))
         case = cases.vortex_tets(nx, ny, nz, precision="fp32+acc64")
@@ -313,13 +337,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         tuned = dev.tuning()
     else:
         # The autotuner picks the launch choices on this case (the state is restored after it).
-        tuned, _ = dev.autotune(cfl=case.cfl, rk=case.rk, trial_steps=2)
+        tuned, _ = dev.autotune(cfl=case.cfl, rk=case.rk, local=case.local, trial_steps=2)
     # Warm-up (and graph capture).
-    dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.warmup, graph=True)
+    dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.warmup, graph=True)
     if args.profile:
         # Eager launches for a profiler: the warm-up above, then `steps` steps kernel by kernel.
         t0 = time.perf_counter()
-        r = dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.steps, graph=False)
+        r = dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.steps, graph=False)
         print(json.dumps({"profile": True, "cells": n, "steps": args.steps,
                           "wall_s": time.perf_counter() - t0, "rms": list(r.residuals)}))  # fmt: skip
         dev.close()
@@ -340,7 +364,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(gpu_uuid(local_rank)) as clocks:
         start.record(stream)
-        r = dev.step(cfl=case.cfl, rk=case.rk, n_steps=args.steps, graph=True)
+        r = dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.steps, graph=True)
         end.record(stream)
         end.synchronize()
     barrier()
@@ -358,14 +382,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         dev.upload(u_host)
-        dev.step(cfl=case.cfl, rk=case.rk, n_steps=1, graph=True)
+        dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=1, graph=True)
         dev.download(out=u_host)
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(t1 - t0)
     e2e = whole_job_rate(world, n, e2e_steps, e2e_s)
 
     # -- per-kernel times (CUDA events around every launch on the stepper's stream)
-    kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, n_steps=3)
+    kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=3)
     alg = kernel_bytes(case, case.rk)
     dominant = max((k for k in kt if kt[k][1] > 0), key=lambda k: kt[k][0])
     per_step_launches = kt[dominant][1] / 3
@@ -421,7 +445,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         if world == 1 and not args.no_cpu:
             rate, sample, cores = cpu_throughput(2, 1, args.cpu_threads or host_threads(),
-                                                 parse_triple(args.cpu_slab))  # fmt: skip
+                                                 cpu_slab(args), args.workload)  # fmt: skip
             line["cpu_baseline"] = {"value": rate, "unit": "cell-iterations/s", "cores": cores,
                                     "kind": "port", "sample": sample}  # fmt: skip
         print(json.dumps(line), flush=True)
@@ -446,13 +470,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["tets", "hex"], default="tets")
+    ap.add_argument("--workload", choices=["tets", "hex", "channel"], default="tets")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--cpu-slab", default="240,24,6",
+    ap.add_argument("--cpu-slab", default="",
                     help="lattice NX,NY,NZ each CPU thread steps for the CPU baseline")
     ap.add_argument("--cpu-threads", type=int, default=0,
                     help="threads of the CPU baseline (0: every core this process may use)")
     ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")
+    ap.add_argument("--channel", default="480,150,100", help="bump channel boxes NX,NY,NZ")
     ap.add_argument("--tuning", default="", help="launch choices instead of the autotuner: "
                     "grad_chunk,grad_block,face_mode,face_block,gather_block")
     ap.add_argument("--profile", action="store_true",

@@ -65,6 +65,29 @@ int autan_mesh_build_cells(int64_t n_points, const double* points, int64_t n_cel
                            const int32_t* face_nodes, const int32_t* face_zone, int32_t order,
                            void** mesh, char* err, size_t err_len);
 
+/* The hybrid channel over a Gaussian bump, y_w(x) = bump exp(-25 (x - 1.5)^2), on
+ * [0, extent[0]] x [y_w, extent[1]] x [0, extent[2]] (no counterpart in the reference, whose
+ * meshes come from files; its V&V bump meshes come from gmsh): nx x ny x nz boxes with wall-normal
+ * spacings growing by `ratio` per layer up to layer `stretched`, constant above; rows
+ * [prism_rows[0], prism_rows[1]) split into two triangular prisms per box; in rows
+ * [brick_rows[0], brick_rows[1]) and columns [brick_cols[0], brick_cols[1]), polyhedral 2 x 1
+ * bricks staggered row to row (two half-faces above and below, hexagonal z faces); hexahedra
+ * elsewhere. All faces planar. Zones: 0 inlet (x = 0), 1 outlet, 2 bump wall, 3 top, 4 z = 0,
+ * 5 z = extent[2]. order: owned cell order as autan_lattice.rcm. */
+struct autan_bump_channel {
+  int32_t nx, ny, nz;
+  double extent[3];
+  double bump;
+  double ratio;
+  int32_t stretched;
+  int32_t prism_rows[2];
+  int32_t brick_rows[2];
+  int32_t brick_cols[2];
+  int32_t order;
+};
+int autan_mesh_build_bump_channel(const struct autan_bump_channel* spec, void** mesh, char* err,
+                                  size_t err_len);
+
 void autan_mesh_free(void* mesh);
 
 /* counts[0..11]: n_points, n_cells, n_owned_cells, n_faces, n_interior_faces,

@@ -89,3 +89,36 @@ def test_boundary_code_out_of_range():
     m = M.periodic_box_hex(4, 4, 2, extent=(1, 1, 0.5))
     with pytest.raises(N.NativeError):
         m.gradient_weights(np.full(m.n_boundary_faces, 9, dtype=np.uint8))
+
+
+def test_bump_channel_contract():
+    """The hybrid channel: closed cells of positive volume filling the channel, hexahedra, prisms
+    and polyhedral bricks present, planar faces, zones on the six sides, LSQ weights exact for
+    linear fields with every boundary face kept."""
+    m = M.bump_channel(18, 12, 3, order="morton")
+    ni, no = m.n_interior_faces, m.n_owned_cells
+    assert m.n_cells == no and m.all_planar
+    nfaces = np.diff(m.cell_face_offsets)
+    # 6 faces: hex; 5: prism; 8 to 10: bricks (one or two faces per side, hexagonal ends)
+    assert set(np.unique(nfaces)) >= {5, 6} and nfaces.max() >= 8
+    acc = np.zeros((3, m.n_cells))
+    np.add.at(acc, (slice(None), m.owner), m.face_area)
+    np.add.at(acc, (slice(None), m.neighbour), -m.face_area[:, :ni])
+    assert np.abs(acc).max() < 1e-14
+    assert np.all(m.cell_volume > 0)
+    xs = np.linspace(0.0, 3.0, 200001)
+    area = np.trapezoid(1.0 - 0.05 * np.exp(-25 * (xs - 1.5) ** 2), xs)
+    assert m.cell_volume.sum() == pytest.approx(0.5 * area, rel=1e-4)
+    assert set(np.unique(m.boundary_zone)) == {0, 1, 2, 3, 4, 5}
+    kind = np.zeros(m.n_boundary_faces, dtype=np.uint8)
+    w = m.gradient_weights(kind)
+    a = np.array([0.3, -1.2, 0.7])
+    xc, xf = m.cell_centroid, m.face_centroid
+    so, st = m.stencil_offsets, m.stencil
+    for c in range(no):
+        g = np.zeros(3)
+        for k in range(so[c], so[c + 1]):
+            e = st[k]
+            x = xc[:, e] if e >= 0 else xf[:, -e - 1]
+            g += (a @ (x - xc[:, c])) * w[:, k]
+        assert np.allclose(g, a, rtol=1e-9, atol=1e-9)

@@ -302,3 +302,34 @@ def test_conservation_jittered_box_within_gate_bound():
     E, D = sums[0], sums[1]
     assert np.all(D > 0)
     assert np.all(np.abs(E) / D <= tau), np.abs(E) / D
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
+def test_bump_channel_local_steps(precision):
+    """The hybrid bump channel (hexahedra, prisms, polyhedral bricks; AUSM+-up, total-pressure
+    inlet, static-pressure outlet, slip walls), 5 SSP-RK3 steps with local time steps at CFL 1.5,
+    against the oracle in the same precision: the inlet state's pow/exp/log are CUDA's on the device
+    and the C library's in the oracle, so the bound is 1e-12 relative in FP64 and 1e-5 in
+    fp32+acc64 (a last-place difference of the float inlet state carried through 5 steps)."""
+    case = cases.bump_channel(24, 12, 4, precision=precision, steps=5)
+    u_d, r, rms_d, _ = run_device(case, case.steps, local=True)
+    u_o, rms_o, _, bad = run_oracle(case, case.steps, local=True)
+    assert bad == -1 and r.invalid_cell is None
+    bound = 1e-12 if precision == "fp64" else 1e-5
+    assert rel_err(u_d, u_o) <= bound
+    assert rel_err(rms_d, rms_o) <= 1e3 * bound
+
+
+def test_bump_channel_conservation_gate():
+    """D2 gate 7 on the hybrid channel after 20 local steps (fp32+acc64): the device's E_k / D_k
+    within tau = max(64 2^-52, 2 gamma_(d+2)) for every equation."""
+    case = cases.bump_channel(30, 15, 4, steps=20)
+    with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+        dev.upload(case.u0)
+        dev.step(cfl=case.cfl, rk=case.rk, n_steps=case.steps, local=True)
+        sums, d = dev.conservation()
+    m = d + 2
+    tau = max(64 * 2.0**-52, 2 * m * 2.0**-53 / (1 - m * 2.0**-53))
+    E, D = sums[0], sums[1]
+    assert np.all(np.isfinite(sums)) and np.all(D > 0)
+    assert np.all(np.abs(E) / D <= tau), np.abs(E) / D
