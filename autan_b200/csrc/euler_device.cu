@@ -421,37 +421,65 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
     }
     const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
     const int len = __ldg(d.st_len + c);
-    for (int j0 = 0; j0 < len; j0 += CHUNK) {
-      C e4[CHUNK][4], wn[CHUNK][5];
+    // One stencil entry {w, index} and its value wn, added in stencil order.
+    auto add_entry = [&](const C* e, const C* wn) {
 #pragma unroll
-      for (int q = 0; q < CHUNK; ++q)
-        if (j0 + q < len)
-          load_words<P, sizeof(C) == 8>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice), 0, 4, e4[q]);
-#pragma unroll
-      for (int q = 0; q < CHUNK; ++q) {
-        if (j0 + q < len) {
-          const int e = index_of(e4[q][3]);
-          load5<P>(e >= 0 ? d.prim + static_cast<long long>(e) * kPrimW
-                          : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
-                   wn[q]);
-        }
+      for (int i = 0; i < 5; ++i) {
+        const C dw = wn[i] - wc[i];
+        acc[3 * i] += static_cast<double>(dw * e[0]);
+        acc[3 * i + 1] += static_cast<double>(dw * e[1]);
+        acc[3 * i + 2] += static_cast<double>(dw * e[2]);
       }
 #pragma unroll
-      for (int q = 0; q < CHUNK; ++q) {
-        if (j0 + q < len) {
+      for (int i = 0; i < 5; ++i) {
+        if (wn[i] < lo[i]) lo[i] = wn[i];
+        if (wn[i] > hi[i]) hi[i] = wn[i];
+      }
+    };
+    auto row = [&](int j, C* e) {
+      load_words<P, sizeof(C) == 8>(d.st + 4 * (base + static_cast<long long>(j) * kSlice), 0, 4, e);
+    };
+    auto gather = [&](const C* e, C* w) {
+      const int x = index_of(e[3]);
+      load5<P>(x >= 0 ? d.prim + static_cast<long long>(x) * kPrimW
+                      : d.prim_b + static_cast<long long>(-x - 1) * kPrimB,
+               w);
+    };
+    if constexpr (CHUNK == 0) {
+      // Software pipeline: while entry j is added, the gather of entry j + 1 and the row of entry
+      // j + 2 are in flight.
+      C eC[4], eN[4], wC[5], wN[5];
+      if (len > 0) {
+        row(0, eC);
+        gather(eC, wC);
+      }
+      if (len > 1) row(1, eN);
+#pragma unroll 2
+      for (int j = 0; j < len; ++j) {
+        C eF[4];
+        if (j + 1 < len) gather(eN, wN);
+        if (j + 2 < len) row(j + 2, eF);
+        add_entry(eC, wC);
 #pragma unroll
-          for (int i = 0; i < 5; ++i) {
-            const C dw = wn[q][i] - wc[i];
-            acc[3 * i] += static_cast<double>(dw * e4[q][0]);
-            acc[3 * i + 1] += static_cast<double>(dw * e4[q][1]);
-            acc[3 * i + 2] += static_cast<double>(dw * e4[q][2]);
-          }
-#pragma unroll
-          for (int i = 0; i < 5; ++i) {
-            if (wn[q][i] < lo[i]) lo[i] = wn[q][i];
-            if (wn[q][i] > hi[i]) hi[i] = wn[q][i];
-          }
+        for (int k = 0; k < 4; ++k) {
+          eC[k] = eN[k];
+          eN[k] = eF[k];
         }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) wC[k] = wN[k];
+      }
+    } else {
+      for (int j0 = 0; j0 < len; j0 += CHUNK) {
+        C e4[CHUNK][4], wn[CHUNK][5];
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q < len) row(j0 + q, e4[q]);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q < len) gather(e4[q], wn[q]);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q < len) add_entry(e4[q], wn[q]);
       }
     }
     // include_own_value (:517-521); out: phi, then grad, then padding.
@@ -1365,7 +1393,8 @@ struct Tuning {
   int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather
   int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
   int gather_block = 256;  // threads per block of the store-gather sum
-  int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies
+  int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies;
+                         // 2: loaded by each thread, software-pipelined (chunk unused)
   static constexpr int kCount = 6;
   void to(int32_t* p) const {
     p[0] = grad_chunk;
@@ -1396,7 +1425,7 @@ void Tuning::validate() const {
   if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
-  if (grad_mode != 0 && grad_mode != 1) fail("E1101: grad_mode is 0 or 1");
+  if (grad_mode < 0 || grad_mode > 2) fail("E1101: grad_mode is 0, 1 or 2");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
   if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
     fail("E1101: block sizes are multiples of 32 in [32, 256]");
@@ -1920,10 +1949,11 @@ class Impl final : public Stepper {
     if (second_) {
       double best_ms = 1e300;
       Tuning keep = best;
-      for (int mode : {0, 1})
+      for (int mode : {0, 1, 2})
       for (int chunk : {1, 2, 4, 8})
         for (int block : {64, 128, 256}) {
           if (mode == 0 && chunk == 8) continue;
+          if (mode == 2 && chunk != 1) continue;
           if (mode == 1 && (chunk == 1 || block > 128)) continue;
           Tuning t = keep;
           t.grad_mode = mode;
@@ -2224,7 +2254,9 @@ class Impl final : public Stepper {
             launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, blocks(n_, bs), bs, sm, d, cfl, loc);
           return;
         }
-        if (tuning_.grad_chunk == 1)
+        if (tuning_.grad_mode == 2)
+          launch_as(kGradients, k_gradients<P, L, D, 0>, gs, bs, d, cfl, loc);
+        else if (tuning_.grad_chunk == 1)
           launch_as(kGradients, k_gradients<P, L, D, 1>, gs, bs, d, cfl, loc);
         else if (tuning_.grad_chunk == 2)
           launch_as(kGradients, k_gradients<P, L, D, 2>, gs, bs, d, cfl, loc);

@@ -167,7 +167,8 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * cell recomputes its faces' fluxes; 1 store-gather: each face's flux once into a face scratch,
  * then summed per cell), [3] threads per block of the face kernel, [4] of the store-gather sum,
  * [5] gradient staging (0: each thread loads its stencil rows; 1: each block's rows staged into
- * shared memory by TMA bulk copies, at most 128 threads per block).
+ * shared memory by TMA bulk copies, at most 128 threads per block; 2: as 0, software-pipelined:
+ * the next entry's gather and the row after it in flight while an entry is added).
  * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
  * (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,

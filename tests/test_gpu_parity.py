@@ -197,7 +197,7 @@ def test_tuning_variants_are_bit_identical(precision):
     case = cases.vortex_tets(16, 16, 6, steps=3, precision=precision)
     u_o, *_ = run_oracle(case, case.steps)
     no = case.mesh.n_owned_cells
-    for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 4)):
+    for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 2), (1, 4), (1, 8), (2, 1)):
         for mode in (0, 1):
             for block in (64, 128) if gmode else (64, 256):
                 with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
