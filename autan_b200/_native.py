@@ -114,6 +114,22 @@ class StepResult(C.Structure):
     ]
 
 
+class MarchResult(C.Structure):
+    """struct autan_march_result of include/autan_euler_device.h."""
+
+    _fields_ = [
+        ("iterations", i64),
+        ("steps", i64),
+        ("converged", i32),
+        ("plateau_mask", i32),
+        ("first", f64 * 5),
+        ("last", f64 * 5),
+        ("time_step", f64),
+        ("gpu_ms", f64),
+        ("invalid_cell", i64),
+    ]
+
+
 def _bind(lib: C.CDLL) -> None:
     def fn(name: str, res, *args):
         f = getattr(lib, name)
@@ -125,6 +141,8 @@ def _bind(lib: C.CDLL) -> None:
        P(vp), C.c_char_p, sz)  # fmt: skip
     fn("autan_mesh_build_bump_channel", C.c_int, P(BumpChannel), P(vp), C.c_char_p, sz)
     fn("autan_mesh_free", None, vp)
+    fn("autan_convergence_iteration", C.c_int, P(f64), i64, f64, P(f64), P(i64), P(i32), C.c_char_p,
+       sz)  # fmt: skip
     fn("autan_mesh_counts", None, vp, P(i64))
     fn("autan_mesh_array", C.c_int, vp, C.c_char_p, P(vp), P(i64), P(i32))
     fn("autan_mesh_gradient_weights", C.c_int, vp, P(u8), P(f64), C.c_char_p, sz)
@@ -158,6 +176,8 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_boundary_pressure", C.c_int, vp, P(f64), P(f64), P(f64), C.c_char_p,
            sz)  # fmt: skip
         fn("autan_euler_device_conservation", C.c_int, vp, P(f64), P(i32), C.c_char_p, sz)
+        fn("autan_euler_device_march", C.c_int, vp, f64, f64, i32, i32, i64, i32, f64, P(f64),
+           P(MarchResult), C.c_char_p, sz)  # fmt: skip
     if hasattr(lib, "autan_exact_rms_static"):
         fn("autan_exact_rms_static", C.c_int, vp, i64, i64, i32, vp, vp, C.c_char_p, sz)
 

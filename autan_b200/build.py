@@ -42,7 +42,7 @@ NVCC_FLAGS = [
 
 HOST_SOURCES = ["setup.cpp"]
 CUDA_SOURCES = ["euler_device.cu", "norms_static.cu"]
-HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp"]
+HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp", "convergence.hpp"]
 
 
 def _newer(src: Path, obj: Path, deps: list[Path]) -> bool:

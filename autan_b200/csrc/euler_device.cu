@@ -44,6 +44,7 @@
 
 #include "autan_euler_device.h"
 #include "euler_bodies.cuh"
+#include "convergence.hpp"
 #include "exact_sum.cuh"
 
 namespace autan_b200 {
@@ -2437,6 +2438,59 @@ Stepper* as_stepper(void* h) {
 
 }  // namespace autan_b200
 
+namespace autan_b200 {
+
+// A steady march to the convergence rule (runtime/src/run.cpp:2351-2389), `batch` steps per
+// captured-graph call, the rule fed each step's residual RMS from the history.
+void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_steps, int batch,
+           double orders, const double* floors, autan_march_result* out) {
+  if (out == nullptr) fail("E1101: null result");
+  if (max_steps < 1 || batch < 1) fail("E1101: max_steps and batch must be positive");
+  if (!(orders > 0.0)) fail("E1101: orders must be positive");
+  Convergence conv(orders, floors);
+  autan_march_result res{};
+  res.invalid_cell = -1;
+  std::vector<double> rms(5ULL * batch);
+  std::vector<double> dts(static_cast<size_t>(batch));
+  cudaEvent_t t0 = nullptr;
+  cudaEvent_t t1 = nullptr;
+  check(cudaEventCreate(&t0), "event");
+  check(cudaEventCreate(&t1), "event");
+  check(cudaEventRecord(t0, h->stream), "event");
+  long long taken = 0;
+  while (taken < max_steps && !res.converged && res.invalid_cell < 0) {
+    const long long n = std::min<long long>(batch, max_steps - taken);
+    autan_euler_step_result r{};
+    h->step(cfl, dt, local, rk, n, true, &r);
+    h->history(n, rms.data(), dts.data());
+    for (long long i = 0; i < n; ++i) {
+      for (int k = 0; k < 5; ++k) res.last[k] = rms[5 * i + k];
+      res.time_step = dts[i];
+      if (conv.add(rms.data() + 5 * i)) {
+        res.converged = 1;
+        res.iterations = taken + i + 1;
+        res.plateau_mask = conv.plateau_mask();
+        break;
+      }
+    }
+    taken += n;
+    res.invalid_cell = r.invalid_cell;
+  }
+  check(cudaEventRecord(t1, h->stream), "event");
+  check(cudaEventSynchronize(t1), "event");
+  float ms = 0.0f;
+  check(cudaEventElapsedTime(&ms, t0, t1), "event");
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (!res.converged) res.iterations = taken;
+  res.steps = taken;
+  res.gpu_ms = ms;
+  for (int k = 0; k < 5; ++k) res.first[k] = conv.first()[k];
+  *out = res;
+}
+
+}  // namespace autan_b200
+
 using namespace autan_b200;
 
 extern "C" {
@@ -2642,6 +2696,12 @@ int autan_euler_device_conservation(void* handle, double* sums, int32_t* max_fac
     const int d = h->conservation(sums);
     if (max_faces != nullptr) *max_faces = d;
   });
+}
+
+int autan_euler_device_march(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                             int64_t max_steps, int32_t batch, double orders, const double* floors,
+                             autan_march_result* out, char* err, size_t err_len) {
+  AUTAN_CALL(march(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, out));
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {

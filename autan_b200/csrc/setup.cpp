@@ -2,6 +2,8 @@
 // and BC-aware least-squares weights, in the layouts of Autan's mesh contract
 // (docs/contracts/mesh.md). Every function cites the reference function it stands in for.
 #include "autan_b200_setup.h"
+#include "autan_euler_device.h"
+#include "convergence.hpp"
 
 #include <algorithm>
 #include <array>
@@ -1067,6 +1069,24 @@ int autan_mesh_build_bump_channel(const autan_bump_channel* spec, void** mesh, c
 }
 
 void autan_mesh_free(void* mesh) { delete static_cast<Mesh*>(mesh); }
+
+int autan_convergence_iteration(const double* residuals, int64_t n, double orders,
+                                const double* floors, int64_t* iteration, int32_t* plateau_mask,
+                                char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if ((residuals == nullptr && n > 0) || iteration == nullptr) fail("E1101", "null argument");
+    autan_b200::Convergence conv(orders, floors);
+    *iteration = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (conv.add(residuals + 5 * i)) {
+        *iteration = i + 1;
+        if (plateau_mask != nullptr) *plateau_mask = conv.plateau_mask();
+        return;
+      }
+    }
+    if (plateau_mask != nullptr) *plateau_mask = 0;
+  });
+}
 
 void autan_mesh_counts(const void* mesh, int64_t* counts) {
   const auto& m = *static_cast<const Mesh*>(mesh);

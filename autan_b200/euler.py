@@ -240,6 +240,23 @@ class EulerDevice:
         self._u_keep = np.ascontiguousarray(u, dtype=np.float64).reshape(5, self.n_cells)
         return N.ptr(self._u_keep, C.c_double)
 
+    def march(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
+              max_steps: int = 1000, batch: int = 50, orders: float = 8.0,
+              floors=None) -> dict:  # fmt: skip
+        """A steady march to the convergence rule (autan_euler_device_march): steps until every
+        equation's RMS has dropped `orders` decades (or sits on a round-off plateau at most 10
+        `floors` high), at most max_steps."""
+        out = N.MarchResult()
+        fl = None if floors is None else np.ascontiguousarray(floors, dtype=np.float64)
+        self._call("autan_euler_device_march", float(cfl), float(dt), int(local), int(rk),
+                   int(max_steps), int(batch), float(orders),
+                   None if fl is None else N.ptr(fl, C.c_double), C.byref(out))  # fmt: skip
+        return dict(iterations=int(out.iterations), steps=int(out.steps),
+                    converged=bool(out.converged), plateau_mask=int(out.plateau_mask),
+                    first=np.array(out.first[:]), last=np.array(out.last[:]),
+                    time_step=float(out.time_step), gpu_ms=float(out.gpu_ms),
+                    invalid_cell=None if out.invalid_cell < 0 else int(out.invalid_cell))  # fmt: skip
+
     def history(self, count: int) -> tuple[np.ndarray, np.ndarray]:
         rms = np.zeros((count, 5))
         dt = np.zeros(count)
@@ -329,3 +346,44 @@ def _result(out: N.StepResult) -> StepResult:
         invalid_cell=None if out.invalid_cell < 0 else int(out.invalid_cell),
         steps=int(out.steps),
     )
+
+
+# runtime/include/autan/runtime/physics.hpp: round_off_floor = 2^-24 (half an FP32 ulp at 1).
+ROUND_OFF_FLOOR = 0.5 * 2.0**-23
+
+
+def residual_scales(mesh: Mesh, density: float, pressure: float, speed: float,
+                    gamma: float = 1.4) -> np.ndarray:  # fmt: skip
+    """Phi_k, the constant flux scales of the Euler residual (EulerPhysics::residual_scales,
+    physics/src/euler_physics.cpp:440-476): the RMS over owned cells of each cell's total face
+    area (exact sums), times rho q, rho q^2 (three momenta) and rho q h, q = |u| + c,
+    h = c^2 / (gamma - 1) + |u|^2 / 2."""
+    import math
+
+    nf, ni = mesh.n_faces, mesh.n_interior_faces
+    area = mesh.face_area_magnitude
+    surface = np.zeros(mesh.n_cells)
+    np.add.at(surface, mesh.owner[:nf], area[:nf])
+    np.add.at(surface, mesh.neighbour[:ni], area[:ni])
+    own = surface[: mesh.n_owned_cells]
+    rms_area = math.sqrt(math.fsum(own * own) / math.fsum(np.ones(own.size)))
+    c = math.sqrt(gamma * pressure / density)
+    q = speed + c
+    h = c * c / (gamma - 1.0) + 0.5 * speed * speed
+    mass = density * q * rms_area
+    momentum = mass * q
+    return np.array([mass, momentum, momentum, momentum, mass * h])
+
+
+def convergence_iteration(residuals, orders: float, floors=None) -> tuple[int, int]:
+    """The convergence rule on a residual history (autan_convergence_iteration): the first
+    1-based iteration at which it holds (0: none) and its plateau mask."""
+    r = np.ascontiguousarray(residuals, dtype=np.float64).reshape(-1, 5)
+    fl = None if floors is None else np.ascontiguousarray(floors, dtype=np.float64)
+    it = C.c_int64()
+    mask = C.c_int32()
+    err = N.errbuf()
+    N.check(N.lib().autan_convergence_iteration(N.ptr(r, C.c_double), r.shape[0], float(orders),
+                                                None if fl is None else N.ptr(fl, C.c_double),
+                                                C.byref(it), C.byref(mask), err, len(err)), err)  # fmt: skip
+    return int(it.value), int(mask.value)

@@ -201,6 +201,32 @@ int autan_euler_device_boundary_pressure(void* handle, const double* u, double* 
  * tau = max(64 2^-52, 2 gamma_(d+2)) (docs/validation/acceptance.md, D2 gate 7). */
 int autan_euler_device_conservation(void* handle, double* sums, int32_t* max_faces, char* err,
                                     size_t err_len);
+/* The result of a march to convergence. */
+struct autan_march_result {
+  int64_t iterations;   /* the iteration at which the rule held, or the steps taken if it never did */
+  int64_t steps;        /* steps taken: up to batch - 1 more than `iterations` (the last batch) */
+  int32_t converged;    /* 1 when the rule held */
+  int32_t plateau_mask; /* bit e: equation e converged on a round-off plateau */
+  double first[5];      /* the residual RMS of iteration 1 */
+  double last[5];       /* the residual RMS of iteration `iterations` */
+  double time_step;     /* that iteration's global step */
+  double gpu_ms;        /* device time of the march (CUDA events on the handle's stream) */
+  int64_t invalid_cell; /* as autan_euler_step_result, -1 if none; the march stops at one */
+};
+
+/* A steady march (runtime/src/run.cpp:2351-2389): steps of autan_euler_device_step, `batch` per
+ * captured-graph call, until every equation's RMS residual has dropped `orders` decades from its
+ * reference or, with `floors` (round_off_floor * Phi_k, 5 values; NULL: no plateau rule), sits on
+ * a round-off plateau at most 10 floors high (runtime/include/autan/runtime/round_off.hpp), or
+ * until max_steps. The rule as autan_convergence_iteration. */
+int autan_euler_device_march(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                             int64_t max_steps, int32_t batch, double orders, const double* floors,
+                             struct autan_march_result* out, char* err, size_t err_len);
+/* The convergence rule alone, on a residual history (n iterations x 5, row-major): *iteration the
+ * first (1-based) at which it holds, 0 if none; *plateau_mask (may be NULL) as above. Host only. */
+int autan_convergence_iteration(const double* residuals, int64_t n, double orders,
+                                const double* floors, int64_t* iteration, int32_t* plateau_mask,
+                                char* err, size_t err_len);
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);
 /* The handle's cudaStream_t. */

@@ -232,3 +232,55 @@ def load_case(path) -> tuple[dict, dict, dict]:
     scheme = {k[len("scheme_"):]: (z[k].tolist()) for k in z if k.startswith("scheme_")}
     rest = {k: v for k, v in z.items() if k not in mesh_keys and not k.startswith("scheme_")}
     return mesh, scheme, rest
+
+
+def convergence_iteration(residuals, orders, floors=None):
+    """The steady convergence decision restated in Python (runtime/src/run.cpp:2351-2389,
+    runtime/include/autan/runtime/round_off.hpp RoundOffExemption and ResidualPlateau): the first
+    1-based iteration at which every equation met its drop or sits on a round-off plateau, and the
+    plateau mask then; (0, 0) if never."""
+    drop = 10.0 ** (-orders)
+    first = None
+    zero = exempt = None
+    floor0 = 0.0
+    plats = [dict(window=[0.0] * 100, ref=float("inf"), count=0, since=0) for _ in range(5)]
+
+    def plateau_add(pl, v):
+        pl["window"][pl["count"] % 100] = v
+        pl["count"] += 1
+        if pl["count"] >= 100:
+            srt = sorted(pl["window"])
+            level = (srt[49] + srt[50]) / 2
+            if level < 0.9 * pl["ref"]:
+                pl["ref"] = level
+                pl["since"] = pl["count"]
+        return pl["since"] > 0 and pl["count"] - pl["since"] >= 100
+
+    def drop_ref(e):
+        return max(first[1:4]) if 1 <= e <= 3 else first[e]
+
+    def woken_ref(e):
+        return drop_ref(e) if 1 <= e <= 3 else max(first)
+
+    for it, r in enumerate(np.asarray(residuals, dtype=np.float64).reshape(-1, 5), start=1):
+        if first is None:
+            first = [float(x) for x in r]
+            floor0 = 1e-12 * max(first)
+            zero = [x < floor0 for x in first]
+            exempt = list(zero)
+        for e in range(5):
+            if exempt[e] and r[e] > floor0:
+                exempt[e] = False
+        ok, mask = True, 0
+        for e in range(5):
+            flat = plateau_add(plats[e], float(r[e]))
+            woken = zero[e] and not exempt[e]
+            ref = woken_ref(e) if woken else drop_ref(e)
+            met = exempt[e] or r[e] <= ref * drop
+            plateau = floors is not None and flat and r[e] <= 10.0 * floors[e]
+            if not met and plateau:
+                mask |= 1 << e
+            ok = ok and (met or plateau)
+        if ok:
+            return it, mask
+    return 0, 0

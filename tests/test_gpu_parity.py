@@ -333,3 +333,30 @@ def test_bump_channel_conservation_gate():
     E, D = sums[0], sums[1]
     assert np.all(np.isfinite(sums)) and np.all(D > 0)
     assert np.all(np.abs(E) / D <= tau), np.abs(E) / D
+
+
+def test_march_to_convergence_matches_the_oracle():
+    """A steady march (autan_euler_device_march, batches of 7 graph-launched steps) of a small
+    channel (state inlet, pressure outlet, slip walls; no exp/log on the path), fp64, local steps at
+    CFL 1.5, to a 2-decade drop: the same converged iteration and the same residual bits as the
+    oracle's steps fed to the rule's restatement."""
+    from autan_b200 import mesh as M
+
+    case = cases.bump_channel(12, 6, 2, precision="fp64")
+    kind, data = case.bc_kind.copy(), case.bc_data.copy()
+    inlet = kind == M.BC_INLET
+    kind[inlet] = M.BC_STATE
+    data[:, inlet] = np.array([1.0, 0.5, 0.0, 0.0, 1.0 / 1.4])[:, None]
+    with EulerDevice(case.mesh, case.scheme, kind, data) as dev:
+        dev.upload(case.u0)
+        res = dev.march(cfl=1.5, local=True, rk=3, max_steps=2000, batch=7, orders=2.0)
+    assert res["converged"] and res["invalid_cell"] is None
+    assert 0 <= res["steps"] - res["iterations"] < 7
+    md = cases.oracle_mesh_dict(cases.Case("march", case.mesh, case.scheme, kind, data, case.u0,
+                                           3, 1.5, 1, True))  # fmt: skip
+    o = O.Oracle(md, case.scheme.as_dict(), kind, data)
+    u = case.u0.copy()
+    norms = [o.step(u, rk=3, cfl=1.5, local=True)[0] for _ in range(res["steps"])]
+    it, mask = O.convergence_iteration(np.array(norms), 2.0)
+    assert (it, mask) == (res["iterations"], res["plateau_mask"])
+    assert bits_equal(res["first"], norms[0]) and bits_equal(res["last"], norms[it - 1])
