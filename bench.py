@@ -307,6 +307,33 @@ def workload_config(args) -> dict:
     }
 
 
+def run_converge(args, case, dev, tuned) -> None:
+    """A steady march to `--converge` decades (autan_euler_device_march), fp32+acc64 with the
+    round-off plateau floors of the case's freestream (runtime/src/run.cpp:1874-1897)."""
+    from autan_b200.euler import ROUND_OFF_FLOOR, residual_scales
+
+    floors = None
+    if case.scheme.precision != "fp64":
+        u0 = case.u0[:, 0]
+        rho = float(u0[0])
+        speed = float(np.linalg.norm(u0[1:4]) / rho)
+        p = float((case.scheme.gamma - 1.0) * (u0[4] - 0.5 * rho * speed * speed))
+        floors = ROUND_OFF_FLOOR * residual_scales(case.mesh, rho, p, speed, case.scheme.gamma)
+    res = dev.march(cfl=case.cfl, local=case.local, rk=case.rk, max_steps=args.max_steps,
+                    batch=200, orders=args.converge, floors=floors)  # fmt: skip
+    n = case.mesh.n_owned_cells
+    print(json.dumps({
+        "metric": f"GPU time to a {args.converge:g}-decade residual drop",
+        "value": res["gpu_ms"] / 1e3, "unit": "s", "higher_is_better": False,
+        "converged": res["converged"], "iterations": res["iterations"], "steps": res["steps"],
+        "plateau_mask": res["plateau_mask"], "first_rms": list(res["first"]),
+        "last_rms": list(res["last"]), "cells": n,
+        "cell_iterations_per_s": n * res["steps"] / (res["gpu_ms"] / 1e3),
+        "config": dict(workload_config(args), tuning=tuned, start="freestream"),
+    }), flush=True)  # fmt: skip
+    dev.close()
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     import torch
 
@@ -338,6 +365,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     else:
         # The autotuner picks the launch choices on this case (the state is restored after it).
         tuned, _ = dev.autotune(cfl=case.cfl, rk=case.rk, local=case.local, trial_steps=2)
+    if args.converge > 0:
+        run_converge(args, case, dev, tuned)
+        return
     # Warm-up (and graph capture).
     dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.warmup, graph=True)
     if args.profile:
@@ -480,6 +510,11 @@ def main() -> None:
     ap.add_argument("--channel", default="480,150,100", help="bump channel boxes NX,NY,NZ")
     ap.add_argument("--tuning", default="", help="launch choices instead of the autotuner: "
                     "grad_chunk,grad_block,face_mode,face_block,gather_block")
+    ap.add_argument("--converge", type=float, default=0.0,
+                    help="instead of the throughput line: march the workload from its start to "
+                         "this many decades of residual drop (round-off plateau rule in "
+                         "fp32+acc64) and print iterations and GPU time")
+    ap.add_argument("--max-steps", type=int, default=100000, help="step cap of --converge")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()
