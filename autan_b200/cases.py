@@ -147,3 +147,147 @@ def bump_channel(nx=480, ny=150, nz=100, mach=0.5, precision="fp32+acc64", steps
     u0 = np.ascontiguousarray(np.repeat(free[:, None], mesh.n_cells, axis=1))
     return Case("bump-channel", mesh, scheme, kind, data, u0, rk=3, cfl=1.5, steps=steps,
                 local=True)  # fmt: skip
+
+
+MESH_KEYS = ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces", "n_owned_interior_faces",
+             "n_owned_faces")  # fmt: skip
+
+
+def union(meshes, weights) -> tuple[dict, np.ndarray, np.ndarray]:
+    """The disjoint union of meshes without ghost cells, in the mesh contract's layout: cells of
+    mesh k after those of meshes < k; interior faces of every mesh (in mesh order), then boundary
+    faces of every mesh; each cell's faces still in increasing order. weights: each mesh's LSQ
+    weights (3 x its stencil entries). Returns the mesh arrays (a dict, as EulerDevice and the
+    oracle take them), the concatenated weights and the cell offsets of the meshes."""
+    for m in meshes:
+        if m.n_cells != m.n_owned_cells:
+            raise ValueError("union: meshes with ghost cells are not supported")
+    nc = np.array([m.n_cells for m in meshes])
+    ni = np.array([m.n_interior_faces for m in meshes])
+    nb = np.array([m.n_faces - m.n_interior_faces for m in meshes])
+    coff = np.concatenate([[0], np.cumsum(nc)])
+    ioff = np.concatenate([[0], np.cumsum(ni)])
+    boff = np.concatenate([[0], np.cumsum(nb)])
+    NI, NF = int(ioff[-1]), int(ioff[-1] + boff[-1])
+
+    def new_face(k, f):
+        f = np.asarray(f, dtype=np.int64)
+        return np.where(f < ni[k], f + ioff[k], NI + boff[k] + (f - ni[k]))
+
+    owner = np.empty(NF, dtype=np.int32)
+    neighbour = np.empty(NI, dtype=np.int32)
+    face_zone = np.empty(NF, dtype=np.int32)
+    vec = {key: np.empty((d, NF)) for key, d in (("face_normal", 3), ("face_centroid", 3),
+                                                  ("face_area", 3), ("face_moment", 9))}  # fmt: skip
+    area = np.empty(NF)
+    for k, m in enumerate(meshes):
+        src_i = slice(0, ni[k])
+        dst_i = slice(ioff[k], ioff[k + 1])
+        src_b = slice(ni[k], ni[k] + nb[k])
+        dst_b = slice(NI + boff[k], NI + boff[k + 1])
+        for src, dst in ((src_i, dst_i), (src_b, dst_b)):
+            owner[dst] = m.owner[src] + coff[k]
+            face_zone[dst] = m.face_zone[src]
+            area[dst] = m.face_area_magnitude[src]
+            for key in vec:
+                vec[key][:, dst] = getattr(m, key).reshape(vec[key].shape[0], -1)[:, src]
+        neighbour[dst_i] = m.neighbour + coff[k]
+    cfo, cf, so, st = [np.zeros(1, dtype=np.int64)], [], [np.zeros(1, dtype=np.int64)], []
+    for k, m in enumerate(meshes):
+        cfo.append(m.cell_face_offsets[1:] + cfo[-1][-1])
+        cf.append(new_face(k, m.cell_faces).astype(np.int32))
+        so.append(m.stencil_offsets[1:] + so[-1][-1])
+        e = m.stencil.astype(np.int64)
+        st.append(np.where(e >= 0, e + coff[k], -(new_face(k, -e - 1) + 1)).astype(np.int32))
+    d = dict(n_cells=int(coff[-1]), n_owned_cells=int(coff[-1]), n_faces=NF, n_interior_faces=NI,
+             n_owned_interior_faces=NI, n_owned_faces=NF, owner=owner, neighbour=neighbour,
+             face_zone=face_zone, face_area_magnitude=area,
+             cell_face_offsets=np.concatenate(cfo), cell_faces=np.concatenate(cf),
+             ghost_owner=np.zeros(0, dtype=np.int32),
+             cell_centroid=np.concatenate([m.cell_centroid for m in meshes], axis=1),
+             cell_volume=np.concatenate([m.cell_volume for m in meshes]),
+             stencil_offsets=np.concatenate(so), stencil=np.concatenate(st))  # fmt: skip
+    d.update(vec)
+    d["face_moment"] = d["face_moment"].reshape(-1)
+    w = np.concatenate([np.asarray(x).reshape(3, -1) for x in weights], axis=1)
+    d["stencil_lsq_weight"] = w
+    d["all_planar"] = all(m.all_planar for m in meshes)
+    return d, w, coff
+
+
+@dataclass
+class Batch:
+    """Many steady bump-channel cases as one union mesh (autan_euler_device_set_cases)."""
+
+    mesh: dict
+    weights: np.ndarray
+    cell_offsets: np.ndarray
+    scheme: Scheme
+    bc_kind: np.ndarray
+    bc_data: np.ndarray
+    u0: np.ndarray
+    params: list  # per case: dict(cells, mach, angle, bump, boxes)
+    cfl: float = 1.5
+    rk: int = 3
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.mesh["n_owned_cells"])
+
+
+def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precision="fp32+acc64",
+               inlet="farfield") -> Batch:  # fmt: skip
+    """Batched steady bump channels: per case (numpy default_rng(seed)) a cell count log-uniform
+    in `cells`, Mach ~ U(0.3, 0.75), flow angle ~ U(-4, 4) degrees, bump height ~ U(0.02, 0.10).
+    Each case's channel has about the requested cells (boxes in the ratio 3 : 1 : 1 / 2 of the
+    channel's extent, hybrid rows as bump_channel). Inflow and outflow faces take the farfield
+    state of the case's freestream (rho = 1, p = 1 / gamma, speed Mach, at the flow angle in the
+    x-y plane); bump, top and z sides slip. A common scheme (second order, Venkatakrishnan K = 5)
+    and reference state (Mach 0.5 along x) serve every case; local steps make the cases
+    independent. inlet="state": the inflow faces take the freestream as a given state and the
+    outflow faces its static pressure (no exp/log on the path, for bit-exact tests)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(cells[0]), np.log(cells[1])
+    g = GAMMA
+    p = 1.0 / g
+    meshes, weights, kinds, datas, u0s, params = [], [], [], [], [], []
+    for _ in range(n_cases):
+        target = float(np.exp(rng.uniform(lo, hi)))
+        mach = float(rng.uniform(0.3, 0.75))
+        angle = float(rng.uniform(-4.0, 4.0))
+        bump = float(rng.uniform(0.02, 0.10))
+        # cells ~ 1.111 nx ny nz with nx = 6 a, ny = 2 a, nz = a
+        a = max(2, int(round((target / (1.111 * 12.0)) ** (1.0 / 3.0))))
+        nx, ny, nz = 6 * a, 2 * a, a
+        m = M.bump_channel(nx, ny, nz, bump=bump)
+        zone = m.boundary_zone
+        kind = np.full(m.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
+        data = np.zeros((5, m.n_boundary_faces))
+        t = np.radians(angle)
+        w = np.array([1.0, mach * np.cos(t), mach * np.sin(t), 0.0, p])
+        io = (zone == M.ZONE_INLET) | (zone == M.ZONE_OUTLET)
+        if inlet == "state":
+            kind[zone == M.ZONE_INLET] = M.BC_STATE
+            data[:, zone == M.ZONE_INLET] = w[:, None]
+            kind[zone == M.ZONE_OUTLET] = M.BC_OUTLET
+            data[4, zone == M.ZONE_OUTLET] = p
+        else:
+            kind[io] = M.BC_FARFIELD
+            data[:, io] = w[:, None]
+        meshes.append(m)
+        weights.append(m.gradient_weights(kind))
+        kinds.append(kind)
+        datas.append(data)
+        free = conserved(*(np.array(x) for x in w), g)
+        u0s.append(np.repeat(free[:, None], m.n_cells, axis=1))
+        params.append(dict(cells=m.n_cells, mach=mach, angle=angle, bump=bump, boxes=(nx, ny, nz)))
+    d, wts, coff = union(meshes, weights)
+    ref = conserved(np.array(1.0), np.array(0.5), np.array(0.0), np.array(0.0), np.array(p), g)
+    scheme = Scheme(flux=flux, second_order=True, limiter=True, venkat_k=5.0, length=1.0, gamma=g,
+                    gas_constant=1.0 / g, mach_ref=0.5, scale=(1.0, 0.5, 0.5, 0.5, p),
+                    reference=tuple(float(x) for x in ref), precision=precision,
+                    planar=bool(d["all_planar"]))  # fmt: skip
+    for m in meshes:
+        m.close()
+    return Batch(d, wts, coff, scheme, np.concatenate(kinds), np.concatenate(datas, axis=1),
+                 np.ascontiguousarray(np.concatenate(u0s, axis=1)), params)  # fmt: skip

@@ -121,7 +121,16 @@ struct Dev {
   const C* f_m;     // 9 x n_if, warped meshes only
   const C* b_m;     // 9 x nb
   Control* ctl;
+  // Batched cases (null without): the case of each owned cell and whether each case still steps.
+  const int* case_of;
+  const unsigned char* active;
 };
+
+// Whether owned cell c takes part (its case has not stopped).
+template <class P>
+__device__ __forceinline__ bool cell_active(const Dev<P>& d, int c) {
+  return d.active == nullptr || d.active[d.case_of[c]] != 0;
+}
 
 __device__ __forceinline__ int index_of(float x) { return __float_as_int(x); }
 __device__ __forceinline__ int index_of(double x) {
@@ -394,7 +403,7 @@ template <class P, bool LIMIT, bool DT, int CHUNK>
 __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n;
+  const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
   if (threadIdx.x == 0) {
     // The block's stencil rows and incidence records (contiguous in the sliced layout) to L2.
@@ -629,7 +638,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
   }
   if (!bounded_wait(&bar, d.ctl)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n;
+  const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
   if (live) {
     C wc[5];
@@ -740,7 +749,7 @@ __global__ void __launch_bounds__(256) k_spectral(Dev<P> d, double cfl, int loca
                                                   double* dt_out) {
   using C = typename P::C;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n;
+  const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
   if (live) {
     C wc[5];
@@ -958,7 +967,7 @@ __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stag
                                                     double wb, int local, int last) {
   using C = typename P::C;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n) return;
+  if (c >= d.n || !cell_active(d, c)) return;
   C wc[5], gc[15], pc[5];
   cell_recon<P, SECOND>(d, c, wc, pc, gc);
   const double vol = __ldg(d.volume + c);
@@ -1016,6 +1025,7 @@ __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux
   if (f >= d.n_if) return;
   C fr[kFace], wl[5], gl[15], pl[5], wr[5], gr[15], pr[5], out[8];
   load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
+  if (!cell_active(d, index_of(fr[7]))) return;
   cell_recon<P, SECOND>(d, index_of(fr[7]), wl, pl, gl);
   cell_recon<P, SECOND>(d, index_of(fr[11]), wr, pr, gr);
   interior_flux<P, FLUX, PLANAR>(d, f, fr, wl, gl, pl, wr, gr, pr, out);
@@ -1031,6 +1041,7 @@ __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flu
   if (b >= nbo) return;
   C br[kBface], wc[5], gc[15], pc[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
+  if (!cell_active(d, index_of(br[13]))) return;
   cell_recon<P, SECOND>(d, index_of(br[13]), wc, pc, gc);
   boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
   out[5] = out[6] = out[7] = C(0);
@@ -1045,7 +1056,7 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
                                                 double wa, double wb, int local, int last) {
   using C = typename P::C;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n) return;
+  if (c >= d.n || !cell_active(d, c)) return;
   const double vol = __ldg(d.volume + c);
   CellIn in;
   load_cell_in(d, c, mode, stage, local, in);
@@ -1130,6 +1141,62 @@ __global__ void k_norm_finish(Control* ctl, int n, int record) {
     }
     if (record) ctl->hist_dt[slot] = ctl->dt;
   }
+}
+
+// Batched cases: the exact sums of R_k^2 per case. A block whose cells all lie in one case adds
+// into shared words and flushes them once; a block over a case boundary adds each warp's terms,
+// grouped by case, to the global words of their cases.
+__global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, int n,
+                                                           const int* case_of,
+                                                           unsigned long long* words) {
+  __shared__ unsigned long long sh[5 * kWords];
+  const long long c0 = static_cast<long long>(blockIdx.x) * blockDim.x;
+  const long long c1 = min(c0 + static_cast<long long>(blockDim.x), static_cast<long long>(n)) - 1;
+  const long long c = c0 + threadIdx.x;
+  const int first = case_of[c0], last = case_of[c1];
+  if (first == last) {
+    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+      warp_exact_add_nonneg(sh + k * kWords, r * r);
+    }
+    __syncthreads();
+    unsigned long long* dst = words + static_cast<long long>(first) * 5 * kWords;
+    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+      const unsigned long long v = sh[i];
+      if (v != 0) atomicAdd(&dst[i], v);
+    }
+    return;
+  }
+  const unsigned full = 0xffffffffu;
+  const int mine = c < n ? case_of[c] : -1;
+  unsigned todo = __ballot_sync(full, mine >= 0);
+  while (todo != 0) {
+    const int kc = __shfl_sync(full, mine, __ffs(todo) - 1);
+    const bool in = mine == kc;
+    const unsigned group = __ballot_sync(full, in);
+    unsigned long long* dst = words + static_cast<long long>(kc) * 5 * kWords;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double r = in ? res[k * static_cast<long long>(n) + c] : 0.0;
+      warp_exact_add_nonneg(dst + k * kWords, r * r);
+    }
+    todo &= ~group;
+  }
+}
+
+// Per case and equation (q = 5 case + k): rms = sqrt(sum / cells of the case) into this step's
+// row of the case history; the words are cleared for the next step.
+__global__ void k_case_norm_finish(unsigned long long* words, const double* cells, int n_cases,
+                                   const Control* ctl, double* hist) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 5 * n_cases) return;
+  unsigned long long* w = words + static_cast<long long>(q) * kWords;
+  const double rms = sqrt(exact_value(w) / cells[q / 5]);
+  hist[(ctl->step % kHistory) * 5LL * n_cases + q] = rms;
+  for (int i = 0; i < kWords; ++i) w[i] = 0;
 }
 
 // The start of a step: clears the sums and the validity marks, sets the global step (fixed) or
@@ -1457,6 +1524,10 @@ class Stepper {
   virtual void face_parts(const double* u, double* res_faces, double* face_flux) = 0;
   virtual void boundary_pressure(const double* u, double* p, double* force) = 0;
   virtual int conservation(double* sums) = 0;
+  virtual void set_cases(int n_cases, const int64_t* cell_offsets) = 0;
+  virtual void set_active(const uint8_t* active) = 0;
+  virtual void case_history(long long count, double* rms) = 0;
+  virtual int n_cases() const = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
@@ -1691,6 +1762,8 @@ class Impl final : public Stepper {
     d_.f_m = f_m_.as<C>();
     d_.b_m = b_m_.as<C>();
     d_.ctl = ctl_.as<Control>();
+    d_.case_of = nullptr;
+    d_.active = nullptr;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     if (tuning_.face_mode == 1) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
@@ -2204,6 +2277,57 @@ class Impl final : public Stepper {
     return max_faces_;
   }
 
+  // Batched cases: owned cells [cell_offsets[k], cell_offsets[k + 1]) form case k.
+  void set_cases(int n_cases, const int64_t* off) override {
+    if (n_cases < 1 || off == nullptr) fail("E1101: at least one case and its cell offsets");
+    if (off[0] != 0 || off[n_cases] != n_) fail("E1101: case offsets must span the owned cells");
+    std::vector<int> case_of(std::max(n_, 1), 0);
+    std::vector<double> cells(n_cases);
+    for (int k = 0; k < n_cases; ++k) {
+      if (off[k + 1] <= off[k]) fail("E1101: every case needs at least one cell");
+      cells[k] = static_cast<double>(off[k + 1] - off[k]);
+      for (int64_t c = off[k]; c < off[k + 1]; ++c) case_of[c] = k;
+    }
+    drop_graph();
+    n_cases_ = n_cases;
+    case_of_ = upload(case_of, stream);
+    case_cells_ = upload(cells, stream);
+    case_words_.alloc(5ULL * kWords * n_cases * sizeof(unsigned long long));
+    case_hist_.alloc(static_cast<size_t>(kHistory) * 5 * n_cases * sizeof(double));
+    active_.alloc(static_cast<size_t>(n_cases));
+    check(cudaMemsetAsync(case_words_.ptr(), 0, case_words_.bytes(), stream), "cases");
+    check(cudaMemsetAsync(case_hist_.ptr(), 0, case_hist_.bytes(), stream), "cases");
+    check(cudaMemsetAsync(active_.ptr(), 1, active_.bytes(), stream), "cases");
+    d_.case_of = case_of_.as<int>();
+    d_.active = active_.as<unsigned char>();
+    check(cudaStreamSynchronize(stream), "cases");
+  }
+
+  void set_active(const uint8_t* active) override {
+    if (n_cases_ == 0) fail("E1101: no cases set");
+    check(cudaMemcpyAsync(active_.ptr(), active, static_cast<size_t>(n_cases_), cudaMemcpyHostToDevice,
+                          stream), "active");
+    check(cudaStreamSynchronize(stream), "active");
+  }
+
+  // The last `count` steps' per-case RMS (count x n_cases x 5), oldest first.
+  void case_history(long long count, double* rms) override {
+    if (n_cases_ == 0) fail("E1101: no cases set");
+    long long step = 0;
+    check(cudaMemcpyAsync(&step, &d_.ctl->step, sizeof(step), cudaMemcpyDeviceToHost, stream), "history");
+    check(cudaStreamSynchronize(stream), "history");
+    const long long n = std::min<long long>({count, step, kHistory});
+    const size_t row = 5ULL * n_cases_ * sizeof(double);
+    for (long long i = 0; i < n; ++i) {
+      const long long slot = (step - n + i) % kHistory;
+      check(cudaMemcpyAsync(rms + i * 5LL * n_cases_, case_hist_.as<double>() + slot * 5LL * n_cases_,
+                            row, cudaMemcpyDeviceToHost, stream), "history");
+    }
+    check(cudaStreamSynchronize(stream), "history");
+  }
+
+  int n_cases() const override { return n_cases_; }
+
   // Calls body(flux, planar, second) with the scheme's compile-time choices.
   template <class B>
   void dispatch_faces(B&& body) {
@@ -2307,6 +2431,14 @@ class Impl final : public Stepper {
         launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
                   static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
         launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        if (n_cases_ > 0) {
+          launch_as(kNorms, k_case_norm_sums, blocks(n_), kBlock,
+                    static_cast<const double*>(res_.as<double>()), n_,
+                    static_cast<const int*>(case_of_.as<int>()), case_words_.as<unsigned long long>());
+          launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
+                    case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
+                    n_cases_, static_cast<const Control*>(d_.ctl), case_hist_.as<double>());
+        }
       }
     }
     launch(k_end_step, 1, 32, d_.ctl);
@@ -2374,6 +2506,8 @@ class Impl final : public Stepper {
   Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
   Buffer bface_r64_, face_mult_, cons_words_;  // boundary pressure and conservation
+  Buffer case_of_, case_cells_, case_words_, case_hist_, active_;  // batched cases
+  int n_cases_ = 0;
   double pref64_ = 0.0;
   int max_faces_ = 0;
   Buffer face_, f_m_, bface_, b_m_, source_;
@@ -2487,6 +2621,68 @@ void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_
   res.gpu_ms = ms;
   for (int k = 0; k < 5; ++k) res.first[k] = conv.first()[k];
   *out = res;
+}
+
+// The batched march: one convergence rule per case, fed that case's row of each step's per-case
+// RMS; a case that meets its rule stops stepping (its cells are skipped from the next batch on).
+void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long long max_steps,
+                 int batch, double orders, const double* floors, int64_t* iterations,
+                 int32_t* converged, int64_t* steps_taken, double* gpu_ms) {
+  const int nk = h->n_cases();
+  if (nk == 0) fail("E1101: no cases set");
+  if (max_steps < 1 || batch < 1) fail("E1101: max_steps and batch must be positive");
+  if (!(orders > 0.0)) fail("E1101: orders must be positive");
+  if (iterations == nullptr || converged == nullptr) fail("E1101: null outputs");
+  std::vector<Convergence> conv;
+  conv.reserve(nk);
+  for (int k = 0; k < nk; ++k) conv.emplace_back(orders, floors != nullptr ? floors + 5 * k : nullptr);
+  std::vector<uint8_t> active(nk, 1);
+  for (int k = 0; k < nk; ++k) {
+    iterations[k] = 0;
+    converged[k] = 0;
+  }
+  h->set_active(active.data());
+  std::vector<double> rms(5ULL * nk * batch);
+  cudaEvent_t t0 = nullptr;
+  cudaEvent_t t1 = nullptr;
+  check(cudaEventCreate(&t0), "event");
+  check(cudaEventCreate(&t1), "event");
+  check(cudaEventRecord(t0, h->stream), "event");
+  long long taken = 0;
+  int left = nk;
+  while (taken < max_steps && left > 0) {
+    const long long n = std::min<long long>(batch, max_steps - taken);
+    autan_euler_step_result r{};
+    h->step(cfl, dt, local, rk, n, true, &r);
+    h->case_history(n, rms.data());
+    bool changed = false;
+    for (int k = 0; k < nk; ++k) {
+      if (!active[k]) continue;
+      for (long long i = 0; i < n; ++i) {
+        if (conv[k].add(rms.data() + (i * nk + k) * 5)) {
+          iterations[k] = taken + i + 1;
+          converged[k] = 1;
+          active[k] = 0;
+          changed = true;
+          --left;
+          break;
+        }
+      }
+    }
+    taken += n;
+    if (changed) h->set_active(active.data());
+    if (r.invalid_cell >= 0) break;
+  }
+  check(cudaEventRecord(t1, h->stream), "event");
+  check(cudaEventSynchronize(t1), "event");
+  float ms = 0.0f;
+  check(cudaEventElapsedTime(&ms, t0, t1), "event");
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  for (int k = 0; k < nk; ++k)
+    if (!converged[k]) iterations[k] = taken;
+  if (steps_taken != nullptr) *steps_taken = taken;
+  if (gpu_ms != nullptr) *gpu_ms = ms;
 }
 
 }  // namespace autan_b200
@@ -2702,6 +2898,34 @@ int autan_euler_device_march(void* handle, double cfl, double dt, int32_t local,
                              int64_t max_steps, int32_t batch, double orders, const double* floors,
                              autan_march_result* out, char* err, size_t err_len) {
   AUTAN_CALL(march(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, out));
+}
+
+int autan_euler_device_set_cases(void* handle, int32_t n_cases, const int64_t* cell_offsets,
+                                 char* err, size_t err_len) {
+  AUTAN_CALL(h->set_cases(n_cases, cell_offsets));
+}
+
+int autan_euler_device_set_active(void* handle, const uint8_t* active, char* err, size_t err_len) {
+  AUTAN_CALL({
+    if (active == nullptr) fail("E1101: null active flags");
+    h->set_active(active);
+  });
+}
+
+int autan_euler_device_case_history(void* handle, int64_t count, double* rms, char* err,
+                                    size_t err_len) {
+  AUTAN_CALL({
+    if (rms == nullptr) fail("E1101: null output");
+    h->case_history(count, rms);
+  });
+}
+
+int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                                   int64_t max_steps, int32_t batch, double orders,
+                                   const double* floors, int64_t* iterations, int32_t* converged,
+                                   int64_t* steps, double* gpu_ms, char* err, size_t err_len) {
+  AUTAN_CALL(march_cases(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, iterations,
+                         converged, steps, gpu_ms));
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {

@@ -257,6 +257,40 @@ class EulerDevice:
                     time_step=float(out.time_step), gpu_ms=float(out.gpu_ms),
                     invalid_cell=None if out.invalid_cell < 0 else int(out.invalid_cell))  # fmt: skip
 
+    # -- batched cases
+    def set_cases(self, cell_offsets) -> None:
+        """Case k = owned cells [cell_offsets[k], cell_offsets[k + 1]) of the union mesh."""
+        off = np.ascontiguousarray(cell_offsets, dtype=np.int64)
+        self.n_cases = off.size - 1
+        self._call("autan_euler_device_set_cases", int(self.n_cases), N.ptr(off, C.c_int64))
+
+    def set_active(self, active) -> None:
+        a = np.ascontiguousarray(active, dtype=np.uint8)
+        self._call("autan_euler_device_set_active", N.ptr(a, C.c_uint8))
+
+    def case_history(self, count: int) -> np.ndarray:
+        """Per-case RMS of the last `count` steps of the last step call: count x cases x 5."""
+        out = np.zeros((count, self.n_cases, 5))
+        self._call("autan_euler_device_case_history", int(count), N.ptr(out, C.c_double))
+        return out
+
+    def march_cases(self, cfl: float = 0.8, dt: float = 0.0, local: bool = True, rk: int = 3,
+                    max_steps: int = 1000, batch: int = 50, orders: float = 8.0,
+                    floors=None) -> dict:  # fmt: skip
+        """The batched march (autan_euler_device_march_cases): each case to the convergence rule,
+        stopping at the end of the batch in which it converged."""
+        it = np.zeros(self.n_cases, dtype=np.int64)
+        conv = np.zeros(self.n_cases, dtype=np.int32)
+        steps = C.c_int64()
+        ms = C.c_double()
+        fl = None if floors is None else np.ascontiguousarray(floors, dtype=np.float64)
+        self._call("autan_euler_device_march_cases", float(cfl), float(dt), int(local), int(rk),
+                   int(max_steps), int(batch), float(orders),
+                   None if fl is None else N.ptr(fl, C.c_double), N.ptr(it, C.c_int64),
+                   N.ptr(conv, C.c_int32), C.byref(steps), C.byref(ms))  # fmt: skip
+        return dict(iterations=it, converged=conv.astype(bool), steps=int(steps.value),
+                    gpu_ms=float(ms.value))
+
     def history(self, count: int) -> tuple[np.ndarray, np.ndarray]:
         rms = np.zeros((count, 5))
         dt = np.zeros(count)

@@ -227,6 +227,29 @@ int autan_euler_device_march(void* handle, double cfl, double dt, int32_t local,
 int autan_convergence_iteration(const double* residuals, int64_t n, double orders,
                                 const double* floors, int64_t* iteration, int32_t* plateau_mask,
                                 char* err, size_t err_len);
+/* Batched cases (many steady cases advanced together; no counterpart in the reference, which runs
+ * one case per process): the handle's mesh is the disjoint union of the cases' meshes, case k's
+ * owned cells [cell_offsets[k], cell_offsets[k + 1]) (n_cases + 1 offsets from 0 to
+ * n_owned_cells). Every kernel of a stage runs once over all cases; with local time steps the
+ * cases do not interact. Each step then also records each case's RMS residual (exact sums over its
+ * cells), and a case whose active flag is 0 is skipped: its state no longer changes. */
+int autan_euler_device_set_cases(void* handle, int32_t n_cases, const int64_t* cell_offsets,
+                                 char* err, size_t err_len);
+/* One flag per case, nonzero: the case steps. */
+int autan_euler_device_set_active(void* handle, const uint8_t* active, char* err, size_t err_len);
+/* The per-case RMS of the last `count` steps of the last step call: count x n_cases x 5, oldest
+ * first. */
+int autan_euler_device_case_history(void* handle, int64_t count, double* rms, char* err,
+                                    size_t err_len);
+/* The batched march: steps (`batch` per captured-graph call) until every case has met the
+ * convergence rule of autan_euler_device_march (floors: 5 per case or NULL), each case stopping at
+ * the end of the batch in which it converged, or until max_steps. iterations[k] (n_cases): the
+ * iteration at which case k converged, or the steps taken; converged[k]: 1 if it did; *steps: steps
+ * taken; *gpu_ms: device time. */
+int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t local, int32_t rk,
+                                   int64_t max_steps, int32_t batch, double orders,
+                                   const double* floors, int64_t* iterations, int32_t* converged,
+                                   int64_t* steps, double* gpu_ms, char* err, size_t err_len);
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);
 /* The handle's cudaStream_t. */
