@@ -153,15 +153,35 @@ MESH_KEYS = ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces", "n_owned
              "n_owned_faces")  # fmt: skip
 
 
+UNION_KEYS = ("owner", "neighbour", "face_zone", "face_area_magnitude", "face_normal",
+              "face_centroid", "face_area", "face_moment", "cell_face_offsets", "cell_faces",
+              "cell_centroid", "cell_volume", "stencil_offsets", "stencil")  # fmt: skip
+
+
+def compact(m: M.Mesh, moments: bool = True) -> "SimpleNamespace":
+    """The arrays of a mesh that a union needs, detached from its native handle (closed here)."""
+    from types import SimpleNamespace
+
+    keys = UNION_KEYS if moments else tuple(k for k in UNION_KEYS if k != "face_moment")
+    out = SimpleNamespace(**{k: getattr(m, k) for k in keys},
+                          **{k: getattr(m, k) for k in MESH_KEYS}, all_planar=m.all_planar)  # fmt: skip
+    if not moments:
+        out.face_moment = None
+    m.close()
+    return out
+
+
 def union(meshes, weights) -> tuple[dict, np.ndarray, np.ndarray]:
     """The disjoint union of meshes without ghost cells, in the mesh contract's layout: cells of
     mesh k after those of meshes < k; interior faces of every mesh (in mesh order), then boundary
-    faces of every mesh; each cell's faces still in increasing order. weights: each mesh's LSQ
-    weights (3 x its stencil entries). Returns the mesh arrays (a dict, as EulerDevice and the
-    oracle take them), the concatenated weights and the cell offsets of the meshes."""
+    faces of every mesh; each cell's faces still in increasing order. meshes: Mesh objects or their
+    compact() arrays (face_moment None: all planar, left out); weights: each mesh's LSQ weights
+    (3 x its stencil entries). Returns the mesh arrays (a dict, as EulerDevice and the oracle take
+    them), the concatenated weights and the cell offsets of the meshes."""
     for m in meshes:
         if m.n_cells != m.n_owned_cells:
             raise ValueError("union: meshes with ghost cells are not supported")
+    moments = all(getattr(m, "face_moment", None) is not None for m in meshes)
     nc = np.array([m.n_cells for m in meshes])
     ni = np.array([m.n_interior_faces for m in meshes])
     nb = np.array([m.n_faces - m.n_interior_faces for m in meshes])
@@ -177,8 +197,10 @@ def union(meshes, weights) -> tuple[dict, np.ndarray, np.ndarray]:
     owner = np.empty(NF, dtype=np.int32)
     neighbour = np.empty(NI, dtype=np.int32)
     face_zone = np.empty(NF, dtype=np.int32)
-    vec = {key: np.empty((d, NF)) for key, d in (("face_normal", 3), ("face_centroid", 3),
-                                                  ("face_area", 3), ("face_moment", 9))}  # fmt: skip
+    shapes = [("face_normal", 3), ("face_centroid", 3), ("face_area", 3)]
+    if moments:
+        shapes.append(("face_moment", 9))
+    vec = {key: np.empty((d, NF)) for key, d in shapes}
     area = np.empty(NF)
     for k, m in enumerate(meshes):
         src_i = slice(0, ni[k])
@@ -208,7 +230,7 @@ def union(meshes, weights) -> tuple[dict, np.ndarray, np.ndarray]:
              cell_volume=np.concatenate([m.cell_volume for m in meshes]),
              stencil_offsets=np.concatenate(so), stencil=np.concatenate(st))  # fmt: skip
     d.update(vec)
-    d["face_moment"] = d["face_moment"].reshape(-1)
+    d["face_moment"] = d["face_moment"].reshape(-1) if moments else np.zeros(0)
     w = np.concatenate([np.asarray(x).reshape(3, -1) for x in weights], axis=1)
     d["stencil_lsq_weight"] = w
     d["all_planar"] = all(m.all_planar for m in meshes)
@@ -274,20 +296,21 @@ def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precisi
         else:
             kind[io] = M.BC_FARFIELD
             data[:, io] = w[:, None]
-        meshes.append(m)
         weights.append(m.gradient_weights(kind))
         kinds.append(kind)
         datas.append(data)
         free = conserved(*(np.array(x) for x in w), g)
         u0s.append(np.repeat(free[:, None], m.n_cells, axis=1))
-        params.append(dict(cells=m.n_cells, mach=mach, angle=angle, bump=bump, boxes=(nx, ny, nz)))
+        from autan_b200.euler import residual_scales
+
+        params.append(dict(cells=m.n_cells, mach=mach, angle=angle, bump=bump, boxes=(nx, ny, nz),
+                           phi=residual_scales(m, 1.0, p, mach, g)))  # fmt: skip
+        meshes.append(compact(m, moments=not m.all_planar))
     d, wts, coff = union(meshes, weights)
     ref = conserved(np.array(1.0), np.array(0.5), np.array(0.0), np.array(0.0), np.array(p), g)
     scheme = Scheme(flux=flux, second_order=True, limiter=True, venkat_k=5.0, length=1.0, gamma=g,
                     gas_constant=1.0 / g, mach_ref=0.5, scale=(1.0, 0.5, 0.5, 0.5, p),
                     reference=tuple(float(x) for x in ref), precision=precision,
                     planar=bool(d["all_planar"]))  # fmt: skip
-    for m in meshes:
-        m.close()
     return Batch(d, wts, coff, scheme, np.concatenate(kinds), np.concatenate(datas, axis=1),
                  np.ascontiguousarray(np.concatenate(u0s, axis=1)), params)  # fmt: skip

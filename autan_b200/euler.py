@@ -107,6 +107,9 @@ def mesh_arrays(mesh: Mesh | dict, weights: np.ndarray | None) -> tuple[N.MeshAr
     np_t = {C.c_int32: np.int32, C.c_int64: np.int64, C.c_double: np.float64}
     for k, t in spec.items():
         a = np.ascontiguousarray(get(k), dtype=np_t[t])
+        if a.size == 0 and k == "face_moment":
+            m.face_moment = None  # no moments: every face planar (the ABI's NULL)
+            continue
         if a.size == 0:
             a = np.zeros(1, dtype=np_t[t])
         keep.append(a)

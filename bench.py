@@ -285,6 +285,15 @@ def run_reference(args, rank: int, world: int) -> None:
 
 
 def workload_config(args) -> dict:
+    if args.workload == "batch":
+        lo, hi = (int(v) for v in args.cells.split(","))
+        return {"workload": f"{args.cases} batched steady bump channels (seed {args.seed}), cells "
+                            f"log-uniform in [{lo}, {hi}], Mach U(0.3, 0.75), flow angle U(-4, 4) "
+                            "deg, bump U(0.02, 0.10), farfield inflow/outflow, slip walls, Roe, LSQ "
+                            "face2 + Venkatakrishnan K=5, SSP-RK3 with local steps at CFL 1.5, "
+                            "fp32+acc64; every stage kernel one launch over all cases",
+                "parallelism": f"replicas x{args.gpus}",
+                "l2": "working set of every step larger than the 126 MB L2"}  # fmt: skip
     if args.workload == "channel":
         nx, ny, nz = (int(v) for v in args.channel.split(","))
         return {"workload": f"steady subsonic bump channel, {nx}x{ny}x{nz} boxes as hybrid "
@@ -334,6 +343,28 @@ def run_converge(args, case, dev, tuned) -> None:
     dev.close()
 
 
+def run_converge_batch(args, batch, dev, tuned) -> None:
+    """The batched march to `--converge` decades, each case with its own plateau floors."""
+    from autan_b200.euler import ROUND_OFF_FLOOR
+
+    floors = np.stack([ROUND_OFF_FLOOR * p["phi"] for p in batch.params])
+    res = dev.march_cases(cfl=batch.cfl, local=True, rk=batch.rk, max_steps=args.max_steps,
+                          batch=100, orders=args.converge, floors=floors)  # fmt: skip
+    cells = np.array([p["cells"] for p in batch.params])
+    it = res["iterations"]
+    print(json.dumps({
+        "metric": f"GPU time to a {args.converge:g}-decade residual drop of every case",
+        "value": res["gpu_ms"] / 1e3, "unit": "s", "higher_is_better": False,
+        "cases": len(cells), "cells": int(cells.sum()), "converged": int(res["converged"].sum()),
+        "steps": res["steps"], "iterations_min": int(it.min()), "iterations_median": float(np.median(it)),
+        "iterations_max": int(it.max()),
+        "cell_iterations": int((cells * it).sum()),
+        "cell_iterations_per_s": float((cells * it).sum() / (res["gpu_ms"] / 1e3)),
+        "config": dict(workload_config(args), tuning=tuned, start="freestream"),
+    }), flush=True)  # fmt: skip
+    dev.close()
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     import torch
 
@@ -348,7 +379,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     from autan_b200 import cases
     from autan_b200.euler import EulerDevice
 
-    if args.workload == "hex":
+    batch = None
+    if args.workload == "batch":
+        import types
+
+        lo, hi = (int(v) for v in args.cells.split(","))
+        batch = cases.bump_batch(args.cases, seed=args.seed, cells=(lo, hi))
+        case = types.SimpleNamespace(mesh=types.SimpleNamespace(**batch.mesh), scheme=batch.scheme,
+                                     bc_kind=batch.bc_kind, bc_data=batch.bc_data, u0=batch.u0,
+                                     cfl=batch.cfl, rk=batch.rk, local=True)  # fmt: skip
+    elif args.workload == "hex":
         case = cases.vortex_hex()
     elif args.workload == "channel":
         case = cases.bump_channel(*(int(v) for v in args.channel.split(",")))
@@ -356,7 +396,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         nx, ny, nz = (int(v) for v in args.lattice.split(","))
         case = cases.vortex_tets(nx, ny, nz, precision="fp32+acc64")
     n = case.mesh.n_owned_cells
-    dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
+    if batch is not None:
+        dev = EulerDevice(batch.mesh, batch.scheme, batch.bc_kind, batch.bc_data,
+                          weights=batch.weights, device=local_rank)  # fmt: skip
+        dev.set_cases(batch.cell_offsets)
+    else:
+        dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
     dev.upload(case.u0)
     stream = torch.cuda.ExternalStream(dev.stream)
     if args.tuning:
@@ -366,7 +411,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         # The autotuner picks the launch choices on this case (the state is restored after it).
         tuned, _ = dev.autotune(cfl=case.cfl, rk=case.rk, local=case.local, trial_steps=2)
     if args.converge > 0:
-        run_converge(args, case, dev, tuned)
+        if batch is not None:
+            run_converge_batch(args, batch, dev, tuned)
+        else:
+            run_converge(args, case, dev, tuned)
         return
     # Warm-up (and graph capture).
     dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.warmup, graph=True)
@@ -500,7 +548,10 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["tets", "hex", "channel"], default="tets")
+    ap.add_argument("--workload", choices=["tets", "hex", "channel", "batch"], default="tets")
+    ap.add_argument("--cases", type=int, default=256, help="batch: number of channel cases")
+    ap.add_argument("--cells", default="20000,500000", help="batch: cell range LO,HI (log-uniform)")
+    ap.add_argument("--seed", type=int, default=0, help="batch: seed of the case parameters")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-slab", default="",
                     help="lattice NX,NY,NZ each CPU thread steps for the CPU baseline")
