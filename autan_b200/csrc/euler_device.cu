@@ -1430,7 +1430,9 @@ Sliced slice_rows(const std::vector<long long>& off) {
     }
     s.start[sl] = static_cast<int>(run);
     run += longest * kSlice;
-    if (run >= std::numeric_limits<int>::max() / 4) fail("E1101: stencil too large for int32 offsets");
+    // Slice starts are int32 entries (word offsets, 4 per entry, are formed in 64 bits).
+    if (run >= std::numeric_limits<int>::max() - 2 * kSlice)
+      fail("E1101: stencil too large for int32 offsets");
   }
   s.start.back() = static_cast<int>(run);
   s.total = run;
