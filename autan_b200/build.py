@@ -41,7 +41,7 @@ NVCC_FLAGS = [
 ]
 
 HOST_SOURCES = ["setup.cpp"]
-CUDA_SOURCES = ["euler_device.cu", "norms_static.cu"]
+CUDA_SOURCES = ["euler_device.cu", "norms_static.cu", "mlp.cu"]
 HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp", "convergence.hpp"]
 
 

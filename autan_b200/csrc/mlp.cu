@@ -1,0 +1,814 @@
+// The learned warm start: a small MLP (BF16 weights and activations, FP32 accumulation) trained
+// and evaluated by this file's own tensor-core kernels, and the exact wall distance it takes as an
+// input. C ABI: include/autan_mlp.h.
+//
+// Layout: activations are row-major [rows x padded width] BF16, every layer's width padded to a
+// multiple of 16 (inputs) or 8 (outputs) with zeros; weights W [out x in] BF16 (and their
+// transposes for the backward pass), FP32 master copies with Adam moments. The dense kernel is
+// C[M x N] = A[M x K] B[N x K]^T with warp-level mma.sync m16n8k16 (BF16 in, FP32 accumulate),
+// bias and GELU fused in its epilogue; the weight gradient C[N x K] = dZ^T A sums 128-row chunks
+// into per-chunk partials that a second kernel adds in chunk order, so training is deterministic.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "autan_mlp.h"
+
+namespace autan_b200 {
+namespace mlp {
+
+using bf16 = __nv_bfloat16;
+
+struct Failure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+[[noreturn]] void fail(const std::string& what) { throw Failure(what); }
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fail(std::string("E1300: ") + what + ": " + cudaGetErrorString(e));
+}
+
+constexpr int kMaxWidth = 128;
+constexpr int kRowsPerBlock = 64;  // dense kernel: 4 warps x 16 rows
+constexpr int kChunk = 128;        // weight-gradient rows per partial
+
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+  return static_cast<uint32_t>(__bfloat16_as_ushort(lo)) |
+         (static_cast<uint32_t>(__bfloat16_as_ushort(hi)) << 16);
+}
+
+// D = A B + C for one m16n8k16 tile (PTX mma.sync, row.col, BF16 operands, FP32 accumulators).
+__device__ __forceinline__ void mma16816(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ float gelu(float z) {
+  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  const float pdf = expf(-0.5f * z * z) * 0.39894228040143268f;
+  return cdf + z * pdf;
+}
+
+// C[M x N] = A[M x K] B[N x K]^T + bias: A (lda), B (ldb) BF16 row-major, K a multiple of 16, N a
+// multiple of 8 and at most 128. Epilogue: z = C + bias into Z (FP32, ldz, may be null); then
+// GELU(z) (ACT) or z, into Y (BF16, ldy) or Yf (FP32, ldy). 128 threads: warp w the rows
+// [16 w, 16 w + 16) of the block's 64.
+template <bool ACT>
+__global__ void __launch_bounds__(128) k_dense(const bf16* A, int lda, int M, int K, const bf16* B,
+                                               int ldb, int N, const float* bias, float* Z, int ldz,
+                                               bf16* Y, float* Yf, int ldy) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int sk = K + 8;  // padded row stride (bank spread)
+  bf16* As = reinterpret_cast<bf16*>(smem);
+  bf16* Bs = As + kRowsPerBlock * sk;
+  const int row0 = blockIdx.x * kRowsPerBlock;
+  for (int i = threadIdx.x; i < kRowsPerBlock * K; i += blockDim.x) {
+    const int r = i / K, k = i % K;
+    As[r * sk + k] = row0 + r < M ? A[static_cast<long long>(row0 + r) * lda + k] : __float2bfloat16(0.0f);
+  }
+  for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
+    const int n = i / K, k = i % K;
+    Bs[n * sk + k] = B[static_cast<long long>(n) * ldb + k];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  float acc[16][4];
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[j][q] = 0.0f;
+  const bf16* ar = As + (16 * warp) * sk;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    uint32_t a[4];
+    a[0] = pack2(ar[g * sk + k0 + 2 * t], ar[g * sk + k0 + 2 * t + 1]);
+    a[1] = pack2(ar[(g + 8) * sk + k0 + 2 * t], ar[(g + 8) * sk + k0 + 2 * t + 1]);
+    a[2] = pack2(ar[g * sk + k0 + 2 * t + 8], ar[g * sk + k0 + 2 * t + 9]);
+    a[3] = pack2(ar[(g + 8) * sk + k0 + 2 * t + 8], ar[(g + 8) * sk + k0 + 2 * t + 9]);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      if (8 * j < N) {
+        const bf16* br = Bs + (8 * j + g) * sk + k0;
+        uint32_t b[2];
+        b[0] = pack2(br[2 * t], br[2 * t + 1]);
+        b[1] = pack2(br[2 * t + 8], br[2 * t + 9]);
+        mma16816(acc[j], a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (8 * j >= N) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = row0 + 16 * warp + g + (q >= 2 ? 8 : 0);
+      const int n = 8 * j + 2 * t + (q & 1);
+      if (r >= M) continue;
+      const float z = acc[j][q] + (bias != nullptr ? bias[n] : 0.0f);
+      if (Z != nullptr) Z[static_cast<long long>(r) * ldz + n] = z;
+      const float y = ACT ? gelu(z) : z;
+      if (Y != nullptr) Y[static_cast<long long>(r) * ldy + n] = __float2bfloat16(y);
+      if (Yf != nullptr) Yf[static_cast<long long>(r) * ldy + n] = y;
+    }
+  }
+}
+
+// Partial weight gradients: for the 128-row chunk blockIdx.x, P[chunk][N x K] = dZ_chunk^T A_chunk
+// (dZ BF16 [M x N], A BF16 [M x K]; N, K multiples of 16, at most 128). 256 threads: warp w the
+// gradient rows [16 w, 16 w + 16) (warps beyond N / 16 idle).
+constexpr int kWgradSmem = 2 * kChunk * (kMaxWidth + 8) * 2;
+
+__global__ void __launch_bounds__(256) k_wgrad(const bf16* dZ, int ldz, const bf16* A, int lda,
+                                               int M, int N, int K, float* partial) {
+  extern __shared__ __align__(16) unsigned char wsm[];
+  auto Ds = reinterpret_cast<bf16 (*)[kMaxWidth + 8]>(wsm);
+  auto As = reinterpret_cast<bf16 (*)[kMaxWidth + 8]>(wsm + kChunk * (kMaxWidth + 8) * 2);
+  const int m0 = blockIdx.x * kChunk;
+  for (int i = threadIdx.x; i < kChunk * N; i += blockDim.x) {
+    const int r = i / N, n = i % N;
+    Ds[r][n] = m0 + r < M ? dZ[static_cast<long long>(m0 + r) * ldz + n] : __float2bfloat16(0.0f);
+  }
+  for (int i = threadIdx.x; i < kChunk * K; i += blockDim.x) {
+    const int r = i / K, k = i % K;
+    As[r][k] = m0 + r < M ? A[static_cast<long long>(m0 + r) * lda + k] : __float2bfloat16(0.0f);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  if (16 * warp >= N) return;
+  float acc[16][4];
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[j][q] = 0.0f;
+  const int n0 = 16 * warp;
+  for (int r0 = 0; r0 < kChunk; r0 += 16) {
+    // A operand (m16 x k16): element (i, r) = dZ[r0 + r][n0 + i]
+    uint32_t a[4];
+    a[0] = pack2(Ds[r0 + 2 * t][n0 + g], Ds[r0 + 2 * t + 1][n0 + g]);
+    a[1] = pack2(Ds[r0 + 2 * t][n0 + g + 8], Ds[r0 + 2 * t + 1][n0 + g + 8]);
+    a[2] = pack2(Ds[r0 + 2 * t + 8][n0 + g], Ds[r0 + 2 * t + 9][n0 + g]);
+    a[3] = pack2(Ds[r0 + 2 * t + 8][n0 + g + 8], Ds[r0 + 2 * t + 9][n0 + g + 8]);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      if (8 * j < K) {
+        // B operand (k16 x n8): element (r, c) = A[r0 + r][8 j + c]
+        uint32_t b[2];
+        b[0] = pack2(As[r0 + 2 * t][8 * j + g], As[r0 + 2 * t + 1][8 * j + g]);
+        b[1] = pack2(As[r0 + 2 * t + 8][8 * j + g], As[r0 + 2 * t + 9][8 * j + g]);
+        mma16816(acc[j], a, b);
+      }
+    }
+  }
+  float* out = partial + static_cast<long long>(blockIdx.x) * N * K;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    if (8 * j >= K) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int n = n0 + g + (q >= 2 ? 8 : 0);
+      const int k = 8 * j + 2 * t + (q & 1);
+      out[n * K + k] = acc[j][q];
+    }
+  }
+}
+
+// grad[i] = sum over chunks c (in order) of partial[c][i]; the bias gradient of the layer's
+// columns likewise from the column sums of dZ (FP32) over the rows.
+__global__ void k_sum_partials(const float* partial, int chunks, int size, float* grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= size) return;
+  float s = 0.0f;
+  for (int c = 0; c < chunks; ++c) s += partial[static_cast<long long>(c) * size + i];
+  grad[i] = s;
+}
+__global__ void k_column_sums(const float* dz, int ld, int M, int N, float* out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float s = 0.0f;
+  for (int r = 0; r < M; ++r) s += dz[static_cast<long long>(r) * ld + n];
+  out[n] = s;
+}
+
+// Standardised inputs of rows idx (or 0..n-1) as BF16 [n x ldx] (zero padding).
+__global__ void k_inputs(const float* x, int inputs, const int* idx, int n, const float* mean,
+                         const float* sd, bf16* out, int ldx) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<long long>(n) * ldx) return;
+  const long long r = i / ldx;
+  const int c = static_cast<int>(i % ldx);
+  float v = 0.0f;
+  if (c < inputs) {
+    const long long src = idx != nullptr ? idx[r] : r;
+    v = (x[src * inputs + c] - mean[c]) / sd[c];
+  }
+  out[i] = __float2bfloat16(v);
+}
+
+// Output layer loss and gradient: pred (FP32 [n x ld]) against the standardised targets of rows
+// idx; dpred = 2 (pred - t) / (n outputs) as FP32 and BF16; per-row squared errors into se.
+__global__ void k_loss(const float* pred, int ld, const float* y, int outputs, const int* idx,
+                       int n, const float* mean, const float* sd, float* dz, bf16* dzb, float* se) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const long long src = idx != nullptr ? idx[r] : r;
+  float s = 0.0f;
+  const float scale = 2.0f / (static_cast<float>(n) * outputs);
+  for (int c = 0; c < ld; ++c) {
+    float g = 0.0f;
+    if (c < outputs) {
+      const float t = (y[src * outputs + c] - mean[c]) / sd[c];
+      const float d = pred[static_cast<long long>(r) * ld + c] - t;
+      s += d * d;
+      g = scale * d;
+    }
+    dz[static_cast<long long>(r) * ld + c] = g;
+    dzb[static_cast<long long>(r) * ld + c] = __float2bfloat16(g);
+  }
+  se[r] = s;
+}
+
+// dZ of a hidden layer from the gradient of its activation dA (FP32): dZ = dA GELU'(Z).
+__global__ void k_gelu_back(const float* dA, const float* Z, long long count, float* dz, bf16* dzb) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float g = dA[i] * gelu_grad(Z[i]);
+  dz[i] = g;
+  dzb[i] = __float2bfloat16(g);
+}
+
+__global__ void k_adam(float* p, const float* g, float* m, float* v, long long count, float lr,
+                       float c1, float c2) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float gi = g[i];
+  m[i] = 0.9f * m[i] + 0.1f * gi;
+  v[i] = 0.999f * v[i] + 0.001f * gi * gi;
+  const float mh = m[i] / c1, vh = v[i] / c2;
+  p[i] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// BF16 weights W [np x kp] and W^T [kp x np] (zero padded) from the FP32 master W [out x in].
+__global__ void k_round_weights(const float* w, int out, int in, bf16* wb, int kp, bf16* wt, int np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np * kp) return;
+  const int n = i / kp, k = i % kp;
+  const float x = n < out && k < in ? w[n * in + k] : 0.0f;
+  wb[n * kp + k] = __float2bfloat16(x);
+  wt[k * np + n] = __float2bfloat16(x);
+}
+
+__global__ void k_outputs(const float* pred, int ld, int outputs, int n, const float* mean,
+                          const float* sd, float* y) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<long long>(n) * outputs) return;
+  const long long r = i / outputs;
+  const int c = static_cast<int>(i % outputs);
+  y[i] = pred[r * ld + c] * sd[c] + mean[c];
+}
+
+// ---------------------------------------------------------------- wall distance
+
+struct V3 {
+  double x, y, z;
+};
+__device__ __forceinline__ V3 sub3(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 axpy(V3 a, double s, V3 d) {
+  return {a.x + s * d.x, a.y + s * d.y, a.z + s * d.z};
+}
+
+// Distance from p to triangle (a, b, c): the closest point by the Voronoi regions of the
+// triangle's vertices, edges and face (Ericson, Real-Time Collision Detection, 2005, sec. 5.1.5).
+__device__ double point_triangle(V3 p, V3 a, V3 b, V3 c) {
+  const V3 ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
+  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  V3 q;
+  if (d1 <= 0.0 && d2 <= 0.0) {
+    q = a;
+  } else {
+    const V3 bp = sub3(p, b);
+    const double d3 = dot(ab, bp), d4 = dot(ac, bp);
+    const V3 cp = sub3(p, c);
+    const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    const double vc = d1 * d4 - d3 * d2;
+    const double vb = d5 * d2 - d1 * d6;
+    const double va = d3 * d6 - d5 * d4;
+    if (d3 >= 0.0 && d4 <= d3) {
+      q = b;
+    } else if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+      q = axpy(a, d1 / (d1 - d3), ab);
+    } else if (d6 >= 0.0 && d5 <= d6) {
+      q = c;
+    } else if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+      q = axpy(a, d2 / (d2 - d6), ac);
+    } else if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+      q = axpy(b, (d4 - d3) / ((d4 - d3) + (d5 - d6)), sub3(c, b));
+    } else {
+      const double den = 1.0 / (va + vb + vc);
+      q = axpy(axpy(a, vb * den, ab), vc * den, ac);
+    }
+  }
+  const V3 d = sub3(p, q);
+  return sqrt(dot(d, d));
+}
+
+__global__ void k_wall_distance(const double* tri, const int64_t* tri_off, const double* pts,
+                                const int* case_of, long long n, double* out) {
+  const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = case_of[i];
+  const V3 p{pts[i], pts[n + i], pts[2 * n + i]};
+  double best = __longlong_as_double(0x7ff0000000000000LL);
+  for (int64_t t = tri_off[k]; t < tri_off[k + 1]; ++t) {
+    const double* q = tri + 9 * t;
+    const double d = point_triangle(p, {q[0], q[1], q[2]}, {q[3], q[4], q[5]}, {q[6], q[7], q[8]});
+    if (d < best) best = d;
+  }
+  out[i] = best;
+}
+
+// ---------------------------------------------------------------- host
+
+struct Buf {
+  void* p = nullptr;
+  size_t n = 0;
+  Buf() = default;
+  explicit Buf(size_t bytes) { alloc(bytes); }
+  Buf(const Buf&) = delete;
+  Buf& operator=(const Buf&) = delete;
+  ~Buf() {
+    if (p != nullptr) cudaFree(p);
+  }
+  void alloc(size_t bytes) {
+    if (p != nullptr) cudaFree(p);
+    p = nullptr;
+    n = bytes;
+    if (bytes > 0) check(cudaMalloc(&p, bytes), "cudaMalloc");
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+int pad(int x, int m) { return (x + m - 1) / m * m; }
+int blocks(long long n, int b) { return static_cast<int>(std::max<long long>(1, (n + b - 1) / b)); }
+
+struct Layer {
+  int in, out;   // logical sizes
+  int kp, np;    // padded (K multiple of 16; N multiple of 16, 8 for the output)
+  long long w0;  // offset of W in the parameter vector, then b at w0 + out * in
+};
+
+class Net {
+ public:
+  Net(int inputs, int width, int layers, int outputs, uint64_t seed, int device)
+      : inputs_(inputs), width_(width), outputs_(outputs), device_(device) {
+    if (width < 16 || width > kMaxWidth || width % 16 != 0) fail("E1101: width is 16 to 128, a multiple of 16");
+    if (inputs < 1 || inputs > width || outputs < 1 || outputs > width || layers < 1)
+      fail("E1101: inputs and outputs 1 to width, at least one hidden layer");
+    check(cudaSetDevice(device), "cudaSetDevice");
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    long long off = 0;
+    for (int l = 0; l <= layers; ++l) {
+      Layer L;
+      L.in = l == 0 ? inputs : width;
+      L.out = l == layers ? outputs : width;
+      L.kp = pad(L.in, 16);
+      L.np = l == layers ? pad(L.out, 16) : width;
+      L.w0 = off;
+      off += static_cast<long long>(L.out) * L.in + L.out;
+      layers_.push_back(L);
+    }
+    count_ = off;
+    std::vector<float> p(count_, 0.0f);
+    std::mt19937_64 rng(seed);
+    for (const Layer& L : layers_) {
+      const float a = std::sqrt(6.0f / static_cast<float>(L.in + L.out));
+      std::uniform_real_distribution<float> u(-a, a);
+      for (long long i = 0; i < static_cast<long long>(L.out) * L.in; ++i) p[L.w0 + i] = u(rng);
+    }
+    params_.alloc(count_ * 4);
+    grad_.alloc(count_ * 4);
+    m_.alloc(count_ * 4);
+    v_.alloc(count_ * 4);
+    check(cudaMemsetAsync(m_.p, 0, count_ * 4, stream_), "memset");
+    check(cudaMemsetAsync(v_.p, 0, count_ * 4, stream_), "memset");
+    for (const Layer& L : layers_) {
+      wb_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
+      wt_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
+    }
+    std::vector<float> ones(std::max(inputs, outputs), 1.0f), zeros(std::max(inputs, outputs), 0.0f);
+    in_mean_.alloc(inputs * 4);
+    in_sd_.alloc(inputs * 4);
+    out_mean_.alloc(outputs * 4);
+    out_sd_.alloc(outputs * 4);
+    set_scaling(zeros.data(), ones.data(), zeros.data(), ones.data());
+    set_parameters(p.data());
+  }
+  ~Net() {
+    cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(stream_);
+  }
+
+  long long count() const { return count_; }
+
+  void set_scaling(const float* im, const float* is, const float* om, const float* os) {
+    for (int i = 0; i < inputs_; ++i)
+      if (!(is[i] > 0.0f)) fail("E1101: input standard deviations must be positive");
+    for (int i = 0; i < outputs_; ++i)
+      if (!(os[i] > 0.0f)) fail("E1101: output standard deviations must be positive");
+    copy(in_mean_, im, inputs_ * 4);
+    copy(in_sd_, is, inputs_ * 4);
+    copy(out_mean_, om, outputs_ * 4);
+    copy(out_sd_, os, outputs_ * 4);
+    sync();
+  }
+
+  void set_parameters(const float* p) {
+    copy(params_, p, count_ * 4);
+    round_weights();
+    sync();
+  }
+  void get_parameters(float* p) {
+    check(cudaMemcpyAsync(p, params_.p, count_ * 4, cudaMemcpyDeviceToHost, stream_), "params");
+    sync();
+  }
+
+  void set_data(const float* x, const float* y, long long n) {
+    if (n < 1) fail("E1101: empty training set");
+    n_data_ = n;
+    x_.alloc(static_cast<size_t>(n) * inputs_ * 4);
+    y_.alloc(static_cast<size_t>(n) * outputs_ * 4);
+    copy(x_, x, static_cast<size_t>(n) * inputs_ * 4);
+    copy(y_, y, static_cast<size_t>(n) * outputs_ * 4);
+    sync();
+  }
+
+  // Forward and backward of `rows` rows (x: raw inputs, y: raw targets, idx: rows of them or null);
+  // the gradient into grad_, the loss returned.
+  float forward_backward(const float* x, const float* y, const int* idx, int rows) {
+    ensure_work(rows);
+    const int L = static_cast<int>(layers_.size());
+    launch_inputs(x, idx, rows);
+    forward(rows, true);
+    const Layer& last = layers_[L - 1];
+    k_loss<<<blocks(rows, 128), 128, 0, stream_>>>(zf(L - 1), last.np, y, outputs_, idx, rows,
+                                                   out_mean_.as<float>(), out_sd_.as<float>(),
+                                                   dz_.as<float>(), dzb_.as<bf16>(), se_.as<float>());
+    check(cudaGetLastError(), "loss");
+    for (int l = L - 1; l >= 0; --l) {
+      const Layer& Ly = layers_[l];
+      const bf16* a_prev = act(l - 1);
+      const int lda = l == 0 ? layers_[0].kp : width_;
+      // weight gradient, padded [np x kp], then the logical [out x in] part and the bias
+      const int chunks = blocks(rows, kChunk);
+      const int size = Ly.np * Ly.kp;
+      ensure(partial_, static_cast<size_t>(chunks) * size * 4);
+      ensure(wfull_, static_cast<size_t>(size) * 4);
+      if (!wgrad_attr_) {
+        check(cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem),
+              "smem");
+        wgrad_attr_ = true;
+      }
+      k_wgrad<<<chunks, 256, kWgradSmem, stream_>>>(dzb_.as<bf16>(), Ly.np, a_prev, lda, rows, Ly.np,
+                                                   Ly.kp, partial_.as<float>());
+      check(cudaGetLastError(), "wgrad");
+      k_sum_partials<<<blocks(size, 256), 256, 0, stream_>>>(partial_.as<float>(), chunks, size,
+                                                             wfull_.as<float>());
+      check(cudaGetLastError(), "wgrad sum");
+      check(cudaMemcpy2DAsync(grad_.as<float>() + Ly.w0, Ly.in * 4, wfull_.as<float>(), Ly.kp * 4,
+                              Ly.in * 4, Ly.out, cudaMemcpyDeviceToDevice, stream_),
+            "wgrad copy");
+      k_column_sums<<<blocks(Ly.out, 128), 128, 0, stream_>>>(
+          dz_.as<float>(), Ly.np, rows, Ly.out, grad_.as<float>() + Ly.w0 + static_cast<long long>(Ly.out) * Ly.in);
+      check(cudaGetLastError(), "bias grad");
+      if (l == 0) break;
+      // dA_{l-1} = dZ_l W_l: the dense kernel on W^T [kp x np]
+      const Layer& Lp = layers_[l - 1];
+      launch_dense<false>(dzb_.as<bf16>(), Ly.np, rows, Ly.np, wt_[l]->as<bf16>(), Ly.np, Ly.kp,
+                          nullptr, da_.as<float>(), Ly.kp, nullptr, nullptr, Ly.kp);
+      k_gelu_back<<<blocks(static_cast<long long>(rows) * Lp.np, 256), 256, 0, stream_>>>(
+          da_.as<float>(), zf(l - 1), static_cast<long long>(rows) * Lp.np, dz_.as<float>(),
+          dzb_.as<bf16>());
+      check(cudaGetLastError(), "gelu back");
+    }
+    std::vector<float> se(rows);
+    check(cudaMemcpyAsync(se.data(), se_.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
+    sync();
+    double s = 0.0;
+    for (float v : se) s += v;
+    return static_cast<float>(s / (static_cast<double>(rows) * outputs_));
+  }
+
+  void train(int epochs, int batch, float lr, uint64_t seed, float* loss) {
+    if (n_data_ == 0) fail("E1101: no training data");
+    if (batch < 128 || batch % 128 != 0) fail("E1101: batch must be a positive multiple of 128");
+    std::mt19937_64 rng(seed);
+    std::vector<int> perm(n_data_);
+    for (long long i = 0; i < n_data_; ++i) perm[i] = static_cast<int>(i);
+    ensure(idx_, static_cast<size_t>(n_data_) * 4);
+    for (int e = 0; e < epochs; ++e) {
+      std::shuffle(perm.begin(), perm.end(), rng);
+      copy(idx_, perm.data(), static_cast<size_t>(n_data_) * 4);
+      double sum = 0.0;
+      long long steps = 0;
+      for (long long r0 = 0; r0 + batch <= n_data_; r0 += batch) {
+        sum += forward_backward(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch);
+        ++t_;
+        const float c1 = 1.0f - std::pow(0.9f, static_cast<float>(t_));
+        const float c2 = 1.0f - std::pow(0.999f, static_cast<float>(t_));
+        k_adam<<<blocks(count_, 256), 256, 0, stream_>>>(params_.as<float>(), grad_.as<float>(),
+                                                         m_.as<float>(), v_.as<float>(), count_, lr, c1, c2);
+        check(cudaGetLastError(), "adam");
+        round_weights();
+        ++steps;
+      }
+      if (loss != nullptr) loss[e] = static_cast<float>(steps > 0 ? sum / steps : 0.0);
+    }
+    sync();
+  }
+
+  void predict(const float* x, long long n, float* y, bool device_ptrs) {
+    const long long chunk = 1 << 18;
+    Buf xd, yd;
+    if (!device_ptrs) {
+      xd.alloc(static_cast<size_t>(n) * inputs_ * 4);
+      yd.alloc(static_cast<size_t>(n) * outputs_ * 4);
+      copy(xd, x, static_cast<size_t>(n) * inputs_ * 4);
+    }
+    const float* xs = device_ptrs ? x : xd.as<float>();
+    float* ys = device_ptrs ? y : yd.as<float>();
+    const int L = static_cast<int>(layers_.size());
+    for (long long r0 = 0; r0 < n; r0 += chunk) {
+      const int rows = static_cast<int>(std::min(chunk, n - r0));
+      ensure_work(rows);
+      launch_inputs(xs + r0 * inputs_, nullptr, rows);
+      forward(rows, false);
+      k_outputs<<<blocks(static_cast<long long>(rows) * outputs_, 256), 256, 0, stream_>>>(
+          zf(L - 1), layers_[L - 1].np, outputs_, rows, out_mean_.as<float>(), out_sd_.as<float>(),
+          ys + r0 * outputs_);
+      check(cudaGetLastError(), "outputs");
+    }
+    if (!device_ptrs)
+      check(cudaMemcpyAsync(y, yd.p, static_cast<size_t>(n) * outputs_ * 4, cudaMemcpyDeviceToHost, stream_),
+            "predict");
+    sync();
+  }
+
+  // One forward and backward pass on host rows, no update: the loss and the gradient.
+  float gradient(const float* x, const float* y, int n, float* g) {
+    Buf xd(static_cast<size_t>(n) * inputs_ * 4), yd(static_cast<size_t>(n) * outputs_ * 4);
+    copy(xd, x, static_cast<size_t>(n) * inputs_ * 4);
+    copy(yd, y, static_cast<size_t>(n) * outputs_ * 4);
+    const float l = forward_backward(xd.as<float>(), yd.as<float>(), nullptr, n);
+    grad_to(g);
+    return l;
+  }
+
+  void grad_to(float* g) {
+    check(cudaMemcpyAsync(g, grad_.p, count_ * 4, cudaMemcpyDeviceToHost, stream_), "grad");
+    sync();
+  }
+  void copy_in(Buf& b, const void* host, size_t bytes) { copy(b, host, bytes); }
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+
+ private:
+  template <bool ACT>
+  void launch_dense(const bf16* A, int lda, int M, int K, const bf16* B, int ldb, int N,
+                    const float* bias, float* Z, int ldz, bf16* Y, float* Yf, int ldy) {
+    const size_t smem = static_cast<size_t>(kRowsPerBlock + N) * (K + 8) * 2;
+    if (smem > 48 * 1024)
+      check(cudaFuncSetAttribute(k_dense<ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)), "smem");
+    k_dense<ACT><<<blocks(M, kRowsPerBlock), 128, smem, stream_>>>(A, lda, M, K, B, ldb, N, bias, Z,
+                                                                  ldz, Y, Yf, ldy);
+    check(cudaGetLastError(), "dense");
+  }
+  void forward(int rows, bool keep) {
+    (void)keep;
+    const int L = static_cast<int>(layers_.size());
+    for (int l = 0; l < L; ++l) {
+      const Layer& Ly = layers_[l];
+      const bf16* a = act(l - 1);
+      const int lda = l == 0 ? layers_[0].kp : width_;
+      const float* bias = params_.as<float>() + Ly.w0 + static_cast<long long>(Ly.out) * Ly.in;
+      // biases of padded output columns: the parameter vector holds `out` of them; padded
+      // columns read beyond into the next layer's weights, so the output layer uses its own pad
+      const float* b = Ly.np == Ly.out ? bias : padded_bias(l);
+      if (l < L - 1) {
+        launch_dense<true>(a, lda, rows, Ly.kp, wb_[l]->as<bf16>(), Ly.kp, Ly.np, b, zf(l), Ly.np,
+                           act_b(l), nullptr, Ly.np);
+      } else {
+        launch_dense<false>(a, lda, rows, Ly.kp, wb_[l]->as<bf16>(), Ly.kp, Ly.np, b, zf(l), Ly.np,
+                            nullptr, nullptr, Ly.np);
+      }
+    }
+  }
+  const float* padded_bias(int l) {
+    const Layer& Ly = layers_[l];
+    ensure(pbias_, static_cast<size_t>(kMaxWidth) * 4);
+    check(cudaMemsetAsync(pbias_.p, 0, kMaxWidth * 4, stream_), "bias");
+    check(cudaMemcpyAsync(pbias_.p, params_.as<float>() + Ly.w0 + static_cast<long long>(Ly.out) * Ly.in,
+                          Ly.out * 4, cudaMemcpyDeviceToDevice, stream_), "bias");
+    return pbias_.as<float>();
+  }
+  void launch_inputs(const float* x, const int* idx, int rows) {
+    const int ldx = layers_[0].kp;
+    k_inputs<<<blocks(static_cast<long long>(rows) * ldx, 256), 256, 0, stream_>>>(
+        x, inputs_, idx, rows, in_mean_.as<float>(), in_sd_.as<float>(), x0_.as<bf16>(), ldx);
+    check(cudaGetLastError(), "inputs");
+  }
+  void round_weights() {
+    for (size_t l = 0; l < layers_.size(); ++l) {
+      const Layer& Ly = layers_[l];
+      k_round_weights<<<blocks(static_cast<long long>(Ly.np) * Ly.kp, 256), 256, 0, stream_>>>(
+          params_.as<float>() + Ly.w0, Ly.out, Ly.in, wb_[l]->as<bf16>(), Ly.kp, wt_[l]->as<bf16>(),
+          Ly.np);
+      check(cudaGetLastError(), "round weights");
+    }
+  }
+  const bf16* act(int l) { return l < 0 ? x0_.as<bf16>() : act_b(l); }
+  bf16* act_b(int l) { return acts_.as<bf16>() + static_cast<long long>(l) * work_rows_ * width_; }
+  float* zf(int l) { return zs_.as<float>() + static_cast<long long>(l) * work_rows_ * kMaxWidth; }
+  void ensure_work(int rows) {
+    if (rows <= work_rows_) return;
+    work_rows_ = rows;
+    const long long L = static_cast<long long>(layers_.size());
+    x0_.alloc(static_cast<size_t>(rows) * layers_[0].kp * 2);
+    acts_.alloc(static_cast<size_t>(L) * rows * width_ * 2);
+    zs_.alloc(static_cast<size_t>(L) * rows * kMaxWidth * 4);
+    dz_.alloc(static_cast<size_t>(rows) * kMaxWidth * 4);
+    dzb_.alloc(static_cast<size_t>(rows) * kMaxWidth * 2);
+    da_.alloc(static_cast<size_t>(rows) * kMaxWidth * 4);
+    se_.alloc(static_cast<size_t>(rows) * 4);
+  }
+  void ensure(Buf& b, size_t bytes) {
+    if (b.n < bytes) b.alloc(bytes);
+  }
+  void copy(Buf& b, const void* host, size_t bytes) {
+    check(cudaMemcpyAsync(b.p, host, bytes, cudaMemcpyHostToDevice, stream_), "copy");
+  }
+  void sync() { check(cudaStreamSynchronize(stream_), "sync"); }
+
+  int inputs_, width_, outputs_, device_;
+  cudaStream_t stream_ = nullptr;
+  std::vector<Layer> layers_;
+  long long count_ = 0;
+  long long t_ = 0;
+  long long n_data_ = 0;
+  int work_rows_ = 0;
+  bool wgrad_attr_ = false;
+  Buf params_, grad_, m_, v_, in_mean_, in_sd_, out_mean_, out_sd_, x_, y_, idx_;
+  Buf x0_, acts_, zs_, dz_, dzb_, da_, se_, partial_, wfull_, pbias_;
+  std::vector<std::unique_ptr<Buf>> wb_, wt_;
+};
+
+int fail_to(char* err, size_t len, const std::string& what) {
+  if (err != nullptr && len > 0) snprintf(err, len, "%s", what.c_str());
+  return 1;
+}
+
+template <class F>
+int guarded(char* err, size_t len, F&& body) {
+  try {
+    body();
+    return 0;
+  } catch (const Failure& e) {
+    return fail_to(err, len, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail_to(err, len, "E1103: out of host memory");
+  } catch (const std::exception& e) {
+    return fail_to(err, len, std::string("E1100: ") + e.what());
+  }
+}
+
+Net* as_net(void* h) {
+  if (h == nullptr) fail("E1101: null handle");
+  return static_cast<Net*>(h);
+}
+
+}  // namespace mlp
+}  // namespace autan_b200
+
+using namespace autan_b200::mlp;
+
+extern "C" {
+
+int autan_mlp_create(int32_t inputs, int32_t width, int32_t layers, int32_t outputs, uint64_t seed,
+                     int32_t device, void** handle, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (handle == nullptr) fail("E1101: null handle");
+    *handle = new Net(inputs, width, layers, outputs, seed, device < 0 ? 0 : device);
+  });
+}
+
+void autan_mlp_destroy(void* handle) { delete static_cast<Net*>(handle); }
+
+int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,
+                          const float* out_mean, const float* out_std, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!in_mean || !in_std || !out_mean || !out_std) fail("E1101: null scaling");
+    as_net(handle)->set_scaling(in_mean, in_std, out_mean, out_std);
+  });
+}
+
+int64_t autan_mlp_parameter_count(void* handle) {
+  return handle == nullptr ? 0 : static_cast<Net*>(handle)->count();
+}
+
+int autan_mlp_get_parameters(void* handle, float* params, int64_t count, char* err,
+                             size_t err_len) {
+  return guarded(err, err_len, [&] {
+    Net* n = as_net(handle);
+    if (params == nullptr || count != n->count()) fail("E1101: parameter count mismatch");
+    n->get_parameters(params);
+  });
+}
+
+int autan_mlp_set_parameters(void* handle, const float* params, int64_t count, char* err,
+                             size_t err_len) {
+  return guarded(err, err_len, [&] {
+    Net* n = as_net(handle);
+    if (params == nullptr || count != n->count()) fail("E1101: parameter count mismatch");
+    n->set_parameters(params);
+  });
+}
+
+int autan_mlp_set_data(void* handle, const float* x, const float* y, int64_t n, char* err,
+                       size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (x == nullptr || y == nullptr) fail("E1101: null data");
+    as_net(handle)->set_data(x, y, n);
+  });
+}
+
+int autan_mlp_train(void* handle, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                    float* loss, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] { as_net(handle)->train(epochs, batch, lr, seed, loss); });
+}
+
+int autan_mlp_gradient(void* handle, const float* x, const float* y, int64_t n, float* loss,
+                       float* grad, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    Net* net = as_net(handle);
+    if (x == nullptr || y == nullptr || grad == nullptr || n < 1 || n > (1 << 20))
+      fail("E1101: 1 to 2^20 rows and non-null arrays");
+    const float l = net->gradient(x, y, static_cast<int>(n), grad);
+    if (loss != nullptr) *loss = l;
+  });
+}
+
+int autan_mlp_predict(void* handle, const float* x, int64_t n, float* y, int32_t device_ptrs,
+                      char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (x == nullptr || y == nullptr || n < 0) fail("E1101: null arrays");
+    if (n == 0) return;
+    as_net(handle)->predict(x, n, y, device_ptrs != 0);
+  });
+}
+
+int autan_wall_distance(const double* triangles, const int64_t* tri_offsets, const double* points,
+                        const int64_t* point_offsets, int32_t n_cases, int64_t n_points,
+                        double* distance, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!tri_offsets || !points || !point_offsets || !distance || n_cases < 1 || n_points < 0)
+      fail("E1101: null or empty arguments");
+    if (point_offsets[0] != 0 || point_offsets[n_cases] != n_points)
+      fail("E1101: point offsets must span the points");
+    const int64_t nt = tri_offsets[n_cases];
+    std::vector<int> case_of(std::max<int64_t>(n_points, 1), 0);
+    for (int k = 0; k < n_cases; ++k)
+      for (int64_t i = point_offsets[k]; i < point_offsets[k + 1]; ++i) case_of[i] = k;
+    Buf t(static_cast<size_t>(std::max<int64_t>(nt, 1)) * 9 * 8), to((n_cases + 1) * 8),
+        p(static_cast<size_t>(std::max<int64_t>(n_points, 1)) * 3 * 8),
+        c(case_of.size() * 4), d(static_cast<size_t>(std::max<int64_t>(n_points, 1)) * 8);
+    if (nt > 0) check(cudaMemcpy(t.p, triangles, nt * 9 * 8, cudaMemcpyHostToDevice), "copy");
+    check(cudaMemcpy(to.p, tri_offsets, (n_cases + 1) * 8, cudaMemcpyHostToDevice), "copy");
+    check(cudaMemcpy(p.p, points, n_points * 3 * 8, cudaMemcpyHostToDevice), "copy");
+    check(cudaMemcpy(c.p, case_of.data(), case_of.size() * 4, cudaMemcpyHostToDevice), "copy");
+    k_wall_distance<<<blocks(n_points, 128), 128>>>(t.as<double>(), to.as<int64_t>(), p.as<double>(),
+                                                    c.as<int>(), n_points, d.as<double>());
+    check(cudaGetLastError(), "wall distance");
+    check(cudaMemcpy(distance, d.p, n_points * 8, cudaMemcpyDeviceToHost), "copy");
+  });
+}
+
+}  // extern "C"

@@ -284,3 +284,108 @@ def convergence_iteration(residuals, orders, floors=None):
         if ok:
             return it, mask
     return 0, 0
+
+
+# ------------------------------------------------------------------ MLP restatement (numpy)
+
+
+def bf16(a):
+    """Round FP32 values to BF16 (nearest, ties to even), returned as FP32."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    out = r.astype(np.uint32).view(np.float32)
+    return np.where(np.isnan(a), a, out)
+
+
+def _erf(x):
+    from math import erf
+
+    return np.vectorize(erf)(x)
+
+
+def mlp_layers(inputs, width, layers, outputs):
+    """(in, out, offset of W) per layer in the parameter vector of autan_mlp (W out x in, then b)."""
+    out, off = [], 0
+    for l in range(layers + 1):
+        i = inputs if l == 0 else width
+        o = outputs if l == layers else width
+        out.append((i, o, off))
+        off += o * i + o
+    return out, off
+
+
+def mlp_forward_backward(params, x, y, scaling, inputs=7, width=128, layers=4, outputs=5,
+                         exact=False):  # fmt: skip
+    """The loss and parameter gradient of the autan_mlp kernels, restated in numpy: BF16 rounding of
+    the standardised inputs, the weights, the hidden activations and the backward dZ, FP32 math
+    (FP64 and no rounding with exact=True, for finite-difference checks)."""
+    dt = np.float64 if exact else np.float32
+    rnd = (lambda a: np.asarray(a, dtype=dt)) if exact else bf16
+    im, isd, om, osd = (np.asarray(v, dtype=dt) for v in scaling)
+    spec, count = mlp_layers(inputs, width, layers, outputs)
+    p = np.asarray(params, dtype=dt)
+    W = [rnd(p[o : o + n_out * n_in].reshape(n_out, n_in)) for n_in, n_out, o in spec]
+    b = [p[o + n_out * n_in : o + n_out * n_in + n_out] for n_in, n_out, o in spec]
+    a = rnd((np.asarray(x, dtype=dt) - im) / isd)
+    acts, zs = [a], []
+    for l in range(layers + 1):
+        z = (acts[-1].astype(dt) @ W[l].T.astype(dt)).astype(dt) + b[l]
+        zs.append(z)
+        if l < layers:
+            g = (0.5 * z * (1.0 + _erf(z / np.sqrt(2.0)))).astype(dt)
+            acts.append(rnd(g))
+    t = (np.asarray(y, dtype=dt) - om) / osd
+    pred = zs[-1]
+    n = pred.shape[0]
+    loss = float(np.sum((pred - t) ** 2) / (n * outputs))
+    dz = (2.0 / (n * outputs)) * (pred - t)
+    grad = np.zeros(count, dtype=dt)
+    for l in range(layers, -1, -1):
+        n_in, n_out, o = spec[l]
+        dzb = rnd(dz)
+        grad[o : o + n_out * n_in] = (dzb.T @ acts[l]).reshape(-1)
+        grad[o + n_out * n_in : o + n_out * n_in + n_out] = dz.sum(axis=0)
+        if l == 0:
+            break
+        da = dzb @ W[l]
+        z = zs[l - 1]
+        cdf = 0.5 * (1.0 + _erf(z / np.sqrt(2.0)))
+        pdf = np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+        dz = (da * (cdf + z * pdf)).astype(dt)
+    return loss, grad
+
+
+def point_triangle(p, a, b, c):
+    """Distance from p to triangle (a, b, c) by the Voronoi regions of its features (Ericson,
+    Real-Time Collision Detection, 2005, sec. 5.1.5), in the kernel's operation order."""
+    def dot(u, v):  # left to right, no fused multiply-add (the kernel's order)
+        return float(u[0]) * float(v[0]) + float(u[1]) * float(v[1]) + float(u[2]) * float(v[2])
+
+    ab, ac, ap = b - a, c - a, p - a
+    d1, d2 = dot(ab, ap), dot(ac, ap)
+    if d1 <= 0.0 and d2 <= 0.0:
+        q = a
+    else:
+        bp = p - b
+        d3, d4 = dot(ab, bp), dot(ac, bp)
+        cp = p - c
+        d5, d6 = dot(ab, cp), dot(ac, cp)
+        vc = d1 * d4 - d3 * d2
+        vb = d5 * d2 - d1 * d6
+        va = d3 * d6 - d5 * d4
+        if d3 >= 0.0 and d4 <= d3:
+            q = b
+        elif vc <= 0.0 and d1 >= 0.0 and d3 <= 0.0:
+            q = a + (d1 / (d1 - d3)) * ab
+        elif d6 >= 0.0 and d5 <= d6:
+            q = c
+        elif vb <= 0.0 and d2 >= 0.0 and d6 <= 0.0:
+            q = a + (d2 / (d2 - d6)) * ac
+        elif va <= 0.0 and (d4 - d3) >= 0.0 and (d5 - d6) >= 0.0:
+            q = b + ((d4 - d3) / ((d4 - d3) + (d5 - d6))) * (c - b)
+        else:
+            den = 1.0 / (va + vb + vc)
+            q = (a + (vb * den) * ab) + (vc * den) * ac
+    d = p - q
+    return float(np.sqrt(dot(d, d)))

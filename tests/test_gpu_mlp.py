@@ -1,0 +1,81 @@
+"""The warm-start MLP's own BF16 tensor-core kernels against the numpy restatement
+(tests/oracle.py mlp_forward_backward): loss and parameter gradient of one forward and backward
+pass, predictions, a training run that fits a smooth field, and the exact wall distance."""
+
+import numpy as np
+import pytest
+
+import oracle as O
+from autan_b200.warmstart import MLP, wall_distance
+
+pytestmark = pytest.mark.gpu
+
+
+def data(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 7)).astype(np.float32)
+    y = np.stack([np.sin(x[:, 0]) * x[:, 1], np.cos(x[:, 2]), x[:, 3] * x[:, 4], np.tanh(x[:, 5]),
+                  0.1 * x[:, 6] ** 2], axis=1).astype(np.float32)  # fmt: skip
+    return x, y
+
+
+def scaling(x, y):
+    return (x.mean(0), x.std(0), y.mean(0), y.std(0))
+
+
+def test_gradient_against_the_restatement():
+    """BF16 operands, FP32 sums in another order: a BF16 rounding of an activation or a dZ may
+    flip; the bounds (1e-4 on the loss, 2e-2 on the gradient's norm) leave room for that."""
+    x, y = data(1000)
+    net = MLP(seed=3)
+    sc = scaling(x, y)
+    net.set_scaling(*sc)
+    p = net.parameters()
+    loss, g = net.gradient(x, y)
+    loss0, g0 = O.mlp_forward_backward(p, x, y, tuple(np.float32(v) for v in sc))
+    assert abs(loss - loss0) <= 1e-4 * loss0
+    assert np.linalg.norm(g - g0) <= 2e-2 * np.linalg.norm(g0)
+    # the output layer's bias gradient is an FP32 column sum of the same dZ: close
+    assert np.allclose(g[-5:], g0[-5:], rtol=1e-3, atol=1e-6)
+
+
+def test_training_fits_a_smooth_field():
+    x, y = data(65536, seed=1)
+    net = MLP(seed=4)
+    net.set_scaling(*scaling(x, y))
+    net.set_data(x, y)
+    loss = net.train(epochs=20, batch=4096, lr=2e-3, seed=5)
+    assert loss[-1] < 0.05 * loss[0], loss
+    xt, yt = data(4096, seed=2)
+    pred = net.predict(xt)
+    assert np.sqrt(np.mean((pred - yt) ** 2)) < 0.3 * np.sqrt(np.mean((yt - yt.mean(0)) ** 2))
+
+
+def test_prediction_matches_the_restatement():
+    x, y = data(3000, seed=6)
+    net = MLP(seed=7)
+    sc = scaling(x, y)
+    net.set_scaling(*sc)
+    p = net.parameters()
+    pred = net.predict(x)
+    # the restatement's standardised prediction (its loss path), de-standardised
+    spec, _ = O.mlp_layers(7, 128, 4, 5)
+    W = [O.bf16(p[o : o + a * b].reshape(b, a)) for a, b, o in spec]
+    bias = [p[o + a * b : o + a * b + b] for a, b, o in spec]
+    act = O.bf16((x - sc[0]) / sc[1])
+    for l in range(5):
+        z = act @ W[l].T + bias[l]
+        act = O.bf16(0.5 * z * (1.0 + O._erf(z / np.sqrt(2.0)))) if l < 4 else z
+    want = act * sc[3] + sc[2]
+    assert np.abs(pred - want).max() <= 2e-2 * np.abs(want).max()
+
+
+def test_wall_distance_bit_for_bit():
+    rng = np.random.default_rng(8)
+    tris = [rng.normal(size=(17, 9)), rng.normal(size=(5, 9))]
+    pts = [rng.normal(size=(3, 300)) * 2, rng.normal(size=(3, 100))]
+    got = wall_distance(tris, pts)
+    for k in range(2):
+        want = [min(O.point_triangle(pts[k][:, i], t[0:3], t[3:6], t[6:9]) for t in tris[k])
+                for i in range(pts[k].shape[1])]  # fmt: skip
+        assert np.array_equal(got[k], np.array(want))
