@@ -234,6 +234,7 @@ def union(meshes, weights) -> tuple[dict, np.ndarray, np.ndarray]:
     w = np.concatenate([np.asarray(x).reshape(3, -1) for x in weights], axis=1)
     d["stencil_lsq_weight"] = w
     d["all_planar"] = all(m.all_planar for m in meshes)
+    d["boundary_offsets"] = boff.astype(np.int64)  # each mesh's first boundary face, from NI
     return d, w, coff
 
 
@@ -258,13 +259,14 @@ class Batch:
 
 
 def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precision="fp32+acc64",
-               inlet="farfield") -> Batch:  # fmt: skip
+               inlet="farfield", walls=False) -> Batch:  # fmt: skip
     """Batched steady bump channels: per case (numpy default_rng(seed)) a cell count log-uniform
     in `cells`, Mach ~ U(0.3, 0.75), flow angle ~ U(-4, 4) degrees, bump height ~ U(0.02, 0.10).
     Each case's channel has about the requested cells (boxes in the ratio 3 : 1 : 1 / 2 of the
     channel's extent, hybrid rows as bump_channel). Inflow and outflow faces take the farfield
     state of the case's freestream (rho = 1, p = 1 / gamma, speed Mach, at the flow angle in the
-    x-y plane); bump, top and z sides slip. A common scheme (second order, Venkatakrishnan K = 5)
+    x-y plane); bump, top and z sides slip. walls: keep each case's bump-wall triangles
+    (params[k]["wall"], t x 9, as WallSurface builds them) for the wall distance. A common scheme (second order, Venkatakrishnan K = 5)
     and reference state (Mach 0.5 along x) serve every case; local steps make the cases
     independent. inlet="state": the inflow faces take the freestream as a given state and the
     outflow faces its static pressure (no exp/log on the path, for bit-exact tests)."""
@@ -305,6 +307,10 @@ def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precisi
 
         params.append(dict(cells=m.n_cells, mach=mach, angle=angle, bump=bump, boxes=(nx, ny, nz),
                            phi=residual_scales(m, 1.0, p, mach, g)))  # fmt: skip
+        if walls:
+            from autan_b200.warmstart import wall_triangles
+
+            params[-1]["wall"] = wall_triangles(m, M.ZONE_BUMP)
         meshes.append(compact(m, moments=not m.all_planar))
     d, wts, coff = union(meshes, weights)
     ref = conserved(np.array(1.0), np.array(0.5), np.array(0.0), np.array(0.0), np.array(p), g)

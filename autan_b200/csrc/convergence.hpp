@@ -27,26 +27,22 @@ class Convergence {
   static constexpr double kRatio = 0.9;        // plateau_ratio
   static constexpr double kBand = 10.0;        // round_off_band
 
-  // floors: round_off_floor * Phi_k per equation, or nullptr for no plateau rule.
-  Convergence(double orders, const double* floors) : drop_(std::pow(10.0, -orders)) {
+  // floors: round_off_floor * Phi_k per equation, or nullptr for no plateau rule. reference: the
+  // residuals the drops are taken from (a continued run's `start.residual_reference`,
+  // run.cpp:2351-2356), or nullptr for the first iteration's.
+  Convergence(double orders, const double* floors, const double* reference = nullptr)
+      : drop_(std::pow(10.0, -orders)) {
     if (floors != nullptr) {
       use_floor_ = true;
       for (int e = 0; e < kEquations; ++e) floor_[e] = floors[e];
     }
+    if (reference != nullptr) set_first(reference);
   }
 
   // This iteration's residuals; true once converged. plateau_mask(): the equations that
   // converged on a plateau rather than by their drop.
   bool add(const double* r) {
-    if (!have_first_) {
-      have_first_ = true;
-      for (int e = 0; e < kEquations; ++e) first_[e] = r[e];
-      zero_floor_ = 1e-12 * *std::max_element(first_.begin(), first_.end());
-      for (int e = 0; e < kEquations; ++e) {
-        zero_[e] = first_[e] < zero_floor_;
-        exempt_[e] = zero_[e];
-      }
-    }
+    if (!have_first_) set_first(r);
     for (int e = 0; e < kEquations; ++e)
       if (exempt_[e] && r[e] > zero_floor_) exempt_[e] = false;
     bool converged = true;
@@ -65,6 +61,16 @@ class Convergence {
   }
 
   int plateau_mask() const { return mask_; }
+
+  void set_first(const double* r) {
+    have_first_ = true;
+    for (int e = 0; e < kEquations; ++e) first_[e] = r[e];
+    zero_floor_ = 1e-12 * *std::max_element(first_.begin(), first_.end());
+    for (int e = 0; e < kEquations; ++e) {
+      zero_[e] = first_[e] < zero_floor_;
+      exempt_[e] = zero_[e];
+    }
+  }
   const std::array<double, kEquations>& first() const { return first_; }
 
  private:

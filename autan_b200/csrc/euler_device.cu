@@ -1761,8 +1761,10 @@ class Impl final : public Stepper {
     d_.n_slices = slices();
     d_.face = face_.as<C>();
     d_.bface = bface_.as<C>();
-    d_.f_m = f_m_.as<C>();
-    d_.b_m = b_m_.as<C>();
+    // No moments on a planar mesh: the pointers stay null (their buffers hold one placeholder
+    // element), so that a kernel guarded by a null test never reads past them.
+    d_.f_m = planar_ ? nullptr : f_m_.as<C>();
+    d_.b_m = planar_ ? nullptr : b_m_.as<C>();
     d_.ctl = ctl_.as<Control>();
     d_.case_of = nullptr;
     d_.active = nullptr;
@@ -2628,8 +2630,9 @@ void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_
 // The batched march: one convergence rule per case, fed that case's row of each step's per-case
 // RMS; a case that meets its rule stops stepping (its cells are skipped from the next batch on).
 void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long long max_steps,
-                 int batch, double orders, const double* floors, int64_t* iterations,
-                 int32_t* converged, int64_t* steps_taken, double* gpu_ms) {
+                 int batch, double orders, const double* floors, const double* reference,
+                 int64_t* iterations, int32_t* converged, double* first, int64_t* steps_taken,
+                 double* gpu_ms) {
   const int nk = h->n_cases();
   if (nk == 0) fail("E1101: no cases set");
   if (max_steps < 1 || batch < 1) fail("E1101: max_steps and batch must be positive");
@@ -2637,7 +2640,9 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
   if (iterations == nullptr || converged == nullptr) fail("E1101: null outputs");
   std::vector<Convergence> conv;
   conv.reserve(nk);
-  for (int k = 0; k < nk; ++k) conv.emplace_back(orders, floors != nullptr ? floors + 5 * k : nullptr);
+  for (int k = 0; k < nk; ++k)
+    conv.emplace_back(orders, floors != nullptr ? floors + 5 * k : nullptr,
+                      reference != nullptr ? reference + 5 * k : nullptr);
   std::vector<uint8_t> active(nk, 1);
   for (int k = 0; k < nk; ++k) {
     iterations[k] = 0;
@@ -2683,6 +2688,12 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
   cudaEventDestroy(t1);
   for (int k = 0; k < nk; ++k)
     if (!converged[k]) iterations[k] = taken;
+  if (first != nullptr)
+    for (int k = 0; k < nk; ++k)
+      for (int e = 0; e < 5; ++e) first[5 * k + e] = conv[k].first()[e];
+  // every case steps again (evaluations after the march see every case)
+  std::fill(active.begin(), active.end(), static_cast<uint8_t>(1));
+  h->set_active(active.data());
   if (steps_taken != nullptr) *steps_taken = taken;
   if (gpu_ms != nullptr) *gpu_ms = ms;
 }
@@ -2924,10 +2935,11 @@ int autan_euler_device_case_history(void* handle, int64_t count, double* rms, ch
 
 int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                    int64_t max_steps, int32_t batch, double orders,
-                                   const double* floors, int64_t* iterations, int32_t* converged,
+                                   const double* floors, const double* reference,
+                                   int64_t* iterations, int32_t* converged, double* first,
                                    int64_t* steps, double* gpu_ms, char* err, size_t err_len) {
-  AUTAN_CALL(march_cases(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, iterations,
-                         converged, steps, gpu_ms));
+  AUTAN_CALL(march_cases(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, reference,
+                         iterations, converged, first, steps, gpu_ms));
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {

@@ -522,6 +522,9 @@ class Net {
     if (batch < 128 || batch % 128 != 0) fail("E1101: batch must be a positive multiple of 128");
     std::mt19937_64 rng(seed);
     std::vector<int> perm(n_data_);
+    const long long per_epoch = n_data_ / batch;
+    const long long total = std::max<long long>(1, per_epoch * epochs);
+    long long done = 0;
     for (long long i = 0; i < n_data_; ++i) perm[i] = static_cast<int>(i);
     ensure(idx_, static_cast<size_t>(n_data_) * 4);
     for (int e = 0; e < epochs; ++e) {
@@ -532,10 +535,14 @@ class Net {
       for (long long r0 = 0; r0 + batch <= n_data_; r0 += batch) {
         sum += forward_backward(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch);
         ++t_;
+        // cosine decay of the learning rate over the call's steps
+        const float rate = lr * 0.5f * (1.0f + std::cos(3.14159265358979f * static_cast<float>(done) / total));
+        ++done;
         const float c1 = 1.0f - std::pow(0.9f, static_cast<float>(t_));
         const float c2 = 1.0f - std::pow(0.999f, static_cast<float>(t_));
         k_adam<<<blocks(count_, 256), 256, 0, stream_>>>(params_.as<float>(), grad_.as<float>(),
-                                                         m_.as<float>(), v_.as<float>(), count_, lr, c1, c2);
+                                                         m_.as<float>(), v_.as<float>(), count_, rate, c1,
+                                                         c2);
         check(cudaGetLastError(), "adam");
         round_weights();
         ++steps;

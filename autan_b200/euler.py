@@ -279,20 +279,25 @@ class EulerDevice:
 
     def march_cases(self, cfl: float = 0.8, dt: float = 0.0, local: bool = True, rk: int = 3,
                     max_steps: int = 1000, batch: int = 50, orders: float = 8.0,
-                    floors=None) -> dict:  # fmt: skip
-        """The batched march (autan_euler_device_march_cases): each case to the convergence rule,
-        stopping at the end of the batch in which it converged."""
+                    floors=None, reference=None) -> dict:  # fmt: skip
+        """The batched march (autan_euler_device_march_cases): each case to the convergence rule
+        (drops from `reference`, n_cases x 5, else from its first iteration), stopping at the end
+        of the batch in which it converged."""
         it = np.zeros(self.n_cases, dtype=np.int64)
         conv = np.zeros(self.n_cases, dtype=np.int32)
+        first = np.zeros((self.n_cases, 5))
         steps = C.c_int64()
         ms = C.c_double()
         fl = None if floors is None else np.ascontiguousarray(floors, dtype=np.float64)
+        rf = None if reference is None else np.ascontiguousarray(reference, dtype=np.float64)
         self._call("autan_euler_device_march_cases", float(cfl), float(dt), int(local), int(rk),
                    int(max_steps), int(batch), float(orders),
-                   None if fl is None else N.ptr(fl, C.c_double), N.ptr(it, C.c_int64),
-                   N.ptr(conv, C.c_int32), C.byref(steps), C.byref(ms))  # fmt: skip
-        return dict(iterations=it, converged=conv.astype(bool), steps=int(steps.value),
-                    gpu_ms=float(ms.value))
+                   None if fl is None else N.ptr(fl, C.c_double),
+                   None if rf is None else N.ptr(rf, C.c_double), N.ptr(it, C.c_int64),
+                   N.ptr(conv, C.c_int32), N.ptr(first, C.c_double), C.byref(steps),
+                   C.byref(ms))  # fmt: skip
+        return dict(iterations=it, converged=conv.astype(bool), first=first,
+                    steps=int(steps.value), gpu_ms=float(ms.value))
 
     def history(self, count: int) -> tuple[np.ndarray, np.ndarray]:
         rms = np.zeros((count, 5))

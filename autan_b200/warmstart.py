@@ -156,3 +156,124 @@ def wall_distance(triangles: list, points: list) -> list:
                                     N.ptr(pts, C.c_double), N.ptr(poff, C.c_int64), len(points),
                                     pts.shape[1], N.ptr(d, C.c_double), err, len(err)), err)  # fmt: skip
     return [d[poff[k] : poff[k + 1]] for k in range(len(points))]
+
+
+# ------------------------------------------------------------------ the experiment
+
+
+def freestream_states(batch) -> np.ndarray:
+    """Each cell's case freestream, conserved (5 x n_cells)."""
+    from autan_b200.cases import GAMMA, conserved
+
+    cols = []
+    for p in batch.params:
+        t = np.radians(p["angle"])
+        w = [1.0, p["mach"] * np.cos(t), p["mach"] * np.sin(t), 0.0, 1.0 / GAMMA]
+        free = conserved(*(np.array(v) for v in w), GAMMA)
+        cols.append(np.repeat(free[:, None], p["cells"], axis=1))
+    return np.concatenate(cols, axis=1)
+
+
+def features(batch) -> np.ndarray:
+    """The MLP inputs of every cell (n_cells x 7): centroid x, y, z, distance to the case's bump
+    wall (exact, on the GPU), the case's Mach number, flow angle (degrees) and bump height."""
+    off = batch.cell_offsets
+    xc = batch.mesh["cell_centroid"]
+    pts = [xc[:, off[k] : off[k + 1]] for k in range(len(batch.params))]
+    dist = wall_distance([p["wall"] for p in batch.params], pts)
+    cols = []
+    for k, p in enumerate(batch.params):
+        n = p["cells"]
+        cols.append(np.column_stack([pts[k].T, dist[k], np.full(n, p["mach"]), np.full(n, p["angle"]),
+                                     np.full(n, p["bump"])]))  # fmt: skip
+    return np.concatenate(cols).astype(np.float32)
+
+
+def floors(batch) -> np.ndarray:
+    from autan_b200.euler import ROUND_OFF_FLOOR
+
+    return np.stack([ROUND_OFF_FLOOR * p["phi"] for p in batch.params])
+
+
+def bump_forces(batch, force) -> np.ndarray:
+    """Per case, the exact sum over its bump-wall faces of the boundary pressure force (3 values),
+    from autan_euler_device_boundary_pressure's per-face forces (3 x n_boundary)."""
+    import math
+
+    ni = batch.mesh["n_interior_faces"]
+    zone = batch.mesh["face_zone"][ni:]
+    boff = batch.mesh["boundary_offsets"]
+    out = np.zeros((len(batch.params), 3))
+    from autan_b200 import mesh as M
+
+    for k in range(len(batch.params)):
+        sel = np.arange(boff[k], boff[k + 1])
+        sel = sel[zone[sel] == M.ZONE_BUMP]
+        out[k] = [math.fsum(force[a, sel]) for a in range(3)]
+    return out
+
+
+def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, reference=None):
+    """The batched march of `batch` from u0 (5 x n_cells), drops taken from `reference` (cases x 5)
+    or each case's first iteration: per-case iterations, GPU time, the converged states and the
+    bump forces."""
+    from autan_b200.euler import EulerDevice
+
+    with EulerDevice(batch.mesh, batch.scheme, batch.bc_kind, batch.bc_data, weights=batch.weights,
+                     device=device) as dev:  # fmt: skip
+        dev.set_cases(batch.cell_offsets)
+        dev.upload(u0)
+        res = dev.march_cases(cfl=batch.cfl, local=True, rk=batch.rk, max_steps=max_steps,
+                              batch=batch_steps, orders=orders, floors=floors(batch),
+                              reference=reference)  # fmt: skip
+        u = dev.download()
+        _, force = dev.boundary_pressure()
+    res["u"] = u
+    res["force"] = bump_forces(batch, force)
+    return res
+
+
+def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30, batch_rows=8192,
+               lr=1e-3, orders=8.0, max_steps=200000, flux="ausm", log=print) -> dict:  # fmt: skip
+    """The learned warm start end to end: train_cases converged cases (seed 1) as training data,
+    the MLP trained on them, then test_cases held-out cases (seed 2) marched from the network's
+    prediction and from the freestream. Returns the timings, iterations and force differences."""
+    import time
+
+    from autan_b200 import cases
+
+    t0 = time.perf_counter()
+    train = cases.bump_batch(train_cases, seed=1, cells=cells, flux=flux, walls=True)
+    log(f"training set: {train_cases} cases, {train.n_cells} cells, set-up {time.perf_counter() - t0:.0f} s")
+    sol = march(train, train.u0, orders=orders, max_steps=max_steps)
+    log(f"training solutions: {int(sol['converged'].sum())} converged, {sol['steps']} steps, "
+        f"{sol['gpu_ms'] / 1e3:.1f} s GPU")  # fmt: skip
+    x = features(train)
+    y = (sol["u"] - freestream_states(train)).T.astype(np.float32)
+    net = MLP(seed=11)
+    net.set_scaling(x.mean(0), np.maximum(x.std(0), 1e-6), y.mean(0), np.maximum(y.std(0), 1e-9))
+    net.set_data(x, y)
+    t1 = time.perf_counter()
+    loss = net.train(epochs=epochs, batch=batch_rows, lr=lr, seed=12)
+    log(f"training: {epochs} epochs, loss {loss[0]:.3e} -> {loss[-1]:.3e}, {time.perf_counter() - t1:.0f} s")
+    test = cases.bump_batch(test_cases, seed=2, cells=cells, flux=flux, walls=True)
+    free = freestream_states(test)
+    cold = march(test, free, orders=orders, max_steps=max_steps)
+    xt = features(test)
+    warm_u0 = free + net.predict(xt).T.astype(np.float64)
+    # the warm start's drops are measured from the freestream start's first residuals, as a run
+    # continued from another state keeps its reference (runtime/src/run.cpp:2351-2356)
+    warm = march(test, warm_u0, orders=orders, max_steps=max_steps, reference=cold["first"])
+    fc, fw = cold["force"], warm["force"]
+    rel = np.abs(fw - fc).max(axis=1) / np.maximum(np.abs(fc).max(axis=1), 1e-300)
+    return dict(train_cases=train_cases, train_cells=train.n_cells, test_cases=test_cases,
+                test_cells=test.n_cells, epochs=epochs, loss_first=float(loss[0]),
+                loss_last=float(loss[-1]),
+                cold_converged=int(cold["converged"].sum()), warm_converged=int(warm["converged"].sum()),
+                cold_gpu_s=cold["gpu_ms"] / 1e3, warm_gpu_s=warm["gpu_ms"] / 1e3,
+                gpu_time_ratio=cold["gpu_ms"] / warm["gpu_ms"],
+                cold_iterations_median=float(np.median(cold["iterations"])),
+                warm_iterations_median=float(np.median(warm["iterations"])),
+                iterations_ratio_median=float(np.median(cold["iterations"] / np.maximum(warm["iterations"], 1))),
+                force_rel_diff_max=float(rel.max()), force_rel_diff_median=float(np.median(rel)),
+                training_solution_gpu_s=sol["gpu_ms"] / 1e3)  # fmt: skip

@@ -343,6 +343,24 @@ def run_converge(args, case, dev, tuned) -> None:
     dev.close()
 
 
+def run_warmstart(args) -> None:
+    """The learned warm start end to end (autan_b200.warmstart.experiment): converged training
+    cases from the batched solver, the MLP trained on the GPU, held-out cases marched from its
+    prediction and from the freestream; one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    from autan_b200 import warmstart
+
+    tr, te, lo, hi, ep = (int(v) for v in args.warmstart.split(","))
+    res = warmstart.experiment(train_cases=tr, test_cases=te, cells=(lo, hi), epochs=ep,
+                               max_steps=args.max_steps, orders=args.converge or 8.0,
+                               log=lambda m: print(m, file=sys.stderr, flush=True))  # fmt: skip
+    print(json.dumps({"metric": "GPU time to convergence, freestream start / warm start",
+                      "value": res["gpu_time_ratio"], "unit": "x", "higher_is_better": True,
+                      **res}), flush=True)  # fmt: skip
+
+
 def run_converge_batch(args, batch, dev, tuned) -> None:
     """The batched march to `--converge` decades, each case with its own plateau floors."""
     from autan_b200.euler import ROUND_OFF_FLOOR
@@ -566,11 +584,17 @@ def main() -> None:
                          "this many decades of residual drop (round-off plateau rule in "
                          "fp32+acc64) and print iterations and GPU time")
     ap.add_argument("--max-steps", type=int, default=100000, help="step cap of --converge")
+    ap.add_argument("--warmstart", default="",
+                    help="run the learned warm start instead: TRAIN,TEST,LO,HI,EPOCHS (training "
+                         "cases, held-out cases, cell range, epochs), e.g. 2048,64,2000,10000,30")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if args.warmstart:
+        run_warmstart(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

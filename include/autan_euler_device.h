@@ -242,13 +242,16 @@ int autan_euler_device_set_active(void* handle, const uint8_t* active, char* err
 int autan_euler_device_case_history(void* handle, int64_t count, double* rms, char* err,
                                     size_t err_len);
 /* The batched march: steps (`batch` per captured-graph call) until every case has met the
- * convergence rule of autan_euler_device_march (floors: 5 per case or NULL), each case stopping at
- * the end of the batch in which it converged, or until max_steps. iterations[k] (n_cases): the
- * iteration at which case k converged, or the steps taken; converged[k]: 1 if it did; *steps: steps
- * taken; *gpu_ms: device time. */
+ * convergence rule of autan_euler_device_march (floors: 5 per case or NULL; reference: 5 per case,
+ * the residuals each case's drop is measured from, as a continued run's start.residual_reference,
+ * or NULL for each case's first iteration), each case stopping at the end of the batch in which it
+ * converged, or until max_steps. iterations[k] (n_cases): the iteration at which case k converged,
+ * or the steps taken; converged[k]: 1 if it did; first (5 per case, may be NULL): the reference
+ * used; *steps: steps taken; *gpu_ms: device time. Every case steps again afterwards. */
 int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                    int64_t max_steps, int32_t batch, double orders,
-                                   const double* floors, int64_t* iterations, int32_t* converged,
+                                   const double* floors, const double* reference,
+                                   int64_t* iterations, int32_t* converged, double* first,
                                    int64_t* steps, double* gpu_ms, char* err, size_t err_len);
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);

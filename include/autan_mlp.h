@@ -40,8 +40,8 @@ int autan_mlp_set_parameters(void* handle, const float* params, int64_t count, c
 int autan_mlp_set_data(void* handle, const float* x, const float* y, int64_t n, char* err,
                        size_t err_len);
 /* Training: `epochs` passes over the data in shuffled minibatches of `batch` rows (a multiple of
- * 128), Adam (beta1 0.9, beta2 0.999, eps 1e-8) at learning rate lr on the mean squared error of the
- * standardised outputs. loss (epochs values, may be NULL): each epoch's mean minibatch loss. */
+ * 128), Adam (beta1 0.9, beta2 0.999, eps 1e-8) at learning rate lr, decayed along a half cosine
+ * over the call's steps, on the mean squared error of the standardised outputs. loss (epochs values, may be NULL): each epoch's mean minibatch loss. */
 int autan_mlp_train(void* handle, int32_t epochs, int32_t batch, float lr, uint64_t seed,
                     float* loss, char* err, size_t err_len);
 /* One forward and backward pass on n rows (host x, y as set_data's), no update: *loss and the
