@@ -18,7 +18,7 @@ extern "C" {
 #endif
 
 /* The network: `inputs` features -> `layers` hidden layers of `width` (GELU, the erf form) ->
- * `outputs`, each layer y = W x + b with W stored [out x in]. width a multiple of 16 (at most 256);
+ * `outputs`, each layer y = W x + b with W stored [out x in]. width a multiple of 16 (at most 128);
  * inputs and outputs at most width. Inputs are standardised (x - mean) / std and outputs
  * de-standardised y std + mean with the statistics of autan_mlp_set_scaling. Weights: Glorot
  * uniform from `seed`, biases zero. */
@@ -41,7 +41,8 @@ int autan_mlp_set_data(void* handle, const float* x, const float* y, int64_t n, 
                        size_t err_len);
 /* Training: `epochs` passes over the data in shuffled minibatches of `batch` rows (a multiple of
  * 128), Adam (beta1 0.9, beta2 0.999, eps 1e-8) at learning rate lr, decayed along a half cosine
- * over the call's steps, on the mean squared error of the standardised outputs. loss (epochs values, may be NULL): each epoch's mean minibatch loss. */
+ * over the call's steps, on the mean squared error of the standardised outputs. loss (epochs
+ * values, may be NULL): each epoch's mean minibatch loss. */
 int autan_mlp_train(void* handle, int32_t epochs, int32_t batch, float lr, uint64_t seed,
                     float* loss, char* err, size_t err_len);
 /* One forward and backward pass on n rows (host x, y as set_data's), no update: *loss and the
