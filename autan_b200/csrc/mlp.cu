@@ -282,6 +282,188 @@ __global__ void k_outputs(const float* pred, int ld, int outputs, int n, const f
   y[i] = pred[r * ld + c] * sd[c] + mean[c];
 }
 
+
+// ---------------------------------------------------------------- tcgen05 engine
+//
+// The same GEMMs on the 5th-generation tensor cores: C[128 x N] = P[128 x K] Q[N x K]^T for one
+// 128-row tile per CTA (4 warps). Both operands are written to shared memory in the K-major
+// canonical layout without swizzle (8-row x 16-byte core matrices: rows 16 bytes apart, row groups
+// 128 bytes apart, 8-element K groups R * 16 bytes apart for an R-row operand); one thread issues
+// K / 16 tcgen05.mma (kind::f16, BF16 in, FP32 accumulator in tensor memory) and commits them to
+// an mbarrier; after a bounded wait each warp reads its 32 accumulator lanes with tcgen05.ld.
+
+constexpr int kTcRows = 128;
+constexpr int kTcWaitLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Byte offset of element (r, k) in a K-major operand of R rows.
+__device__ __forceinline__ uint32_t kmajor(int r, int k, int R) {
+  return static_cast<uint32_t>((k >> 3) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Shared-memory matrix descriptor: start >> 4 at bits [0, 14), leading byte offset (the K-group
+// step) >> 4 at [16, 30), stride byte offset (the row-group step, 128) >> 4 at [32, 46), version 1
+// at [46, 48), no swizzle (layout 0) at [61, 64).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t start, int R) {
+  uint64_t d = static_cast<uint64_t>((start >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>(((R * 16) >> 4) & 0x3FFF) << 16;
+  d |= static_cast<uint64_t>((128 >> 4) & 0x3FFF) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits [4, 6) = 1), BF16 A and B ([7, 10)
+// and [10, 13) = 1), both K-major, N >> 3 at [17, 23), M >> 4 at [24, 29).
+__host__ __device__ constexpr uint32_t tc_idesc(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) |
+         (static_cast<uint32_t>(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ bool tc_try_wait(unsigned long long* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, "
+      "p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// MODE 0: P rows from A (row-major, lda) at row0 + r, Q = B (row-major [N x K], ldb); epilogue as
+// k_dense. MODE 1 (weight-gradient partial of chunk blockIdx.x): P[n][r] = A[m0 + r][n] (dZ, the
+// tile's 128 rows the output neurons, N0 of them real), Q[k][r] = B[m0 + r][k] (the layer input);
+// the partial [N0 x N] into Yf.
+template <int MODE, bool ACT>
+__global__ void __launch_bounds__(128) k_tc_gemm(const bf16* A, int lda, int M, int K, const bf16* B,
+                                                 int ldb, int N, int N0, const float* bias, float* Z,
+                                                 int ldz, bf16* Y, float* Yf, int ldy, int ncols,
+                                                 unsigned int* fault) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ uint32_t tmem_slot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int inner = MODE == 0 ? K : kTcRows;  // the contracted dimension
+  unsigned char* ps = tsm;
+  unsigned char* qs = tsm + kTcRows * inner * 2;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  const long long r0 = static_cast<long long>(blockIdx.x) * kTcRows;
+  if constexpr (MODE == 0) {
+    const int groups = K >> 3;
+    for (int i = threadIdx.x; i < kTcRows * groups; i += blockDim.x) {
+      const int r = i / groups, g = i % groups;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (r0 + r < M) v = *reinterpret_cast<const uint4*>(A + (r0 + r) * lda + 8 * g);
+      *reinterpret_cast<uint4*>(ps + kmajor(r, 8 * g, kTcRows)) = v;
+    }
+    for (int i = threadIdx.x; i < N * groups; i += blockDim.x) {
+      const int n = i / groups, g = i % groups;
+      *reinterpret_cast<uint4*>(qs + kmajor(n, 8 * g, N)) =
+          *reinterpret_cast<const uint4*>(B + static_cast<long long>(n) * ldb + 8 * g);
+    }
+  } else {
+    for (int i = threadIdx.x; i < kTcRows * kTcRows; i += blockDim.x) {
+      const int r = i / kTcRows, n = i % kTcRows;  // row r of the chunk, neuron n
+      bf16 v = __float2bfloat16(0.0f);
+      if (n < N0 && r0 + r < M) v = A[(r0 + r) * lda + n];
+      *reinterpret_cast<bf16*>(ps + kmajor(n, r, kTcRows)) = v;
+    }
+    for (int i = threadIdx.x; i < kTcRows * N; i += blockDim.x) {
+      const int r = i / N, k = i % N;
+      bf16 v = __float2bfloat16(0.0f);
+      if (r0 + r < M) v = B[(r0 + r) * ldb + k];
+      *reinterpret_cast<bf16*>(qs + kmajor(k, r, N)) = v;
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  if (threadIdx.x == 0) {
+    const uint32_t idesc = tc_idesc(N);
+    for (int k0 = 0; k0 < inner; k0 += 16) {
+      const uint64_t a = smem_desc(smem_addr(ps) + (k0 >> 3) * (kTcRows * 16), kTcRows);
+      const uint64_t b = smem_desc(smem_addr(qs) + (k0 >> 3) * (N * 16), N);
+      tc_mma(tmem, a, b, idesc, k0 > 0 ? 1u : 0u);
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(&bar))
+                 : "memory");
+  }
+  bool done = false;
+  for (int it = 0; it < kTcWaitLimit && !done; ++it) done = tc_try_wait(&bar, 0);
+  // one decision per warp (the tensor-memory loads below are warp-collective): a phase seen
+  // complete by any lane is complete
+  done = __any_sync(0xffffffffu, done);
+  if (!done) {
+    // the accumulator never completed: record it, give the MMAs one more bounded wait, free the
+    // tensor memory and leave without an epilogue
+    if (threadIdx.x == 0) atomicExch(fault, 1u);
+    for (int it = 0; it < kTcWaitLimit && !done; ++it) done = tc_try_wait(&bar, 0);
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = 32 * warp + lane;
+    for (int c0 = 0; c0 < N; c0 += 8) {
+      uint32_t v[8];
+      const uint32_t addr = tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c0);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if constexpr (MODE == 0) {
+        const long long r = r0 + row;
+        if (r < M) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int n = c0 + j;
+            const float z = __uint_as_float(v[j]) + (bias != nullptr ? bias[n] : 0.0f);
+            if (Z != nullptr) Z[r * ldz + n] = z;
+            const float y = ACT ? gelu(z) : z;
+            if (Y != nullptr) Y[r * ldy + n] = __float2bfloat16(y);
+            if (Yf != nullptr) Yf[r * ldy + n] = y;
+          }
+        }
+      } else {
+        if (row < N0) {
+          float* out = Yf + static_cast<long long>(blockIdx.x) * N0 * N;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) out[row * N + c0 + j] = __uint_as_float(v[j]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
+                 : "memory");
+}
+
 // ---------------------------------------------------------------- wall distance
 
 struct V3 {
@@ -385,6 +567,8 @@ class Net {
       fail("E1101: inputs and outputs 1 to width, at least one hidden layer");
     check(cudaSetDevice(device), "cudaSetDevice");
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+    fault_.alloc(sizeof(unsigned int));
+    check(cudaMemset(fault_.p, 0, sizeof(unsigned int)), "fault");
     long long off = 0;
     for (int l = 0; l <= layers; ++l) {
       Layer L;
@@ -482,13 +666,22 @@ class Net {
       const int size = Ly.np * Ly.kp;
       ensure(partial_, static_cast<size_t>(chunks) * size * 4);
       ensure(wfull_, static_cast<size_t>(size) * 4);
-      if (!wgrad_attr_) {
-        check(cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem),
-              "smem");
-        wgrad_attr_ = true;
+      if (tc_) {
+        const size_t smem = static_cast<size_t>(kTcRows + Ly.kp) * kTcRows * 2;
+        check(cudaFuncSetAttribute(k_tc_gemm<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)), "smem");
+        k_tc_gemm<1, false><<<chunks, 128, smem, stream_>>>(
+            dzb_.as<bf16>(), Ly.np, rows, kTcRows, a_prev, lda, Ly.kp, Ly.np, nullptr, nullptr, 0,
+            nullptr, partial_.as<float>(), 0, tmem_cols(Ly.kp), fault_.as<unsigned int>());
+      } else {
+        if (!wgrad_attr_) {
+          check(cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem),
+                "smem");
+          wgrad_attr_ = true;
+        }
+        k_wgrad<<<chunks, 256, kWgradSmem, stream_>>>(dzb_.as<bf16>(), Ly.np, a_prev, lda, rows, Ly.np,
+                                                     Ly.kp, partial_.as<float>());
       }
-      k_wgrad<<<chunks, 256, kWgradSmem, stream_>>>(dzb_.as<bf16>(), Ly.np, a_prev, lda, rows, Ly.np,
-                                                   Ly.kp, partial_.as<float>());
       check(cudaGetLastError(), "wgrad");
       k_sum_partials<<<blocks(size, 256), 256, 0, stream_>>>(partial_.as<float>(), chunks, size,
                                                              wfull_.as<float>());
@@ -601,6 +794,16 @@ class Net {
   template <bool ACT>
   void launch_dense(const bf16* A, int lda, int M, int K, const bf16* B, int ldb, int N,
                     const float* bias, float* Z, int ldz, bf16* Y, float* Yf, int ldy) {
+    if (tc_) {
+      const size_t smem = static_cast<size_t>(kTcRows + N) * K * 2;
+      check(cudaFuncSetAttribute(k_tc_gemm<0, ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)), "smem");
+      k_tc_gemm<0, ACT><<<blocks(M, kTcRows), 128, smem, stream_>>>(A, lda, M, K, B, ldb, N, N, bias,
+                                                                   Z, ldz, Y, Yf, ldy, tmem_cols(N),
+                                                                   fault_.as<unsigned int>());
+      check(cudaGetLastError(), "tc dense");
+      return;
+    }
     const size_t smem = static_cast<size_t>(kRowsPerBlock + N) * (K + 8) * 2;
     if (smem > 48 * 1024)
       check(cudaFuncSetAttribute(k_dense<ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -673,7 +876,25 @@ class Net {
   void copy(Buf& b, const void* host, size_t bytes) {
     check(cudaMemcpyAsync(b.p, host, bytes, cudaMemcpyHostToDevice, stream_), "copy");
   }
-  void sync() { check(cudaStreamSynchronize(stream_), "sync"); }
+  void sync() {
+    check(cudaStreamSynchronize(stream_), "sync");
+    unsigned int f = 0;
+    check(cudaMemcpy(&f, fault_.p, sizeof(f), cudaMemcpyDeviceToHost), "fault");
+    if (f != 0) fail("E1201: a tensor-core accumulator wait timed out; results are invalid");
+  }
+  static int tmem_cols(int n) {
+    int c = 32;
+    while (c < n) c *= 2;
+    return c;
+  }
+
+ public:
+  void set_engine(int engine) {
+    if (engine != 0 && engine != 1) fail("E1101: engine 0 (mma.sync) or 1 (tcgen05)");
+    tc_ = engine == 1;
+  }
+
+ private:
 
   int inputs_, width_, outputs_, device_;
   cudaStream_t stream_ = nullptr;
@@ -683,7 +904,8 @@ class Net {
   long long n_data_ = 0;
   int work_rows_ = 0;
   bool wgrad_attr_ = false;
-  Buf params_, grad_, m_, v_, in_mean_, in_sd_, out_mean_, out_sd_, x_, y_, idx_;
+  bool tc_ = false;  // tcgen05 engine
+  Buf params_, grad_, m_, v_, in_mean_, in_sd_, out_mean_, out_sd_, x_, y_, idx_, fault_;
   Buf x0_, acts_, zs_, dz_, dzb_, da_, se_, partial_, wfull_, pbias_;
   std::vector<std::unique_ptr<Buf>> wb_, wt_;
 };
@@ -728,6 +950,10 @@ int autan_mlp_create(int32_t inputs, int32_t width, int32_t layers, int32_t outp
 }
 
 void autan_mlp_destroy(void* handle) { delete static_cast<Net*>(handle); }
+
+int autan_mlp_set_engine(void* handle, int32_t engine, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] { as_net(handle)->set_engine(engine); });
+}
 
 int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,
                           const float* out_mean, const float* out_std, char* err, size_t err_len) {

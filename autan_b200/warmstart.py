@@ -32,6 +32,7 @@ def _bind():
 
     fn("autan_mlp_create", C.c_int, i32, i32, i32, i32, u64, i32, P(vp), C.c_char_p, sz)
     fn("autan_mlp_destroy", None, vp)
+    fn("autan_mlp_set_engine", C.c_int, vp, i32, C.c_char_p, sz)
     fn("autan_mlp_set_scaling", C.c_int, vp, P(f32), P(f32), P(f32), P(f32), C.c_char_p, sz)
     fn("autan_mlp_parameter_count", i64, vp)
     fn("autan_mlp_get_parameters", C.c_int, vp, P(f32), i64, C.c_char_p, sz)
@@ -65,6 +66,10 @@ class MLP:
     def _call(self, name, *args):
         err = N.errbuf()
         N.check(getattr(self.lib, name)(self.h, *args, err, len(err)), err)
+
+    def set_engine(self, engine: int) -> None:
+        """0: mma.sync kernels; 1: tcgen05 (tensor memory) kernels."""
+        self._call("autan_mlp_set_engine", int(engine))
 
     def set_scaling(self, in_mean, in_std, out_mean, out_std):
         a = [_f32(v) for v in (in_mean, in_std, out_mean, out_std)]

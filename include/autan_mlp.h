@@ -25,6 +25,10 @@ extern "C" {
 int autan_mlp_create(int32_t inputs, int32_t width, int32_t layers, int32_t outputs, uint64_t seed,
                      int32_t device, void** handle, char* err, size_t err_len);
 void autan_mlp_destroy(void* handle);
+/* The GEMM engine: 0 warp-level mma.sync m16n8k16 (the default), 1 tcgen05.mma with the
+ * accumulator in tensor memory (128-row tiles, operands staged in shared memory). Both take BF16
+ * operands and accumulate in FP32. */
+int autan_mlp_set_engine(void* handle, int32_t engine, char* err, size_t err_len);
 /* The standardisation: in_mean, in_std (inputs values each), out_mean, out_std (outputs each). */
 int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,
                           const float* out_mean, const float* out_std, char* err, size_t err_len);

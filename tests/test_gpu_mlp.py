@@ -23,11 +23,13 @@ def scaling(x, y):
     return (x.mean(0), x.std(0), y.mean(0), y.std(0))
 
 
-def test_gradient_against_the_restatement():
+@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+def test_gradient_against_the_restatement(engine):
     """BF16 operands, FP32 sums in another order: a BF16 rounding of an activation or a dZ may
     flip; the bounds (1e-4 on the loss, 2e-2 on the gradient's norm) leave room for that."""
     x, y = data(1000)
     net = MLP(seed=3)
+    net.set_engine(engine)
     sc = scaling(x, y)
     net.set_scaling(*sc)
     p = net.parameters()
@@ -39,9 +41,11 @@ def test_gradient_against_the_restatement():
     assert np.allclose(g[-5:], g0[-5:], rtol=1e-3, atol=1e-6)
 
 
-def test_training_fits_a_smooth_field():
+@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+def test_training_fits_a_smooth_field(engine):
     x, y = data(65536, seed=1)
     net = MLP(seed=4)
+    net.set_engine(engine)
     net.set_scaling(*scaling(x, y))
     net.set_data(x, y)
     loss = net.train(epochs=20, batch=4096, lr=2e-3, seed=5)
@@ -51,9 +55,11 @@ def test_training_fits_a_smooth_field():
     assert np.sqrt(np.mean((pred - yt) ** 2)) < 0.3 * np.sqrt(np.mean((yt - yt.mean(0)) ** 2))
 
 
-def test_prediction_matches_the_restatement():
+@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+def test_prediction_matches_the_restatement(engine):
     x, y = data(3000, seed=6)
     net = MLP(seed=7)
+    net.set_engine(engine)
     sc = scaling(x, y)
     net.set_scaling(*sc)
     p = net.parameters()
@@ -79,3 +85,19 @@ def test_wall_distance_bit_for_bit():
         want = [min(O.point_triangle(pts[k][:, i], t[0:3], t[3:6], t[6:9]) for t in tris[k])
                 for i in range(pts[k].shape[1])]  # fmt: skip
         assert np.array_equal(got[k], np.array(want))
+
+
+def test_engines_agree():
+    """tcgen05 (tensor memory accumulators) and mma.sync: the same BF16 operands and FP32 sums in
+    different orders; predictions and gradients within the BF16 flips that allows."""
+    x, y = data(5000, seed=9)
+    out = []
+    for engine in (0, 1):
+        net = MLP(seed=10)
+        net.set_engine(engine)
+        net.set_scaling(*scaling(x, y))
+        out.append((net.predict(x), net.gradient(x, y)))
+    (p0, (l0, g0)), (p1, (l1, g1)) = out
+    assert np.abs(p0 - p1).max() <= 1e-2 * np.abs(p0).max()
+    assert abs(l0 - l1) <= 1e-4 * l0
+    assert np.linalg.norm(g0 - g1) <= 2e-2 * np.linalg.norm(g0)
