@@ -258,8 +258,38 @@ class Batch:
         return int(self.mesh["n_owned_cells"])
 
 
+def batch_parameters(n_cases, seed, cells) -> list[dict]:
+    """The seeded per-case draws of bump_batch (numpy default_rng(seed)), in case order: target
+    cells (log-uniform in `cells`), Mach, flow angle (degrees), bump height, and the boxes."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(cells[0]), np.log(cells[1])
+    out = []
+    for _ in range(n_cases):
+        target = float(np.exp(rng.uniform(lo, hi)))
+        mach = float(rng.uniform(0.3, 0.75))
+        angle = float(rng.uniform(-4.0, 4.0))
+        bump = float(rng.uniform(0.02, 0.10))
+        # cells ~ 1.111 nx ny nz with nx = 6 a, ny = 2 a, nz = a
+        a = max(2, int(round((target / (1.111 * 12.0)) ** (1.0 / 3.0))))
+        out.append(dict(target=target, mach=mach, angle=angle, bump=bump, boxes=(6 * a, 2 * a, a)))
+    return out
+
+
+def shard_cases(params: list[dict], ranks: int) -> list[list[int]]:
+    """Whole cases to ranks, greedy by cell count (largest first to the least loaded rank, ties to
+    the lower rank): each rank's case indices in increasing order."""
+    size = [1.111 * np.prod(p["boxes"]) for p in params]
+    load = [0.0] * ranks
+    out = [[] for _ in range(ranks)]
+    for k in sorted(range(len(params)), key=lambda i: (-size[i], i)):
+        r = min(range(ranks), key=lambda q: (load[q], q))
+        out[r].append(k)
+        load[r] += size[k]
+    return [sorted(o) for o in out]
+
+
 def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precision="fp32+acc64",
-               inlet="farfield", walls=False) -> Batch:  # fmt: skip
+               inlet="farfield", walls=False, select=None) -> Batch:  # fmt: skip
     """Batched steady bump channels: per case (numpy default_rng(seed)) a cell count log-uniform
     in `cells`, Mach ~ U(0.3, 0.75), flow angle ~ U(-4, 4) degrees, bump height ~ U(0.02, 0.10).
     Each case's channel has about the requested cells (boxes in the ratio 3 : 1 : 1 / 2 of the
@@ -269,20 +299,16 @@ def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precisi
     (params[k]["wall"], t x 9, as WallSurface builds them) for the wall distance. A common scheme (second order, Venkatakrishnan K = 5)
     and reference state (Mach 0.5 along x) serve every case; local steps make the cases
     independent. inlet="state": the inflow faces take the freestream as a given state and the
-    outflow faces its static pressure (no exp/log on the path, for bit-exact tests)."""
-    rng = np.random.default_rng(seed)
-    lo, hi = np.log(cells[0]), np.log(cells[1])
+    outflow faces its static pressure (no exp/log on the path, for bit-exact tests). select: the
+    case indices to build (default all), the draws being those of all n_cases."""
+    draws = batch_parameters(n_cases, seed, cells)
     g = GAMMA
     p = 1.0 / g
     meshes, weights, kinds, datas, u0s, params = [], [], [], [], [], []
-    for _ in range(n_cases):
-        target = float(np.exp(rng.uniform(lo, hi)))
-        mach = float(rng.uniform(0.3, 0.75))
-        angle = float(rng.uniform(-4.0, 4.0))
-        bump = float(rng.uniform(0.02, 0.10))
-        # cells ~ 1.111 nx ny nz with nx = 6 a, ny = 2 a, nz = a
-        a = max(2, int(round((target / (1.111 * 12.0)) ** (1.0 / 3.0))))
-        nx, ny, nz = 6 * a, 2 * a, a
+    for k in range(n_cases) if select is None else select:
+        d0 = draws[k]
+        mach, angle, bump = d0["mach"], d0["angle"], d0["bump"]
+        nx, ny, nz = d0["boxes"]
         m = M.bump_channel(nx, ny, nz, bump=bump)
         zone = m.boundary_zone
         kind = np.full(m.n_boundary_faces, M.BC_SLIP, dtype=np.uint8)
@@ -306,7 +332,7 @@ def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precisi
         from autan_b200.euler import residual_scales
 
         params.append(dict(cells=m.n_cells, mach=mach, angle=angle, bump=bump, boxes=(nx, ny, nz),
-                           phi=residual_scales(m, 1.0, p, mach, g)))  # fmt: skip
+                           phi=residual_scales(m, 1.0, p, mach, g), case=k))  # fmt: skip
         if walls:
             from autan_b200.warmstart import wall_triangles
 

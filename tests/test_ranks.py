@@ -11,6 +11,7 @@ import subprocess
 import sys
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 REPO = Path(__file__).resolve().parent.parent
@@ -82,3 +83,50 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 2
     assert line["e2e"]["value"] == line["value"]
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_cases_shard_whole_and_balanced():
+    """The batch workload's sharding: every case on exactly one rank, ranks' cell totals within
+    the largest case of each other, the same draws whatever the number of ranks."""
+    sys.path.insert(0, str(REPO))
+    from autan_b200 import cases
+
+    params = cases.batch_parameters(256, 0, (20_000, 500_000))
+    size = [1.111 * float(np.prod(p["boxes"])) for p in params]
+    for ranks in (1, 2, 4, 8):
+        parts = cases.shard_cases(params, ranks)
+        flat = sorted(k for part in parts for k in part)
+        assert flat == list(range(256))
+        loads = [sum(size[k] for k in part) for part in parts]
+        assert max(loads) - min(loads) <= max(size)
+    assert cases.batch_parameters(256, 0, (20_000, 500_000)) == params
+
+
+def test_reduce_sum_over_ranks_gloo():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_sum_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [g[1] for g in got] == [30.0, 30.0]
+
+
+def _sum_rank(rank: int, world: int, port: int, out) -> None:
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, str(REPO))
+    import torch.distributed as dist
+
+    import bench
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))  # fmt: skip
+    try:
+        out.put((rank, bench.reduce_sum(10.0 + 10.0 * rank, dist)))
+    finally:
+        dist.destroy_process_group()
