@@ -84,18 +84,29 @@ class Convergence {
     return *std::max_element(first_.begin(), first_.end());
   }
 
+  // The median of the last kWindow values kept by a window in arrival order and the same values
+  // sorted (one removal and one insertion per value): the level (sorted[49] + sorted[50]) / 2 is
+  // the one the reference takes from nth_element on a copy of the window.
   struct Plateau {
-    std::array<double, kWindow> window{};
+    std::array<double, kWindow> window{}, sorted{};
     double reference = std::numeric_limits<double>::infinity();
     std::size_t count = 0, since = 0;
     bool add(double value) {
+      std::size_t filled = std::min(count, kWindow);
+      double* const s = sorted.data();
+      if (count >= kWindow) {
+        double* at = std::lower_bound(s, s + filled, window[count % kWindow]);
+        if (at == s + filled) at = s + filled - 1;  // not found (a NaN left the window)
+        std::move(at + 1, s + filled, at);
+        --filled;
+      }
       window[count % kWindow] = value;
+      double* const pos = std::upper_bound(s, s + filled, value);
+      std::move_backward(pos, s + filled, s + filled + 1);
+      *pos = value;
       ++count;
       if (count >= kWindow) {
-        std::array<double, kWindow> sorted = window;
-        const auto upper = sorted.begin() + kWindow / 2;
-        std::nth_element(sorted.begin(), upper, sorted.end());
-        const double level = (*std::max_element(sorted.begin(), upper) + *upper) / 2;
+        const double level = (s[kWindow / 2 - 1] + s[kWindow / 2]) / 2;
         if (level < kRatio * reference) {
           reference = level;
           since = count;

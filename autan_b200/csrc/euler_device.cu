@@ -39,6 +39,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -497,29 +498,48 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
 #pragma unroll
     for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
     const C* g = out + 5;
+    C phi[5];
+    C vol = C(0);
     if constexpr (LIMIT) {
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
         lo[i] = minv(lo[i], wc[i]);
         hi[i] = maxv(hi[i], wc[i]);
+        phi[i] = C(INFINITY);
       }
-      const C vol = static_cast<C>(__ldg(d.volume + c));
-      C phi[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
-      const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+      vol = static_cast<C>(__ldg(d.volume + c));
+    }
+    // One pass over the cell's incidences for both the limiter (its record: rel(x_f, x_c) of this
+    // side) and, with DT, spectral_radius (:1103-1112: the other side's state, the face's normal
+    // and area), each in incidence order.
+    double lam = 0.0;
+    if constexpr (LIMIT || DT) {
+      const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
       const int il = __ldg(d.inc_len + c);
       for (int j = 0; j < il; ++j) {
-        // The limiter record of the incidence: rel(x_f, x_c) of this side.
+        const long long at = 4 * (ib + static_cast<long long>(j) * kSlice);
         C r[4];
-        load_words<P, sizeof(C) == 8>(d.inc_rec + 4 * (ib + static_cast<long long>(j) * kSlice), 0, 4, r);
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
-          if (v < phi[i]) phi[i] = v;
+        load_words<P, sizeof(C) == 8>(d.inc_rec + at, 0, 4, r);
+        C nd[4], wn[5];
+        if constexpr (DT) {
+          load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
+          const int o = index_of(r[3]);
+          load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
+                          : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
+                   wn);
         }
+        if constexpr (LIMIT) {
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+            const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+            if (v < phi[i]) phi[i] = v;
+          }
+        }
+        if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
       }
+    }
+    if constexpr (LIMIT) {
       // at_most_one (:591-593)
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
@@ -532,22 +552,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
     for (int k = 20; k < kRecon; ++k) out[k] = C(0);
     store_recon<P>(d, c, out);
     if constexpr (DT) {
-      // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89) from the
-      // incidence records: the other side and the face's normal and area.
-      const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
-      const int il = __ldg(d.inc_len + c);
-      double lam = 0.0;
-      for (int j = 0; j < il; ++j) {
-        const long long at = 4 * (ib + static_cast<long long>(j) * kSlice);
-        C rr[4], nd[4], wn[5];
-        load_words<P, sizeof(C) == 8>(d.inc_rec + at, 0, 4, rr);
-        load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
-        const int o = index_of(rr[3]);
-        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
-                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
-                 wn);
-        lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
-      }
+      // The cell's CFL step (device_stepper.cuh:84-89).
       dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
     }
@@ -691,26 +696,47 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
     for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
     const C* g = out + 5;
     const C* irow = inc + 4 * (__ldg(d.inc_start + (c >> 5)) - i0 + (c & 31));
+    const C* drow = ndt + (irow - inc);
     const int il = __ldg(d.inc_len + c);
+    C phi[5];
+    C vol = C(0);
     if constexpr (LIMIT) {
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
         lo[i] = minv(lo[i], wc[i]);
         hi[i] = maxv(hi[i], wc[i]);
+        phi[i] = C(INFINITY);
       }
-      const C vol = static_cast<C>(__ldg(d.volume + c));
-      C phi[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) phi[k] = C(INFINITY);
+      vol = static_cast<C>(__ldg(d.volume + c));
+    }
+    // One pass over the staged incidence records for the limiter and, with DT, spectral_radius
+    // (:1103-1112: the other side's state from the limiter record, the normal and area staged).
+    double lam = 0.0;
+    if constexpr (LIMIT || DT) {
       for (int j = 0; j < il; ++j) {
         const C* r = irow + 4 * kSlice * j;
+        C wn[5];
+        if constexpr (DT) {
+          const int o = index_of(r[3]);
+          load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
+                          : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
+                   wn);
+        }
+        if constexpr (LIMIT) {
 #pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
-          if (v < phi[i]) phi[i] = v;
+          for (int i = 0; i < 5; ++i) {
+            const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+            const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+            if (v < phi[i]) phi[i] = v;
+          }
+        }
+        if constexpr (DT) {
+          const C* nd = drow + 4 * kSlice * j;
+          lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
         }
       }
+    }
+    if constexpr (LIMIT) {
       // at_most_one (:591-593)
 #pragma unroll
       for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
@@ -723,19 +749,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
     for (int k = 20; k < kRecon; ++k) out[k] = C(0);
     store_recon<P>(d, c, out);
     if constexpr (DT) {
-      // spectral_radius (:1103-1112) and the cell's CFL step (device_stepper.cuh:84-89).
-      // Each incidence's other side from the limiter record, its normal and area staged.
-      const C* drow = ndt + (irow - inc);
-      double lam = 0.0;
-      for (int j = 0; j < il; ++j) {
-        const int o = index_of(irow[4 * kSlice * j + 3]);
-        const C* nd = drow + 4 * kSlice * j;
-        C wn[5];
-        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
-                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
-                 wn);
-        lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
-      }
+      // The cell's CFL step (device_stepper.cuh:84-89).
       dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
     }
@@ -1143,48 +1157,75 @@ __global__ void k_norm_finish(Control* ctl, int n, int record) {
   }
 }
 
-// Batched cases: the exact sums of R_k^2 per case. A block whose cells all lie in one case adds
-// into shared words and flushes them once; a block over a case boundary adds each warp's terms,
-// grouped by case, to the global words of their cases.
+// Batched cases: the exact sums of R_k^2 per case. Each block walks kCaseSpan consecutive chunks
+// of blockDim.x cells: a chunk inside one case adds into words private to each warp (shared
+// memory), flushed to that case's global words when the case changes and at the end; a chunk over
+// a case boundary adds each warp's terms, grouped by case, to the global words of their cases.
+constexpr int kCaseSpan = 8;
+
 __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, int n,
                                                            const int* case_of,
                                                            unsigned long long* words) {
-  __shared__ unsigned long long sh[5 * kWords];
-  const long long c0 = static_cast<long long>(blockIdx.x) * blockDim.x;
-  const long long c1 = min(c0 + static_cast<long long>(blockDim.x), static_cast<long long>(n)) - 1;
-  const long long c = c0 + threadIdx.x;
-  const int first = case_of[c0], last = case_of[c1];
-  if (first == last) {
-    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
-      warp_exact_add_nonneg(sh + k * kWords, r * r);
-    }
-    __syncthreads();
-    unsigned long long* dst = words + static_cast<long long>(first) * 5 * kWords;
+  constexpr int kWarps = kBlock / 32;
+  __shared__ unsigned long long sh[kWarps][5 * kWords];
+  unsigned long long* mine = sh[threadIdx.x >> 5];
+  auto clear = [&]() {
+    for (int i = threadIdx.x; i < kWarps * 5 * kWords; i += blockDim.x) (&sh[0][0])[i] = 0;
+  };
+  auto flush = [&](int kc) {
+    unsigned long long* dst = words + static_cast<long long>(kc) * 5 * kWords;
     for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
-      const unsigned long long v = sh[i];
+      unsigned long long v = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) v += sh[w][i];
       if (v != 0) atomicAdd(&dst[i], v);
     }
-    return;
-  }
-  const unsigned full = 0xffffffffu;
-  const int mine = c < n ? case_of[c] : -1;
-  unsigned todo = __ballot_sync(full, mine >= 0);
-  while (todo != 0) {
-    const int kc = __shfl_sync(full, mine, __ffs(todo) - 1);
-    const bool in = mine == kc;
-    const unsigned group = __ballot_sync(full, in);
-    unsigned long long* dst = words + static_cast<long long>(kc) * 5 * kWords;
+  };
+  clear();
+  __syncthreads();
+  int cur = -1;
+  for (int s = 0; s < kCaseSpan; ++s) {
+    const long long c0 = (static_cast<long long>(blockIdx.x) * kCaseSpan + s) * blockDim.x;
+    if (c0 >= n) break;
+    const long long c1 = min(c0 + static_cast<long long>(blockDim.x), static_cast<long long>(n)) - 1;
+    const long long c = c0 + threadIdx.x;
+    const int first = case_of[c0], last = case_of[c1];
+    if (first == last) {
+      if (first != cur) {
+        if (cur >= 0) {
+          __syncthreads();
+          flush(cur);
+          __syncthreads();
+          clear();
+          __syncthreads();
+        }
+        cur = first;
+      }
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double r = in ? res[k * static_cast<long long>(n) + c] : 0.0;
-      warp_exact_add_nonneg(dst + k * kWords, r * r);
+      for (int k = 0; k < 5; ++k) {
+        const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+        warp_exact_add_nonneg<true>(mine + k * kWords, r * r);
+      }
+    } else {
+      const unsigned full = 0xffffffffu;
+      const int kase = c < n ? case_of[c] : -1;
+      unsigned todo = __ballot_sync(full, kase >= 0);
+      while (todo != 0) {
+        const int kc = __shfl_sync(full, kase, __ffs(todo) - 1);
+        const bool in = kase == kc;
+        const unsigned group = __ballot_sync(full, in);
+        unsigned long long* dst = words + static_cast<long long>(kc) * 5 * kWords;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const double r = in ? res[k * static_cast<long long>(n) + c] : 0.0;
+          warp_exact_add_nonneg(dst + k * kWords, r * r);
+        }
+        todo &= ~group;
+      }
     }
-    todo &= ~group;
   }
+  __syncthreads();
+  if (cur >= 0) flush(cur);
 }
 
 // Per case and equation (q = 5 case + k): rms = sqrt(sum / cells of the case) into this step's
@@ -2436,7 +2477,7 @@ class Impl final : public Stepper {
                   static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
         launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
         if (n_cases_ > 0) {
-          launch_as(kNorms, k_case_norm_sums, blocks(n_), kBlock,
+          launch_as(kNorms, k_case_norm_sums, blocks(n_, kBlock * kCaseSpan), kBlock,
                     static_cast<const double*>(res_.as<double>()), n_,
                     static_cast<const int*>(case_of_.as<int>()), case_words_.as<unsigned long long>());
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
@@ -2657,25 +2698,42 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
   check(cudaEventRecord(t0, h->stream), "event");
   long long taken = 0;
   int left = nk;
+  const int workers = std::max(1, std::min<int>(static_cast<int>(std::thread::hardware_concurrency()),
+                                                 nk / 32));
   while (taken < max_steps && left > 0) {
     const long long n = std::min<long long>(batch, max_steps - taken);
     autan_euler_step_result r{};
     h->step(cfl, dt, local, rk, n, true, &r);
     h->case_history(n, rms.data());
-    bool changed = false;
-    for (int k = 0; k < nk; ++k) {
-      if (!active[k]) continue;
-      for (long long i = 0; i < n; ++i) {
-        if (conv[k].add(rms.data() + (i * nk + k) * 5)) {
-          iterations[k] = taken + i + 1;
-          converged[k] = 1;
-          active[k] = 0;
-          changed = true;
-          --left;
-          break;
+    // Each case's rule over this batch; the cases are independent, so interleaved subsets of
+    // them go to host threads.
+    std::vector<int> done(workers, 0);
+    auto run = [&](int w) {
+      for (int k = w; k < nk; k += workers) {
+        if (!active[k]) continue;
+        for (long long i = 0; i < n; ++i) {
+          if (conv[k].add(rms.data() + (i * nk + k) * 5)) {
+            iterations[k] = taken + i + 1;
+            converged[k] = 1;
+            active[k] = 0;
+            ++done[w];
+            break;
+          }
         }
       }
+    };
+    if (workers == 1) {
+      run(0);
+    } else {
+      std::vector<std::thread> pool;
+      for (int w = 1; w < workers; ++w) pool.emplace_back(run, w);
+      run(0);
+      for (auto& t : pool) t.join();
     }
+    int newly = 0;
+    for (int v : done) newly += v;
+    const bool changed = newly > 0;
+    left -= newly;
     taken += n;
     if (changed) h->set_active(active.data());
     if (r.invalid_cell >= 0) break;

@@ -238,47 +238,116 @@ def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, re
     return res
 
 
+def _case_table(batch, cold, warm, rel) -> list[dict]:
+    """Per test case: its draws, cells, both marches' iterations and convergence, force difference."""
+    return [dict(case=p["case"], mach=p["mach"], angle=p["angle"], bump=p["bump"], cells=p["cells"],
+                 cold_iterations=int(cold["iterations"][k]), warm_iterations=int(warm["iterations"][k]),
+                 cold_converged=bool(cold["converged"][k]), warm_converged=bool(warm["converged"][k]),
+                 force_rel_diff=float(rel[k]))
+            for k, p in enumerate(batch.params)]  # fmt: skip
+
+
+def _force_difference(cold, warm) -> np.ndarray:
+    fc, fw = cold["force"], warm["force"]
+    return np.abs(fw - fc).max(axis=1) / np.maximum(np.abs(fc).max(axis=1), 1e-300)
+
+
+def warm_start(net, batch) -> np.ndarray:
+    """The network's starting state of every cell of `batch` (5 x n_cells): freestream + prediction."""
+    return freestream_states(batch) + net.predict(features(batch)).T.astype(np.float64)
+
+
+def save_network(net, path, x_mean, x_std, y_mean, y_std, **extra) -> None:
+    """The trained network (FP32 master parameters) and its standardisation, as a .npz."""
+    np.savez(path, params=net.parameters(), x_mean=x_mean, x_std=x_std, y_mean=y_mean, y_std=y_std,
+             **extra)  # fmt: skip
+
+
+def load_network(path, seed=11) -> MLP:
+    """A network saved by save_network."""
+    z = np.load(path)
+    net = MLP(seed=seed)
+    net.set_scaling(z["x_mean"], z["x_std"], z["y_mean"], z["y_std"])
+    net.set_parameters(z["params"])
+    return net
+
+
 def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30, batch_rows=8192,
-               lr=1e-3, orders=8.0, max_steps=200000, flux="ausm", log=print) -> dict:  # fmt: skip
+               lr=1e-3, orders=8.0, max_steps=200000, flux="ausm", log=print, save=None,
+               load=None) -> dict:  # fmt: skip
     """The learned warm start end to end: train_cases converged cases (seed 1) as training data,
     the MLP trained on them, then test_cases held-out cases (seed 2) marched from the network's
-    prediction and from the freestream. Returns the timings, iterations and force differences."""
+    prediction and from the freestream. The GPU-time comparison is made on the cases that converge
+    from both starts, re-marched as a batch of their own from each start (a batch's GPU time
+    follows its cells' iterations: converged cases' cells are skipped); cases that stall above the
+    rule's plateau band run to max_steps from either start and are reported apart. save: write the
+    trained network (.npz); load: take it from such a file instead of training. Returns the
+    timings, iterations, force differences and a per-case table."""
     import time
 
     from autan_b200 import cases
 
-    t0 = time.perf_counter()
-    train = cases.bump_batch(train_cases, seed=1, cells=cells, flux=flux, walls=True)
-    log(f"training set: {train_cases} cases, {train.n_cells} cells, set-up {time.perf_counter() - t0:.0f} s")
-    sol = march(train, train.u0, orders=orders, max_steps=max_steps)
-    log(f"training solutions: {int(sol['converged'].sum())} converged, {sol['steps']} steps, "
-        f"{sol['gpu_ms'] / 1e3:.1f} s GPU")  # fmt: skip
-    x = features(train)
-    y = (sol["u"] - freestream_states(train)).T.astype(np.float32)
-    net = MLP(seed=11)
-    net.set_scaling(x.mean(0), np.maximum(x.std(0), 1e-6), y.mean(0), np.maximum(y.std(0), 1e-9))
-    net.set_data(x, y)
-    t1 = time.perf_counter()
-    loss = net.train(epochs=epochs, batch=batch_rows, lr=lr, seed=12)
-    log(f"training: {epochs} epochs, loss {loss[0]:.3e} -> {loss[-1]:.3e}, {time.perf_counter() - t1:.0f} s")
+    out = dict(train_cases=train_cases, test_cases=test_cases, epochs=epochs)
+    if load is None:
+        t0 = time.perf_counter()
+        train = cases.bump_batch(train_cases, seed=1, cells=cells, flux=flux, walls=True)
+        log(f"training set: {train_cases} cases, {train.n_cells} cells, set-up {time.perf_counter() - t0:.0f} s")
+        sol = march(train, train.u0, orders=orders, max_steps=max_steps)
+        log(f"training solutions: {int(sol['converged'].sum())} converged, {sol['steps']} steps, "
+            f"{sol['gpu_ms'] / 1e3:.1f} s GPU")  # fmt: skip
+        x = features(train)
+        y = (sol["u"] - freestream_states(train)).T.astype(np.float32)
+        net = MLP(seed=11)
+        scaling = (x.mean(0), np.maximum(x.std(0), 1e-6), y.mean(0), np.maximum(y.std(0), 1e-9))
+        net.set_scaling(*scaling)
+        net.set_data(x, y)
+        t1 = time.perf_counter()
+        loss = net.train(epochs=epochs, batch=batch_rows, lr=lr, seed=12)
+        log(f"training: {epochs} epochs, loss {loss[0]:.3e} -> {loss[-1]:.3e}, {time.perf_counter() - t1:.0f} s")
+        if save is not None:
+            save_network(net, save, *scaling, loss=loss, train_iterations=sol["iterations"],
+                         train_converged=sol["converged"])  # fmt: skip
+        out.update(train_cells=train.n_cells, train_converged=int(sol["converged"].sum()),
+                   loss_first=float(loss[0]), loss_last=float(loss[-1]),
+                   training_solution_gpu_s=sol["gpu_ms"] / 1e3, training_steps=int(sol["steps"]),
+                   train_iterations_median=float(np.median(sol["iterations"])))  # fmt: skip
+    else:
+        net = load_network(load)
+        z = np.load(load)
+        if "loss" in z:
+            out.update(loss_first=float(z["loss"][0]), loss_last=float(z["loss"][-1]),
+                       train_converged=int(z["train_converged"].sum()))  # fmt: skip
     test = cases.bump_batch(test_cases, seed=2, cells=cells, flux=flux, walls=True)
-    free = freestream_states(test)
-    cold = march(test, free, orders=orders, max_steps=max_steps)
-    xt = features(test)
-    warm_u0 = free + net.predict(xt).T.astype(np.float64)
+    cold = march(test, freestream_states(test), orders=orders, max_steps=max_steps)
     # the warm start's drops are measured from the freestream start's first residuals, as a run
     # continued from another state keeps its reference (runtime/src/run.cpp:2351-2356)
-    warm = march(test, warm_u0, orders=orders, max_steps=max_steps, reference=cold["first"])
-    fc, fw = cold["force"], warm["force"]
-    rel = np.abs(fw - fc).max(axis=1) / np.maximum(np.abs(fc).max(axis=1), 1e-300)
-    return dict(train_cases=train_cases, train_cells=train.n_cells, test_cases=test_cases,
-                test_cells=test.n_cells, epochs=epochs, loss_first=float(loss[0]),
-                loss_last=float(loss[-1]),
-                cold_converged=int(cold["converged"].sum()), warm_converged=int(warm["converged"].sum()),
-                cold_gpu_s=cold["gpu_ms"] / 1e3, warm_gpu_s=warm["gpu_ms"] / 1e3,
-                gpu_time_ratio=cold["gpu_ms"] / warm["gpu_ms"],
-                cold_iterations_median=float(np.median(cold["iterations"])),
-                warm_iterations_median=float(np.median(warm["iterations"])),
-                iterations_ratio_median=float(np.median(cold["iterations"] / np.maximum(warm["iterations"], 1))),
-                force_rel_diff_max=float(rel.max()), force_rel_diff_median=float(np.median(rel)),
-                training_solution_gpu_s=sol["gpu_ms"] / 1e3)  # fmt: skip
+    warm = march(test, warm_start(net, test), orders=orders, max_steps=max_steps,
+                 reference=cold["first"])  # fmt: skip
+    rel = _force_difference(cold, warm)
+    table = _case_table(test, cold, warm, rel)
+    both = np.flatnonzero(cold["converged"] & warm["converged"])
+    log(f"test: {len(both)} of {test_cases} cases converge from both starts")
+    out.update(test_cells=test.n_cells, cold_converged=int(cold["converged"].sum()),
+               warm_converged=int(warm["converged"].sum()), both_converged=int(len(both)),
+               all_cold_gpu_s=cold["gpu_ms"] / 1e3, all_warm_gpu_s=warm["gpu_ms"] / 1e3)  # fmt: skip
+    if len(both):
+        sub = cases.bump_batch(test_cases, seed=2, cells=cells, flux=flux, walls=True,
+                               select=[int(k) for k in both])  # fmt: skip
+        limit = int(max(cold["iterations"][both].max(), warm["iterations"][both].max())) + 200
+        cold_b = march(sub, freestream_states(sub), orders=orders, max_steps=limit)
+        warm_b = march(sub, warm_start(net, sub), orders=orders, max_steps=limit,
+                       reference=cold_b["first"])  # fmt: skip
+        ci, wi = cold["iterations"][both], warm["iterations"][both]
+        cw = np.array([p["cells"] for p in sub.params], dtype=np.float64)
+        out.update(cold_gpu_s=cold_b["gpu_ms"] / 1e3, warm_gpu_s=warm_b["gpu_ms"] / 1e3,
+                   gpu_time_ratio=cold_b["gpu_ms"] / warm_b["gpu_ms"],
+                   cold_iterations_median=float(np.median(ci)),
+                   warm_iterations_median=float(np.median(wi)),
+                   iterations_ratio_median=float(np.median(ci / np.maximum(wi, 1))),
+                   cell_iterations_ratio=float((cw * ci).sum() / (cw * np.maximum(wi, 1)).sum()),
+                   force_rel_diff_max=float(rel[both].max()),
+                   force_rel_diff_median=float(np.median(rel[both])),
+                   subset_iterations_match=bool(np.array_equal(cold_b["iterations"], ci)
+                                                and np.array_equal(warm_b["iterations"], wi)))  # fmt: skip
+    out["cases"] = table
+    return out

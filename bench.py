@@ -367,9 +367,10 @@ def run_warmstart(args) -> None:
     tr, te, lo, hi, ep = (int(v) for v in args.warmstart.split(","))
     res = warmstart.experiment(train_cases=tr, test_cases=te, cells=(lo, hi), epochs=ep,
                                max_steps=args.max_steps, orders=args.converge or 8.0,
-                               log=lambda m: print(m, file=sys.stderr, flush=True))  # fmt: skip
+                               log=lambda m: print(m, file=sys.stderr, flush=True),
+                               save=args.save_network or None, load=args.load_network or None)  # fmt: skip
     print(json.dumps({"metric": "GPU time to convergence, freestream start / warm start",
-                      "value": res["gpu_time_ratio"], "unit": "x", "higher_is_better": True,
+                      "value": res.get("gpu_time_ratio"), "unit": "x", "higher_is_better": True,
                       **res}), flush=True)  # fmt: skip
 
 
@@ -604,6 +605,10 @@ def main() -> None:
     ap.add_argument("--warmstart", default="",
                     help="run the learned warm start instead: TRAIN,TEST,LO,HI,EPOCHS (training "
                          "cases, held-out cases, cell range, epochs), e.g. 2048,64,2000,10000,30")
+    ap.add_argument("--save-network", default="",
+                    help="with --warmstart: write the trained network to this .npz")
+    ap.add_argument("--load-network", default="",
+                    help="with --warmstart: take the network from this .npz instead of training")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()

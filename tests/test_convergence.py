@@ -66,3 +66,19 @@ def test_residual_scales_of_the_channel():
     assert phi[1] == phi[2] == phi[3] == pytest.approx(phi[0] * (0.5 + c))
     assert phi[4] == pytest.approx(phi[0] * (c * c / (g - 1) + 0.125))
     assert np.all(ROUND_OFF_FLOOR * phi > 0)
+
+
+@pytest.mark.parametrize("seed", [5, 6, 7, 8])
+def test_plateau_with_repeated_values(seed):
+    """Residuals quantised to a few levels (many equal values in the median window) and a slow
+    staircase down onto the plateau: the window's median, kept incrementally, against the
+    restatement's nth_element on each window."""
+    rng = np.random.default_rng(seed)
+    n = 3000
+    floors = np.full(5, 1e-6)
+    base = np.maximum(np.exp(-0.006 * np.arange(n))[:, None] * np.ones(5), 1.5e-6)
+    levels = rng.choice([0.9, 1.0, 1.1, 1.2], size=(n, 5))
+    r = np.round(base * levels, 8)
+    got = convergence_iteration(r, 8.0, floors)
+    assert got == O.convergence_iteration(r, 8.0, floors)
+    assert got[0] > 0

@@ -101,3 +101,23 @@ def test_engines_agree():
     assert np.abs(p0 - p1).max() <= 1e-2 * np.abs(p0).max()
     assert abs(l0 - l1) <= 1e-4 * l0
     assert np.linalg.norm(g0 - g1) <= 2e-2 * np.linalg.norm(g0)
+
+
+def test_experiment_small_round_trip(tmp_path):
+    """The warm-start experiment end to end on a few small channels: the result's fields, one row
+    per test case, the subset re-march reproducing each case's iterations, and a saved network
+    that, loaded, starts the test cases the same way (same iterations, same forces)."""
+    from autan_b200 import warmstart
+
+    path = tmp_path / "net.npz"
+    res = warmstart.experiment(train_cases=3, test_cases=3, cells=(300, 500), epochs=2,
+                               batch_rows=256, max_steps=4000, save=path, log=lambda m: None)  # fmt: skip
+    assert len(res["cases"]) == 3
+    assert res["both_converged"] == sum(r["cold_converged"] and r["warm_converged"] for r in res["cases"])
+    if res["both_converged"]:
+        assert res["subset_iterations_match"]
+        assert res["gpu_time_ratio"] > 0
+    again = warmstart.experiment(train_cases=3, test_cases=3, cells=(300, 500), max_steps=4000,
+                                 load=path, log=lambda m: None)  # fmt: skip
+    assert [r["warm_iterations"] for r in again["cases"]] == [r["warm_iterations"] for r in res["cases"]]
+    assert [r["force_rel_diff"] for r in again["cases"]] == [r["force_rel_diff"] for r in res["cases"]]
