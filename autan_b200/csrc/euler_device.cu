@@ -125,6 +125,10 @@ struct Dev {
   // Batched cases (null without): the case of each owned cell and whether each case still steps.
   const int* case_of;
   const unsigned char* active;
+  // Per 32 consecutive owned interior (boundary) faces: the case of all their owners, or -1 when
+  // they span two cases; a warp of a stopped case leaves before reading its face records.
+  const int* face_warp_case;
+  const int* bface_warp_case;
 };
 
 // Whether owned cell c takes part (its case has not stopped).
@@ -1037,6 +1041,10 @@ __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux
   using C = typename P::C;
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.n_if) return;
+  if (d.face_warp_case != nullptr) {
+    const int kc = __ldg(d.face_warp_case + (f >> 5));
+    if (kc >= 0 && d.active[kc] == 0) return;
+  }
   C fr[kFace], wl[5], gl[15], pl[5], wr[5], gr[15], pr[5], out[8];
   load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
   if (!cell_active(d, index_of(fr[7]))) return;
@@ -1053,6 +1061,10 @@ __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flu
   using C = typename P::C;
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbo) return;
+  if (d.bface_warp_case != nullptr) {
+    const int kc = __ldg(d.bface_warp_case + (b >> 5));
+    if (kc >= 0 && d.active[kc] == 0) return;
+  }
   C br[kBface], wc[5], gc[15], pc[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
   if (!cell_active(d, index_of(br[13]))) return;
@@ -1155,6 +1167,18 @@ __global__ void k_norm_finish(Control* ctl, int n, int record) {
     }
     if (record) ctl->hist_dt[slot] = ctl->dt;
   }
+}
+
+// Batched cases: for each 32 consecutive face records (`width` words, the owner's index at word
+// `owner`), the case of all their owners, or -1 when they span two cases.
+template <class C>
+__global__ void k_warp_case(const C* rec, int width, int owner, int count, const int* case_of,
+                            int* out) {
+  const long long f = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int kc = f < count ? case_of[index_of(rec[f * width + owner])] : -2;
+  const int first = __shfl_sync(0xffffffffu, kc, 0);
+  const bool same = __all_sync(0xffffffffu, kc == first || kc == -2);
+  if ((threadIdx.x & 31) == 0 && f < count) out[f >> 5] = same ? first : -1;
 }
 
 // Batched cases: the exact sums of R_k^2 per case. Each block walks kCaseSpan consecutive chunks
@@ -1809,6 +1833,8 @@ class Impl final : public Stepper {
     d_.ctl = ctl_.as<Control>();
     d_.case_of = nullptr;
     d_.active = nullptr;
+    d_.face_warp_case = nullptr;
+    d_.bface_warp_case = nullptr;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     if (tuning_.face_mode == 1) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
@@ -2345,6 +2371,16 @@ class Impl final : public Stepper {
     check(cudaMemsetAsync(active_.ptr(), 1, active_.bytes(), stream), "cases");
     d_.case_of = case_of_.as<int>();
     d_.active = active_.as<unsigned char>();
+    face_warp_case_.alloc(static_cast<size_t>(std::max((nif_ + 31) / 32, 1)) * sizeof(int));
+    bface_warp_case_.alloc(static_cast<size_t>(std::max((nbo_ + 31) / 32, 1)) * sizeof(int));
+    if (nif_ > 0)
+      launch(k_warp_case<C>, blocks(nif_), kBlock, static_cast<const C*>(face_.as<C>()), kFace, 7,
+             nif_, static_cast<const int*>(case_of_.as<int>()), face_warp_case_.as<int>());
+    if (nbo_ > 0)
+      launch(k_warp_case<C>, blocks(nbo_), kBlock, static_cast<const C*>(bface_.as<C>()), kBface, 13,
+             nbo_, static_cast<const int*>(case_of_.as<int>()), bface_warp_case_.as<int>());
+    d_.face_warp_case = face_warp_case_.as<int>();
+    d_.bface_warp_case = bface_warp_case_.as<int>();
     check(cudaStreamSynchronize(stream), "cases");
   }
 
@@ -2552,6 +2588,7 @@ class Impl final : public Stepper {
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
   Buffer bface_r64_, face_mult_, cons_words_;  // boundary pressure and conservation
   Buffer case_of_, case_cells_, case_words_, case_hist_, active_;  // batched cases
+  Buffer face_warp_case_, bface_warp_case_;
   int n_cases_ = 0;
   double pref64_ = 0.0;
   int max_faces_ = 0;

@@ -295,8 +295,14 @@ def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30
         sol = march(train, train.u0, orders=orders, max_steps=max_steps)
         log(f"training solutions: {int(sol['converged'].sum())} converged, {sol['steps']} steps, "
             f"{sol['gpu_ms'] / 1e3:.1f} s GPU")  # fmt: skip
-        x = features(train)
-        y = (sol["u"] - freestream_states(train)).T.astype(np.float32)
+        # the training rows: the cells of the cases that converged (a stalled case's last state is
+        # not a steady solution)
+        keep = np.repeat(sol["converged"].astype(bool), [p["cells"] for p in train.params])
+        if not keep.any():
+            log("no training case converged: training on every case's last state")
+            keep[:] = True
+        x = features(train)[keep]
+        y = (sol["u"] - freestream_states(train)).T.astype(np.float32)[keep]
         net = MLP(seed=11)
         scaling = (x.mean(0), np.maximum(x.std(0), 1e-6), y.mean(0), np.maximum(y.std(0), 1e-9))
         net.set_scaling(*scaling)
@@ -308,6 +314,7 @@ def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30
             save_network(net, save, *scaling, loss=loss, train_iterations=sol["iterations"],
                          train_converged=sol["converged"])  # fmt: skip
         out.update(train_cells=train.n_cells, train_converged=int(sol["converged"].sum()),
+                   train_rows=int(keep.sum()),
                    loss_first=float(loss[0]), loss_last=float(loss[-1]),
                    training_solution_gpu_s=sol["gpu_ms"] / 1e3, training_steps=int(sol["steps"]),
                    train_iterations_median=float(np.median(sol["iterations"])))  # fmt: skip
