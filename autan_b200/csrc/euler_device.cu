@@ -399,6 +399,97 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr, long long bytes) {
   }
 }
 
+// The block's stencil rows and incidence records (contiguous in the sliced layout) to L2.
+template <class P, bool LIMIT, bool DT>
+__device__ __forceinline__ void prefetch_block_rows(const Dev<P>& d) {
+  using C = typename P::C;
+  const int s0 = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x) >> 5);
+  const int s1 = min(s0 + static_cast<int>(blockDim.x >> 5), d.n_slices);
+  if (s0 < s1) {
+    const long long e0 = __ldg(d.st_start + s0), e1 = __ldg(d.st_start + s1);
+    const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s1);
+    prefetch_l2(d.st + 4 * e0, (e1 - e0) * 4 * static_cast<long long>(sizeof(C)));
+    if (LIMIT || DT) prefetch_l2(d.inc_rec + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+    if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+  }
+}
+
+// The end of a cell's gradient loop (kernels/euler.py:517-521, :563-608, :1103-1112): the FP64
+// sums rounded to the gradient, the bounds with the cell's own value, then one pass over the
+// cell's incidences for the limiter and, with DT, the spectral radius and the cell's CFL step
+// (returned; 0 without DT); the reconstruction record stored.
+template <class P, bool LIMIT, bool DT>
+__device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const typename P::C* wc,
+                                                const double* acc, typename P::C* lo,
+                                                typename P::C* hi, double cfl, int local) {
+  using C = typename P::C;
+  // include_own_value (:517-521); out: phi, then grad, then padding.
+  C out[kRecon];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
+  const C* g = out + 5;
+  C phi[5];
+  C vol = C(0);
+  if constexpr (LIMIT) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      lo[i] = minv(lo[i], wc[i]);
+      hi[i] = maxv(hi[i], wc[i]);
+      phi[i] = C(INFINITY);
+    }
+    vol = static_cast<C>(__ldg(d.volume + c));
+  }
+  // One pass over the cell's incidences for both the limiter (its record: rel(x_f, x_c) of this
+  // side) and, with DT, spectral_radius (:1103-1112: the other side's state, the face's normal
+  // and area), each in incidence order.
+  double lam = 0.0;
+  if constexpr (LIMIT || DT) {
+    const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+    const int il = __ldg(d.inc_len + c);
+    for (int j = 0; j < il; ++j) {
+      const long long at = 4 * (ib + static_cast<long long>(j) * kSlice);
+      C r[4];
+      load_words<P, sizeof(C) == 8>(d.inc_rec + at, 0, 4, r);
+      C nd[4], wn[5];
+      if constexpr (DT) {
+        load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
+        const int o = index_of(r[3]);
+        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
+                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
+                 wn);
+      }
+      if constexpr (LIMIT) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+          if (v < phi[i]) phi[i] = v;
+        }
+      }
+      if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
+    }
+  }
+  if constexpr (LIMIT) {
+    // at_most_one (:591-593)
+#pragma unroll
+    for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
+  } else {
+    // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
+#pragma unroll
+    for (int i = 0; i < 5; ++i) out[i] = C(1.0);
+  }
+#pragma unroll
+  for (int k = 20; k < kRecon; ++k) out[k] = C(0);
+  store_recon<P>(d, c, out);
+  if constexpr (DT) {
+    // The cell's CFL step (device_stepper.cuh:84-89).
+    const double dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
+    if (local) d.dt_local[c] = dt;
+    return dt;
+  }
+  return 0.0;
+}
+
 // gradients (kernels/euler.py:540-549) then limiter (:596-608), one thread per owned cell: the LSQ
 // gradient over the face2 stencil with FP64 sums, the bounds over the stencil and the cell, then
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
@@ -410,18 +501,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
-  if (threadIdx.x == 0) {
-    // The block's stencil rows and incidence records (contiguous in the sliced layout) to L2.
-    const int s0 = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x) >> 5);
-    const int s1 = min(s0 + static_cast<int>(blockDim.x >> 5), d.n_slices);
-    if (s0 < s1) {
-      const long long e0 = __ldg(d.st_start + s0), e1 = __ldg(d.st_start + s1);
-      const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s1);
-      prefetch_l2(d.st + 4 * e0, (e1 - e0) * 4 * static_cast<long long>(sizeof(C)));
-      if (LIMIT || DT) prefetch_l2(d.inc_rec + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
-      if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
-    }
-  }
+  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -497,69 +577,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
           if (j0 + q < len) add_entry(e4[q], wn[q]);
       }
     }
-    // include_own_value (:517-521); out: phi, then grad, then padding.
-    C out[kRecon];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
-    const C* g = out + 5;
-    C phi[5];
-    C vol = C(0);
-    if constexpr (LIMIT) {
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        lo[i] = minv(lo[i], wc[i]);
-        hi[i] = maxv(hi[i], wc[i]);
-        phi[i] = C(INFINITY);
-      }
-      vol = static_cast<C>(__ldg(d.volume + c));
-    }
-    // One pass over the cell's incidences for both the limiter (its record: rel(x_f, x_c) of this
-    // side) and, with DT, spectral_radius (:1103-1112: the other side's state, the face's normal
-    // and area), each in incidence order.
-    double lam = 0.0;
-    if constexpr (LIMIT || DT) {
-      const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
-      const int il = __ldg(d.inc_len + c);
-      for (int j = 0; j < il; ++j) {
-        const long long at = 4 * (ib + static_cast<long long>(j) * kSlice);
-        C r[4];
-        load_words<P, sizeof(C) == 8>(d.inc_rec + at, 0, 4, r);
-        C nd[4], wn[5];
-        if constexpr (DT) {
-          load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
-          const int o = index_of(r[3]);
-          load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
-                          : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
-                   wn);
-        }
-        if constexpr (LIMIT) {
-#pragma unroll
-          for (int i = 0; i < 5; ++i) {
-            const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-            const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
-            if (v < phi[i]) phi[i] = v;
-          }
-        }
-        if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
-      }
-    }
-    if constexpr (LIMIT) {
-      // at_most_one (:591-593)
-#pragma unroll
-      for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
-    } else {
-      // Second order without limiter: phi = 1 (physics/src/euler.cpp:195).
-#pragma unroll
-      for (int i = 0; i < 5; ++i) out[i] = C(1.0);
-    }
-#pragma unroll
-    for (int k = 20; k < kRecon; ++k) out[k] = C(0);
-    store_recon<P>(d, c, out);
-    if constexpr (DT) {
-      // The cell's CFL step (device_stepper.cuh:84-89).
-      dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
-      if (local) d.dt_local[c] = dt;
-    }
+    dt = gradient_tail<P, LIMIT, DT>(d, c, wc, acc, lo, hi, cfl, local);
   }
   if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
@@ -757,6 +775,146 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
       dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
       if (local) d.dt_local[c] = dt;
     }
+  }
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+// ---------------------------------------------------------------- asynchronous-copy ring
+
+// Per-thread asynchronous copies into shared memory (cp.async): .cg (16 bytes, L2 only) for the
+// streamed stencil rows, .ca (4, 8 or 16 bytes, through L1) for the gathered neighbour records,
+// whose neighbours are shared by nearby cells. Completion is tracked per thread by commit groups.
+__device__ __forceinline__ void cp_async_cg16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+template <int B>
+__device__ __forceinline__ void cp_async_ca(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(B)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Bytes of shared memory per thread of k_gradients_ring at depth `depth` (C of `word` bytes):
+// depth + 1 neighbour records of 5 words and 2 depth + 1 stencil rows of 4 words.
+constexpr int ring_bytes(int depth, int word) {
+  return (depth + 1) * 5 * word + (2 * depth + 1) * 4 * word;
+}
+
+// gradients + limiter (as k_gradients), the stencil walked with asynchronous copies: each thread
+// keeps a ring in shared memory of its next D neighbour records and next 2D stencil rows, so D
+// gathers are in flight without holding registers. Entry j's group (its neighbour record, and
+// the row of entry j + D) is the D-th newest when entry j is added: cp.async.wait_group D - 1. A
+// slot is refilled one entry after it was read (D + 1 record slots, 2D + 1 row slots). Entries
+// are added in stencil order, so the sums are those of k_gradients bit for bit. MINB: the blocks of
+// 128 threads per SM the registers are sized for (6: no spills; 8: 64 registers).
+template <class P, bool LIMIT, bool DT, int D, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_gradients_ring(Dev<P> d, double cfl, int local) {
+  using C = typename P::C;
+  constexpr int kW = 16 / static_cast<int>(sizeof(C));   // words per 16-byte piece
+  constexpr int kG16 = 5 / kW;                            // whole pieces of a record's 5 words
+  constexpr int kGRem = (5 % kW) * static_cast<int>(sizeof(C));  // bytes after them
+  constexpr int kR16 = 4 / kW;                            // pieces of a stencil row
+  constexpr int kGS = D + 1, kRS = 2 * D + 1;             // record and row slots
+  static_assert(kGRem == 4 || kGRem == 8, "a record's tail is one word");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nt = blockDim.x, t = threadIdx.x;
+  // Regions, each piece interleaved over the block's threads (conflict-free 128-bit accesses):
+  // records' whole pieces, records' tails, rows.
+  unsigned char* const g16 = smem_raw;
+  unsigned char* const grem = g16 + kGS * kG16 * nt * 16;
+  unsigned char* const r16 = grem + kGS * nt * kGRem;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n && cell_active(d, c);
+  double dt = 0.0;
+  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  if (live) {
+    C wc[5];
+    load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
+    }
+    const long long base = __ldg(d.st_start + (c >> 5)) + (c & 31);
+    const int len = __ldg(d.st_len + c);
+    const C* rows = d.st + 4 * base;
+    auto rpiece = [&](int slot, int q) { return r16 + ((slot * kR16 + q) * nt + t) * 16; };
+    auto issue_row = [&](int j, int slot) {
+      const C* src = rows + 4LL * kSlice * j;
+#pragma unroll
+      for (int q = 0; q < kR16; ++q) cp_async_cg16(rpiece(slot, q), src + q * kW);
+    };
+    auto row_index = [&](int slot) {
+      return index_of(reinterpret_cast<const C*>(rpiece(slot, kR16 - 1))[kW - 1]);
+    };
+    auto issue_gather = [&](int x, int slot) {
+      const C* src = x >= 0 ? d.prim + static_cast<long long>(x) * kPrimW
+                            : d.prim_b + static_cast<long long>(-x - 1) * kPrimB;
+#pragma unroll
+      for (int q = 0; q < kG16; ++q) cp_async_ca<16>(g16 + ((slot * kG16 + q) * nt + t) * 16, src + q * kW);
+      cp_async_ca<kGRem>(grem + (slot * nt + t) * kGRem, src + kG16 * kW);
+    };
+    // Prologue: rows 0 .. D-1 (waited for), then per entry g < D its record and the row of g + D.
+    for (int j = 0; j < D && j < len; ++j) issue_row(j, j);
+    cp_async_commit();
+    cp_async_wait<0>();
+#pragma unroll
+    for (int g = 0; g < D; ++g) {
+      if (g < len) issue_gather(row_index(g), g);
+      if (g + D < len) issue_row(g + D, g + D);
+      cp_async_commit();
+    }
+    int gs = 0, rs = 0;           // slots of entry j's record and row
+    int gw = D, rw = 2 * D;       // slots the next record and row go to
+    int rn = D;                   // slot of the row of entry j + D
+    for (int j = 0; j < len; ++j) {
+      cp_async_wait<D - 1>();
+      C wn[5], e[4];
+#pragma unroll
+      for (int q = 0; q < kG16; ++q) {
+        const C* v = reinterpret_cast<const C*>(g16 + ((gs * kG16 + q) * nt + t) * 16);
+#pragma unroll
+        for (int w = 0; w < kW; ++w) wn[q * kW + w] = v[w];
+      }
+      wn[4] = *reinterpret_cast<const C*>(grem + (gs * nt + t) * kGRem);
+#pragma unroll
+      for (int q = 0; q < kR16; ++q) {
+        const C* v = reinterpret_cast<const C*>(rpiece(rs, q));
+#pragma unroll
+        for (int w = 0; w < kW; ++w) e[q * kW + w] = v[w];
+      }
+      const int x = j + D < len ? row_index(rn) : 0;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const C dw = wn[i] - wc[i];
+        acc[3 * i] += static_cast<double>(dw * e[0]);
+        acc[3 * i + 1] += static_cast<double>(dw * e[1]);
+        acc[3 * i + 2] += static_cast<double>(dw * e[2]);
+      }
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        if (wn[i] < lo[i]) lo[i] = wn[i];
+        if (wn[i] > hi[i]) hi[i] = wn[i];
+      }
+      if (j + D < len) issue_gather(x, gw);
+      if (j + 2 * D < len) issue_row(j + 2 * D, rw);
+      cp_async_commit();
+      gs = gs + 1 == kGS ? 0 : gs + 1;
+      gw = gw + 1 == kGS ? 0 : gw + 1;
+      rs = rs + 1 == kRS ? 0 : rs + 1;
+      rw = rw + 1 == kRS ? 0 : rw + 1;
+      rn = rn + 1 == kRS ? 0 : rn + 1;
+    }
+    cp_async_wait<0>();
+    dt = gradient_tail<P, LIMIT, DT>(d, c, wc, acc, lo, hi, cfl, local);
   }
   if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
@@ -1529,7 +1687,9 @@ struct Tuning {
   int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
   int gather_block = 256;  // threads per block of the store-gather sum
   int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies;
-                         // 2: loaded by each thread, software-pipelined (chunk unused)
+                         // 2: loaded by each thread, software-pipelined (chunk unused);
+                         // 3: a per-thread ring of asynchronous copies, chunk entries deep;
+                         // 4: as 3 with the registers capped at 64 (8 blocks of 128 per SM)
   static constexpr int kCount = 6;
   void to(int32_t* p) const {
     p[0] = grad_chunk;
@@ -1560,7 +1720,10 @@ void Tuning::validate() const {
   if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
-  if (grad_mode < 0 || grad_mode > 2) fail("E1101: grad_mode is 0, 1 or 2");
+  if (grad_mode >= 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
+    fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
+  if (grad_mode < 0 || grad_mode > 4) fail("E1101: grad_mode is 0 to 4");
+  if (grad_mode >= 3 && grad_block > 128) fail("E1101: the ring gradient kernel takes <= 128 threads");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
   if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
     fail("E1101: block sizes are multiples of 32 in [32, 256]");
@@ -2094,12 +2257,12 @@ class Impl final : public Stepper {
     if (second_) {
       double best_ms = 1e300;
       Tuning keep = best;
-      for (int mode : {0, 1, 2})
+      for (int mode : {0, 1, 2, 3, 4})
       for (int chunk : {1, 2, 4, 8})
         for (int block : {64, 128, 256}) {
           if (mode == 0 && chunk == 8) continue;
           if (mode == 2 && chunk != 1) continue;
-          if (mode == 1 && (chunk == 1 || block > 128)) continue;
+          if ((mode == 1 || mode >= 3) && (chunk == 1 || block > 128)) continue;
           Tuning t = keep;
           t.grad_mode = mode;
           t.grad_chunk = chunk;
@@ -2458,6 +2621,21 @@ class Impl final : public Stepper {
             launch_smem(kGradients, k_gradients_tma<P, L, D, 8>, blocks(n_, bs), bs, sm, d, cfl, loc);
           else
             launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, blocks(n_, bs), bs, sm, d, cfl, loc);
+          return;
+        }
+        if (tuning_.grad_mode >= 3) {
+          const int w = static_cast<int>(sizeof(C));
+          const bool tight = tuning_.grad_mode == 4;
+          if (tuning_.grad_chunk == 2) {
+            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 2, 8>, gs, bs, bs * ring_bytes(2, w), d, cfl, loc);
+            else launch_smem(kGradients, k_gradients_ring<P, L, D, 2, 6>, gs, bs, bs * ring_bytes(2, w), d, cfl, loc);
+          } else if (tuning_.grad_chunk == 8) {
+            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 8, 8>, gs, bs, bs * ring_bytes(8, w), d, cfl, loc);
+            else launch_smem(kGradients, k_gradients_ring<P, L, D, 8, 6>, gs, bs, bs * ring_bytes(8, w), d, cfl, loc);
+          } else {
+            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 4, 8>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
+            else launch_smem(kGradients, k_gradients_ring<P, L, D, 4, 6>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
+          }
           return;
         }
         if (tuning_.grad_mode == 2)

@@ -197,7 +197,8 @@ def test_tuning_variants_are_bit_identical(precision):
     case = cases.vortex_tets(16, 16, 6, steps=3, precision=precision)
     u_o, *_ = run_oracle(case, case.steps)
     no = case.mesh.n_owned_cells
-    for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 2), (1, 4), (1, 8), (2, 1)):
+    for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 2), (1, 4), (1, 8), (2, 1), (3, 2), (3, 4),
+                         (3, 8), (4, 4), (4, 8)):
         for mode in (0, 1):
             for block in (64, 128) if gmode else (64, 256):
                 with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
@@ -208,6 +209,26 @@ def test_tuning_variants_are_bit_identical(precision):
                     dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
                     u = dev.download()
                 assert bits_equal(u[:, :no], u_o[:, :no]), (gmode, chunk, mode, block)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
+def test_gradient_stagings_agree_on_the_channel(precision):
+    """The hybrid bump channel (hexahedra, prisms and polyhedral bricks: about 23 stencil entries
+    per cell, boundary faces in the stencils, local steps): every gradient staging and depth gives
+    the bits of the per-thread loads."""
+    case = cases.bump_channel(24, 10, 4, steps=3, precision=precision)
+    out = {}
+    for gmode, chunk, block in ((0, 1, 128), (1, 4, 128), (2, 1, 64), (3, 2, 64), (3, 4, 128),
+                                (3, 8, 128), (4, 4, 128), (4, 8, 64)):  # fmt: skip
+        with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+            dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=1, face_block=128,
+                           gather_block=128, grad_mode=gmode)  # fmt: skip
+            dev.upload(case.u0)
+            dev.step(cfl=case.cfl, local=True, rk=3, n_steps=case.steps)
+            out[(gmode, chunk, block)] = dev.download()
+    first = out[(0, 1, 128)]
+    for k, u in out.items():
+        assert bits_equal(u, first), k
 
 
 def test_autotune_leaves_the_solution_unchanged():
