@@ -513,7 +513,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     peak, peak_kind = measured_hbm_peak()
     step_ms = ms / args.steps
     step_bytes = sum(alg.values())
-    traffic = committed_traffic(dominant, n)
+    family = {"tets": "tets", "channel": "channel", "batch": "channel"}.get(args.workload, args.workload)
+    traffic = committed_traffic(dominant, n, family)
     line = None
     if rank == 0:
         line = {
@@ -565,15 +566,17 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(line), flush=True)
 
 
-def committed_traffic(kernel: str, n_cells: int):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.md, a
-    line `traffic <kernel> <bytes per launch> <cells>` scaled to this case's cells), else None."""
+def committed_traffic(kernel: str, n_cells: int, mesh: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries (profiles/traffic.md, a
+    line `traffic <kernel> <bytes per launch> <cells> <mesh>` captured on a smaller case of the same
+    mesh family, scaled to this case's cells), else None. mesh: "tets" (the vortex lattices) or
+    "channel" (the hybrid bump channels, single or batched)."""
     p = REPO / "profiles" / "traffic.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
         f = line.strip().strip("`").split()
-        if len(f) == 4 and f[0] == "traffic" and f[1] == kernel:
+        if len(f) == 5 and f[0] == "traffic" and f[1] == kernel and f[4] == mesh:
             return float(f[2]) * n_cells / float(f[3])
     return None
 
