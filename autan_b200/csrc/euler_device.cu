@@ -137,6 +137,18 @@ __device__ __forceinline__ bool cell_active(const Dev<P>& d, int c) {
   return d.active == nullptr || d.active[d.case_of[c]] != 0;
 }
 
+// Whether this block's cells (blockDim.x consecutive owned cells) all belong to one stopped case:
+// the block then leaves before prefetching or staging its stencil rows. Uniform over the block.
+template <class P>
+__device__ __forceinline__ bool block_idle(const Dev<P>& d) {
+  if (d.active == nullptr) return false;
+  const long long c0 = static_cast<long long>(blockIdx.x) * blockDim.x;
+  if (c0 >= d.n) return true;
+  const long long c1 = min(c0 + static_cast<long long>(blockDim.x), static_cast<long long>(d.n)) - 1;
+  const int k0 = d.case_of[c0];
+  return k0 == d.case_of[c1] && d.active[k0] == 0;
+}
+
 __device__ __forceinline__ int index_of(float x) { return __float_as_int(x); }
 __device__ __forceinline__ int index_of(double x) {
   return static_cast<int>(__double_as_longlong(x));
@@ -498,6 +510,7 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 template <class P, bool LIMIT, bool DT, int CHUNK>
 __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
+  if (block_idle(d)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
@@ -642,6 +655,7 @@ __device__ __forceinline__ bool bounded_wait(unsigned long long* bar, Control* c
 template <class P, bool LIMIT, bool DT, int CHUNK>
 __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
+  if (block_idle(d)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ __align__(8) unsigned long long bar;
   const int per_block = blockDim.x / 32;
@@ -814,6 +828,7 @@ constexpr int ring_bytes(int depth, int word) {
 template <class P, bool LIMIT, bool DT, int D, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_gradients_ring(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
+  if (block_idle(d)) return;
   constexpr int kW = 16 / static_cast<int>(sizeof(C));   // words per 16-byte piece
   constexpr int kG16 = 5 / kW;                            // whole pieces of a record's 5 words
   constexpr int kGRem = (5 % kW) * static_cast<int>(sizeof(C));  // bytes after them
