@@ -823,10 +823,9 @@ constexpr int ring_bytes(int depth, int word) {
 // gathers are in flight without holding registers. Entry j's group (its neighbour record, and
 // the row of entry j + D) is the D-th newest when entry j is added: cp.async.wait_group D - 1. A
 // slot is refilled one entry after it was read (D + 1 record slots, 2D + 1 row slots). Entries
-// are added in stencil order, so the sums are those of k_gradients bit for bit. MINB: the blocks of
-// 128 threads per SM the registers are sized for (6: no spills; 8: 64 registers).
-template <class P, bool LIMIT, bool DT, int D, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_gradients_ring(Dev<P> d, double cfl, int local) {
+// are added in stencil order, so the sums are those of k_gradients bit for bit.
+template <class P, bool LIMIT, bool DT, int D>
+__global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
   if (block_idle(d)) return;
   constexpr int kW = 16 / static_cast<int>(sizeof(C));   // words per 16-byte piece
@@ -1703,8 +1702,7 @@ struct Tuning {
   int gather_block = 256;  // threads per block of the store-gather sum
   int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies;
                          // 2: loaded by each thread, software-pipelined (chunk unused);
-                         // 3: a per-thread ring of asynchronous copies, chunk entries deep;
-                         // 4: as 3 with the registers capped at 64 (8 blocks of 128 per SM)
+                         // 3: a per-thread ring of asynchronous copies, chunk entries deep
   static constexpr int kCount = 6;
   void to(int32_t* p) const {
     p[0] = grad_chunk;
@@ -1735,10 +1733,10 @@ void Tuning::validate() const {
   if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
-  if (grad_mode >= 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
+  if (grad_mode == 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
-  if (grad_mode < 0 || grad_mode > 4) fail("E1101: grad_mode is 0 to 4");
-  if (grad_mode >= 3 && grad_block > 128) fail("E1101: the ring gradient kernel takes <= 128 threads");
+  if (grad_mode < 0 || grad_mode > 3) fail("E1101: grad_mode is 0, 1, 2 or 3");
+  if (grad_mode == 3 && grad_block > 128) fail("E1101: the ring gradient kernel takes <= 128 threads");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
   if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
     fail("E1101: block sizes are multiples of 32 in [32, 256]");
@@ -2272,12 +2270,12 @@ class Impl final : public Stepper {
     if (second_) {
       double best_ms = 1e300;
       Tuning keep = best;
-      for (int mode : {0, 1, 2, 3, 4})
+      for (int mode : {0, 1, 2, 3})
       for (int chunk : {1, 2, 4, 8})
         for (int block : {64, 128, 256}) {
           if (mode == 0 && chunk == 8) continue;
           if (mode == 2 && chunk != 1) continue;
-          if ((mode == 1 || mode >= 3) && (chunk == 1 || block > 128)) continue;
+          if ((mode == 1 || mode == 3) && (chunk == 1 || block > 128)) continue;
           Tuning t = keep;
           t.grad_mode = mode;
           t.grad_chunk = chunk;
@@ -2638,19 +2636,14 @@ class Impl final : public Stepper {
             launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, blocks(n_, bs), bs, sm, d, cfl, loc);
           return;
         }
-        if (tuning_.grad_mode >= 3) {
+        if (tuning_.grad_mode == 3) {
           const int w = static_cast<int>(sizeof(C));
-          const bool tight = tuning_.grad_mode == 4;
-          if (tuning_.grad_chunk == 2) {
-            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 2, 8>, gs, bs, bs * ring_bytes(2, w), d, cfl, loc);
-            else launch_smem(kGradients, k_gradients_ring<P, L, D, 2, 6>, gs, bs, bs * ring_bytes(2, w), d, cfl, loc);
-          } else if (tuning_.grad_chunk == 8) {
-            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 8, 8>, gs, bs, bs * ring_bytes(8, w), d, cfl, loc);
-            else launch_smem(kGradients, k_gradients_ring<P, L, D, 8, 6>, gs, bs, bs * ring_bytes(8, w), d, cfl, loc);
-          } else {
-            if (tight) launch_smem(kGradients, k_gradients_ring<P, L, D, 4, 8>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
-            else launch_smem(kGradients, k_gradients_ring<P, L, D, 4, 6>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
-          }
+          if (tuning_.grad_chunk == 2)
+            launch_smem(kGradients, k_gradients_ring<P, L, D, 2>, gs, bs, bs * ring_bytes(2, w), d, cfl, loc);
+          else if (tuning_.grad_chunk == 8)
+            launch_smem(kGradients, k_gradients_ring<P, L, D, 8>, gs, bs, bs * ring_bytes(8, w), d, cfl, loc);
+          else
+            launch_smem(kGradients, k_gradients_ring<P, L, D, 4>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
           return;
         }
         if (tuning_.grad_mode == 2)

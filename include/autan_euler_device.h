@@ -170,8 +170,7 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * shared memory by TMA bulk copies, at most 128 threads per block; 2: as 0, software-pipelined:
  * the next entry's gather and the row after it in flight while an entry is added; 3: each
  * thread's next [0] neighbour records and 2 x [0] rows in a shared-memory ring filled by
- * asynchronous copies (cp.async), [0] = 2, 4 or 8, at most 128 threads per block; 4: as 3 with
- * the registers capped at 64 per thread).
+ * asynchronous copies (cp.async), [0] = 2, 4 or 8, at most 128 threads per block).
  * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
  * (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,

@@ -198,7 +198,7 @@ def test_tuning_variants_are_bit_identical(precision):
     u_o, *_ = run_oracle(case, case.steps)
     no = case.mesh.n_owned_cells
     for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 2), (1, 4), (1, 8), (2, 1), (3, 2), (3, 4),
-                         (3, 8), (4, 4), (4, 8)):
+                         (3, 8)):
         for mode in (0, 1):
             for block in (64, 128) if gmode else (64, 256):
                 with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
@@ -219,7 +219,7 @@ def test_gradient_stagings_agree_on_the_channel(precision):
     case = cases.bump_channel(24, 10, 4, steps=3, precision=precision)
     out = {}
     for gmode, chunk, block in ((0, 1, 128), (1, 4, 128), (2, 1, 64), (3, 2, 64), (3, 4, 128),
-                                (3, 8, 128), (4, 4, 128), (4, 8, 64)):  # fmt: skip
+                                (3, 8, 128)):  # fmt: skip
         with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
             dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=1, face_block=128,
                            gather_block=128, grad_mode=gmode)  # fmt: skip
