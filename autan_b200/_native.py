@@ -180,6 +180,7 @@ def _bind(lib: C.CDLL) -> None:
            P(MarchResult), C.c_char_p, sz)  # fmt: skip
         fn("autan_euler_device_set_cases", C.c_int, vp, i32, P(i64), C.c_char_p, sz)
         fn("autan_euler_device_set_active", C.c_int, vp, P(u8), C.c_char_p, sz)
+        fn("autan_euler_device_set_case_mach_ref", C.c_int, vp, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_case_history", C.c_int, vp, i64, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_march_cases", C.c_int, vp, f64, f64, i32, i32, i64, i32, f64, P(f64),
            P(f64), P(i64), P(i32), P(f64), P(i64), P(f64), C.c_char_p, sz)  # fmt: skip

@@ -257,6 +257,23 @@ class Batch:
     def n_cells(self) -> int:
         return int(self.mesh["n_owned_cells"])
 
+    @property
+    def mach_ref(self) -> np.ndarray:
+        """Per case, its AUSM+-up cut-off Mach number: the case's own freestream Mach, as a run of
+        the case alone sets Scheme::mach_ref."""
+        return np.array([p["mach"] for p in self.params], dtype=np.float64)
+
+    def open(self, device: int = 0):
+        """The batch on the device: an EulerDevice of the union mesh with the cases and their
+        cut-off Mach numbers set (the caller uploads a state)."""
+        from autan_b200.euler import EulerDevice
+
+        dev = EulerDevice(self.mesh, self.scheme, self.bc_kind, self.bc_data, weights=self.weights,
+                          device=device)  # fmt: skip
+        dev.set_cases(self.cell_offsets)
+        dev.set_case_mach_ref(self.mach_ref)
+        return dev
+
 
 def batch_parameters(n_cases, seed, cells) -> list[dict]:
     """The seeded per-case draws of bump_batch (numpy default_rng(seed)), in case order: target
@@ -296,9 +313,11 @@ def bump_batch(n_cases=256, seed=0, cells=(20_000, 500_000), flux="roe", precisi
     channel's extent, hybrid rows as bump_channel). Inflow and outflow faces take the farfield
     state of the case's freestream (rho = 1, p = 1 / gamma, speed Mach, at the flow angle in the
     x-y plane); bump, top and z sides slip. walls: keep each case's bump-wall triangles
-    (params[k]["wall"], t x 9, as WallSurface builds them) for the wall distance. A common scheme (second order, Venkatakrishnan K = 5)
-    and reference state (Mach 0.5 along x) serve every case; local steps make the cases
-    independent. inlet="state": the inflow faces take the freestream as a given state and the
+    (params[k]["wall"], t x 9, as WallSurface builds them) for the wall distance. A common scheme (second order, Venkatakrishnan K = 5,
+    limiter scales and reference state of Mach 0.5 along x) serves every case, except the AUSM+-up
+    cut-off Mach number, which is each case's own (Batch.mach_ref, set by Batch.open: with one
+    shared cut-off above their Mach number, cases at Mach 0.30-0.42 stall in a limit cycle three
+    decades above their round-off band); local steps make the cases independent. inlet="state": the inflow faces take the freestream as a given state and the
     outflow faces its static pressure (no exp/log on the path, for bit-exact tests). select: the
     case indices to build (default all), the draws being those of all n_cases."""
     draws = batch_parameters(n_cases, seed, cells)

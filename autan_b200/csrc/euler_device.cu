@@ -129,6 +129,9 @@ struct Dev {
   // they span two cases; a warp of a stopped case leaves before reading its face records.
   const int* face_warp_case;
   const int* bface_warp_case;
+  // Per case, the AUSM+-up cut-off Mach number (each case's own freestream Mach), or null for the
+  // scheme's one value.
+  const typename P::C* case_minf;
 };
 
 // Whether owned cell c takes part (its case has not stopped).
@@ -971,6 +974,17 @@ __device__ __forceinline__ void cell_recon(const Dev<P>& d, int c, typename P::C
   }
 }
 
+// The scheme's values for a face of owner cell `owner`: with per-case cut-offs, the AUSM+-up
+// cut-off Mach number of the owner's case (M_co of ausm_up, kernels/euler.py:268-303).
+template <int FLUX, class P>
+__device__ __forceinline__ Params<typename P::C> face_params(const Dev<P>& d, int owner) {
+  Params<typename P::C> p = d.p;
+  if constexpr (FLUX == 2) {
+    if (d.case_minf != nullptr) p.minf = d.case_minf[d.case_of[owner]];
+  }
+  return p;
+}
+
 // The flux of interior face f in its orientation (roe_face / hllc_face / ausm_face,
 // kernels/euler.py:687-753, planar forms :783-844): both sides reconstructed, the numerical flux
 // times the area, plus the warped-face term.
@@ -986,7 +1000,7 @@ __device__ __forceinline__ void interior_flux(const Dev<P>& d, int f, const type
   C fl[5], frr[5], fx[5];
   reconstruct(wl, gl, pl, fr + 4, d.p.pref, fl);
   reconstruct(wr, gr, pr, fr + 8, d.p.pref, frr);
-  numerical_flux<FLUX>(fl, frr, n, d.p, fx);
+  numerical_flux<FLUX>(fl, frr, n, face_params<FLUX>(d, index_of(fr[7])), fx);
   if constexpr (PLANAR) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
@@ -1036,7 +1050,7 @@ __device__ __forceinline__ void boundary_flux(const Dev<P>& d, int b, const type
   } else {
     C wbv[5], fx[5];
     boundary_value(wf, kind, br + 8, n, d.p, wbv);
-    numerical_flux<FLUX>(wf, wbv, n, d.p, fx);
+    numerical_flux<FLUX>(wf, wbv, n, face_params<FLUX>(d, index_of(br[13])), fx);
 #pragma unroll
     for (int k = 0; k < 5; ++k) out[k] = area * fx[k];
   }
@@ -1769,6 +1783,7 @@ class Stepper {
   virtual int conservation(double* sums) = 0;
   virtual void set_cases(int n_cases, const int64_t* cell_offsets) = 0;
   virtual void set_active(const uint8_t* active) = 0;
+  virtual void set_case_mach_ref(const double* mach_ref) = 0;
   virtual void case_history(long long count, double* rms) = 0;
   virtual int n_cases() const = 0;
   cudaStream_t stream = nullptr;
@@ -2011,6 +2026,7 @@ class Impl final : public Stepper {
     d_.active = nullptr;
     d_.face_warp_case = nullptr;
     d_.bface_warp_case = nullptr;
+    d_.case_minf = nullptr;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     if (tuning_.face_mode == 1) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
@@ -2557,6 +2573,20 @@ class Impl final : public Stepper {
              nbo_, static_cast<const int*>(case_of_.as<int>()), bface_warp_case_.as<int>());
     d_.face_warp_case = face_warp_case_.as<int>();
     d_.bface_warp_case = bface_warp_case_.as<int>();
+    d_.case_minf = nullptr;
+    check(cudaStreamSynchronize(stream), "cases");
+  }
+
+  void set_case_mach_ref(const double* mach_ref) override {
+    if (n_cases_ == 0) fail("E1101: no cases set");
+    std::vector<C> v(n_cases_);
+    for (int k = 0; k < n_cases_; ++k) {
+      if (!(mach_ref[k] > 0.0)) fail("E1101: AUSM+-up needs a positive cut-off Mach number");
+      v[k] = static_cast<C>(mach_ref[k]);
+    }
+    drop_graph();
+    case_minf_ = upload(v, stream);
+    d_.case_minf = case_minf_.as<C>();
     check(cudaStreamSynchronize(stream), "cases");
   }
 
@@ -2774,7 +2804,7 @@ class Impl final : public Stepper {
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
   Buffer bface_r64_, face_mult_, cons_words_;  // boundary pressure and conservation
   Buffer case_of_, case_cells_, case_words_, case_hist_, active_;  // batched cases
-  Buffer face_warp_case_, bface_warp_case_;
+  Buffer face_warp_case_, bface_warp_case_, case_minf_;
   int n_cases_ = 0;
   double pref64_ = 0.0;
   int max_faces_ = 0;
@@ -3197,6 +3227,14 @@ int autan_euler_device_march(void* handle, double cfl, double dt, int32_t local,
 int autan_euler_device_set_cases(void* handle, int32_t n_cases, const int64_t* cell_offsets,
                                  char* err, size_t err_len) {
   AUTAN_CALL(h->set_cases(n_cases, cell_offsets));
+}
+
+int autan_euler_device_set_case_mach_ref(void* handle, const double* mach_ref, char* err,
+                                         size_t err_len) {
+  AUTAN_CALL({
+    if (mach_ref == nullptr) fail("E1101: null cut-off Mach numbers");
+    h->set_case_mach_ref(mach_ref);
+  });
 }
 
 int autan_euler_device_set_active(void* handle, const uint8_t* active, char* err, size_t err_len) {

@@ -267,6 +267,13 @@ class EulerDevice:
         self.n_cases = off.size - 1
         self._call("autan_euler_device_set_cases", int(self.n_cases), N.ptr(off, C.c_int64))
 
+    def set_case_mach_ref(self, mach_ref) -> None:
+        """Per case, the AUSM+-up cut-off Mach number (n_cases values) in place of the scheme's."""
+        m = np.ascontiguousarray(mach_ref, dtype=np.float64)
+        if m.size != self.n_cases:
+            raise ValueError("one cut-off Mach number per case")
+        self._call("autan_euler_device_set_case_mach_ref", N.ptr(m, C.c_double))
+
     def set_active(self, active) -> None:
         a = np.ascontiguousarray(active, dtype=np.uint8)
         self._call("autan_euler_device_set_active", N.ptr(a, C.c_uint8))

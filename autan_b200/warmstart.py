@@ -222,11 +222,7 @@ def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, re
     """The batched march of `batch` from u0 (5 x n_cells), drops taken from `reference` (cases x 5)
     or each case's first iteration: per-case iterations, GPU time, the converged states and the
     bump forces."""
-    from autan_b200.euler import EulerDevice
-
-    with EulerDevice(batch.mesh, batch.scheme, batch.bc_kind, batch.bc_data, weights=batch.weights,
-                     device=device) as dev:  # fmt: skip
-        dev.set_cases(batch.cell_offsets)
+    with batch.open(device) as dev:
         dev.upload(u0)
         res = dev.march_cases(cfl=batch.cfl, local=True, rk=batch.rk, max_steps=max_steps,
                               batch=batch_steps, orders=orders, floors=floors(batch),

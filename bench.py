@@ -430,9 +430,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         case = cases.vortex_tets(nx, ny, nz, precision="fp32+acc64")
     n = case.mesh.n_owned_cells
     if batch is not None:
-        dev = EulerDevice(batch.mesh, batch.scheme, batch.bc_kind, batch.bc_data,
-                          weights=batch.weights, device=local_rank)  # fmt: skip
-        dev.set_cases(batch.cell_offsets)
+        dev = batch.open(local_rank)
     else:
         dev = EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data, device=local_rank)
     dev.upload(case.u0)

@@ -239,6 +239,12 @@ int autan_euler_device_set_cases(void* handle, int32_t n_cases, const int64_t* c
                                  char* err, size_t err_len);
 /* One flag per case, nonzero: the case steps. */
 int autan_euler_device_set_active(void* handle, const uint8_t* active, char* err, size_t err_len);
+/* Per case (n_cases values, each positive), the AUSM+-up cut-off Mach number M_co
+ * (Scheme::mach_ref, kernels/euler.py:268-303) of the faces whose owner cell is in the case, in
+ * place of the scheme's one value: each case then steps as its own run with its own mach_ref
+ * would. Reset by autan_euler_device_set_cases. No other flux uses it. */
+int autan_euler_device_set_case_mach_ref(void* handle, const double* mach_ref, char* err,
+                                         size_t err_len);
 /* The per-case RMS of the last `count` steps of the last step call: count x n_cases x 5, oldest
  * first. */
 int autan_euler_device_case_history(void* handle, int64_t count, double* rms, char* err,

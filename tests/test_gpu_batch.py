@@ -30,8 +30,8 @@ def device_of(b):
     return dev
 
 
-def case_oracle(b, k):
-    """Case k alone: its own mesh, boundary data and oracle."""
+def case_oracle(b, k, scheme=None):
+    """Case k alone: its own mesh, boundary data and oracle (with `scheme`, default the batch's)."""
     p = b.params[k]
     m = M.bump_channel(*p["boxes"], bump=p["bump"])
     first = sum(cases_b(b, j) for j in range(k))
@@ -40,8 +40,9 @@ def case_oracle(b, k):
     data = np.ascontiguousarray(b.bc_data[:, first : first + nb])
     c0, c1 = b.cell_offsets[k], b.cell_offsets[k + 1]
     u0 = np.ascontiguousarray(b.u0[:, c0:c1])
-    md = cases.oracle_mesh_dict(cases.Case("k", m, b.scheme, kind, data, u0, 3, 1.5, 1, True))
-    return O.Oracle(md, b.scheme.as_dict(), kind, data), u0
+    sch = b.scheme if scheme is None else scheme
+    md = cases.oracle_mesh_dict(cases.Case("k", m, sch, kind, data, u0, 3, 1.5, 1, True))
+    return O.Oracle(md, sch.as_dict(), kind, data), u0
 
 
 def cases_b(b, j):
@@ -92,3 +93,22 @@ def test_batched_march_converges_each_case_at_its_own_iteration():
         norms = [o.step(uk, rk=3, cfl=b.cfl, local=True)[0] for _ in range(int(res["iterations"][k]))]
         it, _ = O.convergence_iteration(np.array(norms), 2.0)
         assert it == res["iterations"][k], (k, it, res["iterations"][k])
+
+
+def test_per_case_cut_off_mach_numbers():
+    """AUSM+-up with each case's own cut-off Mach number (Batch.open): every case steps bit for bit
+    as its own run whose scheme has mach_ref = the case's Mach number."""
+    import dataclasses
+
+    b = cases.bump_batch(3, seed=2, cells=(800, 3000), precision="fp64", inlet="state", flux="ausm")
+    assert len(set(b.mach_ref)) == 3
+    with b.open() as dev:
+        dev.upload(b.u0)
+        dev.step(cfl=b.cfl, rk=3, n_steps=4, local=True)
+        u = dev.download()
+    for k in range(3):
+        o, uk = case_oracle(b, k, dataclasses.replace(b.scheme, mach_ref=float(b.mach_ref[k])))
+        for _ in range(4):
+            o.step(uk, rk=3, cfl=b.cfl, local=True)
+        c0, c1 = b.cell_offsets[k], b.cell_offsets[k + 1]
+        assert bits_equal(u[:, c0:c1], uk), k
