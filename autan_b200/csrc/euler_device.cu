@@ -402,6 +402,16 @@ __device__ __forceinline__ void load5(const typename P::C* src, typename P::C* w
   }
 }
 
+// The stencil bounds (min and max over the stencil values, kernels/euler.py:510-521) with the
+// hardware min/max. They can differ from the keep-the-first rule only in the sign of a zero bound
+// (a NaN value is passed over by both), and the limiter uses a bound only as dp = bound - w_c:
+// when the sign differs dp is zero, and venkat adds dp only as dp * dp (+0) or as a zero product
+// to a sum of eps2 > 0 and d^2 terms, so phi has the same bits either way.
+__device__ __forceinline__ float bound_min(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float bound_max(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double bound_min(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double bound_max(double a, double b) { return fmax(a, b); }
+
 // Fire-and-forget TMA prefetch of a contiguous range into L2 (cp.async.bulk.prefetch.L2, no shared
 // memory, no completion to wait for): ptr 16-byte aligned, bytes a multiple of 16, issued in
 // pieces of at most 32 KB.
@@ -543,8 +553,8 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
       }
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
-        if (wn[i] < lo[i]) lo[i] = wn[i];
-        if (wn[i] > hi[i]) hi[i] = wn[i];
+        lo[i] = bound_min(lo[i], wn[i]);
+        hi[i] = bound_max(hi[i], wn[i]);
       }
     };
     auto row = [&](int j, C* e) {
@@ -723,8 +733,8 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
           }
 #pragma unroll
           for (int i = 0; i < 5; ++i) {
-            if (wn[q][i] < lo[i]) lo[i] = wn[q][i];
-            if (wn[q][i] > hi[i]) hi[i] = wn[q][i];
+            lo[i] = bound_min(lo[i], wn[q][i]);
+            hi[i] = bound_max(hi[i], wn[q][i]);
           }
         }
       }
@@ -918,8 +928,8 @@ __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl,
       }
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
-        if (wn[i] < lo[i]) lo[i] = wn[i];
-        if (wn[i] > hi[i]) hi[i] = wn[i];
+        lo[i] = bound_min(lo[i], wn[i]);
+        hi[i] = bound_max(hi[i], wn[i]);
       }
       if (j + D < len) issue_gather(x, gw);
       if (j + 2 * D < len) issue_row(j + 2 * D, rw);
