@@ -77,13 +77,20 @@ __global__ void __launch_bounds__(128) k_dense(const bf16* A, int lda, int M, in
   bf16* As = reinterpret_cast<bf16*>(smem);
   bf16* Bs = As + kRowsPerBlock * sk;
   const int row0 = blockIdx.x * kRowsPerBlock;
-  for (int i = threadIdx.x; i < kRowsPerBlock * K; i += blockDim.x) {
-    const int r = i / K, k = i % K;
-    As[r * sk + k] = row0 + r < M ? A[static_cast<long long>(row0 + r) * lda + k] : __float2bfloat16(0.0f);
+  // staged in 16-byte pieces (K, lda, ldb multiples of 8 elements; rows of sk elements stay
+  // 16-byte aligned)
+  const int kv = K / 8;
+  for (int i = threadIdx.x; i < kRowsPerBlock * kv; i += blockDim.x) {
+    const int r = i / kv, v = i % kv;
+    const uint4 val = row0 + r < M
+                          ? *reinterpret_cast<const uint4*>(A + static_cast<long long>(row0 + r) * lda + 8 * v)
+                          : make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(As + r * sk + 8 * v) = val;
   }
-  for (int i = threadIdx.x; i < N * K; i += blockDim.x) {
-    const int n = i / K, k = i % K;
-    Bs[n * sk + k] = B[static_cast<long long>(n) * ldb + k];
+  for (int i = threadIdx.x; i < N * kv; i += blockDim.x) {
+    const int n = i / kv, v = i % kv;
+    *reinterpret_cast<uint4*>(Bs + n * sk + 8 * v) =
+        *reinterpret_cast<const uint4*>(B + static_cast<long long>(n) * ldb + 8 * v);
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -95,18 +102,20 @@ __global__ void __launch_bounds__(128) k_dense(const bf16* A, int lda, int M, in
     for (int q = 0; q < 4; ++q) acc[j][q] = 0.0f;
   const bf16* ar = As + (16 * warp) * sk;
   for (int k0 = 0; k0 < K; k0 += 16) {
+    // fragments as 32-bit pairs of adjacent elements (even offsets: 4-byte aligned)
+    auto pair = [](const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); };
     uint32_t a[4];
-    a[0] = pack2(ar[g * sk + k0 + 2 * t], ar[g * sk + k0 + 2 * t + 1]);
-    a[1] = pack2(ar[(g + 8) * sk + k0 + 2 * t], ar[(g + 8) * sk + k0 + 2 * t + 1]);
-    a[2] = pack2(ar[g * sk + k0 + 2 * t + 8], ar[g * sk + k0 + 2 * t + 9]);
-    a[3] = pack2(ar[(g + 8) * sk + k0 + 2 * t + 8], ar[(g + 8) * sk + k0 + 2 * t + 9]);
+    a[0] = pair(ar + g * sk + k0 + 2 * t);
+    a[1] = pair(ar + (g + 8) * sk + k0 + 2 * t);
+    a[2] = pair(ar + g * sk + k0 + 2 * t + 8);
+    a[3] = pair(ar + (g + 8) * sk + k0 + 2 * t + 8);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       if (8 * j < N) {
         const bf16* br = Bs + (8 * j + g) * sk + k0;
         uint32_t b[2];
-        b[0] = pack2(br[2 * t], br[2 * t + 1]);
-        b[1] = pack2(br[2 * t + 8], br[2 * t + 9]);
+        b[0] = pair(br + 2 * t);
+        b[1] = pair(br + 2 * t + 8);
         mma16816(acc[j], a, b);
       }
     }
@@ -139,13 +148,17 @@ __global__ void __launch_bounds__(256) k_wgrad(const bf16* dZ, int ldz, const bf
   auto Ds = reinterpret_cast<bf16 (*)[kMaxWidth + 8]>(wsm);
   auto As = reinterpret_cast<bf16 (*)[kMaxWidth + 8]>(wsm + kChunk * (kMaxWidth + 8) * 2);
   const int m0 = blockIdx.x * kChunk;
-  for (int i = threadIdx.x; i < kChunk * N; i += blockDim.x) {
-    const int r = i / N, n = i % N;
-    Ds[r][n] = m0 + r < M ? dZ[static_cast<long long>(m0 + r) * ldz + n] : __float2bfloat16(0.0f);
+  // staged in 16-byte pieces (N, K, ldz, lda multiples of 8 elements)
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int i = threadIdx.x; i < kChunk * (N / 8); i += blockDim.x) {
+    const int r = i / (N / 8), v = i % (N / 8);
+    *reinterpret_cast<uint4*>(&Ds[r][8 * v]) =
+        m0 + r < M ? *reinterpret_cast<const uint4*>(dZ + static_cast<long long>(m0 + r) * ldz + 8 * v) : zero;
   }
-  for (int i = threadIdx.x; i < kChunk * K; i += blockDim.x) {
-    const int r = i / K, k = i % K;
-    As[r][k] = m0 + r < M ? A[static_cast<long long>(m0 + r) * lda + k] : __float2bfloat16(0.0f);
+  for (int i = threadIdx.x; i < kChunk * (K / 8); i += blockDim.x) {
+    const int r = i / (K / 8), v = i % (K / 8);
+    *reinterpret_cast<uint4*>(&As[r][8 * v]) =
+        m0 + r < M ? *reinterpret_cast<const uint4*>(A + static_cast<long long>(m0 + r) * lda + 8 * v) : zero;
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -197,12 +210,26 @@ __global__ void k_sum_partials(const float* partial, int chunks, int size, float
   for (int c = 0; c < chunks; ++c) s += partial[static_cast<long long>(c) * size + i];
   grad[i] = s;
 }
-__global__ void k_column_sums(const float* dz, int ld, int M, int N, float* out) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+// Column sums of dz [M x ld] over the rows of chunk blockIdx.y (kChunk rows), columns
+// 32 blockIdx.x + threadIdx.x: each of the block's 8 row lanes sums every 8th row, the lanes are
+// then added in lane order; partial[chunk][n] (summed over the chunks in order by k_sum_partials).
+__global__ void __launch_bounds__(256) k_column_partials(const float* dz, int ld, int M, int N,
+                                                         float* partial) {
+  __shared__ float lane_sum[8][33];
+  const int n = blockIdx.x * 32 + threadIdx.x;
+  const long long r0 = static_cast<long long>(blockIdx.y) * kChunk;
+  const long long r1 = min(r0 + kChunk, static_cast<long long>(M));
   float s = 0.0f;
-  for (int r = 0; r < M; ++r) s += dz[static_cast<long long>(r) * ld + n];
-  out[n] = s;
+  if (n < N)
+    for (long long r = r0 + threadIdx.y; r < r1; r += 8) s += dz[r * ld + n];
+  lane_sum[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && n < N) {
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t += lane_sum[k][threadIdx.x];
+    partial[static_cast<long long>(blockIdx.y) * N + n] = t;
+  }
 }
 
 // Standardised inputs of rows idx (or 0..n-1) as BF16 [n x ldx] (zero padding).
@@ -608,6 +635,7 @@ class Net {
   }
   ~Net() {
     cudaStreamSynchronize(stream_);
+    if (se_host_ != nullptr) cudaFreeHost(se_host_);
     cudaStreamDestroy(stream_);
   }
 
@@ -647,7 +675,12 @@ class Net {
 
   // Forward and backward of `rows` rows (x: raw inputs, y: raw targets, idx: rows of them or null);
   // the gradient into grad_, the loss returned.
-  float forward_backward(const float* x, const float* y, const int* idx, int rows) {
+  // The minibatch loss (mean squared error of the standardised outputs). With se_host (pinned,
+  // rows floats) the per-row squared errors are copied there asynchronously and 0 is returned:
+  // the caller sums them (loss_of) after a synchronisation.
+  float forward_backward(const float* x, const float* y, const int* idx, int rows,
+                         float* se_host = nullptr) {
+    if (rows > 65535LL * kChunk) fail("E1101: at most 65535 x 128 rows in one forward-backward pass");
     ensure_work(rows);
     const int L = static_cast<int>(layers_.size());
     launch_inputs(x, idx, rows);
@@ -689,9 +722,14 @@ class Net {
       check(cudaMemcpy2DAsync(grad_.as<float>() + Ly.w0, Ly.in * 4, wfull_.as<float>(), Ly.kp * 4,
                               Ly.in * 4, Ly.out, cudaMemcpyDeviceToDevice, stream_),
             "wgrad copy");
-      k_column_sums<<<blocks(Ly.out, 128), 128, 0, stream_>>>(
-          dz_.as<float>(), Ly.np, rows, Ly.out, grad_.as<float>() + Ly.w0 + static_cast<long long>(Ly.out) * Ly.in);
+      // bias gradient: column sums of dZ per row chunk into the (now free) partials, then summed
+      k_column_partials<<<dim3((Ly.out + 31) / 32, chunks), dim3(32, 8), 0, stream_>>>(
+          dz_.as<float>(), Ly.np, rows, Ly.out, partial_.as<float>());
       check(cudaGetLastError(), "bias grad");
+      k_sum_partials<<<blocks(Ly.out, 256), 256, 0, stream_>>>(
+          partial_.as<float>(), chunks, Ly.out,
+          grad_.as<float>() + Ly.w0 + static_cast<long long>(Ly.out) * Ly.in);
+      check(cudaGetLastError(), "bias grad sum");
       if (l == 0) break;
       // dA_{l-1} = dZ_l W_l: the dense kernel on W^T [kp x np]
       const Layer& Lp = layers_[l - 1];
@@ -702,11 +740,19 @@ class Net {
           dzb_.as<bf16>());
       check(cudaGetLastError(), "gelu back");
     }
+    if (se_host != nullptr) {
+      check(cudaMemcpyAsync(se_host, se_.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
+      return 0.0f;
+    }
     std::vector<float> se(rows);
     check(cudaMemcpyAsync(se.data(), se_.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
     sync();
+    return loss_of(se.data(), rows);
+  }
+
+  float loss_of(const float* se, int rows) const {
     double s = 0.0;
-    for (float v : se) s += v;
+    for (int i = 0; i < rows; ++i) s += se[i];
     return static_cast<float>(s / (static_cast<double>(rows) * outputs_));
   }
 
@@ -720,13 +766,22 @@ class Net {
     long long done = 0;
     for (long long i = 0; i < n_data_; ++i) perm[i] = static_cast<int>(i);
     ensure(idx_, static_cast<size_t>(n_data_) * 4);
+    // an epoch's per-row squared errors, copied without a synchronisation per step
+    const size_t staged = static_cast<size_t>(per_epoch) * batch;
+    if (staged > se_host_n_) {
+      if (se_host_ != nullptr) cudaFreeHost(se_host_);
+      se_host_ = nullptr;
+      se_host_n_ = 0;
+      check(cudaMallocHost(reinterpret_cast<void**>(&se_host_), staged * sizeof(float)), "cudaMallocHost");
+      se_host_n_ = staged;
+    }
     for (int e = 0; e < epochs; ++e) {
       std::shuffle(perm.begin(), perm.end(), rng);
       copy(idx_, perm.data(), static_cast<size_t>(n_data_) * 4);
-      double sum = 0.0;
       long long steps = 0;
       for (long long r0 = 0; r0 + batch <= n_data_; r0 += batch) {
-        sum += forward_backward(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch);
+        forward_backward(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch,
+                         se_host_ + static_cast<size_t>(steps) * batch);
         ++t_;
         // cosine decay of the learning rate over the call's steps
         const float rate = lr * 0.5f * (1.0f + std::cos(3.14159265358979f * static_cast<float>(done) / total));
@@ -740,6 +795,9 @@ class Net {
         round_weights();
         ++steps;
       }
+      sync();
+      double sum = 0.0;
+      for (long long q = 0; q < steps; ++q) sum += loss_of(se_host_ + static_cast<size_t>(q) * batch, batch);
       if (loss != nullptr) loss[e] = static_cast<float>(steps > 0 ? sum / steps : 0.0);
     }
     sync();
@@ -906,6 +964,8 @@ class Net {
   bool wgrad_attr_ = false;
   bool tc_ = false;  // tcgen05 engine
   Buf params_, grad_, m_, v_, in_mean_, in_sd_, out_mean_, out_sd_, x_, y_, idx_, fault_;
+  float* se_host_ = nullptr;  // pinned: an epoch's per-row squared errors
+  size_t se_host_n_ = 0;
   Buf x0_, acts_, zs_, dz_, dzb_, da_, se_, partial_, wfull_, pbias_;
   std::vector<std::unique_ptr<Buf>> wb_, wt_;
 };
