@@ -411,18 +411,40 @@ __global__ void __launch_bounds__(128) k_tc_gemm(const bf16* A, int lda, int M, 
           *reinterpret_cast<const uint4*>(B + static_cast<long long>(n) * ldb + 8 * g);
     }
   } else {
-    for (int i = threadIdx.x; i < kTcRows * kTcRows; i += blockDim.x) {
-      const int r = i / kTcRows, n = i % kTcRows;  // row r of the chunk, neuron n
-      bf16 v = __float2bfloat16(0.0f);
-      if (n < N0 && r0 + r < M) v = A[(r0 + r) * lda + n];
-      *reinterpret_cast<bf16*>(ps + kmajor(n, r, kTcRows)) = v;
-    }
-    for (int i = threadIdx.x; i < kTcRows * N; i += blockDim.x) {
-      const int r = i / N, k = i % N;
-      bf16 v = __float2bfloat16(0.0f);
-      if (r0 + r < M) v = B[(r0 + r) * ldb + k];
-      *reinterpret_cast<bf16*>(qs + kmajor(k, r, N)) = v;
-    }
+    // Both operands transposed (the contraction runs over the chunk's rows): 8 x 8 blocks in two
+    // halves, eight 8-byte loads of 8 rows' 4 columns, transposed in registers, four 16-byte
+    // stores of one column's 8 rows (contiguous in the K-major layout). Columns n >= N0 of A are zero (N0 and
+    // N multiples of 8; lda, ldb multiples of 8 elements).
+    auto block8 = [&](const bf16* src, int ld, int cols, int bound, unsigned char* dst, int R) {
+      const int nb = cols >> 3;
+      for (int i = threadIdx.x; i < (kTcRows >> 3) * nb; i += blockDim.x) {
+        const int rb = i / nb, cb = i % nb;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // columns 4 h .. 4 h + 3 of the block
+          uint32_t w[8][2];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const long long r = r0 + 8 * rb + q;
+            uint2 v = make_uint2(0u, 0u);
+            if (8 * cb < bound && r < M) v = *reinterpret_cast<const uint2*>(src + r * ld + 8 * cb + 4 * h);
+            w[q][0] = v.x;
+            w[q][1] = v.y;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const unsigned sel = (j & 1) ? 0x7632u : 0x5410u;  // high or low halves of two words
+            uint4 o;
+            o.x = __byte_perm(w[0][j >> 1], w[1][j >> 1], sel);
+            o.y = __byte_perm(w[2][j >> 1], w[3][j >> 1], sel);
+            o.z = __byte_perm(w[4][j >> 1], w[5][j >> 1], sel);
+            o.w = __byte_perm(w[6][j >> 1], w[7][j >> 1], sel);
+            *reinterpret_cast<uint4*>(dst + kmajor(8 * cb + 4 * h + j, 8 * rb, R)) = o;
+          }
+        }
+      }
+    };
+    block8(A, lda, kTcRows, N0, ps, kTcRows);  // element (n, r) of dZ^T
+    block8(B, ldb, N, N, qs, N);               // element (k, r) of A_prev^T
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
