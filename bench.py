@@ -172,25 +172,36 @@ def gpu_uuid(device: int) -> str:
 
 def cpu_throughput(steps: int, warmup: int, threads: int,
                    slab: tuple[int, int, int] = (240, 24, 6),
-                   workload: str = "tets") -> tuple[float, str, int]:  # fmt: skip
+                   workload: str = "tets", min_seconds: float = 0.0) -> tuple[float, str, int]:  # fmt: skip
     """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
-    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64), or for the
-    channel workload its own channel of `slab` boxes; the rate of the whole host."""
+    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64), for the channel
+    workload its own channel of `slab` boxes, for the batch workload its own 20 000-cell channel of
+    the batch's distribution and scheme (the first draw of seed 0); the rate of the whole host.
+    `steps` steps, then more until at least `min_seconds` have passed."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle as O
     from autan_b200 import cases
 
-    if workload == "channel":
-        case = cases.bump_channel(*slab, steps=1)
+    if workload == "batch":
+        b = cases.bump_batch(1, seed=0, cells=(20_000, 20_000))
+        md, sch, kind, data, u0 = b.mesh, b.scheme.as_dict(), b.bc_kind, b.bc_data, b.u0
+        cfl, local, cells = b.cfl, True, b.n_cells
+        what = f"{b.params[0]['boxes'][0]}x{b.params[0]['boxes'][1]}x{b.params[0]['boxes'][2]} batch channel"
     else:
-        case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
-    md = cases.oracle_mesh_dict(case)
-    sch = case.scheme.as_dict()
-    oracles = [O.Oracle(md, sch, case.bc_kind, case.bc_data) for _ in range(threads)]
-    states = [case.u0.copy() for _ in range(threads)]
+        if workload == "channel":
+            case = cases.bump_channel(*slab, steps=1)
+            what = f"{slab[0]}x{slab[1]}x{slab[2]} channel"
+        else:
+            case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
+            what = f"{slab[0]}x{slab[1]}x{slab[2]} slab of the benchmark lattice"
+        md, sch = cases.oracle_mesh_dict(case), case.scheme.as_dict()
+        kind, data, u0 = case.bc_kind, case.bc_data, case.u0
+        cfl, local, cells = case.cfl, case.local, case.mesh.n_owned_cells
+    oracles = [O.Oracle(md, sch, kind, data) for _ in range(threads)]
+    states = [u0.copy() for _ in range(threads)]
 
     def one_step(i):
-        oracles[i].step(states[i], rk=3, cfl=case.cfl, local=case.local)
+        oracles[i].step(states[i], rk=3, cfl=cfl, local=local)
 
     def all_threads():
         ts = [threading.Thread(target=one_step, args=(i,)) for i in range(threads)]
@@ -202,14 +213,14 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
     for _ in range(warmup):
         all_threads()
     t0 = time.perf_counter()
-    for _ in range(steps):
+    done = 0
+    while done < steps or time.perf_counter() - t0 < min_seconds:
         all_threads()
+        done += 1
     elapsed = time.perf_counter() - t0
-    cells = case.mesh.n_owned_cells
-    rate = cells * threads * steps / elapsed
-    what = "channel" if workload == "channel" else "slab of the benchmark lattice"
-    sample = (f"{threads} threads x {steps} SSP-RK3 steps of a {slab[0]}x{slab[1]}x{slab[2]} {what} "
-              f"({cells} cells), CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
+    rate = cells * threads * done / elapsed
+    sample = (f"{threads} threads x {done} SSP-RK3 steps of a {what} ({cells} cells each), "
+              f"CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
     return rate, sample, threads
 
 
@@ -558,7 +569,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         if world == 1 and not args.no_cpu:
             rate, sample, cores = cpu_throughput(2, 1, args.cpu_threads or host_threads(),
-                                                 cpu_slab(args), args.workload)  # fmt: skip
+                                                 cpu_slab(args), args.workload, min_seconds=10.0)  # fmt: skip
             line["cpu_baseline"] = {"value": rate, "unit": "cell-iterations/s", "cores": cores,
                                     "kind": "port", "sample": sample}  # fmt: skip
         print(json.dumps(line), flush=True)
