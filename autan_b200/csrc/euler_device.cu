@@ -453,16 +453,18 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 #pragma unroll
   for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
   const C* g = out + 5;
-  C phi[5];
-  C vol = C(0);
+  // phi, and the limiter's per-cell arguments (the same in every face's venkat call): the
+  // bounds' distances from the cell value and eps^2.
+  C phi[5], dmax[5], dmin[5], eps2[5];
   if constexpr (LIMIT) {
+    const C vol = static_cast<C>(__ldg(d.volume + c));
 #pragma unroll
     for (int i = 0; i < 5; ++i) {
-      lo[i] = minv(lo[i], wc[i]);
-      hi[i] = maxv(hi[i], wc[i]);
+      dmax[i] = maxv(hi[i], wc[i]) - wc[i];
+      dmin[i] = minv(lo[i], wc[i]) - wc[i];
+      eps2[i] = d.p.scale[i] * vol;
       phi[i] = C(INFINITY);
     }
-    vol = static_cast<C>(__ldg(d.volume + c));
   }
   // One pass over the cell's incidences for both the limiter (its record: rel(x_f, x_c) of this
   // side) and, with DT, spectral_radius (:1103-1112: the other side's state, the face's normal
@@ -487,7 +489,7 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
           const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+          const C v = venkat(dd, dmax[i], dmin[i], eps2[i]);
           if (v < phi[i]) phi[i] = v;
         }
       }
@@ -747,16 +749,16 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
     const C* irow = inc + 4 * (__ldg(d.inc_start + (c >> 5)) - i0 + (c & 31));
     const C* drow = ndt + (irow - inc);
     const int il = __ldg(d.inc_len + c);
-    C phi[5];
-    C vol = C(0);
+    C phi[5], dmax[5], dmin[5], eps2[5];
     if constexpr (LIMIT) {
+      const C vol = static_cast<C>(__ldg(d.volume + c));
 #pragma unroll
       for (int i = 0; i < 5; ++i) {
-        lo[i] = minv(lo[i], wc[i]);
-        hi[i] = maxv(hi[i], wc[i]);
+        dmax[i] = maxv(hi[i], wc[i]) - wc[i];
+        dmin[i] = minv(lo[i], wc[i]) - wc[i];
+        eps2[i] = d.p.scale[i] * vol;
         phi[i] = C(INFINITY);
       }
-      vol = static_cast<C>(__ldg(d.volume + c));
     }
     // One pass over the staged incidence records for the limiter and, with DT, spectral_radius
     // (:1103-1112: the other side's state from the limiter record, the normal and area staged).
@@ -775,7 +777,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
 #pragma unroll
           for (int i = 0; i < 5; ++i) {
             const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-            const C v = venkat(dd, hi[i] - wc[i], lo[i] - wc[i], d.p.scale[i] * vol);
+            const C v = venkat(dd, dmax[i], dmin[i], eps2[i]);
             if (v < phi[i]) phi[i] = v;
           }
         }
