@@ -489,8 +489,9 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
           const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          const C v = venkat(dd, dmax[i], dmin[i], eps2[i]);
-          if (v < phi[i]) phi[i] = v;
+          // venkat's value is >= 0 and never -0 (its numerator adds 2 d dp, >= 0, to
+          // dp^2 + eps2 >= +0), or NaN: the hardware min is then the keep-the-first min
+          phi[i] = bound_min(phi[i], venkat(dd, dmax[i], dmin[i], eps2[i]));
         }
       }
       if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
@@ -777,8 +778,9 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
 #pragma unroll
           for (int i = 0; i < 5; ++i) {
             const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-            const C v = venkat(dd, dmax[i], dmin[i], eps2[i]);
-            if (v < phi[i]) phi[i] = v;
+            // venkat's value is >= 0 and never -0 (its numerator adds 2 d dp, >= 0, to
+            // dp^2 + eps2 >= +0), or NaN: the hardware min is then the keep-the-first min
+            phi[i] = bound_min(phi[i], venkat(dd, dmax[i], dmin[i], eps2[i]));
           }
         }
         if constexpr (DT) {
