@@ -8,7 +8,7 @@
 //                    neighbour's whole reconstruction data is one cache line, read with 16-byte
 //                    vector loads; three record buffers rotate through the RK stages;
 //   FP64 SoA         u (conserved), RK stage, RK4 accumulator, residual, volume (streamed);
-//   stencil          face2 entries, each {w_x, w_y, w_z, cell or -(b + 1)} in 16 B (fp32), in a
+//   stencil          face2 entries, each {w_x, w_y, w_z, cell or n + b} in 16 B (fp32), in a
 //                    sliced ELLPACK layout (32 cells per slice, entry j of cell c at
 //                    start[c / 32] + 32 j + c % 32): a warp reads entry j of its cells as 512
 //                    contiguous bytes;
@@ -95,11 +95,11 @@ struct Dev {
   int n_if;  // owned interior faces
   Params<C> p;
   double ref[5];
-  const C* prim;      // kPrimW x n: the primitives this stage reads
+  const C* prim;      // kPrimW x n: the primitives this stage reads, then its boundary states
   C* prim_next;       // the primitives this stage writes
   C* recon;           // phi and grad of this stage: kRecon / kGroup groups of kGroup x n words
   long long rstride;  // words from one group to the next (kGroup x n)
-  C* prim_b;       // kPrimB x nb
+  C* prim_b;       // kPrimB x nb: this stage's boundary states (prim's buffer after n records)
   double* u;
   double* stage;
   double* racc;
@@ -114,7 +114,8 @@ struct Dev {
   const int* inc_len;
   const int* inc_code;
   const C* inc_rec;  // 4 per incidence, sliced: rel(x_f, x_c) of the cell's side, the other side
-                     // (its cell's value index, or -(b + 1) for boundary face b)
+                     // (its cell's value index, or n + b for boundary face b: the primitive
+                     // buffers hold the boundary states after the cells)
   const C* inc_dt;   // 4 per incidence, sliced: the face's unit normal and area
   int n_slices;
   const C* face;    // kFace per owned interior face
@@ -481,9 +482,7 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
       if constexpr (DT) {
         load_words<P, sizeof(C) == 8>(d.inc_dt + at, 0, 4, nd);
         const int o = index_of(r[3]);
-        load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
-                        : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
-                 wn);
+        load5<P>(d.prim + static_cast<long long>(o) * kPrimW, wn);
       }
       if constexpr (LIMIT) {
 #pragma unroll
@@ -565,9 +564,7 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
     };
     auto gather = [&](const C* e, C* w) {
       const int x = index_of(e[3]);
-      load5<P>(x >= 0 ? d.prim + static_cast<long long>(x) * kPrimW
-                      : d.prim_b + static_cast<long long>(-x - 1) * kPrimB,
-               w);
+      load5<P>(d.prim + static_cast<long long>(x) * kPrimW, w);
     };
     if constexpr (CHUNK == 0) {
       // Software pipeline: while entry j is added, the gather of entry j + 1 and the row of entry
@@ -718,9 +715,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
       for (int q = 0; q < kChunk; ++q) {
         if (j0 + q < len) {
           const int e = index_of(row[4 * kSlice * (j0 + q) + 3]);
-          load5<P>(e >= 0 ? d.prim + static_cast<long long>(e) * kPrimW
-                          : d.prim_b + static_cast<long long>(-e - 1) * kPrimB,
-                   wn[q]);
+          load5<P>(d.prim + static_cast<long long>(e) * kPrimW, wn[q]);
         }
       }
 #pragma unroll
@@ -770,9 +765,7 @@ __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int
         C wn[5];
         if constexpr (DT) {
           const int o = index_of(r[3]);
-          load5<P>(o >= 0 ? d.prim + static_cast<long long>(o) * kPrimW
-                          : d.prim_b + static_cast<long long>(-o - 1) * kPrimB,
-                   wn);
+          load5<P>(d.prim + static_cast<long long>(o) * kPrimW, wn);
         }
         if constexpr (LIMIT) {
 #pragma unroll
@@ -887,8 +880,7 @@ __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl,
       return index_of(reinterpret_cast<const C*>(rpiece(slot, kR16 - 1))[kW - 1]);
     };
     auto issue_gather = [&](int x, int slot) {
-      const C* src = x >= 0 ? d.prim + static_cast<long long>(x) * kPrimW
-                            : d.prim_b + static_cast<long long>(-x - 1) * kPrimB;
+      const C* src = d.prim + static_cast<long long>(x) * kPrimW;
 #pragma unroll
       for (int q = 0; q < kG16; ++q) cp_async_ca<16>(g16 + ((slot * kG16 + q) * nt + t) * 16, src + q * kW);
       cp_async_ca<kGRem>(grem + (slot * nt + t) * kGRem, src + kG16 * kW);
@@ -1930,11 +1922,12 @@ class Impl final : public Stepper {
         // The other side: the owner for the neighbour's incidence and the reverse, or the face.
         const C* q = v >= 0 ? face.data() + static_cast<long long>(f) * kFace
                             : bface_host_.data() + static_cast<long long>(f - ni_) * kBface;
-        irec[4 * at + 3] = v >= 0 ? ((v & 1) ? q[7] : q[11]) : index_bits<C>(v);
+        irec[4 * at + 3] = v >= 0 ? ((v & 1) ? q[7] : q[11]) : index_bits<C>(n_ + (f - ni_));
         for (int a = 0; a < 4; ++a) idt[4 * at + a] = q[a];
       }
     }
-    // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, value index or -(b + 1)}.
+    // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, record}: the record of a cell
+    // value (its value index) or of boundary face b's state (n + b).
     const bool has_stencil =
         m.stencil != nullptr && m.stencil_offsets != nullptr && m.stencil_lsq_weight != nullptr;
     std::vector<long long> soff(n_ + 1, 0);
@@ -1953,7 +1946,7 @@ class Impl final : public Stepper {
         } else {
           const int f = -e - 1;
           if (f < ni_ || f >= nf_) fail("E1101: a stencil entry is not a boundary face");
-          v = -(f - ni_ + 1);
+          v = n_ + (f - ni_);  // the boundary state's record, after the cells' records
         }
         C* q = ste.data() + 4 * st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
         for (int a = 0; a < 3; ++a) q[a] = static_cast<C>(m.stencil_lsq_weight[a * nst + k]);
@@ -1978,9 +1971,9 @@ class Impl final : public Stepper {
       max_faces_ = std::max<int>(max_faces_, static_cast<int>(m.cell_face_offsets[c + 1] - m.cell_face_offsets[c]));
     // Device arrays.
     const size_t n5 = 5ULL * n_;
-    for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * n_ * sizeof(C));
+    // each primitive buffer holds the owned cells' records, then the boundary faces' states
+    for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * (n_ + std::max(nb_, 1)) * sizeof(C));
     recon_.alloc(static_cast<size_t>(kRecon) * n_ * sizeof(C));
-    prim_b_.alloc(static_cast<size_t>(kPrimB) * std::max(nb_, 1) * sizeof(C));
     u_.alloc(n5 * sizeof(double));
     stage_.alloc(n5 * sizeof(double));
     racc_.alloc(n5 * sizeof(double));
@@ -2003,14 +1996,14 @@ class Impl final : public Stepper {
     f_m_ = upload(fm, stream);
     bface_ = upload(bface_host_, stream);
     b_m_ = upload(bm, stream);
-    for (Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
+    for (Buffer* b : {&u_, &stage_, &racc_, &res_, &dt_local_, &ctl_})
       check(cudaMemsetAsync(b->ptr(), 0, b->bytes(), stream), "memset");
     for (auto& b : prim_) check(cudaMemsetAsync(b.ptr(), 0, b.bytes(), stream), "memset");
     check(cudaMemsetAsync(recon_.ptr(), 0, recon_.bytes(), stream), "memset");
     d_.n = n_;
     d_.nb = nb_;
     d_.n_if = nif_;
-    d_.prim_b = prim_b_.as<C>();
+    d_.prim_b = prim_[0].as<C>() + static_cast<long long>(kPrimW) * n_;
     d_.recon = recon_.as<C>();
     d_.rstride = static_cast<long long>(kGroup) * n_;
     d_.u = u_.as<double>();
@@ -2053,7 +2046,7 @@ class Impl final : public Stepper {
 
   long long device_bytes() const override {
     long long t = 0;
-    for (const Buffer* b : {&prim_b_, &u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
+    for (const Buffer* b : {&u_, &stage_, &racc_, &res_, &dt_local_, &ctl_, &volume_,
                             &st_start_, &st_len_, &st_e_, &inc_start_, &inc_len_, &inc_code_,
                             &face_, &f_m_, &bface_, &b_m_, &source_, &flux_, &bflux_,
                             &inc_rec_, &inc_dt_, &bface_r64_, &face_mult_, &cons_words_})
@@ -2440,6 +2433,7 @@ class Impl final : public Stepper {
   Dev<P> with_rec(int in, int out) const {
     Dev<P> d = d_;
     d.prim = prim_[in].as<C>();
+    d.prim_b = prim_[in].as<C>() + static_cast<long long>(kPrimW) * n_;  // this stage's boundary states
     d.prim_next = prim_[out].as<C>();
     return d;
   }
@@ -2814,7 +2808,7 @@ class Impl final : public Stepper {
   Dev<P> d_{};
   Buffer prim_[3];  // primitive records, rotated through the stages
   Buffer recon_;    // phi and grad of the current stage
-  Buffer prim_b_, u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
+  Buffer u_, stage_, racc_, res_, dt_local_, ctl_, volume_;
   Buffer st_start_, st_len_, st_e_, inc_start_, inc_len_, inc_code_, inc_rec_, inc_dt_;
   Buffer bface_r64_, face_mult_, cons_words_;  // boundary pressure and conservation
   Buffer case_of_, case_cells_, case_words_, case_hist_, active_;  // batched cases
