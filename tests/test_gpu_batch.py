@@ -112,3 +112,23 @@ def test_per_case_cut_off_mach_numbers():
             o.step(uk, rk=3, cfl=b.cfl, local=True)
         c0, c1 = b.cell_offsets[k], b.cell_offsets[k + 1]
         assert bits_equal(u[:, c0:c1], uk), k
+
+
+def test_per_case_cut_off_mach_numbers_are_checked():
+    """One positive cut-off per case, and only after set_cases: anything else is refused with the
+    library's error code, and the handle keeps working."""
+    from autan_b200._native import NativeError
+
+    b = small_batch()
+    with EulerDevice(b.mesh, b.scheme, bc_kind=b.bc_kind, bc_data=b.bc_data, weights=b.weights) as dev:
+        dev.n_cases = 3
+        with pytest.raises(NativeError, match="E1101"):
+            dev.set_case_mach_ref([0.5, 0.5, 0.5])  # no cases set yet
+        dev.set_cases(b.cell_offsets)
+        with pytest.raises(NativeError, match="E1101"):
+            dev.set_case_mach_ref([0.5, 0.0, 0.5])
+        with pytest.raises(ValueError):
+            dev.set_case_mach_ref([0.5, 0.5])
+        dev.set_case_mach_ref([0.4, 0.5, 0.6])
+        dev.upload(b.u0)
+        dev.step(cfl=b.cfl, rk=3, n_steps=2, local=True)
