@@ -665,8 +665,16 @@ __device__ __forceinline__ bool bounded_wait(unsigned long long* bar, Control* c
 // stencil rows and per-incidence limiter records staged into shared memory by one TMA bulk copy
 // each (the slices' rows are contiguous in the sliced layout): the block's whole streaming input
 // is in flight at once, and the threads then only gather their neighbours' primitives (L2).
+// In fp32+acc64, registers sized for 6 blocks of 128 per SM (80 a thread) up to 4 entries in
+// flight; the 8-entry form and the FP64 policy keep their own (they spill under that bound).
+template <class P>
+constexpr int staged_min_blocks(int chunk) {
+  return (chunk >= 8 || sizeof(typename P::C) == 8) ? 1 : 6;
+}
 template <class P, bool LIMIT, bool DT, int CHUNK>
-__global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
+__global__ void __launch_bounds__(128, staged_min_blocks<P>(CHUNK)) k_gradients_tma(Dev<P> d,
+                                                                                    double cfl,
+                                                                                    int local) {
   using C = typename P::C;
   if (block_idle(d)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
