@@ -522,8 +522,19 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
 // are read CHUNK at a time (their loads, then the neighbours' loads, all in flight together) and
 // added in stencil order. With DT, also the cell's CFL step and the block's minimum.
+// Two entries in flight in fp32+acc64: registers sized for 7 blocks of 128 per SM (at most 128
+// threads a block); the other forms take up to 256 threads.
+template <class P>
+constexpr int unstaged_threads(int chunk) {
+  return (chunk == 2 && sizeof(typename P::C) == 4) ? 128 : 256;
+}
+template <class P>
+constexpr int unstaged_min_blocks(int chunk) {
+  return (chunk == 2 && sizeof(typename P::C) == 4) ? 7 : 1;
+}
 template <class P, bool LIMIT, bool DT, int CHUNK>
-__global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int local) {
+__global__ void __launch_bounds__(unstaged_threads<P>(CHUNK), unstaged_min_blocks<P>(CHUNK))
+    k_gradients(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
   if (block_idle(d)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1758,6 +1769,8 @@ void Tuning::validate() const {
   auto block_ok = [](int b) { return b >= 32 && b <= 256 && b % 32 == 0; };
   if (grad_mode == 0 && grad_chunk != 1 && grad_chunk != 2 && grad_chunk != 4)
     fail("E1101: grad_chunk is 1, 2 or 4");
+  if (grad_mode == 0 && grad_chunk == 2 && grad_block > 128)
+    fail("E1101: the gradient kernel with 2 entries in flight takes <= 128 threads");
   if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
@@ -2305,6 +2318,7 @@ class Impl final : public Stepper {
       for (int chunk : {1, 2, 4, 8})
         for (int block : {64, 128, 256}) {
           if (mode == 0 && chunk == 8) continue;
+          if (mode == 0 && chunk == 2 && block > 128) continue;
           if (mode == 2 && chunk != 1) continue;
           if ((mode == 1 || mode == 3) && (chunk == 1 || block > 128)) continue;
           Tuning t = keep;

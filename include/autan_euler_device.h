@@ -163,16 +163,16 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
                                     int64_t n_steps, double* ms, int64_t* launches, char* err,
                                     size_t err_len);
 /* Launch choices of the hot kernels (6 values): [0] stencil entries the gradient kernel loads
- * together (1, 2 or 4; 2, 4 or 8 when staged), [1] its threads per block, [2] face strategy (0 gather-recompute: each
- * cell recomputes its faces' fluxes; 1 store-gather: each face's flux once into a face scratch,
- * then summed per cell), [3] threads per block of the face kernel, [4] of the store-gather sum,
- * [5] gradient staging (0: each thread loads its stencil rows; 1: each block's rows staged into
- * shared memory by TMA bulk copies, at most 128 threads per block; 2: as 0, software-pipelined:
- * the next entry's gather and the row after it in flight while an entry is added; 3: each
- * thread's next [0] neighbour records and 2 x [0] rows in a shared-memory ring filled by
- * asynchronous copies (cp.async), [0] = 2, 4 or 8, at most 128 threads per block).
- * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
- * (codegen/include/autan/kernels/strategy.hpp:14-21). */
+ * together (1, 2 or 4, where 2 takes at most 128 threads per block; 2, 4 or 8 when staged), [1]
+ * its threads per block, [2] face strategy (0 gather-recompute: each cell recomputes its faces'
+ * fluxes; 1 store-gather: each face's flux once into a face scratch, then summed per cell), [3]
+ * threads per block of the face kernel, [4] of the store-gather sum, [5] gradient staging (0:
+ * each thread loads its stencil rows; 1: each block's rows staged into shared memory by TMA bulk
+ * copies, at most 128 threads per block; 2: as 0, software-pipelined: the next entry's gather and
+ * the row after it in flight while an entry is added; 3: each thread's next [0] neighbour records
+ * and 2 x [0] rows in a shared-memory ring filled by asynchronous copies (cp.async), [0] = 2, 4
+ * or 8, at most 128 threads per block). Every choice gives the same bits. No counterpart in the
+ * reference beyond its Strategy enum (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
                                   size_t err_len);
 int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, char* err,
