@@ -522,19 +522,8 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
 // are read CHUNK at a time (their loads, then the neighbours' loads, all in flight together) and
 // added in stencil order. With DT, also the cell's CFL step and the block's minimum.
-// Two entries in flight in fp32+acc64: registers sized for 7 blocks of 128 per SM (at most 128
-// threads a block); the other forms take up to 256 threads.
-template <class P>
-constexpr int unstaged_threads(int chunk) {
-  return (chunk == 2 && sizeof(typename P::C) == 4) ? 128 : 256;
-}
-template <class P>
-constexpr int unstaged_min_blocks(int chunk) {
-  return (chunk == 2 && sizeof(typename P::C) == 4) ? 7 : 1;
-}
 template <class P, bool LIMIT, bool DT, int CHUNK>
-__global__ void __launch_bounds__(unstaged_threads<P>(CHUNK), unstaged_min_blocks<P>(CHUNK))
-    k_gradients(Dev<P> d, double cfl, int local) {
+__device__ __forceinline__ void gradients_cells(const Dev<P>& d, double cfl, int local) {
   using C = typename P::C;
   if (block_idle(d)) return;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -619,6 +608,19 @@ __global__ void __launch_bounds__(unstaged_threads<P>(CHUNK), unstaged_min_block
   if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int local) {
+  gradients_cells<P, LIMIT, DT, CHUNK>(d, cfl, local);
+}
+
+// Two entries in flight in fp32+acc64, registers sized for 7 blocks of 128 per SM (at most 128
+// threads a block): 72 registers instead of 80. Only this form gets the bound; given to the
+// others it makes them spill.
+template <class P, bool LIMIT, bool DT>
+__global__ void __launch_bounds__(128, 7) k_gradients_occ7(Dev<P> d, double cfl, int local) {
+  gradients_cells<P, LIMIT, DT, 2>(d, cfl, local);
+}
+
 // ---------------------------------------------------------------- TMA bulk staging
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -676,16 +678,8 @@ __device__ __forceinline__ bool bounded_wait(unsigned long long* bar, Control* c
 // stencil rows and per-incidence limiter records staged into shared memory by one TMA bulk copy
 // each (the slices' rows are contiguous in the sliced layout): the block's whole streaming input
 // is in flight at once, and the threads then only gather their neighbours' primitives (L2).
-// In fp32+acc64, registers sized for 6 blocks of 128 per SM (80 a thread) up to 4 entries in
-// flight; the 8-entry form and the FP64 policy keep their own (they spill under that bound).
-template <class P>
-constexpr int staged_min_blocks(int chunk) {
-  return (chunk >= 8 || sizeof(typename P::C) == 8) ? 1 : 6;
-}
 template <class P, bool LIMIT, bool DT, int CHUNK>
-__global__ void __launch_bounds__(128, staged_min_blocks<P>(CHUNK)) k_gradients_tma(Dev<P> d,
-                                                                                    double cfl,
-                                                                                    int local) {
+__device__ __forceinline__ void gradients_staged_cells(const Dev<P>& d, double cfl, int local) {
   using C = typename P::C;
   if (block_idle(d)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -820,6 +814,19 @@ __global__ void __launch_bounds__(128, staged_min_blocks<P>(CHUNK)) k_gradients_
     }
   }
   if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
+  gradients_staged_cells<P, LIMIT, DT, CHUNK>(d, cfl, local);
+}
+
+// fp32+acc64 with up to 4 entries in flight, registers sized for 6 blocks of 128 per SM: the
+// stage-0 form (with the time step) drops from 94 to 80 registers. The 8-entry form and the FP64
+// policy spill under that bound and keep k_gradients_tma.
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__global__ void __launch_bounds__(128, 6) k_gradients_tma_occ6(Dev<P> d, double cfl, int local) {
+  gradients_staged_cells<P, LIMIT, DT, CHUNK>(d, cfl, local);
 }
 
 // ---------------------------------------------------------------- asynchronous-copy ring
@@ -2688,12 +2695,20 @@ class Impl final : public Stepper {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
         if (tuning_.grad_mode == 1) {
           const int sm = static_cast<int>(staged_smem(bs, D));
-          if (tuning_.grad_chunk == 2)
-            launch_smem(kGradients, k_gradients_tma<P, L, D, 2>, blocks(n_, bs), bs, sm, d, cfl, loc);
-          else if (tuning_.grad_chunk == 8)
-            launch_smem(kGradients, k_gradients_tma<P, L, D, 8>, blocks(n_, bs), bs, sm, d, cfl, loc);
-          else
-            launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, blocks(n_, bs), bs, sm, d, cfl, loc);
+          const int gb = blocks(n_, bs);
+          if (tuning_.grad_chunk == 8) {
+            launch_smem(kGradients, k_gradients_tma<P, L, D, 8>, gb, bs, sm, d, cfl, loc);
+          } else if constexpr (sizeof(C) == 4) {  // fp32+acc64: the 6-blocks-per-SM bound
+            if (tuning_.grad_chunk == 2)
+              launch_smem(kGradients, k_gradients_tma_occ6<P, L, D, 2>, gb, bs, sm, d, cfl, loc);
+            else
+              launch_smem(kGradients, k_gradients_tma_occ6<P, L, D, 4>, gb, bs, sm, d, cfl, loc);
+          } else {
+            if (tuning_.grad_chunk == 2)
+              launch_smem(kGradients, k_gradients_tma<P, L, D, 2>, gb, bs, sm, d, cfl, loc);
+            else
+              launch_smem(kGradients, k_gradients_tma<P, L, D, 4>, gb, bs, sm, d, cfl, loc);
+          }
           return;
         }
         if (tuning_.grad_mode == 3) {
@@ -2706,14 +2721,18 @@ class Impl final : public Stepper {
             launch_smem(kGradients, k_gradients_ring<P, L, D, 4>, gs, bs, bs * ring_bytes(4, w), d, cfl, loc);
           return;
         }
-        if (tuning_.grad_mode == 2)
+        if (tuning_.grad_mode == 2) {
           launch_as(kGradients, k_gradients<P, L, D, 0>, gs, bs, d, cfl, loc);
-        else if (tuning_.grad_chunk == 1)
+        } else if (tuning_.grad_chunk == 1) {
           launch_as(kGradients, k_gradients<P, L, D, 1>, gs, bs, d, cfl, loc);
-        else if (tuning_.grad_chunk == 2)
-          launch_as(kGradients, k_gradients<P, L, D, 2>, gs, bs, d, cfl, loc);
-        else
+        } else if (tuning_.grad_chunk == 2) {
+          if constexpr (sizeof(C) == 4)  // fp32+acc64: the 7-blocks-per-SM bound
+            launch_as(kGradients, k_gradients_occ7<P, L, D>, gs, bs, d, cfl, loc);
+          else
+            launch_as(kGradients, k_gradients<P, L, D, 2>, gs, bs, d, cfl, loc);
+        } else {
           launch_as(kGradients, k_gradients<P, L, D, 4>, gs, bs, d, cfl, loc);
+        }
       };
       if (limiter_) {
         if (dt) go(std::true_type{}, std::true_type{});
