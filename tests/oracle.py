@@ -95,6 +95,11 @@ class Oracle:
             t = types.get(k, f64)
             dt = {i32: np.int32, i64: np.int64, f64: np.float64}[t]
             a = np.ascontiguousarray(mesh[k], dtype=dt)
+            if a.size == 0 and k == "face_moment":
+                # no moments (planar meshes): NULL, as the C side reads 9 x n_faces of them
+                # whenever the pointer is set
+                setattr(m, k, None)
+                continue
             if a.size == 0:
                 a = np.zeros(1, dtype=dt)
             self.keep[k] = a

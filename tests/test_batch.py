@@ -54,3 +54,16 @@ def test_union_residual_is_each_cases_residual():
         ok = O.Oracle(md, b.scheme.as_dict(), kind, data)
         want = ok.residual(np.ascontiguousarray(u[:, c0:c1]))
         assert np.array_equal(res[:, c0:c1].view(np.int64), want.view(np.int64))
+
+
+def test_oracle_takes_no_moments_for_a_planar_union():
+    """A planar batch's union mesh carries no face moments (an empty array); the oracle must get a
+    NULL pointer for them, not a stand-in element: its set-up reads 9 x n_faces moments from any
+    pointer it is given."""
+    b = cases.bump_batch(2, seed=0, cells=(300, 500))
+    assert b.mesh["all_planar"] and np.asarray(b.mesh["face_moment"]).size == 0
+    o = O.Oracle(b.mesh, b.scheme.as_dict(), b.bc_kind, b.bc_data)
+    assert not o.mesh.face_moment  # NULL
+    u = b.u0.copy()
+    o.step(u, rk=3, cfl=b.cfl, local=True)
+    assert np.all(np.isfinite(u))
