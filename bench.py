@@ -157,6 +157,70 @@ class ClockSampler:
         }
 
 
+class NvmlClockSampler:
+    """The SM clock and the clock-event reasons read through NVML by a host thread about every
+    millisecond while the timed region runs (nvidia-smi's sampling period can exceed a short
+    region). Reading only: no setting of the GPU is changed."""
+
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}  # fmt: skip
+
+    def __init__(self, uuid: str):
+        import pynvml
+
+        self.nvml = pynvml
+        pynvml.nvmlInit()
+        self.handle = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        self.samples = []
+        self.stop = threading.Event()
+        self.thread = None
+
+    def sample(self):
+        n = self.nvml
+        self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
+                             int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))))  # fmt: skip
+
+    def run(self):
+        while not self.stop.is_set():
+            self.sample()
+            time.sleep(0.001)
+
+    def __enter__(self):
+        self.sample()
+        self.thread = threading.Thread(target=self.run, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.thread.join()
+        self.sample()
+        try:
+            self.nvml.nvmlShutdown()
+        except Exception:
+            pass
+
+    def summary(self) -> dict:
+        reasons = set()
+        for _, bits in self.samples:
+            for name, attr in self.REASONS.items():
+                if bits & getattr(self.nvml, attr):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml"}  # fmt: skip
+
+
+def clock_sampler(uuid: str):
+    """NVML sampling when it is available, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(uuid)
+    except Exception:
+        return ClockSampler(uuid)
+
+
 def gpu_uuid(device: int) -> str:
     import torch
 
@@ -482,7 +546,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     launches0 = dev.counters()["launches"]
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(gpu_uuid(local_rank)) as clocks:
+    with clock_sampler(gpu_uuid(local_rank)) as clocks:
         start.record(stream)
         r = dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.steps, graph=True)
         end.record(stream)

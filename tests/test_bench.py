@@ -22,3 +22,28 @@ def test_traffic_is_per_mesh_family_and_scales_with_cells():
     assert bench.committed_traffic("gradients", 2 * 994_600, "channel") == pytest.approx(2 * channel)
     assert bench.committed_traffic("faces", 1000, "tets") is None
     assert bench.committed_traffic("gradients", 1000, "hex") is None
+
+
+def test_nvml_clock_sampler_against_a_fake_nvml(monkeypatch):
+    """The clock record of the timed region read through NVML (here a fake: 1900 MHz under a
+    1965 MHz maximum with the power cap active): median clock, maximum, the active reasons by
+    name, and samples taken through a short region."""
+    import time
+    import types
+
+    fake = types.SimpleNamespace(
+        nvmlInit=lambda: None, nvmlShutdown=lambda: None, NVML_CLOCK_SM=1,
+        nvmlDeviceGetHandleByUUID=lambda uuid: "handle",
+        nvmlDeviceGetMaxClockInfo=lambda h, c: 1965, nvmlDeviceGetClockInfo=lambda h, c: 1900,
+        nvmlDeviceGetCurrentClocksEventReasons=lambda h: 0x4,
+        nvmlClocksEventReasonHwSlowdown=0x8, nvmlClocksEventReasonHwThermalSlowdown=0x40,
+        nvmlClocksEventReasonSwThermalSlowdown=0x20, nvmlClocksEventReasonSwPowerCap=0x4,
+    )  # fmt: skip
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    clocks = bench.clock_sampler("GPU-0")
+    assert isinstance(clocks, bench.NvmlClockSampler)
+    with clocks:
+        time.sleep(0.03)
+    s = clocks.summary()
+    assert s["sm_mhz"] == 1900 and s["sm_max_mhz"] == 1965
+    assert s["reasons"] == ["sw_power_cap"] and s["samples"] >= 3
