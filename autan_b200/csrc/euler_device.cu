@@ -70,6 +70,7 @@ constexpr int kRecon = 24;  // reconstruction words per cell: phi 0-4, grad 5-19
 constexpr int kFace = 12;   // interior face record width
 constexpr int kBface = 16;  // boundary face record width
 constexpr int kPrimB = 8;   // boundary state record width
+static_assert(kPrimB == kPrimW, "boundary states share the primitive buffers' record index (n + b)");
 
 // Step control in device memory: written by the kernels, read by the host after a batch.
 struct Control {

@@ -180,8 +180,11 @@ class NvmlClockSampler:
 
     def sample(self):
         n = self.nvml
-        self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
-                             int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))))  # fmt: skip
+        try:
+            self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
+                                 int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))))  # fmt: skip
+        except Exception:  # a failed read leaves the record short; the bench goes on
+            pass
 
     def run(self):
         while not self.stop.is_set():
@@ -209,8 +212,9 @@ class NvmlClockSampler:
             for name, attr in self.REASONS.items():
                 if bits & getattr(self.nvml, attr):
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml"}  # fmt: skip
+        sm = [c for c, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}  # fmt: skip
 
 
 def clock_sampler(uuid: str):

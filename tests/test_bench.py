@@ -47,3 +47,22 @@ def test_nvml_clock_sampler_against_a_fake_nvml(monkeypatch):
     s = clocks.summary()
     assert s["sm_mhz"] == 1900 and s["sm_max_mhz"] == 1965
     assert s["reasons"] == ["sw_power_cap"] and s["samples"] >= 3
+
+
+def test_nvml_clock_sampler_survives_failed_reads(monkeypatch):
+    """An NVML read that fails leaves the clock record short (here empty) without stopping the
+    timed region."""
+    import types
+
+    def fail(*a):
+        raise RuntimeError("NVML read failed")
+
+    fake = types.SimpleNamespace(
+        nvmlInit=lambda: None, nvmlShutdown=lambda: None, NVML_CLOCK_SM=1,
+        nvmlDeviceGetHandleByUUID=lambda uuid: "handle", nvmlDeviceGetMaxClockInfo=lambda h, c: 1965,
+        nvmlDeviceGetClockInfo=fail, nvmlDeviceGetCurrentClocksEventReasons=fail,
+    )  # fmt: skip
+    monkeypatch.setitem(sys.modules, "pynvml", fake)
+    with bench.clock_sampler("GPU-0") as clocks:
+        pass
+    assert clocks.summary()["sm_mhz"] is None and clocks.summary()["samples"] == 0
