@@ -244,19 +244,24 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
     """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
     slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64), for the channel
     workload its own channel of `slab` boxes, for the batch workload its own 20 000-cell channel of
-    the batch's distribution and scheme (the first draw of seed 0); the rate of the whole host.
+    the batch's distribution and scheme (the first draw of seed 0), for the hex workload its own
+    copy of the 8 192-cell vortex (fp64, classical RK4); the rate of the whole host.
     `steps` steps, then more until at least `min_seconds` have passed."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle as O
     from autan_b200 import cases
 
+    rk = 3
     if workload == "batch":
         b = cases.bump_batch(1, seed=0, cells=(20_000, 20_000))
         md, sch, kind, data, u0 = b.mesh, b.scheme.as_dict(), b.bc_kind, b.bc_data, b.u0
         cfl, local, cells = b.cfl, True, b.n_cells
         what = f"{b.params[0]['boxes'][0]}x{b.params[0]['boxes'][1]}x{b.params[0]['boxes'][2]} batch channel"
     else:
-        if workload == "channel":
+        if workload == "hex":
+            case = cases.vortex_hex(steps=1)
+            what = "64x64x2 hexahedral vortex (fp64)"
+        elif workload == "channel":
             case = cases.bump_channel(*slab, steps=1)
             what = f"{slab[0]}x{slab[1]}x{slab[2]} channel"
         else:
@@ -264,12 +269,12 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
             what = f"{slab[0]}x{slab[1]}x{slab[2]} slab of the benchmark lattice"
         md, sch = cases.oracle_mesh_dict(case), case.scheme.as_dict()
         kind, data, u0 = case.bc_kind, case.bc_data, case.u0
-        cfl, local, cells = case.cfl, case.local, case.mesh.n_owned_cells
+        cfl, local, cells, rk = case.cfl, case.local, case.mesh.n_owned_cells, case.rk
     oracles = [O.Oracle(md, sch, kind, data) for _ in range(threads)]
     states = [u0.copy() for _ in range(threads)]
 
     def one_step(i):
-        oracles[i].step(states[i], rk=3, cfl=cfl, local=local)
+        oracles[i].step(states[i], rk=rk, cfl=cfl, local=local)
 
     def all_threads():
         ts = [threading.Thread(target=one_step, args=(i,)) for i in range(threads)]
@@ -287,7 +292,8 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
         done += 1
     elapsed = time.perf_counter() - t0
     rate = cells * threads * done / elapsed
-    sample = (f"{threads} threads x {done} SSP-RK3 steps of a {what} ({cells} cells each), "
+    kind_of_step = "SSP-RK3" if rk == 3 else "RK4"
+    sample = (f"{threads} threads x {done} {kind_of_step} steps of a {what} ({cells} cells each), "
               f"CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
     return rate, sample, threads
 
