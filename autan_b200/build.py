@@ -41,8 +41,9 @@ NVCC_FLAGS = [
 ]
 
 HOST_SOURCES = ["setup.cpp"]
-CUDA_SOURCES = ["euler_device.cu", "norms_static.cu", "mlp.cu"]
-HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp", "convergence.hpp"]
+CUDA_SOURCES = ["euler_device.cu", "norms_static.cu", "mlp.cu", "setup_device.cu"]
+HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp", "convergence.hpp",
+           "setup_rules.cuh"]
 
 
 def _newer(src: Path, obj: Path, deps: list[Path]) -> bool:

@@ -4,6 +4,7 @@
 #include "autan_b200_setup.h"
 #include "autan_euler_device.h"
 #include "convergence.hpp"
+#include "setup_rules.cuh"
 
 #include <algorithm>
 #include <array>
@@ -18,6 +19,7 @@
 
 namespace {
 
+namespace setup = autan_b200::setup;
 using i32 = std::int32_t;
 using i64 = std::int64_t;
 using Vec = std::array<double, 3>;
@@ -572,56 +574,24 @@ void compute_geometry(Mesh& m) {
   }
 }
 
-// cell_stencil, face2 kind (codegen/cpp/geometry.cpp:432-560): the face neighbours and their face
-// neighbours (the cell itself left out), ascending, then the boundary faces of the cell and of its
-// face neighbours, ascending, each as -(f + 1).
+// The face2 stencil of every cell (owned and ghost) with the shared rule of setup_rules.cuh
+// (codegen/cpp/geometry.cpp:432, StencilKind::face2): one pass, each cell's entries appended.
+setup::MeshView view_of(const Mesh& m) {
+  return {m.n_cells, m.n_owned, m.n_faces, m.n_interior, m.cell_face_offsets.data(),
+          m.cell_faces.data(), m.owner.data(), m.neighbour.data(), m.cell_centroid.data(),
+          m.face_centroid.data()};
+}
+
 void face2_stencil(Mesh& m) {
-  const auto nc = static_cast<std::size_t>(m.n_cells);
-  const i32 nint = m.n_interior;
-  m.stencil_offsets.assign(nc + 1, 0);
+  const setup::MeshView v = view_of(m);
+  m.stencil_offsets.assign(static_cast<std::size_t>(m.n_cells) + 1, 0);
   m.stencil.clear();
-  std::vector<i32> listed(nc, -1), blisted(static_cast<std::size_t>(m.n_faces - nint), -1);
-  std::vector<i32> cells, bfaces;
-  auto across = [&](i32 c, i32 f) { return m.owner[f] == c ? m.neighbour[f] : m.owner[f]; };
+  std::vector<i32> buf(setup::kMaxCandidates), row(setup::kMaxCandidates);
   for (i32 c = 0; c < m.n_cells; ++c) {
-    cells.clear();
-    bfaces.clear();
-    listed[c] = c;
-    auto add_cell = [&](i32 n) {
-      if (listed[n] != c) {
-        listed[n] = c;
-        cells.push_back(n);
-      }
-    };
-    auto add_bface = [&](i32 f) {
-      auto& mark = blisted[f - nint];
-      if (mark != c) {
-        mark = c;
-        bfaces.push_back(f);
-      }
-    };
-    for (i64 k = m.cell_face_offsets[c]; k < m.cell_face_offsets[c + 1]; ++k) {
-      const i32 f = m.cell_faces[k];
-      if (f >= nint) {
-        add_bface(f);
-        continue;
-      }
-      const i32 n = across(c, f);
-      add_cell(n);
-      for (i64 k2 = m.cell_face_offsets[n]; k2 < m.cell_face_offsets[n + 1]; ++k2) {
-        const i32 f2 = m.cell_faces[k2];
-        if (f2 >= nint) {
-          add_bface(f2);
-        } else {
-          add_cell(across(n, f2));
-        }
-      }
-    }
-    std::sort(cells.begin(), cells.end());
-    std::sort(bfaces.begin(), bfaces.end());
-    m.stencil.insert(m.stencil.end(), cells.begin(), cells.end());
-    for (const i32 f : bfaces) m.stencil.push_back(-f - 1);
-    m.stencil_offsets[c + 1] = static_cast<i64>(m.stencil.size());
+    const int len = setup::face2_entries(v, c, buf.data(), setup::kMaxCandidates, row.data());
+    if (len < 0) fail("E1102", "a cell's face2 stencil has more than 512 candidates");
+    m.stencil.insert(m.stencil.end(), row.begin(), row.begin() + len);
+    m.stencil_offsets[static_cast<std::size_t>(c) + 1] = static_cast<i64>(m.stencil.size());
   }
 }
 
@@ -940,64 +910,14 @@ Mesh bump_channel(const autan_bump_channel& s) {
 
 // ------------------------------------------------------------------ gradient weights
 
-// Euler::Impl::compute_gradient_weights (physics/src/euler.cpp:340-416), for the owned cells.
+// The least-squares weights of the owned cells (physics/src/euler.cpp:340-416), one cell at a
+// time with the shared rule of setup_rules.cuh; ghost cells' weights stay 0.
 void gradient_weights(const Mesh& m, const std::uint8_t* kind, double* w) {
-  const auto nc = static_cast<std::size_t>(m.n_cells);
-  const auto nf = static_cast<std::size_t>(m.n_faces);
-  const auto ni = static_cast<std::size_t>(m.n_interior);
-  const auto nst = m.stencil.size();
+  const setup::MeshView v = view_of(m);
+  const auto nst = static_cast<i64>(m.stencil.size());
   std::fill(w, w + 3 * nst, 0.0);
-  constexpr double coordinate_eps = std::numeric_limits<double>::epsilon();
-  std::vector<std::array<double, 4>> offs;
-  for (std::size_t c = 0; c < static_cast<std::size_t>(m.n_owned); ++c) {
-    const auto begin = static_cast<std::size_t>(m.stencil_offsets[c]);
-    const auto end = static_cast<std::size_t>(m.stencil_offsets[c + 1]);
-    auto weights = [&](bool all_boundaries) {
-      std::array<double, 9> a{};
-      offs.clear();
-      for (std::size_t k = begin; k < end; ++k) {
-        const i32 e = m.stencil[k];
-        std::array<double, 3> x{};
-        bool used = true;
-        if (e >= 0) {
-          for (std::size_t j = 0; j < 3; ++j) x[j] = m.cell_centroid[j * nc + static_cast<std::size_t>(e)];
-        } else {
-          const auto f = static_cast<std::size_t>(-e - 1);
-          used = all_boundaries || kind[f - ni] == 0;
-          for (std::size_t j = 0; j < 3; ++j) x[j] = m.face_centroid[j * nf + f];
-        }
-        std::array<double, 4> dk{};
-        for (std::size_t j = 0; j < 3; ++j) {
-          const double xc = m.cell_centroid[j * nc + c];
-          const double round_off = 64 * coordinate_eps * std::max(std::abs(x[j]), std::abs(xc));
-          dk[j] = x[j] - xc;
-          if (std::abs(dk[j]) <= round_off) dk[j] = 0.0;
-        }
-        dk[3] = used ? 1.0 / (dk[0] * dk[0] + dk[1] * dk[1] + dk[2] * dk[2]) : 0.0;
-        for (std::size_t u = 0; u < 3; ++u)
-          for (std::size_t v = 0; v < 3; ++v) a[3 * u + v] += dk[3] * dk[u] * dk[v];
-        offs.push_back(dk);
-      }
-      const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
-                         a[2] * (a[3] * a[7] - a[4] * a[6]);
-      const double sc = a[0] * a[4] * a[8];
-      if (!(std::abs(det) > 1e-10 * std::abs(sc))) return false;
-      const std::array<double, 9> inv = {
-          (a[4] * a[8] - a[5] * a[7]) / det, (a[2] * a[7] - a[1] * a[8]) / det,
-          (a[1] * a[5] - a[2] * a[4]) / det, (a[5] * a[6] - a[3] * a[8]) / det,
-          (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
-          (a[3] * a[7] - a[4] * a[6]) / det, (a[1] * a[6] - a[0] * a[7]) / det,
-          (a[0] * a[4] - a[1] * a[3]) / det};
-      for (std::size_t k = begin; k < end; ++k) {
-        const auto& dk = offs[k - begin];
-        for (std::size_t u = 0; u < 3; ++u)
-          w[u * nst + k] =
-              dk[3] * (inv[3 * u] * dk[0] + inv[3 * u + 1] * dk[1] + inv[3 * u + 2] * dk[2]);
-      }
-      return true;
-    };
-    if (!weights(false)) weights(true);
-  }
+  for (i32 c = 0; c < m.n_owned; ++c)
+    setup::lsq_cell_weights(v, c, m.stencil_offsets.data(), m.stencil.data(), kind, w, nst);
 }
 
 int fail_to(char* err, std::size_t len, const std::string& what) {

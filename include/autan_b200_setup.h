@@ -118,6 +118,40 @@ int autan_mesh_array(const void* mesh, const char* name, const void** ptr, int64
 int autan_mesh_gradient_weights(const void* mesh, const uint8_t* bc_kind, double* weights,
                                 char* err, size_t err_len);
 
+/* ---- the gradient set-up on the GPU -------------------------------------------------------
+ * The face2 stencil of every cell (codegen/cpp/geometry.cpp:432, StencilKind::face2) and the
+ * least-squares weights of the owned cells (physics/src/euler.cpp:340-416) computed by kernels, one
+ * thread per cell, with the same per-cell rules as the host set-up above: the stencil and weights
+ * equal those of autan_mesh_build_* and autan_mesh_gradient_weights bit for bit. For meshes whose
+ * host set-up would dominate (millions of cells, large batches of cases). The mesh is given by its
+ * arrays (host pointers, the mesh contract's layouts), as autan_euler_device_create takes it. */
+struct autan_setup_mesh {
+  int32_t n_cells, n_owned_cells, n_faces, n_interior_faces;
+  const int64_t* cell_face_offsets; /* n_cells + 1 */
+  const int32_t* cell_faces;
+  const int32_t* owner;         /* n_faces */
+  const int32_t* neighbour;     /* n_interior_faces */
+  const double* cell_centroid;  /* 3 x n_cells (ghost cells: their images' centroids) */
+  const double* face_centroid;  /* 3 x n_faces */
+};
+/* Copies the mesh arrays to `device` and computes the stencil there; *n_stencil receives its
+ * length. E1102 when a cell gathers more than 512 stencil candidates. */
+int autan_setup_device_create(const struct autan_setup_mesh* mesh, int32_t device, void** handle,
+                              int64_t* n_stencil, char* err, size_t err_len);
+/* The weights for the boundary codes bc_kind (n_faces - n_interior_faces, the codes of
+ * autan_euler_device.h); *retried (may be NULL) receives the number of cells that needed every
+ * boundary face in their fit. */
+int autan_setup_device_weights(void* handle, const uint8_t* bc_kind, int64_t* retried, char* err,
+                               size_t err_len);
+/* Copies the stencil offsets (n_cells + 1), entries (n_stencil) and weights (3 x n_stencil, after
+ * autan_setup_device_weights) to host arrays; any may be NULL. */
+int autan_setup_device_download(void* handle, int64_t* stencil_offsets, int32_t* stencil,
+                                double* weights, char* err, size_t err_len);
+/* Device times in ms (CUDA events on the handle's stream): [0] copying the mesh arrays, [1] the
+ * stencil, [2] the last weights. */
+void autan_setup_device_times(void* handle, double* ms);
+void autan_setup_device_free(void* handle);
+
 #ifdef __cplusplus
 }
 #endif
