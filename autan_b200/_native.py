@@ -76,6 +76,23 @@ class Scheme(C.Structure):
     ]
 
 
+class SetupMesh(C.Structure):
+    """struct autan_setup_mesh of include/autan_b200_setup.h."""
+
+    _fields_ = [
+        ("n_cells", i32),
+        ("n_owned_cells", i32),
+        ("n_faces", i32),
+        ("n_interior_faces", i32),
+        ("cell_face_offsets", P(i64)),
+        ("cell_faces", P(i32)),
+        ("owner", P(i32)),
+        ("neighbour", P(i32)),
+        ("cell_centroid", P(f64)),
+        ("face_centroid", P(f64)),
+    ]
+
+
 class MeshArrays(C.Structure):
     """struct autan_euler_mesh of include/autan_euler_device.h."""
 
@@ -161,6 +178,7 @@ def _bind(lib: C.CDLL) -> None:
            C.c_char_p, sz)  # fmt: skip
         fn("autan_euler_device_evaluate", C.c_int, vp, P(StepResult), C.c_char_p, sz)
         fn("autan_euler_device_sync", C.c_int, vp, C.c_char_p, sz)
+        fn("autan_euler_device_set_stall_test", C.c_int, vp, i32, C.c_char_p, sz)
         fn("autan_euler_device_stream", vp, vp)
         fn("autan_euler_device_counters", C.c_int, vp, P(i64), C.c_char_p, sz)
         fn("autan_euler_device_gradients", C.c_int, vp, P(f64), P(f64), C.c_char_p, sz)
@@ -184,6 +202,12 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_case_history", C.c_int, vp, i64, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_march_cases", C.c_int, vp, f64, f64, i32, i32, i64, i32, f64, P(f64),
            P(f64), P(i64), P(i32), P(f64), P(i64), P(f64), C.c_char_p, sz)  # fmt: skip
+    if hasattr(lib, "autan_setup_device_create"):
+        fn("autan_setup_device_create", C.c_int, P(SetupMesh), i32, P(vp), P(i64), C.c_char_p, sz)
+        fn("autan_setup_device_weights", C.c_int, vp, P(u8), P(i64), C.c_char_p, sz)
+        fn("autan_setup_device_download", C.c_int, vp, P(i64), P(i32), P(f64), C.c_char_p, sz)
+        fn("autan_setup_device_times", None, vp, P(f64))
+        fn("autan_setup_device_free", None, vp)
     if hasattr(lib, "autan_exact_rms_static"):
         fn("autan_exact_rms_static", C.c_int, vp, i64, i64, i32, vp, vp, C.c_char_p, sz)
 

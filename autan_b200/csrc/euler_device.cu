@@ -80,6 +80,10 @@ struct Control {
   long long step;                // steps taken since the last reset
   double dt;                     // the global step of the current step
   unsigned long long fault;      // a bounded device wait timed out
+  // Nonzero once a primitive record written since the last state upload holds a value that is not
+  // finite or whose magnitude reaches 2^60 (sticky until the next upload): the gradient kernels'
+  // scaled integer-pipe widening is exact only below that bound and falls back to cvt above it.
+  unsigned long long special;
   double rms[5];
   unsigned long long words[5][kWords];
   double hist_rms[kHistory][5];
@@ -134,6 +138,13 @@ struct Dev {
   // Per case, the AUSM+-up cut-off Mach number (each case's own freestream Mach), or null for the
   // scheme's one value.
   const typename P::C* case_minf;
+  // 1 when every LSQ weight is finite and below 2^40 in magnitude (checked at create): with
+  // Control::special clear, the gradient sums may then be widened on the integer pipe.
+  int wide_ok;
+  // Test hook of the failure detection (0 in normal use): with n > 0 every warp of the mode-5
+  // gradient kernel also waits, n polls at most, on an mbarrier that nothing arrives on, so that
+  // the bounded wait runs out and takes the timeout path (fault word, no stores).
+  int stall_polls;
 };
 
 // Whether owned cell c takes part (its case has not stopped).
@@ -286,12 +297,28 @@ __device__ __forceinline__ void store_recon(const Dev<P>& d, int c, const typena
                          out + kGroup * k);
 }
 
+// Whether a primitive value is one the scaled widening of the gradient sums cannot take exactly
+// (not finite, or of magnitude 2^60 or more); recorded in Control::special by every writer of
+// primitive records.
+__device__ __forceinline__ bool special_value(float x) { return !(fabsf(x) < 0x1p60f); }
+__device__ __forceinline__ bool special_value(double x) { return !(fabs(x) < 0x1p60); }
+
+template <class C>
+__device__ __forceinline__ void note_special(const C* w, Control* ctl) {
+  bool s = false;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) s = s || special_value(w[k]);
+  if (s && ctl != nullptr) atomicOr(&ctl->special, 1ULL);
+}
+
 // Writes the primitives of cell c (words 0-7, the padding 5-7 zero).
 template <class P>
-__device__ __forceinline__ void store_prim(typename P::C* prim, int c, const typename P::C* w) {
+__device__ __forceinline__ void store_prim(typename P::C* prim, int c, const typename P::C* w,
+                                           Control* ctl) {
   using C = typename P::C;
   const C t[8] = {w[0], w[1], w[2], w[3], w[4], C(0), C(0), C(0)};
   store_words<P, true>(prim + static_cast<long long>(c) * kPrimW, 0, 8, t);
+  note_special(w, ctl);
 }
 
 // Euler<P>::state then to_primitive: W of the stored state S(u - U_ref) (euler.cpp:925-932,
@@ -305,7 +332,53 @@ __device__ __forceinline__ void prim_of_state(const Dev<P>& d, const double* u, 
   to_primitive(dq, d.p, w);
 }
 
+// CudaStepper::invalid (device_stepper.cuh:107-164): cell c's state as the kernels read it (dq
+// the gauge difference State(u - U_ref) in the compute type: density and pressure finite and
+// positive), then its residual (finite); the least such cells go to Control::bad_state and
+// bad_res.
+template <class P>
+__device__ __forceinline__ void mark_invalid(const Dev<P>& d, int c, const typename P::C* dq,
+                                             const double* res) {
+  using C = typename P::C;
+  const C g = d.p.g;
+  const C r0 = static_cast<C>(d.ref[0]);
+  const C rho = r0 + dq[0];
+  C dm_m = C(0), mr_mr = C(0);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const C mr = static_cast<C>(d.ref[k + 1]);
+    dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
+    mr_mr = mr_mr + mr * mr;
+  }
+  const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
+  const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
+  const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
+                   !(rho > C(0)) || !(pr > C(0));
+  if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
+  bool badr = false;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) badr = badr || !isfinite(res[k]);
+  if (badr) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(c));
+}
+
 // ---------------------------------------------------------------- kernels
+
+// The divergence marks of the device state u and the residual res (FP64 SoA) for evaluate().
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_invalid(Dev<P> d, const double* u, const double* res) {
+  using C = typename P::C;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.n) return;
+  C dq[5];
+  double r[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const long long i = static_cast<long long>(k) * d.n + c;
+    dq[k] = static_cast<C>(u[i] - d.ref[k]);
+    r[k] = res[i];
+  }
+  mark_invalid(d, c, dq, r);
+}
 
 // The primitives of a host state (upload, residual): records of u.
 template <class P>
@@ -317,7 +390,7 @@ __global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typ
   for (int k = 0; k < 5; ++k) uc[k] = u[static_cast<long long>(k) * d.n + c];
   typename P::C w[5], dq[5];
   prim_of_state(d, uc, w, dq);
-  store_prim<P>(rec, c, w);
+  store_prim<P>(rec, c, w, d.ctl);
 }
 
 // boundary_states (kernels/euler.py:455-466): prim_b of every boundary face.
@@ -332,6 +405,7 @@ __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   boundary_value(w, r[7], r + 8, r, d.p, out);
   out[5] = out[6] = out[7] = C(0);
   store_words<P, true>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
+  note_special(out, d.ctl);
 }
 
 // The minimum over a block of positive doubles' bits, then one atomicMin. Every thread of the
@@ -622,6 +696,221 @@ __global__ void __launch_bounds__(128, 7) k_gradients_occ7(Dev<P> d, double cfl,
   gradients_cells<P, LIMIT, DT, 2>(d, cfl, local);
 }
 
+// ---------------------------------------------------------------- integer-pipe widening
+
+// 2^-896 p as a double, exactly, for every finite float p (normal, subnormal or zero, of either
+// sign): the float's sign, exponent and fraction bits placed in a double whose 11-bit exponent
+// field holds the float's 8-bit one (bias 127 read against bias 1023, hence the factor). A signed
+// 32 x 32 -> 64 multiply by 2^29 shifts the bits (its sign extension fills the top three bits of
+// the exponent field with the sign), one AND clears those three bits: two integer instructions in
+// place of one cvt.f64.f32 on the conversion (XU) pipe, which the 15 products of every stencil
+// entry otherwise keep half busy. An infinity or NaN p maps to a finite double: callers take
+// this path only where no product can be one.
+//
+// FP64 sums of these values are 2^-896 times the sums of the same products widened by cvt, bit
+// for bit: while a partial sum is at least 2^-1022 both are rounded to 53 bits at the same
+// relative position; below it the unscaled partial sum is a multiple of 2^-149 under 2^-126
+// (23 significant bits, exact) and the scaled one a multiple of 2^-1045 under 2^-1022, which a
+// subnormal double holds exactly. Multiplying a scaled sum by 2^896 restores it exactly.
+__device__ __forceinline__ double widen_scaled(float p) {
+  double out;
+  asm("{\n\t.reg .b64 t;\n\t.reg .b32 l, h;\n\t"
+      "mul.wide.s32 t, %1, 536870912;\n\t"
+      "mov.b64 {l, h}, t;\n\t"
+      "and.b32 h, h, 0x8FFFFFFF;\n\t"
+      "mov.b64 %0, {l, h};\n\t}"
+      : "=d"(out)
+      : "r"(__float_as_int(p)));
+  return out;
+}
+constexpr double kUnscale = 0x1p896;
+
+// A product widened for the FP64 sums: scaled on the integer pipe (SCALED) or by cvt.
+template <bool SCALED>
+__device__ __forceinline__ double widen(float p) {
+  if constexpr (SCALED) {
+    return widen_scaled(p);
+  } else {
+    return static_cast<double>(p);
+  }
+}
+
+// The products of a stencil entry in the gradient sums are finite and below 2^101 when every
+// primitive read is below 2^60 in magnitude (Control::special clear) and every LSQ weight below
+// 2^40 (Dev::wide_ok, checked at create); their sums then stay below 2^120, so the scaled
+// widening is exact.
+
+// Five words of a record as one 16-byte and one 4-byte load: 5 registers held while the gather is
+// in flight where the 32-byte load holds 8. The two loads read one 32-byte sector.
+__device__ __forceinline__ void load5_narrow(const float* src, float* w) {
+  const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+  w[0] = a.x;
+  w[1] = a.y;
+  w[2] = a.z;
+  w[3] = a.w;
+  w[4] = __ldg(src + 4);
+}
+
+template <bool G5>
+__device__ __forceinline__ void gather5(const float* src, float* w) {
+  if constexpr (G5) {
+    load5_narrow(src, w);
+  } else {
+    load5<Fp32Acc64>(src, w);
+  }
+}
+
+// gradient_tail with the pass over the incidences software-pipelined: the record (and the
+// normal and area) of incidence j + 1 is loaded, and with DT the other side's primitives of
+// incidence j gathered, before incidence j's limiter terms are computed. Same operations in the
+// same order as gradient_tail.
+template <bool LIMIT, bool DT, bool G5>
+__device__ __forceinline__ double gradient_tail_pipelined(const Dev<Fp32Acc64>& d, int c,
+                                                          const float* wc, const double* acc,
+                                                          const float* lo, const float* hi,
+                                                          double cfl, int local) {
+  using P = Fp32Acc64;
+  using C = float;
+  C out[kRecon];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) out[5 + k] = static_cast<C>(acc[k]);
+  const C* g = out + 5;
+  C phi[5], dmax[5], dmin[5], eps2[5];
+  if constexpr (LIMIT) {
+    const C vol = static_cast<C>(__ldg(d.volume + c));
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      dmax[i] = maxv(hi[i], wc[i]) - wc[i];
+      dmin[i] = minv(lo[i], wc[i]) - wc[i];
+      eps2[i] = d.p.scale[i] * vol;
+      phi[i] = C(INFINITY);
+    }
+  }
+  double lam = 0.0;
+  if constexpr (LIMIT || DT) {
+    const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
+    const int il = __ldg(d.inc_len + c);
+    C r[4];
+    if (il > 0) load_words<P>(d.inc_rec + 4 * ib, 0, 4, r);
+    for (int j = 0; j < il; ++j) {
+      C rn[4], nd[4], wn[5];
+      if constexpr (DT) {
+        gather5<G5>(d.prim + static_cast<long long>(index_of(r[3])) * kPrimW, wn);
+        load_words<P>(d.inc_dt + 4 * (ib + static_cast<long long>(j) * kSlice), 0, 4, nd);
+      }
+      if (j + 1 < il)
+        load_words<P>(d.inc_rec + 4 * (ib + static_cast<long long>(j + 1) * kSlice), 0, 4, rn);
+      if constexpr (LIMIT) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
+          phi[i] = bound_min(phi[i], venkat(dd, dmax[i], dmin[i], eps2[i]));
+        }
+      }
+      if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) r[k] = rn[k];
+    }
+  }
+  if constexpr (LIMIT) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) out[i] = minv(phi[i], C(1.0));
+  } else {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) out[i] = C(1.0);
+  }
+#pragma unroll
+  for (int k = 20; k < kRecon; ++k) out[k] = C(0);
+  store_recon<P>(d, c, out);
+  if constexpr (DT) {
+    const double dt = cfl * d.volume[c] / static_cast<double>(static_cast<C>(lam));
+    if (local) d.dt_local[c] = dt;
+    return dt;
+  }
+  return 0.0;
+}
+
+// gradients + limiter (as k_gradients) in fp32+acc64 with the product widening on the integer
+// pipe: WIDE = 1 widens the x and y products of each entry (10 of 15) with widen_scaled, WIDE = 2
+// all 15, the rest through cvt; G5 gathers neighbours with load5_narrow; CHUNK entries are
+// loaded together. Where Control::special is set or a weight is out of range the cells take the
+// cvt loop instead (the same sums, bit for bit).
+template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK>
+__device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, double cfl, int local) {
+  using P = Fp32Acc64;
+  using C = float;
+  if (block_idle(d)) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n && cell_active(d, c);
+  const bool fast = WIDE > 0 && d.wide_ok != 0 && __ldg(&d.ctl->special) == 0ULL;
+  double dt = 0.0;
+  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  if (live) {
+    C wc[5];
+    load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
+    }
+    const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
+    const int len = __ldg(d.st_len + c);
+    auto walk = [&](auto scaled) {
+      constexpr int W = decltype(scaled)::value;
+      for (int j0 = 0; j0 < len; j0 += CHUNK) {
+        C e4[CHUNK][4], wn[CHUNK][5];
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q < len)
+            load_words<P>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice), 0, 4, e4[q]);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q < len)
+            gather5<G5>(d.prim + static_cast<long long>(index_of(e4[q][3])) * kPrimW, wn[q]);
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q) {
+          if (j0 + q < len) {
+#pragma unroll
+            for (int i = 0; i < 5; ++i) {
+              const C dw = wn[q][i] - wc[i];
+              acc[3 * i] += widen<(W >= 1)>(dw * e4[q][0]);
+              acc[3 * i + 1] += widen<(W >= 1)>(dw * e4[q][1]);
+              acc[3 * i + 2] += widen<(W >= 2)>(dw * e4[q][2]);
+            }
+#pragma unroll
+            for (int i = 0; i < 5; ++i) {
+              lo[i] = bound_min(lo[i], wn[q][i]);
+              hi[i] = bound_max(hi[i], wn[q][i]);
+            }
+          }
+        }
+      }
+    };
+    if (fast) {
+      walk(std::integral_constant<int, WIDE>{});
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        acc[3 * i] *= kUnscale;
+        acc[3 * i + 1] *= kUnscale;
+        if (WIDE >= 2) acc[3 * i + 2] *= kUnscale;
+      }
+    } else {
+      walk(std::integral_constant<int, 0>{});
+    }
+    dt = gradient_tail_pipelined<LIMIT, DT, G5>(d, c, wc, acc, lo, hi, cfl, local);
+  }
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_gradients_w(Dev<Fp32Acc64> d, double cfl, int local) {
+  gradients_w_cells<LIMIT, DT, WIDE, G5, CHUNK>(d, cfl, local);
+}
+
 // ---------------------------------------------------------------- TMA bulk staging
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -820,6 +1109,135 @@ __device__ __forceinline__ void gradients_staged_cells(const Dev<P>& d, double c
 template <class P, bool LIMIT, bool DT, int CHUNK>
 __global__ void __launch_bounds__(128) k_gradients_tma(Dev<P> d, double cfl, int local) {
   gradients_staged_cells<P, LIMIT, DT, CHUNK>(d, cfl, local);
+}
+
+// ---------------------------------------------------------------- per-warp TMA row ring
+
+// A warp's 32 cells are one slice: the rows of its entry j are 512 contiguous bytes. Each warp
+// keeps its next R entries' rows in a ring of shared-memory slots, each filled by one 1-D TMA bulk
+// copy (cp.async.bulk, no tensor map, no multicast) that completes on the slot's mbarrier; lane 0
+// refills a slot once the warp has read it. The stencil stream from HBM then runs R entries ahead
+// of the warp without holding registers, and an entry's neighbour index is in shared memory when
+// the warp reaches it, so the gathers start at once: the row load no longer sits in front of every
+// gather. Shared memory per block of 4 warps: 4 R (512 + 8) bytes.
+constexpr int kRingWarps = 4;
+constexpr size_t warp_ring_bytes(int R) {
+  return static_cast<size_t>(kRingWarps) * R * (kSlice * 16 + 8);
+}
+
+// Waits for phase `parity` of a slot's mbarrier, polling at most `polls` times; false on a
+// timeout.
+__device__ __forceinline__ bool slot_wait(unsigned long long* bar, unsigned parity,
+                                          int polls = kWaitLimit) {
+  for (int it = 0; it < polls; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// gradients + limiter (as k_gradients) in fp32+acc64 with the stencil rows streamed through the
+// warp's slot ring; CHUNK entries' gathers in flight at once (their weights read from the slots
+// after the gathers return); G5: 5-word gathers. A slot wait that times out marks Control::fault;
+// the warp then waits, again bounded, for the copies it has issued and stores nothing.
+template <bool LIMIT, bool DT, int R, int CHUNK, bool G5>
+__global__ void __launch_bounds__(128, 7) k_gradients_wring(Dev<Fp32Acc64> d, double cfl, int local) {
+  using P = Fp32Acc64;
+  using C = float;
+  static_assert(R >= CHUNK, "the ring holds at least one chunk");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  if (block_idle(d)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4* ring = reinterpret_cast<float4*>(smem_raw) + warp * R * kSlice;
+  unsigned long long* bar =
+      reinterpret_cast<unsigned long long*>(smem_raw + kRingWarps * R * kSlice * 16) + warp * R;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < d.n && cell_active(d, c);
+  bool ok = true;
+  double dt = 0.0;
+  if (__any_sync(0xffffffffu, live)) {  // uniform over the warp
+    const int s = c >> 5;
+    const long long e0 = __ldg(d.st_start + s);
+    const int L = static_cast<int>((__ldg(d.st_start + s + 1) - e0) / kSlice);
+    const float4* src = reinterpret_cast<const float4*>(d.st) + e0;
+    auto issue = [&](int j) {  // lane 0: entry j's rows into slot j % R
+      const int k = j % R;
+      mbar_expect_tx(&bar[k], kSlice * 16);
+      bulk_to_shared(ring + k * kSlice, src + static_cast<long long>(j) * kSlice, kSlice * 16, &bar[k]);
+    };
+    if (lane == 0) {
+      for (int k = 0; k < R; ++k) mbar_init(&bar[k], 1);
+      for (int j = 0; j < R && j < L; ++j) issue(j);
+    }
+    __syncwarp();
+    if (d.stall_polls > 0) {
+      // test hook: a wait on a barrier nothing arrives on runs out after stall_polls polls
+      __shared__ __align__(8) unsigned long long dead[kRingWarps];
+      if (lane == 0) mbar_init(&dead[warp], 1);
+      __syncwarp();
+      ok = __all_sync(0xffffffffu, slot_wait(&dead[warp], 0, d.stall_polls));
+    }
+    const int len = live ? __ldg(d.st_len + c) : 0;
+    C wc[5] = {C(0), C(0), C(0), C(0), C(0)};
+    if (live) load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
+    double acc[15];
+#pragma unroll
+    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
+    C lo[5], hi[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      lo[k] = C(INFINITY);
+      hi[k] = -C(INFINITY);
+    }
+    int waited = 0;  // entries whose slot has been waited for
+    for (int j0 = 0; ok && j0 < L; j0 += CHUNK) {
+      bool got = true;
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q)
+        if (j0 + q < L) got = got && slot_wait(&bar[(j0 + q) % R], ((j0 + q) / R) & 1);
+      if (!__all_sync(0xffffffffu, got)) {
+        ok = false;
+        break;
+      }
+      waited = j0 + CHUNK < L ? j0 + CHUNK : L;
+      C wn[CHUNK][5];
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q)
+        if (j0 + q < len) {
+          const int x = __float_as_int(ring[((j0 + q) % R) * kSlice + lane].w);
+          gather5<G5>(d.prim + static_cast<long long>(x) * kPrimW, wn[q]);
+        }
+#pragma unroll
+      for (int q = 0; q < CHUNK; ++q) {
+        if (j0 + q < len) {
+          const float4 e = ring[((j0 + q) % R) * kSlice + lane];
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            const C dw = wn[q][i] - wc[i];
+            acc[3 * i] += static_cast<double>(dw * e.x);
+            acc[3 * i + 1] += static_cast<double>(dw * e.y);
+            acc[3 * i + 2] += static_cast<double>(dw * e.z);
+          }
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            lo[i] = bound_min(lo[i], wn[q][i]);
+            hi[i] = bound_max(hi[i], wn[q][i]);
+          }
+        }
+      }
+      __syncwarp();  // every lane has read the chunk's slots
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < CHUNK; ++q)
+          if (j0 + q + R < L) issue(j0 + q + R);
+    }
+    if (!ok) {
+      // a slot wait gave up: mark the fault and wait, bounded, for the copies still in flight
+      if (lane == 0) atomicExch(&d.ctl->fault, 1ULL);
+      for (int j = waited; j < L && j < waited + R; ++j) slot_wait(&bar[j % R], (j / R) & 1);
+    } else if (live) {
+      dt = gradient_tail_pipelined<LIMIT, DT, G5>(d, c, wc, acc, lo, hi, cfl, local);
+    }
+  }
+  if constexpr (DT) block_min_dt(dt, live && ok, &d.ctl->dt_bits);
 }
 
 // fp32+acc64 with up to 4 entries in flight, registers sized for 6 blocks of 128 per SM: the
@@ -1169,30 +1587,8 @@ __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double
   }
   C w[5], dq[5];
   prim_of_state(d, nu, w, dq);
-  store_prim<P>(d.prim_next, c, w);
-  if (last) {
-    // CudaStepper::invalid (device_stepper.cuh:107-164): the new state as the kernels will read
-    // it, in the compute type, then this stage's residual.
-    const C g = d.p.g;
-    const C r0 = static_cast<C>(d.ref[0]);
-    const C rho = r0 + dq[0];
-    C dm_m = C(0), mr_mr = C(0);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const C mr = static_cast<C>(d.ref[k + 1]);
-      dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
-      mr_mr = mr_mr + mr * mr;
-    }
-    const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
-    const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d.p.pref;
-    const bool bad = !isfinite(static_cast<double>(rho)) || !isfinite(static_cast<double>(pr)) ||
-                     !(rho > C(0)) || !(pr > C(0));
-    if (bad) atomicMin(&d.ctl->bad_state, static_cast<unsigned long long>(c));
-    bool badr = false;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) badr = badr || !isfinite(res[k]);
-    if (badr) atomicMin(&d.ctl->bad_res, static_cast<unsigned long long>(c));
-  }
+  store_prim<P>(d.prim_next, c, w, d.ctl);
+  if (last) mark_invalid(d, c, dq, res);
 }
 
 // Gather-recompute: the faces of one owned cell (roe/hllc/ausm _faces and _boundaries), every
@@ -1749,8 +2145,19 @@ struct Tuning {
   int gather_block = 256;  // threads per block of the store-gather sum
   int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies;
                          // 2: loaded by each thread, software-pipelined (chunk unused);
-                         // 3: a per-thread ring of asynchronous copies, chunk entries deep
-  static constexpr int kCount = 6;
+                         // 3: a per-thread ring of asynchronous copies, chunk entries deep;
+                         // 4 (fp32+acc64): loaded by each thread with the products widened on the
+                         // integer pipe (grad_widen), 5-word gathers (grad_narrow), registers
+                         // bounded for grad_minb blocks of 128 per SM;
+                         // 5 (fp32+acc64): each warp's stencil rows streamed by TMA bulk copies
+                         // into a ring of grad_depth shared-memory slots, grad_chunk gathers in
+                         // flight (5-word with grad_narrow)
+  int grad_widen = 0;    // mode 4: products widened by widen_scaled: 0 none, 1 x and y, 2 all
+  int grad_narrow = 0;   // mode 4: 1 gathers neighbours as 16 + 4 bytes instead of 32
+  int grad_minb = 7;     // mode 4: blocks of 128 threads per SM the registers are bounded for
+  int grad_depth = 4;    // mode 5: entries each warp's row ring holds (4 or 8)
+  static constexpr int kCount = 10;
+  static constexpr int kMinCount = 6;  // callers that predate mode 4 pass the first six
   void to(int32_t* p) const {
     p[0] = grad_chunk;
     p[1] = grad_block;
@@ -1758,8 +2165,12 @@ struct Tuning {
     p[3] = face_block;
     p[4] = gather_block;
     p[5] = grad_mode;
+    p[6] = grad_widen;
+    p[7] = grad_narrow;
+    p[8] = grad_minb;
+    p[9] = grad_depth;
   }
-  static Tuning from(const int32_t* p) {
+  static Tuning from(const int32_t* p, int count = kCount) {
     Tuning t;
     t.grad_chunk = p[0];
     t.grad_block = p[1];
@@ -1767,6 +2178,12 @@ struct Tuning {
     t.face_block = p[3];
     t.gather_block = p[4];
     t.grad_mode = p[5];
+    if (count >= kCount) {
+      t.grad_widen = p[6];
+      t.grad_narrow = p[7];
+      t.grad_minb = p[8];
+      t.grad_depth = p[9];
+    }
     t.validate();
     return t;
   }
@@ -1784,7 +2201,19 @@ void Tuning::validate() const {
   if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
   if (grad_mode == 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
-  if (grad_mode < 0 || grad_mode > 3) fail("E1101: grad_mode is 0, 1, 2 or 3");
+  if (grad_mode < 0 || grad_mode > 5) fail("E1101: grad_mode is 0 to 5");
+  if (grad_mode == 5) {
+    if (grad_block != 128) fail("E1101: the mode-5 gradient kernel takes 128 threads");
+    if (grad_chunk != 2 && grad_chunk != 3) fail("E1101: grad_chunk of mode 5 is 2 or 3");
+    if (grad_depth != 4 && grad_depth != 8) fail("E1101: grad_depth is 4 or 8");
+    if (grad_narrow != 0 && grad_narrow != 1) fail("E1101: grad_narrow is 0 or 1");
+  }
+  if (grad_mode == 4) {
+    if (grad_block != 128) fail("E1101: the mode-4 gradient kernel takes 128 threads");
+    if (grad_widen < 0 || grad_widen > 2) fail("E1101: grad_widen is 0, 1 or 2");
+    if (grad_narrow != 0 && grad_narrow != 1) fail("E1101: grad_narrow is 0 or 1");
+    if (grad_chunk != 2 || grad_minb != 7) fail("E1101: mode 4 takes grad_chunk 2, grad_minb 7");
+  }
   if (grad_mode == 3 && grad_block > 128) fail("E1101: the ring gradient kernel takes <= 128 threads");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
   if (!block_ok(grad_block) || !block_ok(face_block) || !block_ok(gather_block))
@@ -1821,6 +2250,7 @@ class Stepper {
   virtual void set_case_mach_ref(const double* mach_ref) = 0;
   virtual void case_history(long long count, double* rms) = 0;
   virtual int n_cases() const = 0;
+  virtual void set_stall_test(int polls) = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
@@ -1965,6 +2395,7 @@ class Impl final : public Stepper {
     st_ = slice_rows(soff);
     const long long nst = has_stencil ? m.stencil_offsets[nc_] : 0;
     std::vector<C> ste(4 * std::max<long long>(st_.total, 1), C(0));
+    bool weights_in_range = true;  // finite and below 2^40: the gradient's scaled widening holds
     for (int c = 0; c < (has_stencil ? n_ : 0); ++c) {
       for (long long k = m.stencil_offsets[c]; k < m.stencil_offsets[c + 1]; ++k) {
         const int e = m.stencil[k];
@@ -1978,7 +2409,10 @@ class Impl final : public Stepper {
           v = n_ + (f - ni_);  // the boundary state's record, after the cells' records
         }
         C* q = ste.data() + 4 * st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
-        for (int a = 0; a < 3; ++a) q[a] = static_cast<C>(m.stencil_lsq_weight[a * nst + k]);
+        for (int a = 0; a < 3; ++a) {
+          q[a] = static_cast<C>(m.stencil_lsq_weight[a * nst + k]);
+          if (!(std::fabs(static_cast<double>(q[a])) < 0x1p40)) weights_in_range = false;
+        }
         q[3] = index_bits<C>(v);
       }
     }
@@ -2063,6 +2497,8 @@ class Impl final : public Stepper {
     d_.face_warp_case = nullptr;
     d_.bface_warp_case = nullptr;
     d_.case_minf = nullptr;
+    d_.wide_ok = (sizeof(C) == 4 && weights_in_range) ? 1 : 0;
+    d_.stall_polls = 0;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     if (tuning_.face_mode == 1) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
@@ -2149,10 +2585,17 @@ class Impl final : public Stepper {
         host[k * static_cast<long long>(nc_) + g] = host[k * static_cast<long long>(nc_) + ghost_owner_[g - n_]];
   }
 
-  void upload_state(const double* u) override {
-    copy_in(u, u_.as<double>());
+  // The primitives of the device state u_ into record buffer 0, where every step starts: a new
+  // state, so Control::special is cleared first and set again by k_store if this state needs it.
+  void store_state() {
+    check(cudaMemsetAsync(&d_.ctl->special, 0, sizeof(unsigned long long), stream), "special");
     launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
            prim_[0].as<C>());
+  }
+
+  void upload_state(const double* u) override {
+    copy_in(u, u_.as<double>());
+    store_state();
     check(cudaStreamSynchronize(stream), "upload");
   }
 
@@ -2173,17 +2616,17 @@ class Impl final : public Stepper {
     enqueue_residual(0);
     launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
     launch(k_norm_finish, 1, 32, d_.ctl, n_, 0);
+    // invalid(): the state, then the residual, marked on the device
+    launch(k_invalid<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
+           static_cast<const double*>(res_.as<double>()));
     check(cudaMemcpyAsync(head_, d_.ctl, kControlHead, cudaMemcpyDeviceToHost, stream), "control");
     check(cudaStreamSynchronize(stream), "evaluate");
     for (int k = 0; k < 5; ++k) out->residuals[k] = head_->rms[k];
     out->time_step = 0.0;
     out->steps = 0;
-    // invalid(): the state, then the residual.
-    std::vector<double> u(5ULL * n_), r(5ULL * n_);
-    check(cudaMemcpyAsync(u.data(), u_.ptr(), u.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
-    check(cudaMemcpyAsync(r.data(), res_.ptr(), r.size() * 8, cudaMemcpyDeviceToHost, stream), "evaluate");
-    check(cudaStreamSynchronize(stream), "evaluate");
-    out->invalid_cell = first_invalid(u, r);
+    out->invalid_cell = head_->bad_state != ~0ULL ? static_cast<int64_t>(head_->bad_state)
+                        : head_->bad_res != ~0ULL ? static_cast<int64_t>(head_->bad_res)
+                                                  : -1;
   }
 
   void step(double cfl, double dt, bool local, int rk, long long n, bool graph,
@@ -2302,8 +2745,7 @@ class Impl final : public Stepper {
     auto restore = [&]() {
       check(cudaMemcpyAsync(u_.ptr(), saved.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),
             "restore state");
-      launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
-             prim_[0].as<C>());
+      store_state();
       check(cudaStreamSynchronize(stream), "restore state");
     };
     ensure_flux_scratch();
@@ -2339,6 +2781,39 @@ class Impl final : public Stepper {
             best = t;
           }
         }
+      if (sizeof(C) == 4 && limiter_)
+        for (int depth : {4, 8})
+          for (int chunk : {2, 3})
+            for (int narrow : {0, 1}) {
+              Tuning t = keep;
+              t.grad_mode = 5;
+              t.grad_block = 128;
+              t.grad_depth = depth;
+              t.grad_chunk = chunk;
+              t.grad_narrow = narrow;
+              const double ms = measure(t, kGradients);
+              if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+              }
+            }
+      if (sizeof(C) == 4 && limiter_)
+        for (int widen : {0, 1, 2})
+          for (int narrow : {0, 1})
+            {
+              Tuning t = keep;
+              t.grad_mode = 4;
+              t.grad_block = 128;
+              t.grad_widen = widen;
+              t.grad_narrow = narrow;
+              t.grad_chunk = 2;
+              t.grad_minb = 7;
+              const double ms = measure(t, kGradients);
+              if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+              }
+            }
     }
     {
       double best_ms = 1e300;
@@ -2653,6 +3128,12 @@ class Impl final : public Stepper {
 
   int n_cases() const override { return n_cases_; }
 
+  void set_stall_test(int polls) override {
+    if (polls < 0) fail("E1101: polls must be >= 0");
+    d_.stall_polls = polls;
+    drop_graph();
+  }
+
   // Calls body(flux, planar, second) with the scheme's compile-time choices.
   template <class B>
   void dispatch_faces(B&& body) {
@@ -2694,6 +3175,19 @@ class Impl final : public Stepper {
       const int gs = blocks(n_, bs);
       auto go = [&](auto lim, auto with_dt) {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
+        if (tuning_.grad_mode == 4 || tuning_.grad_mode == 5) {
+          if constexpr (std::is_same_v<P, Fp32Acc64> && L) {
+            if (tuning_.grad_mode == 5) launch_gradients_ring<D>(d, cfl, loc);
+            else launch_gradients_w<D>(d, cfl, loc);
+            return;
+          }
+          // fp64 or no limiter: the mode-0 form with two entries in flight
+          if constexpr (sizeof(C) == 4)
+            launch_as(kGradients, k_gradients_occ7<P, L, D>, blocks(n_, 128), 128, d, cfl, loc);
+          else
+            launch_as(kGradients, k_gradients<P, L, D, 2>, blocks(n_, 128), 128, d, cfl, loc);
+          return;
+        }
         if (tuning_.grad_mode == 1) {
           const int sm = static_cast<int>(staged_smem(bs, D));
           const int gb = blocks(n_, bs);
@@ -2744,6 +3238,55 @@ class Impl final : public Stepper {
       }
     } else if (dt) {
       launch_as(kSpectral, k_spectral<P>, g, kBlock, d, cfl, loc, static_cast<double*>(nullptr));
+    }
+  }
+
+  // The mode-4 gradient kernel of the tuning's widening, gathers and register bound (fp32+acc64,
+  // limited second order).
+  template <bool D>
+  void launch_gradients_w(const Dev<P>& d, double cfl, int loc) {
+    if constexpr (std::is_same_v<P, Fp32Acc64>) {
+      const int gs = blocks(n_, 128);
+      auto shape = [&](auto wide, auto narrow) {
+        constexpr int W = decltype(wide)::value;
+        constexpr bool G = decltype(narrow)::value;
+        launch_as(kGradients, k_gradients_w<true, D, W, G, 2, 7>, gs, 128, d, cfl, loc);
+      };
+      auto narrow = [&](auto wide) {
+        if (tuning_.grad_narrow) shape(wide, std::true_type{});
+        else shape(wide, std::false_type{});
+      };
+      if (tuning_.grad_widen == 2) narrow(std::integral_constant<int, 2>{});
+      else if (tuning_.grad_widen == 1) narrow(std::integral_constant<int, 1>{});
+      else narrow(std::integral_constant<int, 0>{});
+    }
+  }
+
+  // The mode-5 gradient kernel (per-warp TMA row ring) of the tuning's depth, chunk and gathers.
+  template <bool D>
+  void launch_gradients_ring(const Dev<P>& d, double cfl, int loc) {
+    if constexpr (std::is_same_v<P, Fp32Acc64>) {
+      const int gs = blocks(n_, 128);
+      auto go = [&](auto depth, auto chunk, auto narrow) {
+        constexpr int R = decltype(depth)::value, CH = decltype(chunk)::value;
+        constexpr bool G = decltype(narrow)::value;
+        launch_smem(kGradients, k_gradients_wring<true, D, R, CH, G>, gs, 128, warp_ring_bytes(R),
+                    d, cfl, loc);
+      };
+      using I2 = std::integral_constant<int, 2>;
+      using I3 = std::integral_constant<int, 3>;
+      using I4 = std::integral_constant<int, 4>;
+      using I8 = std::integral_constant<int, 8>;
+      auto by_chunk = [&](auto depth, auto narrow) {
+        if (tuning_.grad_chunk == 3) go(depth, I3{}, narrow);
+        else go(depth, I2{}, narrow);
+      };
+      auto by_narrow = [&](auto depth) {
+        if (tuning_.grad_narrow) by_chunk(depth, std::true_type{});
+        else by_chunk(depth, std::false_type{});
+      };
+      if (tuning_.grad_depth == 8) by_narrow(I8{});
+      else by_narrow(I4{});
     }
   }
 
@@ -2815,32 +3358,6 @@ class Impl final : public Stepper {
     if (graph_ != nullptr) cudaGraphDestroy(graph_);
     graph_exec_ = nullptr;
     graph_ = nullptr;
-  }
-
-  long long first_invalid(const std::vector<double>& u, const std::vector<double>& r) const {
-    const double* ref = d_.ref;
-    const C g = static_cast<C>(scheme_.gamma);
-    const C r0 = static_cast<C>(ref[0]);
-    for (int c = 0; c < n_; ++c) {
-      C dq[5];
-      for (int k = 0; k < 5; ++k) dq[k] = static_cast<C>(u[k * static_cast<long long>(n_) + c] - ref[k]);
-      const C rho = r0 + dq[0];
-      C dm_m = 0, mr_mr = 0;
-      for (int k = 0; k < 3; ++k) {
-        const C mr = static_cast<C>(ref[k + 1]);
-        dm_m = dm_m + dq[k + 1] * (C(2) * mr + dq[k + 1]);
-        mr_mr = mr_mr + mr * mr;
-      }
-      const C dk = (dm_m * r0 - mr_mr * dq[0]) / (rho * r0);
-      const C pr = (g - C(1)) * (dq[4] - C(0.5) * dk) + d_.p.pref;
-      if (!std::isfinite(static_cast<double>(rho)) || !std::isfinite(static_cast<double>(pr)) ||
-          !(rho > C(0)) || !(pr > C(0)))
-        return c;
-    }
-    for (int c = 0; c < n_; ++c)
-      for (int k = 0; k < 5; ++k)
-        if (!std::isfinite(r[k * static_cast<long long>(n_) + c])) return c;
-    return -1;
   }
 
   autan_euler_scheme scheme_;
@@ -3222,15 +3739,19 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
                                   size_t err_len) {
   AUTAN_CALL({
-    if (params == nullptr || count < Tuning::kCount) fail("E1101: 6 tuning parameters expected");
-    h->set_tuning(Tuning::from(params));
+    if (params == nullptr || (count != Tuning::kMinCount && count < Tuning::kCount))
+      fail("E1101: 6 or 10 tuning parameters expected");
+    int32_t all[Tuning::kCount];
+    h->tuning().to(all);
+    for (int i = 0; i < std::min<int>(count, Tuning::kCount); ++i) all[i] = params[i];
+    h->set_tuning(Tuning::from(all));
   });
 }
 
 int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, char* err,
                                   size_t err_len) {
   AUTAN_CALL({
-    if (params == nullptr || count < Tuning::kCount) fail("E1101: room for 6 parameters expected");
+    if (params == nullptr || count < Tuning::kCount) fail("E1101: room for 10 parameters expected");
     h->tuning().to(params);
   });
 }
@@ -3309,6 +3830,10 @@ int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t 
                                    int64_t* steps, double* gpu_ms, char* err, size_t err_len) {
   AUTAN_CALL(march_cases(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, reference,
                          iterations, converged, first, steps, gpu_ms));
+}
+
+int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len) {
+  AUTAN_CALL({ h->set_stall_test(polls); });
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {

@@ -336,27 +336,33 @@ class EulerDevice:
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_KINDS)}
 
     TUNING_KEYS = ("grad_chunk", "grad_block", "face_mode", "face_block", "gather_block",
-                   "grad_mode")
+                   "grad_mode", "grad_widen", "grad_narrow", "grad_minb", "grad_depth")
 
     def tuning(self) -> dict:
-        p = np.zeros(6, dtype=np.int32)
-        self._call("autan_euler_device_get_tuning", N.ptr(p, C.c_int32), 6)
+        p = np.zeros(len(self.TUNING_KEYS), dtype=np.int32)
+        self._call("autan_euler_device_get_tuning", N.ptr(p, C.c_int32), len(p))
         return dict(zip(self.TUNING_KEYS, map(int, p)))
 
     def set_tuning(self, **kw) -> None:
         t = self.tuning()
         t.update(kw)
         p = np.array([t[k] for k in self.TUNING_KEYS], dtype=np.int32)
-        self._call("autan_euler_device_set_tuning", N.ptr(p, C.c_int32), 6)
+        self._call("autan_euler_device_set_tuning", N.ptr(p, C.c_int32), len(p))
 
     def autotune(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
                  trial_steps: int = 2) -> tuple[dict, float]:  # fmt: skip
         """Picks the fastest launch choices on this case; returns them and the ms per step."""
-        p = np.zeros(6, dtype=np.int32)
+        p = np.zeros(len(self.TUNING_KEYS), dtype=np.int32)
         ms = C.c_double()
         self._call("autan_euler_device_autotune", float(cfl), float(dt), int(local), int(rk),
                    int(trial_steps), N.ptr(p, C.c_int32), C.byref(ms))  # fmt: skip
         return dict(zip(self.TUNING_KEYS, map(int, p))), float(ms.value)
+
+    def set_stall_test(self, polls: int) -> None:
+        """Test hook of the failure detection: with polls > 0 the mode-5 gradient kernel's warps
+        also wait on a barrier nothing arrives on, at most `polls` polls, so the next step call
+        fails with E1201; 0 turns it off."""
+        self._call("autan_euler_device_set_stall_test", int(polls))
 
     def sync(self):
         self._call("autan_euler_device_sync")

@@ -162,7 +162,8 @@ int autan_euler_device_time_steps(void* handle, double cfl, double* dt, char* er
 int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                     int64_t n_steps, double* ms, int64_t* launches, char* err,
                                     size_t err_len);
-/* Launch choices of the hot kernels (6 values): [0] stencil entries the gradient kernel loads
+/* Launch choices of the hot kernels (10 values; set_tuning also takes the first 6 alone, the rest
+ * then keep their values): [0] stencil entries the gradient kernel loads
  * together (1, 2 or 4, where 2 takes at most 128 threads per block; 2, 4 or 8 when staged), [1]
  * its threads per block, [2] face strategy (0 gather-recompute: each cell recomputes its faces'
  * fluxes; 1 store-gather: each face's flux once into a face scratch, then summed per cell), [3]
@@ -171,15 +172,22 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * copies, at most 128 threads per block; 2: as 0, software-pipelined: the next entry's gather and
  * the row after it in flight while an entry is added; 3: each thread's next [0] neighbour records
  * and 2 x [0] rows in a shared-memory ring filled by asynchronous copies (cp.async), [0] = 2, 4
- * or 8, at most 128 threads per block). Every choice gives the same bits. No counterpart in the
- * reference beyond its Strategy enum (codegen/include/autan/kernels/strategy.hpp:14-21). */
+ * or 8, at most 128 threads per block; 4, fp32+acc64 only: as 0 with [0] entries loaded together,
+ * 128 threads per block, and [6] 0, 1 or 2: none, the x and y, or all of each entry's 15 products
+ * widened to FP64 on the integer pipe, exactly (2^-896-scaled bit moves) instead of by cvt; [7]
+ * 1: neighbours gathered as 16 + 4 bytes instead of one 32-byte load; [8] 7, the blocks of 128
+ * threads per SM the registers are bounded for, with [0] = 2; 5, fp32+acc64 only: each warp's
+ * stencil rows streamed by TMA bulk copies into a ring of [9] (4 or 8) shared-memory slots ahead of
+ * the warp, [0] (2 or 3) gathers in flight, [7] as for 4, 128 threads per block).
+ * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
+ * (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,
                                   size_t err_len);
 int autan_euler_device_get_tuning(void* handle, int32_t* params, int32_t count, char* err,
                                   size_t err_len);
 /* The autotuner: times candidate launch choices on `trial_steps` steps each of this handle's own
  * case (the device state is restored after every trial), keeps the fastest and returns it in
- * params (6 values) with its ms per step. */
+ * params (10 values, or NULL) with its ms per step. */
 int autan_euler_device_autotune(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                 int32_t trial_steps, int32_t* params, double* ms_per_step,
                                 char* err, size_t err_len);
@@ -261,6 +269,12 @@ int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t 
                                    const double* floors, const double* reference,
                                    int64_t* iterations, int32_t* converged, double* first,
                                    int64_t* steps, double* gpu_ms, char* err, size_t err_len);
+/* Test hook of the failure detection (no counterpart in the reference): with polls > 0 every warp
+ * of the mode-5 gradient kernel also waits, at most `polls` polls, on an mbarrier that nothing
+ * arrives on; the bounded wait runs out, the warp marks the fault word, waits (up to 2^20 polls)
+ * for the copies it has issued and stores nothing, and the step call returns E1201. 0 turns the
+ * hook off; the handle stays usable either way. */
+int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len);
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);
 /* The handle's cudaStream_t. */

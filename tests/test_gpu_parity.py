@@ -209,6 +209,21 @@ def test_tuning_variants_are_bit_identical(precision):
                     dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
                     u = dev.download()
                 assert bits_equal(u[:, :no], u_o[:, :no]), (gmode, chunk, mode, block)
+    if precision == "fp64":
+        return
+    # mode 4: the products widened on the integer pipe (none, x and y, all), 5-word gathers;
+    # mode 5: the per-warp TMA row ring of 4 or 8 slots with 2 or 3 gathers in flight
+    variants = [dict(grad_mode=4, grad_chunk=2, grad_widen=w, grad_narrow=g, grad_minb=7)
+                for w in (0, 1, 2) for g in (0, 1)]
+    variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
+                 for r in (4, 8) for ch in (2, 3) for g in (0, 1)]
+    for v in variants:
+        with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+            dev.set_tuning(grad_block=128, face_mode=1, **v)
+            dev.upload(case.u0)
+            dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
+            u = dev.download()
+        assert bits_equal(u[:, :no], u_o[:, :no]), v
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
@@ -226,6 +241,17 @@ def test_gradient_stagings_agree_on_the_channel(precision):
             dev.upload(case.u0)
             dev.step(cfl=case.cfl, local=True, rk=3, n_steps=case.steps)
             out[(gmode, chunk, block)] = dev.download()
+    if precision != "fp64":
+        variants = [dict(grad_mode=4, grad_chunk=2, grad_widen=w, grad_narrow=g, grad_minb=7)
+                    for w, g in ((0, 1), (1, 0), (2, 1))]
+        variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
+                     for r, ch, g in ((4, 2, 0), (8, 3, 1), (4, 3, 1), (8, 2, 0))]
+        for v in variants:
+            with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+                dev.set_tuning(grad_block=128, face_mode=1, face_block=128, gather_block=128, **v)
+                dev.upload(case.u0)
+                dev.step(cfl=case.cfl, local=True, rk=3, n_steps=case.steps)
+                out[tuple(sorted(v.items()))] = dev.download()
     first = out[(0, 1, 128)]
     for k, u in out.items():
         assert bits_equal(u, first), k
