@@ -1,12 +1,17 @@
 """Benchmark of the explicit Euler residual-and-update path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tets|hex]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload channel|tets|hex|batch]
 
-Workload (default `tets`): the convected isentropic vortex on 2 073 600 jittered Kuhn tetrahedra
-(240 x 240 x 6 lattice, nodes moved by U(-0.2, 0.2) h, seed 0, periodic in x and y, slip in z),
-second-order LSQ face2 gradients with the Venkatakrishnan limiter (K = 5), HLLC, SSP-RK3 at CFL 0.8,
-fp32+acc64. A step is one SSP-RK3 step (three residual evaluations and updates, the CFL time step
-and the exact residual norms). Synthetic data: the vortex field is generated, no dataset is read.
+Workload (default `channel`): the steady subsonic channel over a Gaussian bump, 480 x 150 x 100
+boxes as 8 002 500 hybrid cells (hexahedra, triangular prisms, polyhedral bricks; wall-normal
+stretching 1.1), AUSM+-up, second-order LSQ face2 gradients with the Venkatakrishnan limiter (K = 5),
+total-pressure inlet at Mach 0.5, static-pressure outlet, slip walls, SSP-RK3 with local time steps
+at CFL 1.5, fp32+acc64, from the freestream start. `--workload tets`: the convected isentropic
+vortex on 2 073 600 jittered Kuhn tetrahedra (240 x 240 x 6 lattice, nodes moved by U(-0.2, 0.2) h,
+seed 0, periodic in x and y, slip in z), HLLC, SSP-RK3 at CFL 0.8. A step is one SSP-RK3 step
+(three residual evaluations and updates, the CFL time steps and the exact residual norms).
+Synthetic data: the meshes and fields are generated, no dataset is read.
 
 Metric: cell-iterations per second (cells x steps / s), whole job. `value` is device time (CUDA
 events on the stepper's stream) with the state resident in HBM; `e2e` is the same metric through
@@ -53,10 +58,11 @@ def measured_hbm_peak() -> tuple[float, str]:
 # ------------------------------------------------------------------ algorithmic bytes
 
 
-def kernel_bytes(case, rk: int) -> dict[str, float]:
+def kernel_bytes(case, rk: int, local: bool = False) -> dict[str, float]:
     """Algorithmic bytes of one step per kernel kind: every array a kernel touches, read or written
     once, at its stored size (the rule of the reference's physics/bench/euler_bench.cu:321-372,
-    applied to this layout); re-reads of neighbours' values are not counted."""
+    applied to this layout); re-reads of neighbours' values are not counted. `local`: the CFL
+    steps are per cell (written by the stage-0 gradient launch)."""
     m = case.mesh
     fp32 = case.scheme.precision != "fp64"
     sS = sG = sGV = sC = 4 if fp32 else 8
@@ -75,6 +81,12 @@ def kernel_bytes(case, rk: int) -> dict[str, float]:
         grad = (5 * sS * n + 4 * n + 4 * s + 3 * sGV * s + 5 * sS * nb + inc + 6 * sC * fi
                 + 3 * sC * nbo + 8 * n + 15 * sG * n + 5 * sS * n)  # fmt: skip
     spectral = (5 * sS * n + inc + 8 * fi + 4 * sGV * fi + 4 * sGV * nbo + 5 * sS * nbo + 8 * n)
+    if second:
+        # the stage-0 gradient launch also does the spectral radius and the CFL steps: it reads
+        # the faces' normals and areas besides the gradient's arrays and, with local steps,
+        # writes every cell's step; no separate spectral kernel runs
+        fused = 4 * sGV * (fi + nbo) + (8 * n if local else 0)
+        spectral = 0.0
     face_common = (5 * sS * n + (20 * sS * n if second else 0) + 8 * n + inc + 8 * fi
                    + 4 * sGV * fi + 6 * sC * fi + nbo * (3 * sGV + 3 * sC + 5 * sS + 1 + sGV))  # fmt: skip
     faces = 0.0
@@ -89,7 +101,7 @@ def kernel_bytes(case, rk: int) -> dict[str, float]:
         faces += b
     return {
         "boundary_states": boundary * stages,
-        "gradients": grad * stages,
+        "gradients": grad * stages + (fused if second else 0.0),
         "spectral": spectral,
         "faces": faces,
         "norms": 40.0 * n,
@@ -413,6 +425,36 @@ def workload_config(args) -> dict:
     }
 
 
+def fp64_error(case, dev, steps: int, local_rank: int) -> dict:
+    """The fp32+acc64 state against the FP64 one after `steps` steps of the workload from its
+    start: both run on the device (the fp64 device path equals the CPU FP64 oracle bit for bit on
+    the parity meshes, and is used here because the oracle would take hours at full size). The
+    largest difference of each conserved component, relative to that component's largest
+    magnitude, and the largest of the five."""
+    import dataclasses
+
+    from autan_b200.euler import EulerDevice
+
+    dev.upload(case.u0)
+    dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=steps, graph=True)
+    u32 = dev.download()
+    s64 = dataclasses.replace(case.scheme, precision="fp64")
+    with EulerDevice(case.mesh, s64, case.bc_kind, case.bc_data, device=local_rank) as d64:
+        d64.upload(case.u0)
+        d64.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=steps, graph=True)
+        u64 = d64.download()
+    n = case.mesh.n_owned_cells
+    d, ref = np.abs(u32[:, :n] - u64[:, :n]), np.abs(u64[:, :n])
+    mom = max(ref[1:4].max(), 1e-300)
+    scale = [max(ref[0].max(), 1e-300), mom, mom, mom, max(ref[4].max(), 1e-300)]
+    per = [float(d[k].max() / scale[k]) for k in range(5)]
+    return {"steps": steps, "max_rel": max(per), "per_component_rel": per,
+            "against": "the fp64 device path from the same start (bit-identical to the CPU FP64 "
+                       "oracle at full size on the parity tests); the largest difference of "
+                       "density and energy relative to their largest magnitude, of the momenta "
+                       "relative to the largest momentum magnitude"}  # fmt: skip
+
+
 def run_converge(args, case, dev, tuned) -> None:
     """A steady march to `--converge` decades (autan_euler_device_march), fp32+acc64 with the
     round-off plateau floors of the case's freestream (runtime/src/run.cpp:1874-1897)."""
@@ -587,7 +629,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     # -- per-kernel times (CUDA events around every launch on the stepper's stream)
     kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=3)
-    alg = kernel_bytes(case, case.rk)
+    alg = kernel_bytes(case, case.rk, case.local)
     dominant = max((k for k in kt if kt[k][1] > 0), key=lambda k: kt[k][0])
     per_step_launches = kt[dominant][1] / 3
     avg_ms = kt[dominant][0] / kt[dominant][1]
@@ -598,6 +640,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     step_bytes = sum(alg.values())
     family = {"tets": "tets", "channel": "channel", "batch": "channel"}.get(args.workload, args.workload)
     traffic = committed_traffic(dominant, n, family)
+    error = None
+    if world == 1 and args.error_steps > 0 and args.workload in ("tets", "channel"):
+        error = fp64_error(case, dev, args.error_steps, local_rank)
     line = None
     if rank == 0:
         line = {
@@ -636,6 +681,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "clocks": clocks.summary(),
             "residual_rms": list(map(float, r.residuals)),
         }
+        if error is not None:
+            line["error_vs_fp64"] = error
     dev.close()
     if dist is not None:
         dist.barrier()
@@ -649,19 +696,26 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel
+# kind, averaged over a step's launches, from one ncu capture per mesh family on a smaller case
+# of that family (the capture named beside each entry, under profiles/): (kernel kind, mesh
+# family) -> (bytes per launch, cells of the capture, capture). The bytes per cell do not depend
+# on the lattice size (same stencil, record sizes and cell ordering), so a workload's traffic is
+# the entry scaled to its cells.
+TRAFFIC = {
+    ("gradients", "tets"): (452191659, 1016064, "gradients_occ7_tets_and_channel_1M.md"),
+    ("gradients", "channel"): (695027797, 994600, "gradients_occ7_tets_and_channel_1M.md"),
+}
+
+
 def committed_traffic(kernel: str, n_cells: int, mesh: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summaries (profiles/traffic.md, a
-    line `traffic <kernel> <bytes per launch> <cells> <mesh>` captured on a smaller case of the same
-    mesh family, scaled to this case's cells), else None. mesh: "tets" (the vortex lattices) or
-    "channel" (the hybrid bump channels, single or batched)."""
-    p = REPO / "profiles" / "traffic.md"
-    if not p.exists():
+    """DRAM bytes per launch of `kernel` on `n_cells` cells of mesh family `mesh` ("tets": the
+    vortex lattices; "channel": the hybrid bump channels, single or batched) from TRAFFIC, else
+    None."""
+    entry = TRAFFIC.get((kernel, mesh))
+    if entry is None:
         return None
-    for line in p.read_text().splitlines():
-        f = line.strip().strip("`").split()
-        if len(f) == 5 and f[0] == "traffic" and f[1] == kernel and f[4] == mesh:
-            return float(f[2]) * n_cells / float(f[3])
-    return None
+    return float(entry[0]) * n_cells / float(entry[1])
 
 
 def main() -> None:
@@ -670,7 +724,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["tets", "hex", "channel", "batch"], default="tets")
+    ap.add_argument("--workload", choices=["tets", "hex", "channel", "batch"], default="channel")
     ap.add_argument("--cases", type=int, default=256, help="batch: number of channel cases")
     ap.add_argument("--cells", default="20000,500000", help="batch: cell range LO,HI (log-uniform)")
     ap.add_argument("--seed", type=int, default=0, help="batch: seed of the case parameters")
@@ -695,6 +749,8 @@ def main() -> None:
                     help="with --warmstart: write the trained network to this .npz")
     ap.add_argument("--load-network", default="",
                     help="with --warmstart: take the network from this .npz instead of training")
+    ap.add_argument("--error-steps", type=int, default=100,
+                    help="steps of the fp32+acc64 against fp64 comparison (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()

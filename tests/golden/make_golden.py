@@ -1,8 +1,8 @@
 """Golden vectors of the explicit Euler path from the reference's own kernel source.
 
-Run in a checkout that has the reference at REFERENCE (default /root/reference):
+Run with the reference tree named by the environment (the script reads its kernels/euler.py):
 
-    python tests/golden/make_golden.py
+    AUTAN_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 It imports the reference's `kernels/euler.py` (the DSL module the reference's generator turns into
 the CPU and GPU loops) and calls its @pointwise bodies directly in Python, with the DSL intrinsics
@@ -37,7 +37,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REFERENCE = Path(os.environ.get("AUTAN_REFERENCE", "/root/reference"))
+if "AUTAN_REFERENCE" not in os.environ:
+    raise SystemExit("set AUTAN_REFERENCE to the reference checkout")
+REFERENCE = Path(os.environ["AUTAN_REFERENCE"])
 sys.path.insert(0, str(REPO))
 
 
