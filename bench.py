@@ -21,7 +21,9 @@ over ranks.
 
 `--impl reference` times the reference algorithm on the host cores: the CPU oracle (a C
 restatement of the reference's residual and steps) on one thread per core, each thread stepping
-its own 240 x 24 x 6 slab of the same lattice (207 360 cells) per step.
+its own copy of the workload's CPU sample (cpu_sample: a smaller mesh of the same generator and
+scheme, set up by the reference's own mesh, geometry and stencil code from a committed compact
+mesh, so that this arm loads nothing of this repository's native library).
 """
 
 from __future__ import annotations
@@ -250,38 +252,84 @@ def gpu_uuid(device: int) -> str:
 # ------------------------------------------------------------------ CPU (oracle) throughput
 
 
-def cpu_throughput(steps: int, warmup: int, threads: int,
-                   slab: tuple[int, int, int] = (240, 24, 6),
-                   workload: str = "tets", min_seconds: float = 0.0) -> tuple[float, str, int]:  # fmt: skip
-    """Cell-iterations per second of the CPU oracle: one thread per core, each stepping its own
-    slab (240 x 24 x 6 by default) of the benchmark lattice (SSP-RK3, fp32+acc64), for the channel
-    workload its own channel of `slab` boxes, for the batch workload its own 20 000-cell channel of
-    the batch's distribution and scheme (the first draw of seed 0), for the hex workload its own
-    copy of the 8 192-cell vortex (fp64, classical RK4); the rate of the whole host.
-    `steps` steps, then more until at least `min_seconds` have passed."""
+SAMPLES = {"channel": "channel", "tets": "tets", "hex": "hex", "batch": "batch"}
+SAMPLE_TEXT = {
+    "channel": "a 60x20x10-box hybrid bump channel (13 730 cells) of the 8.0 M-cell workload's "
+               "generator and scheme",
+    "tets": "a 60x24x6 periodic slab (51 840 cells) of the jittered Kuhn-tetrahedra lattice at its "
+            "cell size, HLLC, SSP-RK3",
+    "hex": "the 8 192-cell hexahedral vortex (fp64, first-order Roe, classical RK4)",
+    "batch": "the first channel of the batch (seed 0) drawn at 20 000 cells, Roe, farfield",
+}  # fmt: skip
+
+
+def vortex_state(centroid, beta: float, centre, gamma: float = 1.4) -> np.ndarray:
+    """Shu's isentropic vortex on the freestream rho = p = 1, u = v = 1 (conserved, 5 x cells)."""
+    x, y = centroid[0] - centre[0], centroid[1] - centre[1]
+    r2 = x * x + y * y
+    f = beta / (2.0 * np.pi) * np.exp(0.5 * (1.0 - r2))
+    u, v = 1.0 - f * y, 1.0 + f * x
+    t = 1.0 - (gamma - 1.0) * beta * beta / (8.0 * gamma * np.pi * np.pi) * np.exp(1.0 - r2)
+    rho = t ** (1.0 / (gamma - 1.0))
+    p = rho * t
+    return np.stack([rho, rho * u, rho * v, np.zeros_like(u), p / (gamma - 1.0) +
+                     0.5 * rho * (u * u + v * v)])  # fmt: skip
+
+
+def cpu_sample(workload: str):
+    """The CPU sample of `workload` as the oracle takes it, built without this repository's
+    native library: the compact mesh of tests/golden/cpu_sample_<name>.npz assembled, its FP64
+    geometry and face2 stencil computed by the reference's own code (oracle/_ref: core/src/mesh.cpp
+    assemble, core/src/geometry.cpp compute_geometry, codegen/cpp/geometry.cpp pack_geometry and
+    cell_stencil), ghost images given their owner's geometry shifted by their translation, the
+    least-squares weights by the oracle (physics/src/euler.cpp:340-416). Returns (mesh dict,
+    scheme dict, bc_kind, bc_data, u0, rk, cfl, local, owned cells)."""
     sys.path.insert(0, str(REPO / "tests"))
     import oracle as O
-    from autan_b200 import cases
+    import ref_setup as R
 
-    rk = 3
-    if workload == "batch":
-        b = cases.bump_batch(1, seed=0, cells=(20_000, 20_000))
-        md, sch, kind, data, u0 = b.mesh, b.scheme.as_dict(), b.bc_kind, b.bc_data, b.u0
-        cfl, local, cells = b.cfl, True, b.n_cells
-        what = f"{b.params[0]['boxes'][0]}x{b.params[0]['boxes'][1]}x{b.params[0]['boxes'][2]} batch channel"
+    z = np.load(REPO / "tests" / "golden" / f"cpu_sample_{SAMPLES[workload]}.npz")
+    nc, ng = int(z["n_cells"]), int(z["n_ghost"])
+    owned = nc - ng
+    r = R.reference_setup_arrays(z["points"], z["face_node_offsets"], z["face_nodes"], z["cell0"],
+                                 z["cell1"], z["face_zone"], nc, ng)  # fmt: skip
+    counts = [int(v) for v in r["counts"]]
+    cc, vol = r["cell_centroid"].copy(), r["cell_volume"].copy()
+    g = np.asarray(z["ghost_owner"], dtype=np.int64)
+    if ng:
+        cc[:, owned:] = cc[:, g] + z["ghost_translation"]
+        vol[owned:] = vol[g]
+    md = dict(zip(("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+                   "n_owned_interior_faces", "n_owned_faces"), counts))  # fmt: skip
+    md.update(owner=r["owner"], neighbour=r["neighbour"], cell_face_offsets=r["cell_face_offsets"],
+              cell_faces=r["cell_faces"], ghost_owner=z["ghost_owner"],
+              face_normal=r["face_normal"], face_area_magnitude=r["face_area_magnitude"],
+              face_centroid=r["face_centroid"],
+              face_moment=r["face_moment"] if np.any(r["face_moment"]) else np.zeros(0),
+              cell_centroid=cc, cell_volume=vol, stencil_offsets=r["stencil_offsets"],
+              stencil=r["stencil"])  # fmt: skip
+    kind, data = z["bc_kind"], z["bc_data"]
+    md["stencil_lsq_weight"] = O.gradient_weights(md, kind)
+    start = json.loads(str(z["start"]))
+    if "uniform" in start:
+        u0 = np.repeat(np.array(start["uniform"])[:, None], nc, axis=1)
     else:
-        if workload == "hex":
-            case = cases.vortex_hex(steps=1)
-            what = "64x64x2 hexahedral vortex (fp64)"
-        elif workload == "channel":
-            case = cases.bump_channel(*slab, steps=1)
-            what = f"{slab[0]}x{slab[1]}x{slab[2]} channel"
-        else:
-            case = cases.vortex_tets(*slab, steps=1, precision="fp32+acc64")
-            what = f"{slab[0]}x{slab[1]}x{slab[2]} slab of the benchmark lattice"
-        md, sch = cases.oracle_mesh_dict(case), case.scheme.as_dict()
-        kind, data, u0 = case.bc_kind, case.bc_data, case.u0
-        cfl, local, cells, rk = case.cfl, case.local, case.mesh.n_owned_cells, case.rk
+        u0 = vortex_state(cc, start["vortex"]["beta"], start["vortex"]["centre"])
+        if ng:
+            u0[:, owned:] = u0[:, g]
+    return (md, json.loads(str(z["scheme"])), kind, data, np.ascontiguousarray(u0), int(z["rk"]),
+            float(z["cfl"]), bool(z["local"]), owned)  # fmt: skip
+
+
+def cpu_throughput(steps: int, warmup: int, threads: int, workload: str = "channel",
+                   min_seconds: float = 0.0) -> tuple[float, str, int]:  # fmt: skip
+    """Cell-iterations per second of the CPU oracle on the host: one thread per core, each stepping
+    its own copy of the workload's CPU sample (cpu_sample); the rate of the whole host. `steps`
+    steps, then more until at least `min_seconds` have passed."""
+    sys.path.insert(0, str(REPO / "tests"))
+    import oracle as O
+
+    md, sch, kind, data, u0, rk, cfl, local, cells = cpu_sample(workload)
     oracles = [O.Oracle(md, sch, kind, data) for _ in range(threads)]
     states = [u0.copy() for _ in range(threads)]
 
@@ -305,8 +353,10 @@ def cpu_throughput(steps: int, warmup: int, threads: int,
     elapsed = time.perf_counter() - t0
     rate = cells * threads * done / elapsed
     kind_of_step = "SSP-RK3" if rk == 3 else "RK4"
-    sample = (f"{threads} threads x {done} {kind_of_step} steps of a {what} ({cells} cells each), "
-              f"CPU oracle (C, -O2), {elapsed:.1f} s")  # fmt: skip
+    sample = (f"{threads} threads x {done} {kind_of_step} steps of {SAMPLE_TEXT[workload]}, each "
+              f"thread its own copy; set up by the reference's own mesh assembly, geometry and "
+              f"stencil code with the oracle's weights; stepped by the CPU oracle (C, -O2); "
+              f"{elapsed:.1f} s")  # fmt: skip
     return rate, sample, threads
 
 
@@ -348,14 +398,6 @@ def whole_job_rate(world: int, cells: int, steps: int, seconds: float) -> float:
     return world * cells * steps / seconds
 
 
-def cpu_slab(args) -> tuple[int, int, int]:
-    """Boxes each CPU-baseline thread steps: --cpu-slab, else 240 x 24 x 6 of the tetrahedral
-    lattice or a 60 x 20 x 10 channel."""
-    if args.cpu_slab:
-        return parse_triple(args.cpu_slab)
-    return (60, 20, 10) if args.workload == "channel" else (240, 24, 6)
-
-
 def parse_triple(text: str) -> tuple[int, int, int]:
     a, b, c = (int(v) for v in text.split(","))
     return a, b, c
@@ -369,7 +411,7 @@ def run_reference(args, rank: int, world: int) -> None:
         return
     threads = args.cpu_threads or host_threads()
     rate, sample, cores = cpu_throughput(args.steps, max(1, min(args.warmup, 1)), threads,
-                                         cpu_slab(args), args.workload)  # fmt: skip
+                                         args.workload)  # fmt: skip
     line = {
         "impl": "reference",
         "metric": "cell-iterations/s",
@@ -690,7 +732,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0:
         if world == 1 and not args.no_cpu:
             rate, sample, cores = cpu_throughput(2, 1, args.cpu_threads or host_threads(),
-                                                 cpu_slab(args), args.workload, min_seconds=10.0)  # fmt: skip
+                                                 args.workload, min_seconds=10.0)  # fmt: skip
             line["cpu_baseline"] = {"value": rate, "unit": "cell-iterations/s", "cores": cores,
                                     "kind": "port", "sample": sample}  # fmt: skip
         print(json.dumps(line), flush=True)
@@ -729,8 +771,6 @@ def main() -> None:
     ap.add_argument("--cells", default="20000,500000", help="batch: cell range LO,HI (log-uniform)")
     ap.add_argument("--seed", type=int, default=0, help="batch: seed of the case parameters")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--cpu-slab", default="",
-                    help="lattice NX,NY,NZ each CPU thread steps for the CPU baseline")
     ap.add_argument("--cpu-threads", type=int, default=0,
                     help="threads of the CPU baseline (0: every core this process may use)")
     ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")

@@ -3,6 +3,7 @@
  * (tests/toolchain/check_no_fma.cmake), so that every operation rounds once. */
 #include "euler_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -45,6 +46,81 @@
 #undef EXP
 #undef LOG
 #undef SFX
+
+/* ------------------------------------------------------------------ LSQ weights */
+/* Euler::Impl::compute_gradient_weights (physics/src/euler.cpp:340-416) of the owned cells: the
+ * normal matrix of each cell's stencil offsets weighted by 1 / |d|^2, a boundary face in the fit
+ * only with condition 0 (state) unless the fit without such faces is singular
+ * (|det| <= 1e-10 |a00 a11 a22|, then every boundary face enters), an offset component within 64
+ * ulps of the larger coordinate taken as zero, the inverse by cofactors over the determinant, the
+ * weights s (inverse row . d). Ghost cells' weights stay 0. Here each cell's offsets are kept in a
+ * scratch row between the matrix and the weights. */
+typedef struct {
+  double d[3];
+  double s;
+} lsq_offset;
+
+static int lsq_fit(const oracle_mesh* m, int32_t c, const uint8_t* bc_kind, int every_boundary,
+                   lsq_offset* row, double* w, int64_t n_stencil) {
+  const int64_t first = m->stencil_offsets[c], last = m->stencil_offsets[c + 1];
+  const int64_t nc = m->n_cells, nf = m->n_faces;
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t k = first; k < last; ++k) {
+    const int32_t e = m->stencil[k];
+    const double* x;
+    int64_t stride, at;
+    int fit = 1;
+    if (e >= 0) {
+      x = m->cell_centroid;
+      stride = nc;
+      at = e;
+    } else {
+      x = m->face_centroid;
+      stride = nf;
+      at = -(int64_t)e - 1;
+      fit = every_boundary || bc_kind[at - m->n_interior_faces] == 0;
+    }
+    lsq_offset* q = &row[k - first];
+    for (int j = 0; j < 3; ++j) {
+      const double xo = x[j * stride + at], xc = m->cell_centroid[j * nc + c];
+      const double big = fabs(xo) < fabs(xc) ? fabs(xc) : fabs(xo);
+      const double diff = xo - xc;
+      q->d[j] = fabs(diff) <= 64 * DBL_EPSILON * big ? 0.0 : diff;
+    }
+    q->s = fit ? 1.0 / (q->d[0] * q->d[0] + q->d[1] * q->d[1] + q->d[2] * q->d[2]) : 0.0;
+    for (int u = 0; u < 3; ++u)
+      for (int v = 0; v < 3; ++v) a[3 * u + v] += q->s * q->d[u] * q->d[v];
+  }
+  const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+  if (!(fabs(det) > 1e-10 * fabs(a[0] * a[4] * a[8]))) return 0;
+  const double inv[9] = {(a[4] * a[8] - a[5] * a[7]) / det, (a[2] * a[7] - a[1] * a[8]) / det,
+                         (a[1] * a[5] - a[2] * a[4]) / det, (a[5] * a[6] - a[3] * a[8]) / det,
+                         (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
+                         (a[3] * a[7] - a[4] * a[6]) / det, (a[1] * a[6] - a[0] * a[7]) / det,
+                         (a[0] * a[4] - a[1] * a[3]) / det};
+  for (int64_t k = first; k < last; ++k) {
+    const lsq_offset* q = &row[k - first];
+    for (int u = 0; u < 3; ++u)
+      w[u * n_stencil + k] =
+          q->s * (inv[3 * u] * q->d[0] + inv[3 * u + 1] * q->d[1] + inv[3 * u + 2] * q->d[2]);
+  }
+  return 1;
+}
+
+void oracle_gradient_weights(const oracle_mesh* m, const uint8_t* bc_kind, double* w) {
+  const int64_t n_stencil = m->stencil_offsets[m->n_cells];
+  memset(w, 0, (size_t)(3 * n_stencil) * sizeof(double));
+  int64_t longest = 1;
+  for (int32_t c = 0; c < m->n_owned_cells; ++c) {
+    const int64_t len = m->stencil_offsets[c + 1] - m->stencil_offsets[c];
+    if (len > longest) longest = len;
+  }
+  lsq_offset* row = (lsq_offset*)malloc((size_t)longest * sizeof(lsq_offset));
+  for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    if (!lsq_fit(m, c, bc_kind, 0, row, w, n_stencil)) lsq_fit(m, c, bc_kind, 1, row, w, n_stencil);
+  free(row);
+}
 
 /* ------------------------------------------------------------------ ExactSum */
 /* runtime/src/exact_sum.cpp:22-140: 68 limbs of 32 bits in int64 words, limb i weighing

@@ -82,6 +82,11 @@ void oracle_boundary_pressure(const oracle* o, double* p, double* force);
 void oracle_norms(const double* res, int32_t n_owned, int32_t n_cells, double* rms);
 /* ExactSum (runtime/src/exact_sum.cpp) of n terms, rounded once to the nearest double. */
 double oracle_exact_sum(const double* terms, int64_t n);
+/* Euler::Impl::compute_gradient_weights (physics/src/euler.cpp:340-416): the least-squares
+ * gradient weights of the owned cells over mesh->stencil (w: 3 x n_stencil, written; ghost cells
+ * 0) for the boundary codes bc_kind (n_faces - n_interior_faces). Reads the mesh's stencil and
+ * centroids only (mesh->stencil_lsq_weight is not read). */
+void oracle_gradient_weights(const oracle_mesh* mesh, const uint8_t* bc_kind, double* w);
 /* First invalid cell of a state and residual (euler_physics.cpp:1399-1435), or -1. */
 int64_t oracle_first_invalid(const oracle* o, const double* u, const double* res);
 

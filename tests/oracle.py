@@ -54,6 +54,8 @@ def lib():
         L.oracle_exact_sum.argtypes = [P(f64), i64]
         L.oracle_first_invalid.restype = i64
         L.oracle_first_invalid.argtypes = [vp, P(f64), P(f64)]
+        L.oracle_gradient_weights.restype = None
+        L.oracle_gradient_weights.argtypes = [P(OracleMesh), P(C.c_uint8), P(f64)]
         for n in ("oracle_flux",):
             getattr(L, n).argtypes = [P(OracleScheme), P(f64), P(f64), P(f64), P(f64)]
         L.oracle_boundary_value.argtypes = [P(OracleScheme), P(f64), f64, P(f64), P(f64), P(f64)]
@@ -75,6 +77,43 @@ def scheme_struct(s: dict) -> OracleScheme:
     o.scale[:] = [float(x) for x in s["scale"]]
     o.reference[:] = [float(x) for x in s["reference"]]
     return o
+
+
+def mesh_struct(mesh: dict, keep: dict) -> OracleMesh:
+    """struct oracle_mesh over the dict's arrays (kept alive in `keep`); a missing or empty
+    stencil_lsq_weight is passed as a one-element stand-in, face_moment as NULL."""
+    m = OracleMesh()
+    for k in ("n_cells", "n_owned_cells", "n_faces", "n_interior_faces",
+              "n_owned_interior_faces", "n_owned_faces"):  # fmt: skip
+        setattr(m, k, int(mesh[k]))
+    types = {"owner": i32, "neighbour": i32, "cell_faces": i32, "ghost_owner": i32,
+             "stencil": i32, "cell_face_offsets": i64, "stencil_offsets": i64}  # fmt: skip
+    for k in ("owner", "neighbour", "cell_face_offsets", "cell_faces", "ghost_owner",
+              "face_normal", "face_area_magnitude", "face_centroid", "face_moment",
+              "cell_centroid", "cell_volume", "stencil_offsets", "stencil",
+              "stencil_lsq_weight"):  # fmt: skip
+        t = types.get(k, f64)
+        dt = {i32: np.int32, i64: np.int64, f64: np.float64}[t]
+        a = np.ascontiguousarray(mesh.get(k, np.zeros(0)), dtype=dt)
+        if a.size == 0 and k == "face_moment":
+            setattr(m, k, None)
+            continue
+        if a.size == 0:
+            a = np.zeros(1, dtype=dt)
+        keep[k] = a
+        setattr(m, k, _p(a, t))
+    return m
+
+
+def gradient_weights(mesh: dict, bc_kind) -> np.ndarray:
+    """The oracle's least-squares weights (3 x n_stencil) of the mesh dict's stencil for the
+    boundary codes (Euler::Impl::compute_gradient_weights, physics/src/euler.cpp:340-416)."""
+    keep = {}
+    m = mesh_struct(mesh, keep)
+    kind = np.ascontiguousarray(bc_kind, dtype=np.uint8)
+    w = np.zeros((3, int(np.asarray(mesh["stencil_offsets"])[int(mesh["n_cells"])])))
+    lib().oracle_gradient_weights(C.byref(m), _p(kind, C.c_uint8), _p(w))
+    return w
 
 
 class Oracle:

@@ -46,25 +46,38 @@ def reference_setup(mesh) -> dict[str, np.ndarray]:
     """The reference's set-up of the product mesh `mesh` (autan_b200.mesh.Mesh): its faces given
     face by face with the product's owner / neighbour and node loops, its ghost cells as the
     reference's halo cells (their centroids the product's, as a partitioner supplies them)."""
-    l = lib()
     nf, ni = mesh.n_faces, mesh.n_interior_faces
-    pts = np.ascontiguousarray(mesh.points, dtype=np.float64)
-    fno = np.ascontiguousarray(mesh.face_node_offsets, dtype=np.int64)
-    fn = np.ascontiguousarray(mesh.face_nodes, dtype=np.int32)
-    c0 = np.ascontiguousarray(mesh.owner, dtype=np.int32)
     c1 = np.full(nf, -1, dtype=np.int32)
     c1[:ni] = mesh.neighbour
-    zone = np.ascontiguousarray(mesh.face_zone, dtype=np.int32)
-    n_zones = int(max(zone.max(initial=-1) + 1, 1))
-    n_ghost = mesh.n_cells - mesh.n_owned_cells
     gc = None
-    if n_ghost > 0:
-        gc = np.ascontiguousarray(mesh.cell_centroid[:, mesh.n_owned_cells:], dtype=np.float64)
+    if mesh.n_cells > mesh.n_owned_cells:
+        gc = mesh.cell_centroid[:, mesh.n_owned_cells:]
+    return reference_setup_arrays(mesh.points, mesh.face_node_offsets, mesh.face_nodes, mesh.owner,
+                                  c1, mesh.face_zone, mesh.n_cells,
+                                  mesh.n_cells - mesh.n_owned_cells, gc)  # fmt: skip
+
+
+def reference_setup_arrays(points, face_node_offsets, face_nodes, cell0, cell1, face_zone,
+                           n_cells: int, n_ghost: int, ghost_centroid=None) -> dict[str, np.ndarray]:
+    """The reference's set-up of a mesh given face by face: points 3 x n_points, each face's node
+    loop, the cells on its two sides (cell1 -1 on a boundary face), the boundary zone of each
+    boundary face, the last n_ghost cells periodic images (ghost_centroid 3 x n_ghost, their
+    centroids, or None)."""
+    l = lib()
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    fno = np.ascontiguousarray(face_node_offsets, dtype=np.int64)
+    fn = np.ascontiguousarray(face_nodes, dtype=np.int32)
+    c0 = np.ascontiguousarray(cell0, dtype=np.int32)
+    c1 = np.ascontiguousarray(cell1, dtype=np.int32)
+    nf = c0.size
+    zone = np.ascontiguousarray(face_zone, dtype=np.int32)
+    n_zones = int(max(zone.max(initial=-1) + 1, 1))
+    gc = None if ghost_centroid is None else np.ascontiguousarray(ghost_centroid, dtype=np.float64)
     h = C.c_void_p()
     err = C.create_string_buffer(1024)
     rc = l.ref_setup(pts.shape[1], pts.ctypes.data, nf, fno.ctypes.data, fn.ctypes.data,
-                     c0.ctypes.data, c1.ctypes.data, zone.ctypes.data, n_zones, mesh.n_cells,
-                     n_ghost, None if gc is None else gc.ctypes.data, C.byref(h), err,
+                     c0.ctypes.data, c1.ctypes.data, zone.ctypes.data, n_zones, int(n_cells),
+                     int(n_ghost), None if gc is None else gc.ctypes.data, C.byref(h), err,
                      len(err))  # fmt: skip
     if rc != 0:
         raise RuntimeError(err.value.decode())
@@ -81,7 +94,7 @@ def reference_setup(mesh) -> dict[str, np.ndarray]:
             out[name] = a
     finally:
         l.ref_free(h)
-    nc = mesh.n_cells
+    nc = int(n_cells)
     for k, rows, cols in (("face_area", 3, nf), ("face_centroid", 3, nf), ("face_normal", 3, nf),
                           ("face_moment", 9, nf), ("cell_centroid", 3, nc)):  # fmt: skip
         out[k] = out[k].reshape(rows, cols)

@@ -71,7 +71,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(free_port()), "bench.py",
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3",
-           "--cpu-slab", "12,12,6", "--cpu-threads", "2"]  # fmt: skip
+           "--workload", "hex", "--cpu-threads", "2"]  # fmt: skip
     r = subprocess.run(cmd, cwd=REPO, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
