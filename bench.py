@@ -278,7 +278,7 @@ def vortex_state(centroid, beta: float, centre, gamma: float = 1.4) -> np.ndarra
 
 def cpu_sample(workload: str):
     """The CPU sample of `workload` as the oracle takes it, built without this repository's
-    native library: the compact mesh of tests/golden/cpu_sample_<name>.npz assembled, its FP64
+    native library: the compact mesh of tests/golden/samples/cpu_sample_<name>.npz assembled, its FP64
     geometry and face2 stencil computed by the reference's own code (oracle/_ref: core/src/mesh.cpp
     assemble, core/src/geometry.cpp compute_geometry, codegen/cpp/geometry.cpp pack_geometry and
     cell_stencil), ghost images given their owner's geometry shifted by their translation, the
@@ -288,7 +288,7 @@ def cpu_sample(workload: str):
     import oracle as O
     import ref_setup as R
 
-    z = np.load(REPO / "tests" / "golden" / f"cpu_sample_{SAMPLES[workload]}.npz")
+    z = np.load(REPO / "tests" / "golden" / "samples" / f"cpu_sample_{SAMPLES[workload]}.npz")
     nc, ng = int(z["n_cells"]), int(z["n_ghost"])
     owned = nc - ng
     r = R.reference_setup_arrays(z["points"], z["face_node_offsets"], z["face_nodes"], z["cell0"],

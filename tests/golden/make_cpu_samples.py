@@ -1,6 +1,6 @@
 """The meshes and cases of the CPU baseline samples, written once as compact face-based inputs
-(tests/golden/cpu_sample_<name>.npz) so that the reference arm of bench.py and its CPU baseline
-build their problem without this repository's native library: at run time the reference's own
+(tests/golden/samples/cpu_sample_<name>.npz) so that the reference arm of bench.py and its CPU
+baseline build their problem without this repository's native library: at run time the reference's own
 mesh assembly, geometry and face2 stencil (oracle/_ref) and the oracle's least-squares weights
 set the sample up from these arrays, and the oracle steps it.
 
@@ -38,7 +38,7 @@ def write(name: str, case, start: dict) -> None:
     cell1[: m.n_interior_faces] = m.neighbour
     n_ghost = m.n_cells - m.n_owned_cells
     np.savez_compressed(
-        HERE / f"cpu_sample_{name}.npz",
+        HERE / "samples" / f"cpu_sample_{name}.npz",
         points=m.points, face_node_offsets=m.face_node_offsets, face_nodes=m.face_nodes,
         cell0=m.owner, cell1=cell1, face_zone=m.face_zone, n_cells=m.n_cells, n_ghost=n_ghost,
         ghost_owner=m.ghost_owner if n_ghost else np.zeros(0, np.int32),
