@@ -201,7 +201,7 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_set_case_mach_ref", C.c_int, vp, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_case_history", C.c_int, vp, i64, P(f64), C.c_char_p, sz)
         fn("autan_euler_device_march_cases", C.c_int, vp, f64, f64, i32, i32, i64, i32, f64, P(f64),
-           P(f64), P(i64), P(i32), P(f64), P(i64), P(f64), C.c_char_p, sz)  # fmt: skip
+           P(f64), P(i64), P(i32), P(f64), P(i64), P(f64), P(f64), C.c_char_p, sz)  # fmt: skip
     if hasattr(lib, "autan_setup_device_create"):
         fn("autan_setup_device_create", C.c_int, P(SetupMesh), i32, P(vp), P(i64), C.c_char_p, sz)
         fn("autan_setup_device_weights", C.c_int, vp, P(u8), P(i64), C.c_char_p, sz)

@@ -372,6 +372,25 @@ __device__ __forceinline__ T venkat(T d, T dmax, T dmin, T eps2) {
   return (dp * dp + eps2 + T(2.0) * d * dp) / (dp * dp + T(2.0) * d * d + d * dp + eps2);
 }
 
+// min(phi, venkat(d, dmax, dmin, eps2)) with the hardware min, phi <= 1, the quotient formed only
+// where it can be below phi. venkat's numerator N and denominator D are >= 0 (or NaN); where
+// t = fl(phi D) >= 2^-100 and N >= fl(t (1 + 2^-21)), N > phi D exactly (the two roundings lose less
+// than the factor gains), so N / D > phi, its correctly rounded value is >= phi and the min is phi.
+// Elsewhere (NaN, infinities, tiny products, or N / D possibly below phi) the quotient is formed as
+// venkat forms it. Same bits as bound_min(phi, venkat(...)).
+__device__ __forceinline__ float venkat_min(float phi, float d, float dmax, float dmin, float eps2) {
+  const float dp = d > 0.0f ? dmax : dmin;
+  const float num = dp * dp + eps2 + 2.0f * d * dp;
+  const float den = dp * dp + 2.0f * d * d + d * dp + eps2;
+  const float t = phi * den;
+  if (t >= 0x1p-100f && num >= t * (1.0f + 0x1p-21f)) return phi;
+  return fminf(phi, num / den);
+}
+__device__ __forceinline__ double venkat_min(double phi, double d, double dmax, double dmin,
+                                             double eps2) {
+  return fmin(phi, venkat(d, dmax, dmin, eps2));
+}
+
 // reconstruct (:619-627): W_f = W + phi (grad W . r), the cell value where rho_f or p_f + p_ref
 // would not be positive.
 template <class T>
@@ -439,6 +458,22 @@ __device__ __forceinline__ void numerical_flux(const T* wl, const T* wr, const T
   } else {
     ausm(wl, wr, n, p.g, p.minf, p.pref, f);
   }
+}
+
+// The cell side's sound speed of wave_speed (:1098), the same for every face of the cell.
+template <class T>
+__device__ __forceinline__ T sound_speed(const T* w, T g, T pref) {
+  return sqrt_(g * (w[4] + pref) / w[0]);
+}
+
+// wave_speed (:1091-1100) with the cell side's sound speed cc = sound_speed(wc) given: the same
+// operations in the same order.
+template <class T>
+__device__ __forceinline__ T wave_speed_cc(const T* wc, T cc, const T* wn, const T* n, T area, T g,
+                                           T pref) {
+  const T lc = absv(dot3(wc + 1, n)) + cc;
+  const T ln = absv(dot3(wn + 1, n)) + sqrt_(g * (wn[4] + pref) / wn[0]);
+  return maxv(lc, ln) * area;
 }
 
 // wave_speed (:1091-1100).

@@ -141,6 +141,13 @@ struct Dev {
   // 1 when every LSQ weight is finite and below 2^40 in magnitude (checked at create): with
   // Control::special clear, the gradient sums may then be widened on the integer pipe.
   int wide_ok;
+  // Re-packed launches of batched cases (null: the launch covers every item): the warp tiles
+  // (32 consecutive cells, owned interior faces or owned boundary faces) that hold an item of a
+  // case still stepping; a launch's warp w takes tile w.
+  const int* cell_tiles;
+  const int* face_tiles;
+  const int* bface_tiles;
+  int n_cell_tiles, n_face_tiles, n_bface_tiles;
   // Test hook of the failure detection (0 in normal use): with n > 0 every warp of the mode-5
   // gradient kernel also waits, n polls at most, on an mbarrier that nothing arrives on, so that
   // the bounded wait runs out and takes the timeout path (fault word, no stores).
@@ -163,6 +170,14 @@ __device__ __forceinline__ bool block_idle(const Dev<P>& d) {
   const long long c1 = min(c0 + static_cast<long long>(blockDim.x), static_cast<long long>(d.n)) - 1;
   const int k0 = d.case_of[c0];
   return k0 == d.case_of[c1] && d.active[k0] == 0;
+}
+
+// The item (cell or face) of this thread: blockIdx.x * blockDim.x + threadIdx.x, or, with a tile
+// list, item lane of the list's tile for this thread's warp; -1 past the list's end.
+__device__ __forceinline__ int tile_item(const int* tiles, int n_tiles) {
+  if (tiles == nullptr) return blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  return w < n_tiles ? (__ldg(tiles + w) << 5) + static_cast<int>(threadIdx.x & 31) : -1;
 }
 
 __device__ __forceinline__ int index_of(float x) { return __float_as_int(x); }
@@ -397,8 +412,8 @@ __global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typ
 template <class P>
 __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   using C = typename P::C;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= d.nb) return;
+  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
+  if (b < 0 || b >= d.nb) return;
   C r[kBface], w[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
   load_prim<P>(d.prim, index_of(r[13]), w);
@@ -500,7 +515,25 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr, long long bytes) {
   }
 }
 
-// The block's stencil rows and incidence records (contiguous in the sliced layout) to L2.
+// The block's stencil rows and incidence records (contiguous in the sliced layout) to L2; with a
+// tile list, each warp's own slice (call from one lane of each warp, c its cell or -1).
+template <class P, bool LIMIT, bool DT>
+__device__ __forceinline__ void prefetch_tile_rows(const Dev<P>& d, int c) {
+  using C = typename P::C;
+  if (c < 0) return;
+  const int s0 = c >> 5;
+  if (s0 >= d.n_slices) return;
+  const long long e0 = __ldg(d.st_start + s0), e1 = __ldg(d.st_start + s0 + 1);
+  const long long i0 = __ldg(d.inc_start + s0), i1 = __ldg(d.inc_start + s0 + 1);
+  prefetch_l2(d.st + 4 * e0, (e1 - e0) * 4 * static_cast<long long>(sizeof(C)));
+  if (LIMIT || DT) prefetch_l2(d.inc_rec + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+  if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+}
+
+// Prefetch of a gradient block's rows: the block's slices, or each warp's tile's.
+template <class P, bool LIMIT, bool DT>
+__device__ __forceinline__ void prefetch_rows(const Dev<P>& d, int c);
+
 template <class P, bool LIMIT, bool DT>
 __device__ __forceinline__ void prefetch_block_rows(const Dev<P>& d) {
   using C = typename P::C;
@@ -512,6 +545,15 @@ __device__ __forceinline__ void prefetch_block_rows(const Dev<P>& d) {
     prefetch_l2(d.st + 4 * e0, (e1 - e0) * 4 * static_cast<long long>(sizeof(C)));
     if (LIMIT || DT) prefetch_l2(d.inc_rec + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
     if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
+  }
+}
+
+template <class P, bool LIMIT, bool DT>
+__device__ __forceinline__ void prefetch_rows(const Dev<P>& d, int c) {
+  if (d.cell_tiles == nullptr) {
+    if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  } else if ((threadIdx.x & 31) == 0) {
+    prefetch_tile_rows<P, LIMIT, DT>(d, c);
   }
 }
 
@@ -600,11 +642,11 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 template <class P, bool LIMIT, bool DT, int CHUNK>
 __device__ __forceinline__ void gradients_cells(const Dev<P>& d, double cfl, int local) {
   using C = typename P::C;
-  if (block_idle(d)) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n && cell_active(d, c);
+  if (d.cell_tiles == nullptr && block_idle(d)) return;
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  const bool live = c >= 0 && c < d.n && cell_active(d, c);
   double dt = 0.0;
-  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  prefetch_rows<P, LIMIT, DT>(d, c);
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -783,10 +825,14 @@ __device__ __forceinline__ double gradient_tail_pipelined(const Dev<Fp32Acc64>& 
       dmax[i] = maxv(hi[i], wc[i]) - wc[i];
       dmin[i] = minv(lo[i], wc[i]) - wc[i];
       eps2[i] = d.p.scale[i] * vol;
-      phi[i] = C(INFINITY);
+      // min(1, min over the faces of venkat) as a min from 1: the same value, and a face whose
+      // venkat cannot go below the running min skips its quotient (venkat_min)
+      phi[i] = C(1.0);
     }
   }
   double lam = 0.0;
+  C cc = C(0);
+  if constexpr (DT) cc = sound_speed(wc, d.p.g, d.p.pref);
   if constexpr (LIMIT || DT) {
     const long long ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
     const int il = __ldg(d.inc_len + c);
@@ -804,10 +850,11 @@ __device__ __forceinline__ double gradient_tail_pipelined(const Dev<Fp32Acc64>& 
 #pragma unroll
         for (int i = 0; i < 5; ++i) {
           const C dd = g[3 * i] * r[0] + g[3 * i + 1] * r[1] + g[3 * i + 2] * r[2];
-          phi[i] = bound_min(phi[i], venkat(dd, dmax[i], dmin[i], eps2[i]));
+          phi[i] = venkat_min(phi[i], dd, dmax[i], dmin[i], eps2[i]);
         }
       }
-      if constexpr (DT) lam += static_cast<double>(wave_speed(wc, wn, nd, nd[3], d.p.g, d.p.pref));
+      if constexpr (DT)
+        lam += static_cast<double>(wave_speed_cc(wc, cc, wn, nd, nd[3], d.p.g, d.p.pref));
 #pragma unroll
       for (int k = 0; k < 4; ++k) r[k] = rn[k];
     }
@@ -839,12 +886,12 @@ template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK>
 __device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, double cfl, int local) {
   using P = Fp32Acc64;
   using C = float;
-  if (block_idle(d)) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n && cell_active(d, c);
+  if (d.cell_tiles == nullptr && block_idle(d)) return;
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  const bool live = c >= 0 && c < d.n && cell_active(d, c);
   const bool fast = WIDE > 0 && d.wide_ok != 0 && __ldg(&d.ctl->special) == 0ULL;
   double dt = 0.0;
-  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  prefetch_rows<P, LIMIT, DT>(d, c);
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -1144,13 +1191,13 @@ __global__ void __launch_bounds__(128, 7) k_gradients_wring(Dev<Fp32Acc64> d, do
   using C = float;
   static_assert(R >= CHUNK, "the ring holds at least one chunk");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  if (block_idle(d)) return;
+  if (d.cell_tiles == nullptr && block_idle(d)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4* ring = reinterpret_cast<float4*>(smem_raw) + warp * R * kSlice;
   unsigned long long* bar =
       reinterpret_cast<unsigned long long*>(smem_raw + kRingWarps * R * kSlice * 16) + warp * R;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n && cell_active(d, c);
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  const bool live = c >= 0 && c < d.n && cell_active(d, c);
   bool ok = true;
   double dt = 0.0;
   if (__any_sync(0xffffffffu, live)) {  // uniform over the warp
@@ -1282,7 +1329,7 @@ constexpr int ring_bytes(int depth, int word) {
 template <class P, bool LIMIT, bool DT, int D>
 __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
-  if (block_idle(d)) return;
+  if (d.cell_tiles == nullptr && block_idle(d)) return;
   constexpr int kW = 16 / static_cast<int>(sizeof(C));   // words per 16-byte piece
   constexpr int kG16 = 5 / kW;                            // whole pieces of a record's 5 words
   constexpr int kGRem = (5 % kW) * static_cast<int>(sizeof(C));  // bytes after them
@@ -1296,10 +1343,10 @@ __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl,
   unsigned char* const g16 = smem_raw;
   unsigned char* const grem = g16 + kGS * kG16 * nt * 16;
   unsigned char* const r16 = grem + kGS * nt * kGRem;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n && cell_active(d, c);
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  const bool live = c >= 0 && c < d.n && cell_active(d, c);
   double dt = 0.0;
-  if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
+  prefetch_rows<P, LIMIT, DT>(d, c);
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -1392,8 +1439,8 @@ template <class P>
 __global__ void __launch_bounds__(256) k_spectral(Dev<P> d, double cfl, int local,
                                                   double* dt_out) {
   using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < d.n && cell_active(d, c);
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  const bool live = c >= 0 && c < d.n && cell_active(d, c);
   double dt = 0.0;
   if (live) {
     C wc[5];
@@ -1536,10 +1583,10 @@ __device__ __forceinline__ void load_cell_in(const Dev<P>& d, int c, int mode, i
 template <class P>
 __device__ __forceinline__ void finish_cell(const Dev<P>& d, int c, const double* res,
                                             double vol, int mode, int stage, double wa, double wb,
-                                            int last, const CellIn& in) {
+                                            int last, const CellIn& in, bool store_res = true) {
   using C = typename P::C;
   const bool residual_only = mode == kResidual || mode == kFaceParts;
-  if (residual_only || stage == 0) {
+  if (residual_only || (stage == 0 && store_res)) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) d.res[static_cast<long long>(k) * d.n + c] = res[k];
   }
@@ -1599,8 +1646,8 @@ template <class P, int FLUX, bool PLANAR, bool SECOND>
 __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stage, double wa,
                                                     double wb, int local, int last) {
   using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n || !cell_active(d, c)) return;
+  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  if (c < 0 || c >= d.n || !cell_active(d, c)) return;
   C wc[5], gc[15], pc[5];
   cell_recon<P, SECOND>(d, c, wc, pc, gc);
   const double vol = __ldg(d.volume + c);
@@ -1654,8 +1701,8 @@ constexpr int kFlux = 8;  // flux record width (5 used): one 32-byte sector in f
 template <class P, int FLUX, bool PLANAR, bool SECOND>
 __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux) {
   using C = typename P::C;
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= d.n_if) return;
+  const int f = tile_item(d.face_tiles, d.n_face_tiles);
+  if (f < 0 || f >= d.n_if) return;
   if (d.face_warp_case != nullptr) {
     const int kc = __ldg(d.face_warp_case + (f >> 5));
     if (kc >= 0 && d.active[kc] == 0) return;
@@ -1674,8 +1721,8 @@ __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux
 template <class P, int FLUX, bool PLANAR, bool SECOND>
 __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flux, int nbo) {
   using C = typename P::C;
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbo) return;
+  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
+  if (b < 0 || b >= nbo) return;
   if (d.bface_warp_case != nullptr) {
     const int kc = __ldg(d.bface_warp_case + (b >> 5));
     if (kc >= 0 && d.active[kc] == 0) return;
@@ -1691,13 +1738,66 @@ __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flu
 
 // Store-gather, second half: each owned cell adds its faces' fluxes in increasing face index
 // from the source term (loads of four faces in flight at a time), then finish_cell.
-template <class P>
+// Replicated exact-sum words of the stage-0 norms (NORMS gathers): block b adds its words to
+// replica b % kNormReplicas, so that the blocks' atomics spread over this many copies of each
+// word; k_norm_collect sums the replicas.
+constexpr int kNormReplicas = 64;
+
+template <class P, bool NORMS>
+__device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typename P::C* flux,
+                                            const typename P::C* bflux, int mode, int stage,
+                                            double wa, double wb, int local, int last,
+                                            double* res_out);
+
+// Store-gather sum: each cell's face fluxes added in increasing face index from the source term,
+// then the RK stage (finish_cell). NORMS (face mode 2, a step's stage 0 without batched cases):
+// the squares of the stage-0 residual also go into the exact sums of the RMS norms here, per warp
+// in shared memory and per block into a replica of norm_words, instead of a separate pass over a
+// stored residual (which is then not stored).
+template <class P, bool NORMS>
 __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* flux,
                                                 const typename P::C* bflux, int mode, int stage,
-                                                double wa, double wb, int local, int last) {
+                                                double wa, double wb, int local, int last,
+                                                unsigned long long* norm_words) {
+  if constexpr (!NORMS) {
+    const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+    if (c >= 0 && c < d.n && cell_active(d, c))
+      gather_cell<P, false>(d, c, flux, bflux, mode, stage, wa, wb, local, last, nullptr);
+  } else {
+    // grid-stride over the cells (never re-packed: fused only without batched cases), so that
+    // each block clears and flushes its shared words once for many cells
+    extern __shared__ unsigned long long warp_words[];  // (blockDim.x / 32) x 5 x kWords
+    const int nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < nw * 5 * kWords; i += blockDim.x) warp_words[i] = 0ULL;
+    __syncthreads();
+    unsigned long long* mine = warp_words + (threadIdx.x >> 5) * 5 * kWords;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < d.n;
+         base += stride) {  // block-uniform trip count: every lane reaches the warp adds
+      const long long c = base + threadIdx.x;
+      double res[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      if (c < d.n && cell_active(d, static_cast<int>(c)))
+        gather_cell<P, true>(d, static_cast<int>(c), flux, bflux, mode, stage, wa, wb, local,
+                             last, res);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) warp_exact_add_nonneg<true>(mine + k * kWords, res[k] * res[k]);
+    }
+    __syncthreads();
+    unsigned long long* replica = norm_words + (blockIdx.x % kNormReplicas) * 5 * kWords;
+    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+      unsigned long long v = 0;
+      for (int w = 0; w < nw; ++w) v += warp_words[w * 5 * kWords + i];
+      if (v != 0) atomicAdd(&replica[i], v);
+    }
+  }
+}
+
+template <class P, bool NORMS>
+__device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typename P::C* flux,
+                                            const typename P::C* bflux, int mode, int stage,
+                                            double wa, double wb, int local, int last,
+                                            double* res_out) {
   using C = typename P::C;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= d.n || !cell_active(d, c)) return;
   const double vol = __ldg(d.volume + c);
   CellIn in;
   load_cell_in(d, c, mode, stage, local, in);
@@ -1738,13 +1838,29 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
       }
     }
   }
-  finish_cell(d, c, res, vol, mode, stage, wa, wb, last, in);
+  finish_cell(d, c, res, vol, mode, stage, wa, wb, last, in, !NORMS);
+  if constexpr (NORMS) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) res_out[k] = res[k];
+  }
+}
+
+// The replicas of the fused stage-0 norms summed into the control's words (one block).
+__global__ void k_norm_collect(const unsigned long long* replicas, Control* ctl) {
+  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+    unsigned long long v = 0;
+    for (int r = 0; r < kNormReplicas; ++r) v += replicas[r * 5 * kWords + i];
+    (&ctl->words[0][0])[i] = v;
+  }
 }
 
 // The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176): each
 // warp adds into words of its own in shared memory, the block then sums its warps' words and adds
 // the non-zero ones to the global words.
-__global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, Control* ctl) {
+// With batched cases (case_of, active not null) the cells of stopped cases are left out.
+__global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, Control* ctl,
+                                                      const int* case_of,
+                                                      const unsigned char* active) {
   constexpr int kWarps = kBlock / 32;
   __shared__ unsigned long long sh[kWarps][5 * kWords];
   for (int i = threadIdx.x; i < kWarps * 5 * kWords; i += blockDim.x) (&sh[0][0])[i] = 0;
@@ -1754,8 +1870,9 @@ __global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, 
   for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < n; base += stride) {
     const long long c = base + threadIdx.x;
     double r[5];
+    const bool in = c < n && (active == nullptr || active[case_of[c]] != 0);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) r[k] = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+    for (int k = 0; k < 5; ++k) r[k] = in ? res[k * static_cast<long long>(n) + c] : 0.0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) warp_exact_add_nonneg<true>(mine + k * kWords, r[k] * r[k]);
   }
@@ -1804,6 +1921,7 @@ constexpr int kCaseSpan = 8;
 
 __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, int n,
                                                            const int* case_of,
+                                                           const unsigned char* active,
                                                            unsigned long long* words) {
   constexpr int kWarps = kBlock / 32;
   __shared__ unsigned long long sh[kWarps][5 * kWords];
@@ -1830,6 +1948,7 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
     const long long c = c0 + threadIdx.x;
     const int first = case_of[c0], last = case_of[c1];
     if (first == last) {
+      if (active[first] == 0) continue;  // a stopped case: nothing to add
       if (first != cur) {
         if (cur >= 0) {
           __syncthreads();
@@ -1847,7 +1966,7 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
       }
     } else {
       const unsigned full = 0xffffffffu;
-      const int kase = c < n ? case_of[c] : -1;
+      const int kase = c < n && active[case_of[c]] != 0 ? case_of[c] : -1;
       unsigned todo = __ballot_sync(full, kase >= 0);
       while (todo != 0) {
         const int kc = __shfl_sync(full, kase, __ffs(todo) - 1);
@@ -1881,9 +2000,11 @@ __global__ void k_case_norm_finish(unsigned long long* words, const double* cell
 
 // The start of a step: clears the sums and the validity marks, sets the global step (fixed) or
 // prepares its minimum (CFL).
-__global__ void k_begin(Control* ctl, double dt_fixed) {
+__global__ void k_begin(Control* ctl, double dt_fixed, unsigned long long* norm_replicas) {
   const int t = threadIdx.x;
   for (int i = t; i < 5 * kWords; i += blockDim.x) (&ctl->words[0][0])[i] = 0;
+  if (norm_replicas != nullptr)
+    for (int i = t; i < kNormReplicas * 5 * kWords; i += blockDim.x) norm_replicas[i] = 0;
   if (t == 0) {
     ctl->dt_bits = dt_fixed > 0.0 ? static_cast<unsigned long long>(__double_as_longlong(dt_fixed))
                                   : 0x7ff0000000000000ULL;
@@ -2140,7 +2261,8 @@ struct Counters {
 struct Tuning {
   int grad_chunk = 4;    // stencil entries loaded together by the gradient kernel: 1, 2, 4 (8 staged)
   int grad_block = 128;  // its threads per block
-  int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather
+  int face_mode = 1;     // 0: gather-recompute (each cell computes its faces' fluxes); 1: store-gather;
+                         // 2: store-gather with a step's stage-0 norms summed in its gather
   int face_block = 128;  // threads per block of the face-flux (or gather-recompute) kernel
   int gather_block = 256;  // threads per block of the store-gather sum
   int grad_mode = 1;     // 0: stencil rows loaded by each thread; 1: staged by TMA bulk copies;
@@ -2198,7 +2320,7 @@ void Tuning::validate() const {
     fail("E1101: the gradient kernel with 2 entries in flight takes <= 128 threads");
   if (grad_mode == 1 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the staged kernel is 2, 4 or 8");
-  if (face_mode != 0 && face_mode != 1) fail("E1101: face_mode is 0 or 1");
+  if (face_mode < 0 || face_mode > 2) fail("E1101: face_mode is 0, 1 or 2");
   if (grad_mode == 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
   if (grad_mode < 0 || grad_mode > 5) fail("E1101: grad_mode is 0 to 5");
@@ -2454,6 +2576,8 @@ class Impl final : public Stepper {
     bface_r64_ = upload(r64, stream);
     face_mult_ = upload(mult, stream);
     cons_words_.alloc(20ULL * kWords * sizeof(unsigned long long));
+    norm_words_.alloc(static_cast<size_t>(kNormReplicas) * 5 * kWords * sizeof(unsigned long long));
+    check(cudaMemsetAsync(norm_words_.ptr(), 0, norm_words_.bytes(), stream), "memset");
     inc_dt_ = upload(idt, stream);
     face_ = upload(face, stream);
     f_m_ = upload(fm, stream);
@@ -2497,10 +2621,12 @@ class Impl final : public Stepper {
     d_.face_warp_case = nullptr;
     d_.bface_warp_case = nullptr;
     d_.case_minf = nullptr;
+    d_.cell_tiles = d_.face_tiles = d_.bface_tiles = nullptr;
+    d_.n_cell_tiles = d_.n_face_tiles = d_.n_bface_tiles = 0;
     d_.wide_ok = (sizeof(C) == 4 && weights_in_range) ? 1 : 0;
     d_.stall_polls = 0;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
-    if (tuning_.face_mode == 1) ensure_flux_scratch();
+    if (tuning_.face_mode != 0) ensure_flux_scratch();
     check(cudaStreamSynchronize(stream), "create");
   }
 
@@ -2612,9 +2738,10 @@ class Impl final : public Stepper {
   }
 
   void evaluate(autan_euler_step_result* out) override {
-    launch(k_begin, 1, 256, d_.ctl, 1.0);
+    launch(k_begin, 1, 256, d_.ctl, 1.0, static_cast<unsigned long long*>(nullptr));
     enqueue_residual(0);
-    launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+    launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
+           static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
     launch(k_norm_finish, 1, 32, d_.ctl, n_, 0);
     // invalid(): the state, then the residual, marked on the device
     launch(k_invalid<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
@@ -2727,7 +2854,7 @@ class Impl final : public Stepper {
   void set_tuning(const Tuning& t) override {
     t.validate();
     tuning_ = t;
-    if (t.face_mode == 1) ensure_flux_scratch();  // never inside a graph capture
+    if (t.face_mode != 0) ensure_flux_scratch();  // never inside a graph capture
     drop_graph();
   }
 
@@ -2735,7 +2862,8 @@ class Impl final : public Stepper {
 
   // The autotuner: each candidate launch configuration steps the device state `trial_steps` times
   // (after one untimed step) with event timing; the gradient choices are picked by the gradient
-  // kernel's time, then the face choices by the face kernels' time. The state is restored after
+  // kernel's time, then the face choices by the time of the face kernels and the norms (which
+  // face mode 2 sums inside its gather). The state is restored after
   // every trial, so tuning leaves the solution unchanged. Returns the tuned ms per step.
   double autotune(double cfl, double dt, bool local, int rk, int trial_steps) override {
     if (trial_steps < 1) fail("E1101: trial_steps must be positive");
@@ -2758,7 +2886,8 @@ class Impl final : public Stepper {
       restore();
       double total = 0.0;
       for (int k = 0; k < 6; ++k) total += ms[k];
-      return (kind < 0 ? total : ms[kind]) / trial_steps;
+      const double picked = kind == kFaces ? ms[kFaces] + ms[kNorms] : ms[kind];
+      return (kind < 0 ? total : picked) / trial_steps;
     };
     Tuning best = tuning_;
     if (second_) {
@@ -2818,10 +2947,11 @@ class Impl final : public Stepper {
     {
       double best_ms = 1e300;
       Tuning keep = best;
-      for (int mode : {0, 1})
+      for (int mode : {0, 1, 2})
         for (int block : {64, 128, 256})
           for (int gather : {128, 256}) {
             if (mode == 0 && gather != 256) continue;
+            if (mode == 2 && n_cases_ > 0) continue;  // the same launches as mode 1
             Tuning t = keep;
             t.face_mode = mode;
             t.face_block = block;
@@ -2905,6 +3035,20 @@ class Impl final : public Stepper {
   }
   int norm_blocks() const { return std::min(blocks(n_), 148 * 8); }
 
+  // The grid-stride fused-norm gather: as many blocks as stay resident on the device at once.
+  int norm_gather_grid(int gb, size_t smem) {
+    int& cached = norm_gather_grid_[gb / 32];
+    if (cached == 0) {
+      int per_sm = 0, sms = 0, dev = 0;
+      check(cudaGetDevice(&dev), "device");
+      check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device");
+      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gather<P, true>, gb, smem),
+            "occupancy");
+      cached = std::max(1, per_sm) * std::max(1, sms);
+    }
+    return std::min(cached, blocks(n_, gb));
+  }
+
   template <class K, class... A>
   void launch(K kernel, int grid, int block, A... args) {
     launch_as(kControl, kernel, grid, block, args...);
@@ -2937,6 +3081,14 @@ class Impl final : public Stepper {
 
   Dev<P> with_rec(int in, int out) const {
     Dev<P> d = d_;
+    if (repacked()) {
+      d.cell_tiles = cell_tiles_.as<int>();
+      d.face_tiles = face_tiles_.as<int>();
+      d.bface_tiles = bface_tiles_.as<int>();
+      d.n_cell_tiles = n_cell_tiles_;
+      d.n_face_tiles = n_face_tiles_;
+      d.n_bface_tiles = n_bface_tiles_;
+    }
     d.prim = prim_[in].as<C>();
     d.prim_b = prim_[in].as<C>() + static_cast<long long>(kPrimW) * n_;  // this stage's boundary states
     d.prim_next = prim_[out].as<C>();
@@ -2944,13 +3096,13 @@ class Impl final : public Stepper {
   }
 
   void launch_faces(const Dev<P>& d, int mode, int stage, double wa, double wb, int local,
-                    int last) {
+                    int last, bool norms = false) {
     if (tuning_.face_mode == 0) {
       dispatch_faces([&](auto flux, auto planar, auto second) {
         constexpr int F = decltype(flux)::value;
         constexpr bool PL = decltype(planar)::value, SE = decltype(second)::value;
         const int bs = tuning_.face_block;
-        launch_as(kFaces, k_faces_cell<P, F, PL, SE>, blocks(n_, bs), bs, d, mode, stage, wa, wb,
+        launch_as(kFaces, k_faces_cell<P, F, PL, SE>, cell_grid(bs), bs, d, mode, stage, wa, wb,
                   local, last);
       });
       return;
@@ -2959,8 +3111,17 @@ class Impl final : public Stepper {
     C* fl = flux_.as<C>();
     C* bfl = bflux_.as<C>();
     const int gb = tuning_.gather_block;
-    launch_as(kFaces, k_gather<P>, blocks(n_, gb), gb, d, static_cast<const C*>(fl),
-              static_cast<const C*>(bfl), mode, stage, wa, wb, local, last);
+    if (norms) {
+      const size_t sm = static_cast<size_t>(gb / 32) * 5 * kWords * sizeof(unsigned long long);
+      launch_smem(kFaces, k_gather<P, true>, norm_gather_grid(gb, sm), gb, sm, d,
+                  static_cast<const C*>(fl),
+                  static_cast<const C*>(bfl), mode, stage, wa, wb, local, last,
+                  norm_words_.as<unsigned long long>());
+    } else {
+      launch_as(kFaces, k_gather<P, false>, cell_grid(gb), gb, d, static_cast<const C*>(fl),
+                static_cast<const C*>(bfl), mode, stage, wa, wb, local, last,
+                static_cast<unsigned long long*>(nullptr));
+    }
   }
 
   // Every owned face's flux, once, into the face scratch (the store-gather strategy's first half).
@@ -2972,8 +3133,8 @@ class Impl final : public Stepper {
       constexpr int F = decltype(flux)::value;
       constexpr bool PL = decltype(planar)::value, SE = decltype(second)::value;
       const int bs = tuning_.face_block;
-      launch_as(kFaces, k_face_flux<P, F, PL, SE>, blocks(nif_, bs), bs, d, fl);
-      if (nbo_ > 0) launch_as(kFaces, k_bface_flux<P, F, PL, SE>, blocks(nbo_, bs), bs, d, bfl, nbo_);
+      launch_as(kFaces, k_face_flux<P, F, PL, SE>, face_grid(bs), bs, d, fl);
+      if (nbo_ > 0) launch_as(kFaces, k_bface_flux<P, F, PL, SE>, bface_grid(bs, nbo_), bs, d, bfl, nbo_);
     });
   }
 
@@ -2995,8 +3156,9 @@ class Impl final : public Stepper {
     ensure_flux_scratch();
     const Dev<P> d = with_rec(1, 1);
     launch_flux(d);
-    launch(k_gather<P>, blocks(n_), kBlock, d, static_cast<const C*>(flux_.as<C>()),
-           static_cast<const C*>(bflux_.as<C>()), static_cast<int>(kFaceParts), 0, 0.0, 0.0, 0, 0);
+    launch(k_gather<P, false>, blocks(n_), kBlock, d, static_cast<const C*>(flux_.as<C>()),
+           static_cast<const C*>(bflux_.as<C>()), static_cast<int>(kFaceParts), 0, 0.0, 0.0, 0, 0,
+           static_cast<unsigned long long*>(nullptr));
   }
 
   void face_parts(const double* u, double* res_faces, double* face_flux) override {
@@ -3087,7 +3249,64 @@ class Impl final : public Stepper {
     d_.face_warp_case = face_warp_case_.as<int>();
     d_.bface_warp_case = bface_warp_case_.as<int>();
     d_.case_minf = nullptr;
+    case_offsets_.assign(off, off + n_cases + 1);
+    face_warp_case_h_.assign(static_cast<size_t>((nif_ + 31) / 32), 0);
+    bface_warp_case_h_.assign(static_cast<size_t>((nbo_ + 31) / 32), 0);
+    if (!face_warp_case_h_.empty())
+      check(cudaMemcpyAsync(face_warp_case_h_.data(), face_warp_case_.ptr(),
+                            face_warp_case_h_.size() * sizeof(int), cudaMemcpyDeviceToHost, stream),
+            "cases");
+    if (!bface_warp_case_h_.empty())
+      check(cudaMemcpyAsync(bface_warp_case_h_.data(), bface_warp_case_.ptr(),
+                            bface_warp_case_h_.size() * sizeof(int), cudaMemcpyDeviceToHost, stream),
+            "cases");
+    n_cell_tiles_ = n_face_tiles_ = n_bface_tiles_ = -1;
     check(cudaStreamSynchronize(stream), "cases");
+  }
+
+  // The warp tiles of the cases still stepping (re-packed launches), or none when every case
+  // steps: 32-cell slices overlapping an active case's cells, and the 32-face warps of interior and
+  // boundary faces whose owners include an active case.
+  void repack(const uint8_t* active) {
+    bool all = true;
+    for (int k = 0; k < n_cases_; ++k) all = all && active[k] != 0;
+    drop_graph();
+    if (all) {
+      n_cell_tiles_ = n_face_tiles_ = n_bface_tiles_ = -1;
+      return;
+    }
+    std::vector<int> cells, faces, bfaces;
+    std::vector<uint8_t> mark(static_cast<size_t>((n_ + 31) / 32), 0);
+    for (int k = 0; k < n_cases_; ++k)
+      if (active[k])
+        for (int64_t sl = case_offsets_[k] / 32; sl <= (case_offsets_[k + 1] - 1) / 32; ++sl) mark[sl] = 1;
+    for (size_t sl = 0; sl < mark.size(); ++sl)
+      if (mark[sl]) cells.push_back(static_cast<int>(sl));
+    auto warps = [&](const std::vector<int>& wc, std::vector<int>& out) {
+      for (size_t w = 0; w < wc.size(); ++w)
+        if (wc[w] < 0 || active[wc[w]]) out.push_back(static_cast<int>(w));
+    };
+    warps(face_warp_case_h_, faces);
+    warps(bface_warp_case_h_, bfaces);
+    auto put = [&](Buffer& b, const std::vector<int>& v, int& n) {
+      n = static_cast<int>(v.size());
+      b = upload(v, stream);
+    };
+    put(cell_tiles_, cells, n_cell_tiles_);
+    put(face_tiles_, faces, n_face_tiles_);
+    put(bface_tiles_, bfaces, n_bface_tiles_);
+  }
+
+  // Grids of the step's launches: over the tiles while cases are re-packed, else every item.
+  bool repacked() const { return step_tiles_ && n_cell_tiles_ >= 0; }
+  int cell_grid(int bs) const {
+    return repacked() ? blocks(32LL * std::max(n_cell_tiles_, 1), bs) : blocks(n_, bs);
+  }
+  int face_grid(int bs) const {
+    return repacked() ? blocks(32LL * std::max(n_face_tiles_, 1), bs) : blocks(nif_, bs);
+  }
+  int bface_grid(int bs, int count) const {
+    return repacked() ? blocks(32LL * std::max(n_bface_tiles_, 1), bs) : blocks(count, bs);
   }
 
   void set_case_mach_ref(const double* mach_ref) override {
@@ -3107,6 +3326,7 @@ class Impl final : public Stepper {
     if (n_cases_ == 0) fail("E1101: no cases set");
     check(cudaMemcpyAsync(active_.ptr(), active, static_cast<size_t>(n_cases_), cudaMemcpyHostToDevice,
                           stream), "active");
+    repack(active);
     check(cudaStreamSynchronize(stream), "active");
   }
 
@@ -3167,12 +3387,12 @@ class Impl final : public Stepper {
   // with `dt`, the spectral radius and the CFL step of the step too.
   void enqueue_cells(int in, bool dt, double cfl, bool local) {
     const Dev<P> d = with_rec(in, in);
-    launch_as(kBoundary, k_boundary_states<P>, blocks(nb_), kBlock, d);
-    const int g = blocks(n_);
+    launch_as(kBoundary, k_boundary_states<P>, bface_grid(kBlock, nb_), kBlock, d);
+    const int g = cell_grid(kBlock);
     const int loc = local ? 1 : 0;
     if (second_) {
       const int bs = tuning_.grad_block;
-      const int gs = blocks(n_, bs);
+      const int gs = cell_grid(bs);
       auto go = [&](auto lim, auto with_dt) {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
         if (tuning_.grad_mode == 4 || tuning_.grad_mode == 5) {
@@ -3183,9 +3403,18 @@ class Impl final : public Stepper {
           }
           // fp64 or no limiter: the mode-0 form with two entries in flight
           if constexpr (sizeof(C) == 4)
-            launch_as(kGradients, k_gradients_occ7<P, L, D>, blocks(n_, 128), 128, d, cfl, loc);
+            launch_as(kGradients, k_gradients_occ7<P, L, D>, cell_grid(128), 128, d, cfl, loc);
           else
-            launch_as(kGradients, k_gradients<P, L, D, 2>, blocks(n_, 128), 128, d, cfl, loc);
+            launch_as(kGradients, k_gradients<P, L, D, 2>, cell_grid(128), 128, d, cfl, loc);
+          return;
+        }
+        if (tuning_.grad_mode == 1 && repacked()) {
+          // the staged form copies a block's contiguous slices: over re-packed tiles, the
+          // two-entries form instead
+          if constexpr (sizeof(C) == 4)
+            launch_as(kGradients, k_gradients_occ7<P, L, D>, cell_grid(128), 128, d, cfl, loc);
+          else
+            launch_as(kGradients, k_gradients<P, L, D, 2>, cell_grid(128), 128, d, cfl, loc);
           return;
         }
         if (tuning_.grad_mode == 1) {
@@ -3246,7 +3475,7 @@ class Impl final : public Stepper {
   template <bool D>
   void launch_gradients_w(const Dev<P>& d, double cfl, int loc) {
     if constexpr (std::is_same_v<P, Fp32Acc64>) {
-      const int gs = blocks(n_, 128);
+      const int gs = cell_grid(128);
       auto shape = [&](auto wide, auto narrow) {
         constexpr int W = decltype(wide)::value;
         constexpr bool G = decltype(narrow)::value;
@@ -3266,7 +3495,7 @@ class Impl final : public Stepper {
   template <bool D>
   void launch_gradients_ring(const Dev<P>& d, double cfl, int loc) {
     if constexpr (std::is_same_v<P, Fp32Acc64>) {
-      const int gs = blocks(n_, 128);
+      const int gs = cell_grid(128);
       auto go = [&](auto depth, auto chunk, auto narrow) {
         constexpr int R = decltype(depth)::value, CH = decltype(chunk)::value;
         constexpr bool G = decltype(narrow)::value;
@@ -3300,9 +3529,18 @@ class Impl final : public Stepper {
   // One step. Records rotate through three buffers so that a step starts and ends in buffer 0:
   // RK3 0 -> 1 -> 2 -> 0; RK4 0 -> 1 -> 2 -> 1 -> 0.
   void enqueue_step(const StepKey& k) {
+    struct Tiles {  // the step's launches take the re-packed tiles, nothing else does
+      bool& on;
+      explicit Tiles(bool& f) : on(f) { on = true; }
+      ~Tiles() { on = false; }
+    } tiles(step_tiles_);
     const bool cfl_dt = !(k.dt > 0.0);
     const bool local = cfl_dt && k.local;
-    launch(k_begin, 1, 256, d_.ctl, cfl_dt ? 0.0 : k.dt);
+    // the stage-0 norms fused into the store-gather sum (not with batched cases, whose per-case
+    // norms read the stored residual)
+    const bool fused = tuning_.face_mode == 2 && n_cases_ == 0;
+    launch(k_begin, 1, 256, d_.ctl, cfl_dt ? 0.0 : k.dt,
+           fused ? norm_words_.as<unsigned long long>() : static_cast<unsigned long long*>(nullptr));
     const int stages = k.rk == 3 ? 3 : 4;
     static const int in3[3] = {0, 1, 2}, out3[3] = {1, 2, 0};
     static const int in4[4] = {0, 1, 2, 1}, out4[4] = {1, 2, 1, 0};
@@ -3316,15 +3554,26 @@ class Impl final : public Stepper {
       const double wa = k.rk == 3 ? w3[st][0] : c4[st];
       const double wb = k.rk == 3 ? w3[st][1] : 0.0;
       launch_faces(with_rec(in, out), k.rk == 3 ? kRk3 : kRk4, st, wa, wb, local ? 1 : 0,
-                   st == stages - 1 ? 1 : 0);
+                   st == stages - 1 ? 1 : 0, fused && st == 0);
       if (st == 0) {
-        launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
-                  static_cast<const double*>(res_.as<double>()), n_, d_.ctl);
+        if (fused) {
+          launch_as(kNorms, k_norm_collect, 1, 512,
+                    static_cast<const unsigned long long*>(norm_words_.as<unsigned long long>()),
+                    d_.ctl);
+        } else {
+          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
+                    static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
+                    n_cases_ > 0 ? static_cast<const int*>(case_of_.as<int>()) : nullptr,
+                    n_cases_ > 0 ? static_cast<const unsigned char*>(active_.as<unsigned char>())
+                                 : nullptr);
+        }
         launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
         if (n_cases_ > 0) {
           launch_as(kNorms, k_case_norm_sums, blocks(n_, kBlock * kCaseSpan), kBlock,
                     static_cast<const double*>(res_.as<double>()), n_,
-                    static_cast<const int*>(case_of_.as<int>()), case_words_.as<unsigned long long>());
+                    static_cast<const int*>(case_of_.as<int>()),
+                    static_cast<const unsigned char*>(active_.as<unsigned char>()),
+                    case_words_.as<unsigned long long>());
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
                     case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
                     n_cases_, static_cast<const Control*>(d_.ctl), case_hist_.as<double>());
@@ -3386,6 +3635,15 @@ class Impl final : public Stepper {
   Tuning tuning_;
   size_t staged_smem_[2][5] = {};  // [time step staged][slices per block]
   Buffer flux_, bflux_;  // face scratch of the store-gather strategy
+  Buffer norm_words_;    // kNormReplicas x 5 x kWords: the fused stage-0 norms' exact sums
+  int norm_gather_grid_[9] = {};  // by gather_block / 32
+  // Re-packed launches of batched cases (repack): tile lists, their lengths (-1: none), the
+  // cases' cell offsets and the host copies of the 32-face warps' cases.
+  Buffer cell_tiles_, face_tiles_, bface_tiles_;
+  int n_cell_tiles_ = -1, n_face_tiles_ = -1, n_bface_tiles_ = -1;
+  std::vector<int64_t> case_offsets_;
+  std::vector<int> face_warp_case_h_, bface_warp_case_h_;
+  bool step_tiles_ = false;  // set while enqueue_step records: its launches use the tiles
   Control* head_ = nullptr;  // pinned copy of the control's head
   struct Timed {
     int kind;
@@ -3493,7 +3751,7 @@ void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_
 void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long long max_steps,
                  int batch, double orders, const double* floors, const double* reference,
                  int64_t* iterations, int32_t* converged, double* first, int64_t* steps_taken,
-                 double* gpu_ms) {
+                 double* gpu_ms, double* stop_ms) {
   const int nk = h->n_cases();
   if (nk == 0) fail("E1101: no cases set");
   if (max_steps < 1 || batch < 1) fail("E1101: max_steps and batch must be positive");
@@ -3508,13 +3766,16 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
   for (int k = 0; k < nk; ++k) {
     iterations[k] = 0;
     converged[k] = 0;
+    if (stop_ms != nullptr) stop_ms[k] = -1.0;
   }
   h->set_active(active.data());
   std::vector<double> rms(5ULL * nk * batch);
   cudaEvent_t t0 = nullptr;
   cudaEvent_t t1 = nullptr;
+  cudaEvent_t tb = nullptr;
   check(cudaEventCreate(&t0), "event");
   check(cudaEventCreate(&t1), "event");
+  check(cudaEventCreate(&tb), "event");
   check(cudaEventRecord(t0, h->stream), "event");
   long long taken = 0;
   int left = nk;
@@ -3553,6 +3814,15 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
     int newly = 0;
     for (int v : done) newly += v;
     const bool changed = newly > 0;
+    if (changed && stop_ms != nullptr) {
+      // the device time so far (the batch's steps have completed: step() synchronised)
+      check(cudaEventRecord(tb, h->stream), "event");
+      check(cudaEventSynchronize(tb), "event");
+      float now = 0.0f;
+      check(cudaEventElapsedTime(&now, t0, tb), "event");
+      for (int k = 0; k < nk; ++k)
+        if (converged[k] && stop_ms[k] < 0.0) stop_ms[k] = now;
+    }
     left -= newly;
     taken += n;
     if (changed) h->set_active(active.data());
@@ -3564,6 +3834,10 @@ void march_cases(Stepper* h, double cfl, double dt, bool local, int rk, long lon
   check(cudaEventElapsedTime(&ms, t0, t1), "event");
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  cudaEventDestroy(tb);
+  if (stop_ms != nullptr)
+    for (int k = 0; k < nk; ++k)
+      if (stop_ms[k] < 0.0) stop_ms[k] = ms;
   for (int k = 0; k < nk; ++k)
     if (!converged[k]) iterations[k] = taken;
   if (first != nullptr)
@@ -3827,9 +4101,10 @@ int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t 
                                    int64_t max_steps, int32_t batch, double orders,
                                    const double* floors, const double* reference,
                                    int64_t* iterations, int32_t* converged, double* first,
-                                   int64_t* steps, double* gpu_ms, char* err, size_t err_len) {
+                                   int64_t* steps, double* gpu_ms, double* stop_ms, char* err,
+                                   size_t err_len) {
   AUTAN_CALL(march_cases(h, cfl, dt, local != 0, rk, max_steps, batch, orders, floors, reference,
-                         iterations, converged, first, steps, gpu_ms));
+                         iterations, converged, first, steps, gpu_ms, stop_ms));
 }
 
 int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len) {

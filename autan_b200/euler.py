@@ -295,6 +295,7 @@ class EulerDevice:
         first = np.zeros((self.n_cases, 5))
         steps = C.c_int64()
         ms = C.c_double()
+        stop = np.zeros(self.n_cases)
         fl = None if floors is None else np.ascontiguousarray(floors, dtype=np.float64)
         rf = None if reference is None else np.ascontiguousarray(reference, dtype=np.float64)
         self._call("autan_euler_device_march_cases", float(cfl), float(dt), int(local), int(rk),
@@ -302,9 +303,9 @@ class EulerDevice:
                    None if fl is None else N.ptr(fl, C.c_double),
                    None if rf is None else N.ptr(rf, C.c_double), N.ptr(it, C.c_int64),
                    N.ptr(conv, C.c_int32), N.ptr(first, C.c_double), C.byref(steps),
-                   C.byref(ms))  # fmt: skip
+                   C.byref(ms), N.ptr(stop, C.c_double))  # fmt: skip
         return dict(iterations=it, converged=conv.astype(bool), first=first,
-                    steps=int(steps.value), gpu_ms=float(ms.value))
+                    steps=int(steps.value), gpu_ms=float(ms.value), stop_ms=stop)
 
     def history(self, count: int) -> tuple[np.ndarray, np.ndarray]:
         rms = np.zeros((count, 5))

@@ -224,6 +224,9 @@ def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, re
     bump forces."""
     with batch.open(device) as dev:
         dev.upload(u0)
+        # launch choices from the autotuner on this batch (state restored; every choice has the
+        # same bits)
+        res_tuning, _ = dev.autotune(cfl=batch.cfl, rk=batch.rk, local=True, trial_steps=2)
         res = dev.march_cases(cfl=batch.cfl, local=True, rk=batch.rk, max_steps=max_steps,
                               batch=batch_steps, orders=orders, floors=floors(batch),
                               reference=reference)  # fmt: skip
@@ -231,6 +234,7 @@ def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, re
         _, force = dev.boundary_pressure()
     res["u"] = u
     res["force"] = bump_forces(batch, force)
+    res["tuning"] = res_tuning
     return res
 
 
@@ -270,8 +274,9 @@ def load_network(path, seed=11) -> MLP:
 
 def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30, batch_rows=8192,
                lr=1e-3, orders=8.0, max_steps=200000, flux="ausm", log=print, save=None,
-               load=None) -> dict:  # fmt: skip
-    """The learned warm start end to end: train_cases converged cases (seed 1) as training data,
+               load=None, train_seed=1) -> dict:  # fmt: skip
+    """The learned warm start end to end: train_cases converged cases (seed train_seed) as
+    training data (their batched march's per-case iterations and stop times are reported too),
     the MLP trained on them, then test_cases held-out cases (seed 2) marched from the network's
     prediction and from the freestream. The GPU-time comparison is made on the cases that converge
     from both starts, re-marched as a batch of their own from each start (a batch's GPU time
@@ -286,7 +291,7 @@ def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30
     out = dict(train_cases=train_cases, test_cases=test_cases, epochs=epochs)
     if load is None:
         t0 = time.perf_counter()
-        train = cases.bump_batch(train_cases, seed=1, cells=cells, flux=flux, walls=True)
+        train = cases.bump_batch(train_cases, seed=train_seed, cells=cells, flux=flux, walls=True)
         log(f"training set: {train_cases} cases, {train.n_cells} cells, set-up {time.perf_counter() - t0:.0f} s")
         sol = march(train, train.u0, orders=orders, max_steps=max_steps)
         log(f"training solutions: {int(sol['converged'].sum())} converged, {sol['steps']} steps, "
@@ -313,7 +318,13 @@ def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30
                    train_rows=int(keep.sum()),
                    loss_first=float(loss[0]), loss_last=float(loss[-1]),
                    training_solution_gpu_s=sol["gpu_ms"] / 1e3, training_steps=int(sol["steps"]),
-                   train_iterations_median=float(np.median(sol["iterations"])))  # fmt: skip
+                   train_iterations_median=float(np.median(sol["iterations"])),
+                   train_seed=train_seed, flux=flux, train_tuning=sol["tuning"],
+                   train_cases_table=[dict(cells=int(p["cells"]), mach=float(p["mach"]),
+                                           iterations=int(sol["iterations"][k]),
+                                           converged=bool(sol["converged"][k]),
+                                           stop_s=float(sol["stop_ms"][k]) / 1e3)
+                                      for k, p in enumerate(train.params)])  # fmt: skip
     else:
         net = load_network(load)
         z = np.load(load)

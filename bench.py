@@ -60,7 +60,7 @@ def measured_hbm_peak() -> tuple[float, str]:
 # ------------------------------------------------------------------ algorithmic bytes
 
 
-def kernel_bytes(case, rk: int, local: bool = False) -> dict[str, float]:
+def kernel_bytes(case, rk: int, local: bool = False, fused_norms: bool = False) -> dict[str, float]:
     """Algorithmic bytes of one step per kernel kind: every array a kernel touches, read or written
     once, at its stored size (the rule of the reference's physics/bench/euler_bench.cu:321-372,
     applied to this layout); re-reads of neighbours' values are not counted. `local`: the CFL
@@ -98,15 +98,15 @@ def kernel_bytes(case, rk: int, local: bool = False) -> dict[str, float]:
             b += 40 * n  # stage read
         if rk == 4:
             b += (40 * n if st > 0 else 0) + (40 * n if st < 3 else 0)  # accumulator
-        if st == 0:
-            b += 40 * n  # residual for the norms
+        if st == 0 and not fused_norms:
+            b += 40 * n  # residual for the norms (face mode 2 sums them in the gather instead)
         faces += b
     return {
         "boundary_states": boundary * stages,
         "gradients": grad * stages + (fused if second else 0.0),
         "spectral": spectral,
         "faces": faces,
-        "norms": 40.0 * n,
+        "norms": 0.0 if fused_norms else 40.0 * n,
         "control": 0.0,
     }
 
@@ -537,7 +537,8 @@ def run_warmstart(args) -> None:
     res = warmstart.experiment(train_cases=tr, test_cases=te, cells=(lo, hi), epochs=ep,
                                max_steps=args.max_steps, orders=args.converge or 8.0,
                                log=lambda m: print(m, file=sys.stderr, flush=True),
-                               save=args.save_network or None, load=args.load_network or None)  # fmt: skip
+                               save=args.save_network or None, load=args.load_network or None,
+                               flux=args.flux, train_seed=args.train_seed)  # fmt: skip
     print(json.dumps({"metric": "GPU time to convergence, freestream start / warm start",
                       "value": res.get("gpu_time_ratio"), "unit": "x", "higher_is_better": True,
                       **res}), flush=True)  # fmt: skip
@@ -558,6 +559,11 @@ def run_converge_batch(args, batch, dev, tuned) -> None:
         "cases": len(cells), "cells": int(cells.sum()), "converged": int(res["converged"].sum()),
         "steps": res["steps"], "iterations_min": int(it.min()), "iterations_median": float(np.median(it)),
         "iterations_max": int(it.max()),
+        "stop_s": {"min": float(res["stop_ms"].min()) / 1e3,
+                   "median": float(np.median(res["stop_ms"])) / 1e3,
+                   "max": float(res["stop_ms"].max()) / 1e3,
+                   "per_case": [round(float(v) / 1e3, 3) for v in res["stop_ms"]]},
+        "iterations_per_case": [int(v) for v in it],
         "cell_iterations": int((cells * it).sum()),
         "cell_iterations_per_s": float((cells * it).sum() / (res["gpu_ms"] / 1e3)),
         "config": dict(workload_config(args), tuning=tuned, start="freestream"),
@@ -671,7 +677,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
     # -- per-kernel times (CUDA events around every launch on the stepper's stream)
     kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=3)
-    alg = kernel_bytes(case, case.rk, case.local)
+    alg = kernel_bytes(case, case.rk, case.local, fused_norms=tuned["face_mode"] == 2 and batch is None)
     dominant = max((k for k in kt if kt[k][1] > 0), key=lambda k: kt[k][0])
     per_step_launches = kt[dominant][1] / 3
     avg_ms = kt[dominant][0] / kt[dominant][1]
@@ -776,7 +782,8 @@ def main() -> None:
     ap.add_argument("--lattice", default="240,240,6", help="tetrahedral lattice NX,NY,NZ")
     ap.add_argument("--channel", default="480,150,100", help="bump channel boxes NX,NY,NZ")
     ap.add_argument("--tuning", default="", help="launch choices instead of the autotuner: "
-                    "grad_chunk,grad_block,face_mode,face_block,gather_block")
+                    "grad_chunk,grad_block,face_mode,face_block,gather_block,grad_mode[,"
+                    "grad_widen,grad_narrow,grad_minb,grad_depth]")
     ap.add_argument("--converge", type=float, default=0.0,
                     help="instead of the throughput line: march the workload from its start to "
                          "this many decades of residual drop (round-off plateau rule in "
@@ -785,6 +792,10 @@ def main() -> None:
     ap.add_argument("--warmstart", default="",
                     help="run the learned warm start instead: TRAIN,TEST,LO,HI,EPOCHS (training "
                          "cases, held-out cases, cell range, epochs), e.g. 2048,64,2000,10000,30")
+    ap.add_argument("--flux", default="ausm", choices=["ausm", "roe", "hllc"],
+                    help="with --warmstart: the flux of the training and held-out cases")
+    ap.add_argument("--train-seed", type=int, default=1,
+                    help="with --warmstart: the seed of the training cases' draws")
     ap.add_argument("--save-network", default="",
                     help="with --warmstart: write the trained network to this .npz")
     ap.add_argument("--load-network", default="",

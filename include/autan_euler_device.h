@@ -166,7 +166,9 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * then keep their values): [0] stencil entries the gradient kernel loads
  * together (1, 2 or 4, where 2 takes at most 128 threads per block; 2, 4 or 8 when staged), [1]
  * its threads per block, [2] face strategy (0 gather-recompute: each cell recomputes its faces'
- * fluxes; 1 store-gather: each face's flux once into a face scratch, then summed per cell), [3]
+ * fluxes; 1 store-gather: each face's flux once into a face scratch, then summed per cell; 2 as 1,
+ * with a step's stage-0 residual norms summed inside the gather instead of a pass over a stored
+ * residual, without batched cases), [3]
  * threads per block of the face kernel, [4] of the store-gather sum, [5] gradient staging (0:
  * each thread loads its stencil rows; 1: each block's rows staged into shared memory by TMA bulk
  * copies, at most 128 threads per block; 2: as 0, software-pipelined: the next entry's gather and
@@ -263,12 +265,16 @@ int autan_euler_device_case_history(void* handle, int64_t count, double* rms, ch
  * or NULL for each case's first iteration), each case stopping at the end of the batch in which it
  * converged, or until max_steps. iterations[k] (n_cases): the iteration at which case k converged,
  * or the steps taken; converged[k]: 1 if it did; first (5 per case, may be NULL): the reference
- * used; *steps: steps taken; *gpu_ms: device time. Every case steps again afterwards. */
+ * used; *steps: steps taken; *gpu_ms: device time; stop_ms (n_cases, may be NULL): the device
+ * time from the march's start to the end of the batch in which each case converged (the whole
+ * march's time for a case that did not). Once cases stop, the stage kernels are launched over the
+ * 32-item tiles of the cases still stepping only. Every case steps again afterwards. */
 int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t local, int32_t rk,
                                    int64_t max_steps, int32_t batch, double orders,
                                    const double* floors, const double* reference,
                                    int64_t* iterations, int32_t* converged, double* first,
-                                   int64_t* steps, double* gpu_ms, char* err, size_t err_len);
+                                   int64_t* steps, double* gpu_ms, double* stop_ms, char* err,
+                                   size_t err_len);
 /* Test hook of the failure detection (no counterpart in the reference): with polls > 0 every warp
  * of the mode-5 gradient kernel also waits, at most `polls` polls, on an mbarrier that nothing
  * arrives on; the bounded wait runs out, the warp marks the fault word, waits (up to 2^20 polls)
@@ -291,7 +297,9 @@ int autan_euler_device_counters(void* handle, int64_t* counters, char* err, size
  * Limits: components 1 to 8, n 1 to 2^30 (a sum's words cannot overflow), device index < 64;
  * anything beyond is refused with E1101 before any device work.
  * Scratch: 4544 bytes of module-level device memory per device, found with cudaGetSymbolAddress
- * on the first call for each device (make that first call before any stream capture); each call
+ * on the first call for each device (make that first call before any stream capture) and kept
+ * for the process: the device's primary context must live as long (no cudaDeviceReset between
+ * calls, which would reload the module elsewhere); each call
  * clears the words it uses on `stream` first. Calls that overlap in time on one device share the
  * scratch and race: order them on one stream or wait between them. For callers that cannot
  * allocate at the point of the call (a pool allocator holding all device memory, a path where

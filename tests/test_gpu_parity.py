@@ -193,13 +193,14 @@ def test_conservation_full_size():
 @pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
 def test_tuning_variants_are_bit_identical(precision):
     """Every launch choice of the autotuner's space (gradient chunking and blocks, gather-recompute
-    or store-gather faces) gives the same bits, and equals the oracle."""
+    or store-gather faces, the stage-0 norms in the gather or in their own pass) gives the same
+    bits, states and residual norms, and equals the oracle."""
     case = cases.vortex_tets(16, 16, 6, steps=3, precision=precision)
-    u_o, *_ = run_oracle(case, case.steps)
+    u_o, rms_o, *_ = run_oracle(case, case.steps)
     no = case.mesh.n_owned_cells
     for gmode, chunk in ((0, 1), (0, 2), (0, 4), (1, 2), (1, 4), (1, 8), (2, 1), (3, 2), (3, 4),
                          (3, 8)):
-        for mode in (0, 1):
+        for mode in (0, 1, 2):
             for block in (64, 128) if gmode or chunk == 2 else (64, 256):
                 with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
                     dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=mode,
@@ -207,8 +208,10 @@ def test_tuning_variants_are_bit_identical(precision):
                                    grad_mode=gmode)
                     dev.upload(case.u0)
                     dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
+                    rms, _ = dev.history(case.steps)
                     u = dev.download()
                 assert bits_equal(u[:, :no], u_o[:, :no]), (gmode, chunk, mode, block)
+                assert bits_equal(rms, rms_o), (gmode, chunk, mode, block)
     if precision == "fp64":
         return
     # mode 4: the products widened on the integer pipe (none, x and y, all), 5-word gathers;
@@ -217,13 +220,15 @@ def test_tuning_variants_are_bit_identical(precision):
                 for w in (0, 1, 2) for g in (0, 1)]
     variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
                  for r in (4, 8) for ch in (2, 3) for g in (0, 1)]
-    for v in variants:
+    for i, v in enumerate(variants):
         with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
-            dev.set_tuning(grad_block=128, face_mode=1, **v)
+            dev.set_tuning(grad_block=128, face_mode=1 + i % 2, **v)
             dev.upload(case.u0)
             dev.step(cfl=case.cfl, rk=3, n_steps=case.steps)
+            rms, _ = dev.history(case.steps)
             u = dev.download()
         assert bits_equal(u[:, :no], u_o[:, :no]), v
+        assert bits_equal(rms, rms_o), v
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32+acc64"])
@@ -233,13 +238,15 @@ def test_gradient_stagings_agree_on_the_channel(precision):
     the bits of the per-thread loads."""
     case = cases.bump_channel(24, 10, 4, steps=3, precision=precision)
     out = {}
+    norms = {}
     for gmode, chunk, block in ((0, 1, 128), (1, 4, 128), (2, 1, 64), (3, 2, 64), (3, 4, 128),
                                 (3, 8, 128)):  # fmt: skip
         with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
-            dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=1, face_block=128,
-                           gather_block=128, grad_mode=gmode)  # fmt: skip
+            dev.set_tuning(grad_chunk=chunk, grad_block=block, face_mode=1 + gmode % 2,
+                           face_block=128, gather_block=128, grad_mode=gmode)  # fmt: skip
             dev.upload(case.u0)
             dev.step(cfl=case.cfl, local=True, rk=3, n_steps=case.steps)
+            norms[(gmode, chunk, block)] = dev.history(case.steps)[0]
             out[(gmode, chunk, block)] = dev.download()
     if precision != "fp64":
         variants = [dict(grad_mode=4, grad_chunk=2, grad_widen=w, grad_narrow=g, grad_minb=7)
@@ -255,6 +262,8 @@ def test_gradient_stagings_agree_on_the_channel(precision):
     first = out[(0, 1, 128)]
     for k, u in out.items():
         assert bits_equal(u, first), k
+    for k, r in norms.items():
+        assert bits_equal(r, norms[(0, 1, 128)]), k
 
 
 def test_autotune_leaves_the_solution_unchanged():
