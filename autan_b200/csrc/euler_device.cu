@@ -530,9 +530,6 @@ __device__ __forceinline__ void prefetch_tile_rows(const Dev<P>& d, int c) {
   if (DT) prefetch_l2(d.inc_dt + 4 * i0, (i1 - i0) * 4 * static_cast<long long>(sizeof(C)));
 }
 
-// Prefetch of a gradient block's rows: the block's slices, or each warp's tile's.
-template <class P, bool LIMIT, bool DT>
-__device__ __forceinline__ void prefetch_rows(const Dev<P>& d, int c);
 
 template <class P, bool LIMIT, bool DT>
 __device__ __forceinline__ void prefetch_block_rows(const Dev<P>& d) {
@@ -548,12 +545,26 @@ __device__ __forceinline__ void prefetch_block_rows(const Dev<P>& d) {
   }
 }
 
-template <class P, bool LIMIT, bool DT>
+// Prefetch of a gradient block's rows: the block's slices, or (TILES) each warp's tile's.
+template <class P, bool LIMIT, bool DT, bool TILES = false>
 __device__ __forceinline__ void prefetch_rows(const Dev<P>& d, int c) {
-  if (d.cell_tiles == nullptr) {
+  if constexpr (!TILES) {
     if (threadIdx.x == 0) prefetch_block_rows<P, LIMIT, DT>(d);
-  } else if ((threadIdx.x & 31) == 0) {
-    prefetch_tile_rows<P, LIMIT, DT>(d, c);
+  } else {
+    if ((threadIdx.x & 31) == 0) prefetch_tile_rows<P, LIMIT, DT>(d, c);
+  }
+}
+
+// The owned cell of this thread in a gradient launch: the launch index, or (TILES, re-packed
+// batched launches) the warp's tile's cell. The gradient kernels other than k_gradients_tiles
+// never run over tiles; their cell index then stays a function of the launch index, which the
+// compiler recomputes instead of holding it in a register through the stencil loop.
+template <bool TILES, class P>
+__device__ __forceinline__ int gradient_cell(const Dev<P>& d) {
+  if constexpr (TILES) {
+    return tile_item(d.cell_tiles, d.n_cell_tiles);
+  } else {
+    return static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
   }
 }
 
@@ -639,14 +650,14 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
 // are read CHUNK at a time (their loads, then the neighbours' loads, all in flight together) and
 // added in stencil order. With DT, also the cell's CFL step and the block's minimum.
-template <class P, bool LIMIT, bool DT, int CHUNK>
+template <class P, bool LIMIT, bool DT, int CHUNK, bool TILES = false>
 __device__ __forceinline__ void gradients_cells(const Dev<P>& d, double cfl, int local) {
   using C = typename P::C;
-  if (d.cell_tiles == nullptr && block_idle(d)) return;
-  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
+  if (!TILES && block_idle(d)) return;
+  const int c = gradient_cell<TILES>(d);
   const bool live = c >= 0 && c < d.n && cell_active(d, c);
   double dt = 0.0;
-  prefetch_rows<P, LIMIT, DT>(d, c);
+  prefetch_rows<P, LIMIT, DT, TILES>(d, c);
   if (live) {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
@@ -736,6 +747,17 @@ __global__ void __launch_bounds__(256) k_gradients(Dev<P> d, double cfl, int loc
 template <class P, bool LIMIT, bool DT>
 __global__ void __launch_bounds__(128, 7) k_gradients_occ7(Dev<P> d, double cfl, int local) {
   gradients_cells<P, LIMIT, DT, 2>(d, cfl, local);
+}
+
+// The gradient launch of re-packed batched steps (whatever the tuning): each warp takes the cells
+// of its tile, two entries in flight, 128 threads per block (the fp32+acc64 form bounded for 7
+// blocks per SM as k_gradients_occ7).
+template <class P>
+constexpr int kTilesMinBlocks = sizeof(typename P::C) == 4 ? 7 : 1;
+template <class P, bool LIMIT, bool DT>
+__global__ void __launch_bounds__(128, kTilesMinBlocks<P>) k_gradients_tiles(Dev<P> d, double cfl,
+                                                                             int local) {
+  gradients_cells<P, LIMIT, DT, 2, true>(d, cfl, local);
 }
 
 // ---------------------------------------------------------------- integer-pipe widening
@@ -886,9 +908,9 @@ template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK>
 __device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, double cfl, int local) {
   using P = Fp32Acc64;
   using C = float;
-  if (d.cell_tiles == nullptr && block_idle(d)) return;
-  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
-  const bool live = c >= 0 && c < d.n && cell_active(d, c);
+  if (block_idle(d)) return;
+  const int c = gradient_cell<false>(d);
+  const bool live = c < d.n && cell_active(d, c);
   const bool fast = WIDE > 0 && d.wide_ok != 0 && __ldg(&d.ctl->special) == 0ULL;
   double dt = 0.0;
   prefetch_rows<P, LIMIT, DT>(d, c);
@@ -1191,13 +1213,13 @@ __global__ void __launch_bounds__(128, 7) k_gradients_wring(Dev<Fp32Acc64> d, do
   using C = float;
   static_assert(R >= CHUNK, "the ring holds at least one chunk");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  if (d.cell_tiles == nullptr && block_idle(d)) return;
+  if (block_idle(d)) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4* ring = reinterpret_cast<float4*>(smem_raw) + warp * R * kSlice;
   unsigned long long* bar =
       reinterpret_cast<unsigned long long*>(smem_raw + kRingWarps * R * kSlice * 16) + warp * R;
-  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
-  const bool live = c >= 0 && c < d.n && cell_active(d, c);
+  const int c = gradient_cell<false>(d);
+  const bool live = c < d.n && cell_active(d, c);
   bool ok = true;
   double dt = 0.0;
   if (__any_sync(0xffffffffu, live)) {  // uniform over the warp
@@ -1329,7 +1351,7 @@ constexpr int ring_bytes(int depth, int word) {
 template <class P, bool LIMIT, bool DT, int D>
 __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl, int local) {
   using C = typename P::C;
-  if (d.cell_tiles == nullptr && block_idle(d)) return;
+  if (block_idle(d)) return;
   constexpr int kW = 16 / static_cast<int>(sizeof(C));   // words per 16-byte piece
   constexpr int kG16 = 5 / kW;                            // whole pieces of a record's 5 words
   constexpr int kGRem = (5 % kW) * static_cast<int>(sizeof(C));  // bytes after them
@@ -1343,8 +1365,8 @@ __global__ void __launch_bounds__(128, 6) k_gradients_ring(Dev<P> d, double cfl,
   unsigned char* const g16 = smem_raw;
   unsigned char* const grem = g16 + kGS * kG16 * nt * 16;
   unsigned char* const r16 = grem + kGS * nt * kGRem;
-  const int c = tile_item(d.cell_tiles, d.n_cell_tiles);
-  const bool live = c >= 0 && c < d.n && cell_active(d, c);
+  const int c = gradient_cell<false>(d);
+  const bool live = c < d.n && cell_active(d, c);
   double dt = 0.0;
   prefetch_rows<P, LIMIT, DT>(d, c);
   if (live) {
@@ -3395,6 +3417,10 @@ class Impl final : public Stepper {
       const int gs = cell_grid(bs);
       auto go = [&](auto lim, auto with_dt) {
         constexpr bool L = decltype(lim)::value, D = decltype(with_dt)::value;
+        if (repacked()) {
+          launch_as(kGradients, k_gradients_tiles<P, L, D>, cell_grid(128), 128, d, cfl, loc);
+          return;
+        }
         if (tuning_.grad_mode == 4 || tuning_.grad_mode == 5) {
           if constexpr (std::is_same_v<P, Fp32Acc64> && L) {
             if (tuning_.grad_mode == 5) launch_gradients_ring<D>(d, cfl, loc);
@@ -3402,15 +3428,6 @@ class Impl final : public Stepper {
             return;
           }
           // fp64 or no limiter: the mode-0 form with two entries in flight
-          if constexpr (sizeof(C) == 4)
-            launch_as(kGradients, k_gradients_occ7<P, L, D>, cell_grid(128), 128, d, cfl, loc);
-          else
-            launch_as(kGradients, k_gradients<P, L, D, 2>, cell_grid(128), 128, d, cfl, loc);
-          return;
-        }
-        if (tuning_.grad_mode == 1 && repacked()) {
-          // the staged form copies a block's contiguous slices: over re-packed tiles, the
-          // two-entries form instead
           if constexpr (sizeof(C) == 4)
             launch_as(kGradients, k_gradients_occ7<P, L, D>, cell_grid(128), 128, d, cfl, loc);
           else
