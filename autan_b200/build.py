@@ -43,7 +43,7 @@ NVCC_FLAGS = [
 HOST_SOURCES = ["setup.cpp"]
 CUDA_SOURCES = ["euler_device.cu", "norms_static.cu", "mlp.cu", "setup_device.cu"]
 HEADERS = ["euler_bodies.cuh", "exact_sum.cuh", "device_mesh.hpp", "convergence.hpp",
-           "setup_rules.cuh"]
+           "setup_rules.cuh", "mlp_fused.cuh"]
 
 
 def _newer(src: Path, obj: Path, deps: list[Path]) -> bool:

@@ -8,6 +8,9 @@
 // C[M x N] = A[M x K] B[N x K]^T with warp-level mma.sync m16n8k16 (BF16 in, FP32 accumulate),
 // bias and GELU fused in its epilogue; the weight gradient C[N x K] = dZ^T A sums 128-row chunks
 // into per-chunk partials that a second kernel adds in chunk order, so training is deterministic.
+// Three engines: that warp-level mma.sync path, the same GEMMs a launch per layer on tcgen05, and
+// (width 128, the default) the fused tcgen05 kernel of mlp_fused.cuh that takes each 128-row tile
+// through the whole forward and backward pass in one launch.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -513,6 +516,8 @@ __global__ void __launch_bounds__(128) k_tc_gemm(const bf16* A, int lda, int M, 
                  : "memory");
 }
 
+#include "mlp_fused.cuh"
+
 // ---------------------------------------------------------------- wall distance
 
 struct V3 {
@@ -639,6 +644,13 @@ class Net {
     }
     params_.alloc(count_ * 4);
     grad_.alloc(count_ * 4);
+    {
+      int dev = 0;
+      check(cudaGetDevice(&dev), "device");
+      check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev), "device");
+    }
+    fused_ok_ = width == kMaxWidth && static_cast<int>(layers_.size()) <= fused::kLayersMax;
+    fused_ = fused_ok_;  // the fused tcgen05 engine is the default where it applies
     m_.alloc(count_ * 4);
     v_.alloc(count_ * 4);
     check(cudaMemsetAsync(m_.p, 0, count_ * 4, stream_), "memset");
@@ -646,12 +658,18 @@ class Net {
     for (const Layer& L : layers_) {
       wb_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
       wt_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
+      // the fused engine's operand images (zero padding stays zero: packing writes the weights)
+      wk_img_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
+      wt_img_.emplace_back(std::make_unique<Buf>(static_cast<size_t>(L.np) * L.kp * 2));
+      check(cudaMemsetAsync(wk_img_.back()->p, 0, wk_img_.back()->n, stream_), "memset");
+      check(cudaMemsetAsync(wt_img_.back()->p, 0, wt_img_.back()->n, stream_), "memset");
     }
     std::vector<float> ones(std::max(inputs, outputs), 1.0f), zeros(std::max(inputs, outputs), 0.0f);
     in_mean_.alloc(inputs * 4);
     in_sd_.alloc(inputs * 4);
     out_mean_.alloc(outputs * 4);
     out_sd_.alloc(outputs * 4);
+    build_layout();
     set_scaling(zeros.data(), ones.data(), zeros.data(), ones.data());
     set_parameters(p.data());
   }
@@ -703,6 +721,10 @@ class Net {
   float forward_backward(const float* x, const float* y, const int* idx, int rows,
                          float* se_host = nullptr) {
     if (rows > 65535LL * kChunk) fail("E1101: at most 65535 x 128 rows in one forward-backward pass");
+    if (fused_) {
+      fused_pass(x, y, idx, rows, false, 0.0f, 0.0f, 0.0f);
+      return take_loss(fse_, rows, se_host);
+    }
     ensure_work(rows);
     const int L = static_cast<int>(layers_.size());
     launch_inputs(x, idx, rows);
@@ -762,14 +784,58 @@ class Net {
           dzb_.as<bf16>());
       check(cudaGetLastError(), "gelu back");
     }
+    return take_loss(se_, rows, se_host);
+  }
+
+  // The loss of a pass from its per-row squared errors (se, device): with se_host (pinned) they
+  // are copied there asynchronously and 0 is returned.
+  float take_loss(const Buf& se_dev, int rows, float* se_host) {
     if (se_host != nullptr) {
-      check(cudaMemcpyAsync(se_host, se_.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
+      check(cudaMemcpyAsync(se_host, se_dev.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
       return 0.0f;
     }
     std::vector<float> se(rows);
-    check(cudaMemcpyAsync(se.data(), se_.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
+    check(cudaMemcpyAsync(se.data(), se_dev.p, rows * 4, cudaMemcpyDeviceToHost, stream_), "loss");
     sync();
     return loss_of(se.data(), rows);
+  }
+
+  // The fused engine's pass over `rows` rows (fused::k_fused): the gradient into grad_ and the
+  // per-row squared errors into fse_; with `update`, also the Adam step at rate lr (bias
+  // corrections c1, c2) and the re-packed operand images, in the same second launch.
+  void fused_pass(const float* x, const float* y, const int* idx, int rows, bool update, float lr,
+                  float c1, float c2) {
+    const int tiles = blocks(rows, 128);
+    const int grid = std::min(tiles, sms_);
+    const long long L = static_cast<long long>(layers_.size());
+    ensure(zbuf_, static_cast<size_t>(grid) * (L - 1) * 128 * 128 * 4);
+    ensure(atbuf_, static_cast<size_t>(grid) * lay_.at_bytes);
+    ensure(fpartial_, static_cast<size_t>(grid) * count_ * 4);
+    ensure(fse_, static_cast<size_t>(rows) * 4);
+    fused_attrs();
+    fused::k_fused<true><<<grid, fused::kThreads, fused::kSmem, stream_>>>(
+        lay_, x, y, idx, rows, tiles, zbuf_.as<float>(), atbuf_.as<unsigned char>(),
+        fpartial_.as<float>(), count_, fse_.as<float>(),
+        2.0f / (static_cast<float>(rows) * outputs_), nullptr, fault_.as<unsigned int>());
+    check(cudaGetLastError(), "fused pass");
+    if (update) {
+      fused::k_fused_update<true, true><<<blocks(count_, 256), 256, 0, stream_>>>(
+          lay_, fpartial_.as<float>(), grid, count_, grad_.as<float>(), params_.as<float>(),
+          m_.as<float>(), v_.as<float>(), lr, c1, c2);
+    } else {
+      fused::k_fused_update<false, false><<<blocks(count_, 256), 256, 0, stream_>>>(
+          lay_, fpartial_.as<float>(), grid, count_, grad_.as<float>(), params_.as<float>(),
+          nullptr, nullptr, 0.0f, 1.0f, 1.0f);
+    }
+    check(cudaGetLastError(), "fused update");
+  }
+  void fused_attrs() {
+    if (fused_attr_) return;
+    check(cudaFuncSetAttribute(fused::k_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               fused::kSmem), "smem");
+    check(cudaFuncSetAttribute(fused::k_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               fused::kSmem), "smem");
+    fused_attr_ = true;
   }
 
   float loss_of(const float* se, int rows) const {
@@ -802,6 +868,18 @@ class Net {
       copy(idx_, perm.data(), static_cast<size_t>(n_data_) * 4);
       long long steps = 0;
       for (long long r0 = 0; r0 + batch <= n_data_; r0 += batch) {
+        if (fused_) {
+          // one fused pass and one update launch a step
+          ++t_;
+          const float rate = lr * 0.5f * (1.0f + std::cos(3.14159265358979f * static_cast<float>(done) / total));
+          ++done;
+          const float c1 = 1.0f - std::pow(0.9f, static_cast<float>(t_));
+          const float c2 = 1.0f - std::pow(0.999f, static_cast<float>(t_));
+          fused_pass(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch, true, rate, c1, c2);
+          take_loss(fse_, batch, se_host_ + static_cast<size_t>(steps) * batch);
+          ++steps;
+          continue;
+        }
         forward_backward(x_.as<float>(), y_.as<float>(), idx_.as<int>() + r0, batch,
                          se_host_ + static_cast<size_t>(steps) * batch);
         ++t_;
@@ -838,6 +916,15 @@ class Net {
     const int L = static_cast<int>(layers_.size());
     for (long long r0 = 0; r0 < n; r0 += chunk) {
       const int rows = static_cast<int>(std::min(chunk, n - r0));
+      if (fused_) {
+        const int tiles = blocks(rows, 128);
+        fused_attrs();
+        fused::k_fused<false><<<std::min(tiles, sms_), fused::kThreads, fused::kSmem, stream_>>>(
+            lay_, xs + r0 * inputs_, nullptr, nullptr, rows, tiles, nullptr, nullptr, nullptr, 0,
+            nullptr, 0.0f, ys + r0 * outputs_, fault_.as<unsigned int>());
+        check(cudaGetLastError(), "fused predict");
+        continue;
+      }
       ensure_work(rows);
       launch_inputs(xs + r0 * inputs_, nullptr, rows);
       forward(rows, false);
@@ -934,6 +1021,38 @@ class Net {
           Ly.np);
       check(cudaGetLastError(), "round weights");
     }
+    if (fused_ok_) {  // the fused engine's operand images
+      fused::k_fused_update<false, true><<<blocks(count_, 256), 256, 0, stream_>>>(
+          lay_, nullptr, 0, count_, nullptr, params_.as<float>(), nullptr, nullptr, 0.0f, 1.0f, 1.0f);
+      check(cudaGetLastError(), "pack weights");
+    }
+  }
+  void build_layout() {
+    if (!fused_ok_) return;
+    fused::Layout& P = lay_;
+    P = fused::Layout{};
+    P.layers = static_cast<int>(layers_.size());
+    P.inputs = inputs_;
+    P.outputs = outputs_;
+    long long at = 0;
+    for (size_t l = 0; l < layers_.size(); ++l) {
+      const Layer& Ly = layers_[l];
+      P.in[l] = Ly.in;
+      P.out[l] = Ly.out;
+      P.kp[l] = Ly.kp;
+      P.np[l] = Ly.np;
+      P.w0[l] = Ly.w0;
+      P.at0[l] = at;
+      at += static_cast<long long>(Ly.kp) * 128 * 2;
+      P.wk[l] = P.wkw[l] = wk_img_[l]->as<bf16>();
+      P.wtk[l] = P.wtkw[l] = wt_img_[l]->as<bf16>();
+    }
+    P.at_bytes = at;
+    P.params = params_.as<float>();
+    P.in_mean = in_mean_.as<float>();
+    P.in_sd = in_sd_.as<float>();
+    P.out_mean = out_mean_.as<float>();
+    P.out_sd = out_sd_.as<float>();
   }
   const bf16* act(int l) { return l < 0 ? x0_.as<bf16>() : act_b(l); }
   bf16* act_b(int l) { return acts_.as<bf16>() + static_cast<long long>(l) * work_rows_ * width_; }
@@ -970,9 +1089,14 @@ class Net {
 
  public:
   void set_engine(int engine) {
-    if (engine != 0 && engine != 1) fail("E1101: engine 0 (mma.sync) or 1 (tcgen05)");
+    if (engine < 0 || engine > 2)
+      fail("E1101: engine 0 (mma.sync), 1 (tcgen05 per layer) or 2 (fused tcgen05)");
+    if (engine == 2 && !fused_ok_)
+      fail("E1101: the fused tcgen05 engine takes width 128 and at most 8 weight layers");
     tc_ = engine == 1;
+    fused_ = engine == 2;
   }
+  int engine() const { return fused_ ? 2 : (tc_ ? 1 : 0); }
 
  private:
 
@@ -984,7 +1108,14 @@ class Net {
   long long n_data_ = 0;
   int work_rows_ = 0;
   bool wgrad_attr_ = false;
-  bool tc_ = false;  // tcgen05 engine
+  bool tc_ = false;  // tcgen05 engine, layer per launch
+  bool fused_ = false;     // fused tcgen05 engine (fused::k_fused)
+  bool fused_ok_ = false;  // the network's shape suits it (width 128)
+  bool fused_attr_ = false;
+  int sms_ = 148;
+  fused::Layout lay_{};
+  Buf zbuf_, atbuf_, fpartial_, fse_;
+  std::vector<std::unique_ptr<Buf>> wk_img_, wt_img_;
   Buf params_, grad_, m_, v_, in_mean_, in_sd_, out_mean_, out_sd_, x_, y_, idx_, fault_;
   float* se_host_ = nullptr;  // pinned: an epoch's per-row squared errors
   size_t se_host_n_ = 0;

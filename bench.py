@@ -544,6 +544,48 @@ def run_warmstart(args) -> None:
                       **res}), flush=True)  # fmt: skip
 
 
+def run_mlp_step(args) -> None:
+    """The warm-start MLP's training step (7 -> 4 x 128 GELU -> 5, 8192-row minibatches of 65 536
+    seeded rows, Adam) and its inference (2^20 rows) per engine: 0 mma.sync a kernel per layer,
+    1 tcgen05 a kernel per layer, 2 fused tcgen05. Every train and predict call ends with a stream
+    synchronisation, so host time around a call is the device time of its launches plus launch
+    overhead; one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    from autan_b200.warmstart import MLP
+
+    r = np.random.default_rng(0)
+    x = r.normal(size=(65536, 7)).astype(np.float32)
+    y = r.normal(size=(65536, 5)).astype(np.float32)
+    xp = r.normal(size=(1 << 20, 7)).astype(np.float32)
+    flops_step = 0.0
+    dims = [(7, 128)] + [(128, 128)] * 3 + [(128, 5)]
+    for i, o in dims:  # forward, input gradient (not for the first layer), weight gradient
+        flops_step += 2.0 * 8192 * i * o * (3 if i != 7 else 2)
+    out = {}
+    for engine in (0, 1, 2):
+        net = MLP(seed=1)
+        net.set_engine(engine)
+        net.set_scaling(x.mean(0), x.std(0), y.mean(0), y.std(0))
+        net.set_data(x, y)
+        net.train(epochs=1, batch=8192, lr=1e-3, seed=2)  # warm-up
+        t0 = time.perf_counter()
+        net.train(epochs=args.steps, batch=8192, lr=1e-3, seed=3)
+        step_ms = (time.perf_counter() - t0) * 1e3 / (8 * args.steps)
+        net.predict(xp[:8192])
+        t0 = time.perf_counter()
+        net.predict(xp)
+        pred_ms = (time.perf_counter() - t0) * 1e3
+        out[str(engine)] = {"train_step_ms": step_ms, "train_tflops": flops_step / step_ms / 1e9,
+                            "predict_1M_rows_ms": pred_ms}  # fmt: skip
+        net.close()
+    print(json.dumps({"metric": "warm-start MLP training step (8192 rows) and inference (2^20 rows)",
+                      "unit": "ms", "engines": out,
+                      "note": "host time around synchronising calls; engine 2 is the default"}),
+          flush=True)  # fmt: skip
+
+
 def run_converge_batch(args, batch, dev, tuned) -> None:
     """The batched march to `--converge` decades, each case with its own plateau floors."""
     from autan_b200.euler import ROUND_OFF_FLOOR
@@ -789,6 +831,9 @@ def main() -> None:
                          "this many decades of residual drop (round-off plateau rule in "
                          "fp32+acc64) and print iterations and GPU time")
     ap.add_argument("--max-steps", type=int, default=100000, help="step cap of --converge")
+    ap.add_argument("--mlp-step", action="store_true",
+                    help="instead of the throughput line: time the warm-start MLP's training step "
+                         "and inference per engine (--steps epochs of 8 steps)")
     ap.add_argument("--warmstart", default="",
                     help="run the learned warm start instead: TRAIN,TEST,LO,HI,EPOCHS (training "
                          "cases, held-out cases, cell range, epochs), e.g. 2048,64,2000,10000,30")
@@ -807,6 +852,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if args.mlp_step:
+        run_mlp_step(args)
+        return
     if args.warmstart:
         run_warmstart(args)
         return

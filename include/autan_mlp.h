@@ -25,9 +25,13 @@ extern "C" {
 int autan_mlp_create(int32_t inputs, int32_t width, int32_t layers, int32_t outputs, uint64_t seed,
                      int32_t device, void** handle, char* err, size_t err_len);
 void autan_mlp_destroy(void* handle);
-/* The GEMM engine: 0 warp-level mma.sync m16n8k16 (the default), 1 tcgen05.mma with the
- * accumulator in tensor memory (128-row tiles, operands staged in shared memory). Both take BF16
- * operands and accumulate in FP32. */
+/* The GEMM engine: 0 warp-level mma.sync m16n8k16, a kernel per layer; 1 tcgen05.mma with the
+ * accumulator in tensor memory, a kernel per layer (128-row tiles, operands staged in shared
+ * memory); 2 (width 128 only; the default there, else 0) fused tcgen05: one kernel takes each
+ * 128-row tile through every layer's forward and, for training, backward GEMMs (weights staged by
+ * TMA bulk copies, accumulators in tensor memory), a second sums the tiles' gradients and applies
+ * the Adam step. All take BF16 operands and accumulate in FP32. E1101 for engine 2 at another
+ * width. */
 int autan_mlp_set_engine(void* handle, int32_t engine, char* err, size_t err_len);
 /* The standardisation: in_mean, in_std (inputs values each), out_mean, out_std (outputs each). */
 int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,

@@ -1,6 +1,8 @@
-"""The warm-start MLP's own BF16 tensor-core kernels against the numpy restatement
-(tests/oracle.py mlp_forward_backward): loss and parameter gradient of one forward and backward
-pass, predictions, a training run that fits a smooth field, and the exact wall distance."""
+"""The warm-start MLP's own BF16 tensor-core kernels (three engines: warp-level mma.sync, tcgen05 a
+layer per launch, and the fused tcgen05 kernel that is the default at width 128) against the numpy
+restatement (tests/oracle.py mlp_forward_backward): loss and parameter gradient of one forward and
+backward pass, predictions, a training run that fits a smooth field, and the exact wall
+distance."""
 
 import numpy as np
 import pytest
@@ -23,7 +25,7 @@ def scaling(x, y):
     return (x.mean(0), x.std(0), y.mean(0), y.std(0))
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["mma_sync", "tcgen05", "tcgen05_fused"])
 def test_gradient_against_the_restatement(engine):
     """BF16 operands, FP32 sums in another order: a BF16 rounding of an activation or a dZ may
     flip; the bounds (1e-4 on the loss, 2e-2 on the gradient's norm) leave room for that."""
@@ -41,7 +43,7 @@ def test_gradient_against_the_restatement(engine):
     assert np.allclose(g[-5:], g0[-5:], rtol=1e-3, atol=1e-6)
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["mma_sync", "tcgen05", "tcgen05_fused"])
 def test_training_fits_a_smooth_field(engine):
     x, y = data(65536, seed=1)
     net = MLP(seed=4)
@@ -55,7 +57,7 @@ def test_training_fits_a_smooth_field(engine):
     assert np.sqrt(np.mean((pred - yt) ** 2)) < 0.3 * np.sqrt(np.mean((yt - yt.mean(0)) ** 2))
 
 
-@pytest.mark.parametrize("engine", [0, 1], ids=["mma_sync", "tcgen05"])
+@pytest.mark.parametrize("engine", [0, 1, 2], ids=["mma_sync", "tcgen05", "tcgen05_fused"])
 def test_prediction_matches_the_restatement(engine):
     x, y = data(3000, seed=6)
     net = MLP(seed=7)
@@ -87,20 +89,42 @@ def test_wall_distance_bit_for_bit():
         assert np.array_equal(got[k], np.array(want))
 
 
-def test_engines_agree():
-    """tcgen05 (tensor memory accumulators) and mma.sync: the same BF16 operands and FP32 sums in
-    different orders; predictions and gradients within the BF16 flips that allows."""
-    x, y = data(5000, seed=9)
+@pytest.mark.parametrize("rows", [5000, 40000])
+def test_engines_agree(rows):
+    """tcgen05 per layer, fused tcgen05 (tensor memory accumulators) and mma.sync: the same BF16
+    operands and FP32 sums in different orders; predictions and gradients within the BF16 flips
+    that allows. 40 000 rows: more 128-row tiles than SMs, so fused CTAs take several tiles each."""
+    x, y = data(rows, seed=9)
     out = []
-    for engine in (0, 1):
+    for engine in (0, 1, 2):
         net = MLP(seed=10)
         net.set_engine(engine)
         net.set_scaling(*scaling(x, y))
         out.append((net.predict(x), net.gradient(x, y)))
-    (p0, (l0, g0)), (p1, (l1, g1)) = out
-    assert np.abs(p0 - p1).max() <= 1e-2 * np.abs(p0).max()
-    assert abs(l0 - l1) <= 1e-4 * l0
-    assert np.linalg.norm(g0 - g1) <= 2e-2 * np.linalg.norm(g0)
+    p0, (l0, g0) = out[0]
+    for p1, (l1, g1) in out[1:]:
+        assert np.abs(p0 - p1).max() <= 1e-2 * np.abs(p0).max()
+        assert abs(l0 - l1) <= 1e-4 * l0
+        assert np.linalg.norm(g0 - g1) <= 2e-2 * np.linalg.norm(g0)
+
+
+def test_fused_engine_is_the_default_and_deterministic():
+    """Width 128: the fused engine unless another is chosen; two passes give the same bits (the
+    CTAs' partials are summed in a fixed order); other widths refuse it."""
+    x, y = data(3000, seed=11)
+    runs = []
+    for _ in range(2):
+        net = MLP(seed=12)
+        net.set_scaling(*scaling(x, y))
+        runs.append(net.gradient(x, y))
+    fused = MLP(seed=12)
+    fused.set_engine(2)
+    fused.set_scaling(*scaling(x, y))
+    assert runs[0][0] == runs[1][0] and np.array_equal(runs[0][1], runs[1][1])
+    assert np.array_equal(fused.gradient(x, y)[1], runs[0][1])
+    narrow = MLP(width=64, seed=12)
+    with pytest.raises(Exception, match="E1101"):
+        narrow.set_engine(2)
 
 
 def test_experiment_small_round_trip(tmp_path):
