@@ -821,11 +821,11 @@ class Net {
     if (update) {
       fused::k_fused_update<true, true><<<blocks(count_, 256), 256, 0, stream_>>>(
           lay_, fpartial_.as<float>(), grid, count_, grad_.as<float>(), params_.as<float>(),
-          m_.as<float>(), v_.as<float>(), lr, c1, c2);
+          m_.as<float>(), v_.as<float>(), lr, c1, c2, fault_.as<unsigned int>());
     } else {
       fused::k_fused_update<false, false><<<blocks(count_, 256), 256, 0, stream_>>>(
           lay_, fpartial_.as<float>(), grid, count_, grad_.as<float>(), params_.as<float>(),
-          nullptr, nullptr, 0.0f, 1.0f, 1.0f);
+          nullptr, nullptr, 0.0f, 1.0f, 1.0f, fault_.as<unsigned int>());
     }
     check(cudaGetLastError(), "fused update");
   }
@@ -1023,7 +1023,8 @@ class Net {
     }
     if (fused_ok_) {  // the fused engine's operand images
       fused::k_fused_update<false, true><<<blocks(count_, 256), 256, 0, stream_>>>(
-          lay_, nullptr, 0, count_, nullptr, params_.as<float>(), nullptr, nullptr, 0.0f, 1.0f, 1.0f);
+          lay_, nullptr, 0, count_, nullptr, params_.as<float>(), nullptr, nullptr, 0.0f, 1.0f, 1.0f,
+          nullptr);
       check(cudaGetLastError(), "pack weights");
     }
   }
@@ -1079,7 +1080,11 @@ class Net {
     check(cudaStreamSynchronize(stream_), "sync");
     unsigned int f = 0;
     check(cudaMemcpy(&f, fault_.p, sizeof(f), cudaMemcpyDeviceToHost), "fault");
-    if (f != 0) fail("E1201: a tensor-core accumulator wait timed out; results are invalid");
+    if (f != 0) {
+      // reported once: the word is cleared so that the handle's next call starts clean
+      check(cudaMemset(fault_.p, 0, sizeof(unsigned int)), "fault");
+      fail("E1201: a tensor-core wait timed out; results are invalid");
+    }
   }
   static int tmem_cols(int n) {
     int c = 32;
@@ -1097,6 +1102,12 @@ class Net {
     fused_ = engine == 2;
   }
   int engine() const { return fused_ ? 2 : (tc_ ? 1 : 0); }
+  // Test hook (0 in normal use): the fused kernel's first wait polls a barrier nothing arrives on,
+  // at most `polls` times, and runs out (the call then fails with E1201).
+  void set_stall_test(int polls) {
+    if (polls < 0) fail("E1101: polls must be >= 0");
+    lay_.stall_polls = polls;
+  }
 
  private:
 
@@ -1166,6 +1177,10 @@ void autan_mlp_destroy(void* handle) { delete static_cast<Net*>(handle); }
 
 int autan_mlp_set_engine(void* handle, int32_t engine, char* err, size_t err_len) {
   return guarded(err, err_len, [&] { as_net(handle)->set_engine(engine); });
+}
+
+int autan_mlp_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] { as_net(handle)->set_stall_test(polls); });
 }
 
 int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,

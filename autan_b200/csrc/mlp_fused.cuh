@@ -53,6 +53,10 @@ struct Layout {
   bf16* wtkw[kLayersMax];
   const float* params;  // FP32 master parameters (the biases are read from here)
   const float *in_mean, *in_sd, *out_mean, *out_sd;
+  // Test hook of the failure detection (0 in normal use): with n > 0 every thread first waits, n
+  // polls at most, on an mbarrier that nothing arrives on, so that the bounded wait runs out and
+  // the kernel takes its fault path (fault word, no stores) before any copy or MMA is issued.
+  int stall_polls;
 };
 
 __device__ __forceinline__ void bar_init(unsigned long long* bar) {
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             float* zbuf, unsigned char* atbuf, float* partial, long long count, float* se,
             float scale, float* yout, unsigned int* fault) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ __align__(8) unsigned long long mma_bar, ld_bar[2];
+  __shared__ __align__(8) unsigned long long mma_bar, ld_bar[2], dead_bar;
   __shared__ uint32_t tmem_slot;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = warp & 3, h = warp >> 2;  // TMEM lane quarter, column half
@@ -212,6 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     bar_init(&mma_bar);
     bar_init(&ld_bar[0]);
     bar_init(&ld_bar[1]);
+    bar_init(&dead_bar);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_before();
@@ -229,6 +234,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t mma_par = 0, ld_par = 0, ld_busy = 0;
   bool mma_pending = false;
   bool ok = true;
+  if (P.stall_polls > 0) {  // the test hook: a wait that cannot complete, bounded
+    bool done = false;
+    for (int it = 0; it < P.stall_polls && !done; ++it) done = tc_try_wait(&dead_bar, 0);
+    ok = __syncthreads_and(done ? 1 : 0) != 0;
+  }
 
   // job j's staging (thread 0): W_l or W_l^T, and A_l^T for the backward jobs, into buffer j % 2
   auto issue = [&](int j) {
@@ -463,12 +473,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // grad[p] = the CTAs' partials summed in CTA order; with ADAM, the Adam step of parameter p
 // (as k_adam); with PACK, its BF16 copies into the layer's two operand images (weights only).
+// Nothing is written after a fault of the pass (fault word set; null: no pass).
 template <bool ADAM, bool PACK>
 __global__ void k_fused_update(Layout P, const float* partial, int ctas, long long count,
                                float* grad, float* params, float* m, float* v, float lr, float c1,
-                               float c2) {
+                               float c2, const unsigned int* fault) {
   const long long p = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (p >= count) return;
+  if (fault != nullptr && *reinterpret_cast<const volatile unsigned int*>(fault) != 0u) return;
   if (partial != nullptr) {
     float s = 0.0f;
     for (int c = 0; c < ctas; ++c) s += partial[static_cast<long long>(c) * count + p];

@@ -33,6 +33,7 @@ def _bind():
     fn("autan_mlp_create", C.c_int, i32, i32, i32, i32, u64, i32, P(vp), C.c_char_p, sz)
     fn("autan_mlp_destroy", None, vp)
     fn("autan_mlp_set_engine", C.c_int, vp, i32, C.c_char_p, sz)
+    fn("autan_mlp_set_stall_test", C.c_int, vp, i32, C.c_char_p, sz)
     fn("autan_mlp_set_scaling", C.c_int, vp, P(f32), P(f32), P(f32), P(f32), C.c_char_p, sz)
     fn("autan_mlp_parameter_count", i64, vp)
     fn("autan_mlp_get_parameters", C.c_int, vp, P(f32), i64, C.c_char_p, sz)
@@ -68,8 +69,13 @@ class MLP:
         N.check(getattr(self.lib, name)(self.h, *args, err, len(err)), err)
 
     def set_engine(self, engine: int) -> None:
-        """0: mma.sync kernels; 1: tcgen05 (tensor memory) kernels."""
+        """0: mma.sync kernels; 1: tcgen05 (tensor memory) kernels, a launch per layer; 2: the
+        fused tcgen05 kernel (the default at width 128)."""
         self._call("autan_mlp_set_engine", int(engine))
+
+    def set_stall_test(self, polls: int) -> None:
+        """Test hook: the fused kernel's first wait runs out after `polls` polls (0: off)."""
+        self._call("autan_mlp_set_stall_test", int(polls))
 
     def set_scaling(self, in_mean, in_std, out_mean, out_std):
         a = [_f32(v) for v in (in_mean, in_std, out_mean, out_std)]

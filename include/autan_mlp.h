@@ -33,6 +33,11 @@ void autan_mlp_destroy(void* handle);
  * the Adam step. All take BF16 operands and accumulate in FP32. E1101 for engine 2 at another
  * width. */
 int autan_mlp_set_engine(void* handle, int32_t engine, char* err, size_t err_len);
+/* Test hook of the failure detection (0, the default, in normal use): with polls > 0 every launch
+ * of the fused engine first waits, `polls` polls at most, on an mbarrier that nothing arrives on;
+ * the wait runs out, the kernel records a fault and leaves without stores, and the call fails with
+ * E1201. Setting 0 again restores normal work on the same handle. */
+int autan_mlp_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len);
 /* The standardisation: in_mean, in_std (inputs values each), out_mean, out_std (outputs each). */
 int autan_mlp_set_scaling(void* handle, const float* in_mean, const float* in_std,
                           const float* out_mean, const float* out_std, char* err, size_t err_len);

@@ -8,7 +8,10 @@
   handle then steps a valid state bit for bit as the oracle.
 - A bounded device wait that runs out: the test hook makes every warp of the TMA-ring gradient
   kernel wait a few polls on a barrier that nothing arrives on. The step call returns E1201, and
-  the same handle then steps bit for bit as the oracle."""
+  the same handle then steps bit for bit as the oracle.
+- The same for the warm-start MLP's fused tcgen05 kernel: gradient, predict and train return
+  E1201 and leave the parameters as they were; with the hook off the same handle gives the bits
+  of a fresh network."""
 
 import numpy as np
 import pytest
@@ -17,6 +20,7 @@ import oracle as O
 from autan_b200 import cases
 from autan_b200._native import NativeError
 from autan_b200.euler import EulerDevice
+from autan_b200.warmstart import MLP
 
 pytestmark = pytest.mark.gpu
 
@@ -96,3 +100,29 @@ def test_bounded_wait_runs_out_and_the_handle_recovers():
         _, _, bad = o.step(u_o, rk=3, cfl=case.cfl)
     assert r.invalid_cell is None and bad == -1
     assert same_bits(u_d[:, :no], u_o[:, :no])
+
+
+def test_mlp_bounded_wait_runs_out_and_the_handle_recovers():
+    rng = np.random.default_rng(13)
+    x = rng.normal(size=(2000, 7)).astype(np.float32)
+    y = rng.normal(size=(2000, 5)).astype(np.float32)
+    sc = (x.mean(0), x.std(0), y.mean(0), y.std(0))
+    ref = MLP(seed=14)
+    ref.set_scaling(*sc)
+    loss0, g0 = ref.gradient(x, y)
+    net = MLP(seed=14)
+    net.set_scaling(*sc)
+    net.set_data(x, y)
+    net.set_stall_test(16)
+    with pytest.raises(NativeError, match="E1201"):
+        net.gradient(x, y)
+    with pytest.raises(NativeError, match="E1201"):
+        net.predict(x)
+    with pytest.raises(NativeError, match="E1201"):
+        net.train(epochs=1, batch=1024, lr=1e-3, seed=1)
+    assert np.array_equal(net.parameters(), ref.parameters())  # no update was applied
+    net.set_stall_test(0)
+    loss1, g1 = net.gradient(x, y)
+    assert loss1 == loss0 and np.array_equal(g1, g0)
+    net.close()
+    ref.close()
