@@ -408,12 +408,10 @@ __global__ void __launch_bounds__(kBlock) k_store(Dev<P> d, const double* u, typ
   store_prim<P>(rec, c, w, d.ctl);
 }
 
-// boundary_states (kernels/euler.py:455-466): prim_b of every boundary face.
+// boundary_states (kernels/euler.py:455-466): prim_b of boundary face b.
 template <class P>
-__global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
+__device__ __forceinline__ void boundary_state(const Dev<P>& d, int b) {
   using C = typename P::C;
-  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
-  if (b < 0 || b >= d.nb) return;
   C r[kBface], w[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, r);
   load_prim<P>(d.prim, index_of(r[13]), w);
@@ -421,6 +419,14 @@ __global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
   out[5] = out[6] = out[7] = C(0);
   store_words<P, true>(d.prim_b + static_cast<long long>(b) * kPrimB, 0, 8, out);
   note_special(out, d.ctl);
+}
+
+// ... of every boundary face.
+template <class P>
+__global__ void __launch_bounds__(kBlock) k_boundary_states(Dev<P> d) {
+  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
+  if (b < 0 || b >= d.nb) return;
+  boundary_state(d, b);
 }
 
 // The minimum over a block of positive doubles' bits, then one atomicMin. Every thread of the
@@ -650,15 +656,25 @@ __device__ __forceinline__ double gradient_tail(const Dev<P>& d, int c, const ty
 // phi_k = min(1, min over the cell's faces of venkat(grad W . rel(x_f, x_c), ...)); the entries
 // are read CHUNK at a time (their loads, then the neighbours' loads, all in flight together) and
 // added in stencil order. With DT, also the cell's CFL step and the block's minimum.
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__device__ __forceinline__ double gradient_cell_body(const Dev<P>& d, int c, double cfl, int local);
+
 template <class P, bool LIMIT, bool DT, int CHUNK, bool TILES = false>
 __device__ __forceinline__ void gradients_cells(const Dev<P>& d, double cfl, int local) {
-  using C = typename P::C;
   if (!TILES && block_idle(d)) return;
   const int c = gradient_cell<TILES>(d);
   const bool live = c >= 0 && c < d.n && cell_active(d, c);
   double dt = 0.0;
   prefetch_rows<P, LIMIT, DT, TILES>(d, c);
-  if (live) {
+  if (live) dt = gradient_cell_body<P, LIMIT, DT, CHUNK>(d, c, cfl, local);
+  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
+}
+
+// One owned cell's gradient, bounds and limiter (and, with DT, its CFL step, returned).
+template <class P, bool LIMIT, bool DT, int CHUNK>
+__device__ __forceinline__ double gradient_cell_body(const Dev<P>& d, int c, double cfl, int local) {
+  using C = typename P::C;
+  {
     C wc[5];
     load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
     double acc[15];
@@ -731,9 +747,8 @@ __device__ __forceinline__ void gradients_cells(const Dev<P>& d, double cfl, int
           if (j0 + q < len) add_entry(e4[q], wn[q]);
       }
     }
-    dt = gradient_tail<P, LIMIT, DT>(d, c, wc, acc, lo, hi, cfl, local);
+    return gradient_tail<P, LIMIT, DT>(d, c, wc, acc, lo, hi, cfl, local);
   }
-  if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
 template <class P, bool LIMIT, bool DT, int CHUNK>
@@ -1718,17 +1733,11 @@ __global__ void __launch_bounds__(256) k_faces_cell(Dev<P> d, int mode, int stag
 
 constexpr int kFlux = 8;  // flux record width (5 used): one 32-byte sector in fp32+acc64
 
-// Store-gather, first half (the reference's store strategy, emit_gpu.py): the flux of every owned
-// interior face, once, in its orientation, into the face scratch.
+// The flux of owned interior face f, in its orientation, into the face scratch (none for a face
+// of a stopped case).
 template <class P, int FLUX, bool PLANAR, bool SECOND>
-__global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux) {
+__device__ __forceinline__ void face_flux_body(const Dev<P>& d, int f, typename P::C* flux) {
   using C = typename P::C;
-  const int f = tile_item(d.face_tiles, d.n_face_tiles);
-  if (f < 0 || f >= d.n_if) return;
-  if (d.face_warp_case != nullptr) {
-    const int kc = __ldg(d.face_warp_case + (f >> 5));
-    if (kc >= 0 && d.active[kc] == 0) return;
-  }
   C fr[kFace], wl[5], gl[15], pl[5], wr[5], gr[15], pr[5], out[8];
   load_words<P, kFaceA32<P>>(d.face + static_cast<long long>(f) * kFace, 0, kFace, fr);
   if (!cell_active(d, index_of(fr[7]))) return;
@@ -1739,16 +1748,10 @@ __global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux
   store_words<P, true>(flux + static_cast<long long>(f) * kFlux, 0, kFlux, out);
 }
 
-// ... and of every boundary face of an owned cell (the first n_owned_faces - n_interior_faces).
+// The flux of boundary face b of an owned cell into the boundary-face scratch.
 template <class P, int FLUX, bool PLANAR, bool SECOND>
-__global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flux, int nbo) {
+__device__ __forceinline__ void bface_flux_body(const Dev<P>& d, int b, typename P::C* flux) {
   using C = typename P::C;
-  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
-  if (b < 0 || b >= nbo) return;
-  if (d.bface_warp_case != nullptr) {
-    const int kc = __ldg(d.bface_warp_case + (b >> 5));
-    if (kc >= 0 && d.active[kc] == 0) return;
-  }
   C br[kBface], wc[5], gc[15], pc[5], out[8];
   load_words<P, true>(d.bface + static_cast<long long>(b) * kBface, 0, kBface, br);
   if (!cell_active(d, index_of(br[13]))) return;
@@ -1756,6 +1759,31 @@ __global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flu
   boundary_flux<P, FLUX, PLANAR>(d, b, br, wc, gc, pc, out);
   out[5] = out[6] = out[7] = C(0);
   store_words<P, true>(flux + static_cast<long long>(b) * kFlux, 0, kFlux, out);
+}
+
+// Store-gather, first half (the reference's store strategy, emit_gpu.py): the flux of every owned
+// interior face, once, in its orientation, into the face scratch.
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux) {
+  const int f = tile_item(d.face_tiles, d.n_face_tiles);
+  if (f < 0 || f >= d.n_if) return;
+  if (d.face_warp_case != nullptr) {
+    const int kc = __ldg(d.face_warp_case + (f >> 5));
+    if (kc >= 0 && d.active[kc] == 0) return;
+  }
+  face_flux_body<P, FLUX, PLANAR, SECOND>(d, f, flux);
+}
+
+// ... and of every boundary face of an owned cell (the first n_owned_faces - n_interior_faces).
+template <class P, int FLUX, bool PLANAR, bool SECOND>
+__global__ void __launch_bounds__(256) k_bface_flux(Dev<P> d, typename P::C* flux, int nbo) {
+  const int b = tile_item(d.bface_tiles, d.n_bface_tiles);
+  if (b < 0 || b >= nbo) return;
+  if (d.bface_warp_case != nullptr) {
+    const int kc = __ldg(d.bface_warp_case + (b >> 5));
+    if (kc >= 0 && d.active[kc] == 0) return;
+  }
+  bface_flux_body<P, FLUX, PLANAR, SECOND>(d, b, flux);
 }
 
 // Store-gather, second half: each owned cell adds its faces' fluxes in increasing face index
