@@ -200,10 +200,13 @@ def features(batch) -> np.ndarray:
     return np.concatenate(cols).astype(np.float32)
 
 
-def floors(batch) -> np.ndarray:
+def floors(batch, unit=None) -> np.ndarray:
+    """Each case's round-off floors (cases x 5): unit (default the fp32 round-off unit of the
+    plateau rule, ROUND_OFF_FLOOR) times its residual scales."""
     from autan_b200.euler import ROUND_OFF_FLOOR
 
-    return np.stack([ROUND_OFF_FLOOR * p["phi"] for p in batch.params])
+    u = ROUND_OFF_FLOOR if unit is None else unit
+    return np.stack([u * p["phi"] for p in batch.params])
 
 
 def bump_forces(batch, force) -> np.ndarray:
@@ -224,18 +227,19 @@ def bump_forces(batch, force) -> np.ndarray:
     return out
 
 
-def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, reference=None):
+def march(batch, u0, orders=8.0, max_steps=200000, batch_steps=100, device=0, reference=None,
+          floor_unit=None):
     """The batched march of `batch` from u0 (5 x n_cells), drops taken from `reference` (cases x 5)
-    or each case's first iteration: per-case iterations, GPU time, the converged states and the
-    bump forces."""
+    or each case's first iteration, the plateau rule on floors(batch, floor_unit): per-case
+    iterations, GPU time, the converged states and the bump forces."""
     with batch.open(device) as dev:
         dev.upload(u0)
         # launch choices from the autotuner on this batch (state restored; every choice has the
         # same bits)
         res_tuning, _ = dev.autotune(cfl=batch.cfl, rk=batch.rk, local=True, trial_steps=2)
         res = dev.march_cases(cfl=batch.cfl, local=True, rk=batch.rk, max_steps=max_steps,
-                              batch=batch_steps, orders=orders, floors=floors(batch),
-                              reference=reference)  # fmt: skip
+                              batch=batch_steps, orders=orders,
+                              floors=floors(batch, floor_unit), reference=reference)  # fmt: skip
         u = dev.download()
         _, force = dev.boundary_pressure()
     res["u"] = u
@@ -371,3 +375,33 @@ def experiment(train_cases=2048, test_cases=64, cells=(2_000, 10_000), epochs=30
                                                 and np.array_equal(warm_b["iterations"], wi)))  # fmt: skip
     out["cases"] = table
     return out
+
+
+def fp64_check(load, select, test_cases=32, cells=(20_000, 500_000), orders=11.0,
+               max_steps=400000, flux="roe", log=print) -> dict:
+    """The force difference between the warm and the freestream start where no FP32 round-off
+    plateau stops the march: test cases `select` (the seed-2 draws of `test_cases`, as
+    experiment's test set) in FP64, both starts (the saved network `load`) marched to `orders`
+    decades with FP64 round-off floors (2^-53 of the residual scales), their bump forces compared.
+    Per case: iterations, convergence and the relative force difference."""
+    from autan_b200 import cases
+
+    net = load_network(load)
+    sub = cases.bump_batch(test_cases, seed=2, cells=cells, flux=flux, walls=True,
+                           precision="fp64", select=[int(k) for k in select])  # fmt: skip
+    unit = 2.0**-53
+    cold = march(sub, freestream_states(sub), orders=orders, max_steps=max_steps, floor_unit=unit)
+    warm = march(sub, warm_start(net, sub), orders=orders, max_steps=max_steps,
+                 reference=cold["first"], floor_unit=unit)  # fmt: skip
+    rel = _force_difference(cold, warm)
+    log(f"fp64: {int((cold['converged'] & warm['converged']).sum())} of {len(select)} cases "
+        f"reach {orders:g} decades from both starts")  # fmt: skip
+    return dict(precision="fp64", orders=orders, cells=int(sub.n_cells),
+                cold_gpu_s=cold["gpu_ms"] / 1e3, warm_gpu_s=warm["gpu_ms"] / 1e3,
+                cases=[dict(case=int(p["case"]), mach=float(p["mach"]), cells=int(p["cells"]),
+                            cold_iterations=int(cold["iterations"][k]),
+                            warm_iterations=int(warm["iterations"][k]),
+                            cold_converged=bool(cold["converged"][k]),
+                            warm_converged=bool(warm["converged"][k]),
+                            force_rel_diff=float(rel[k]))
+                       for k, p in enumerate(sub.params)])  # fmt: skip

@@ -544,6 +544,23 @@ def run_warmstart(args) -> None:
                       **res}), flush=True)  # fmt: skip
 
 
+def run_warmstart_fp64(args) -> None:
+    """The warm start's force check in FP64 (autan_b200.warmstart.fp64_check): the selected test
+    cases marched from both starts to --converge decades (default 11) with the saved network
+    --load-network; one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    from autan_b200 import warmstart
+
+    tc, lo, hi = (int(v) for v in args.warmstart_fp64_set.split(","))
+    res = warmstart.fp64_check(args.load_network, [int(v) for v in args.warmstart_fp64.split(",")],
+                               test_cases=tc, cells=(lo, hi), orders=args.converge or 11.0,
+                               max_steps=args.max_steps, flux=args.flux,
+                               log=lambda m: print(m, file=sys.stderr, flush=True))  # fmt: skip
+    print(json.dumps({"metric": "bump force, warm vs freestream start, FP64 march", **res}), flush=True)
+
+
 def run_mlp_step(args) -> None:
     """The warm-start MLP's training step (7 -> 4 x 128 GELU -> 5, 8192-row minibatches of 65 536
     seeded rows, Adam) and its inference (2^20 rows) per engine: 0 mma.sync a kernel per layer,
@@ -831,6 +848,11 @@ def main() -> None:
                          "this many decades of residual drop (round-off plateau rule in "
                          "fp32+acc64) and print iterations and GPU time")
     ap.add_argument("--max-steps", type=int, default=100000, help="step cap of --converge")
+    ap.add_argument("--warmstart-fp64", default="",
+                    help="instead of the throughput line: test cases K1,K2,... of the warm-start "
+                         "test set marched in FP64 from both starts (--load-network)")
+    ap.add_argument("--warmstart-fp64-set", default="32,20000,500000",
+                    help="the warm-start test set the cases are drawn from: CASES,LO,HI")
     ap.add_argument("--mlp-step", action="store_true",
                     help="instead of the throughput line: time the warm-start MLP's training step "
                          "and inference per engine (--steps epochs of 8 steps)")
@@ -854,6 +876,9 @@ def main() -> None:
         ap.error("at least 3 warm-up steps")
     if args.mlp_step:
         run_mlp_step(args)
+        return
+    if args.warmstart_fp64:
+        run_warmstart_fp64(args)
         return
     if args.warmstart:
         run_warmstart(args)
