@@ -2320,7 +2320,7 @@ struct Tuning {
                          // 3: a per-thread ring of asynchronous copies, chunk entries deep;
                          // 4 (fp32+acc64): loaded by each thread with the products widened on the
                          // integer pipe (grad_widen), 5-word gathers (grad_narrow), registers
-                         // bounded for grad_minb blocks of 128 per SM;
+                         // bounded for grad_minb blocks of 128 per SM (chunk 2: 7 or 6; chunk 4: 5);
                          // 5 (fp32+acc64): each warp's stencil rows streamed by TMA bulk copies
                          // into a ring of grad_depth shared-memory slots, grad_chunk gathers in
                          // flight (5-word with grad_narrow)
@@ -2384,7 +2384,8 @@ void Tuning::validate() const {
     if (grad_block != 128) fail("E1101: the mode-4 gradient kernel takes 128 threads");
     if (grad_widen < 0 || grad_widen > 2) fail("E1101: grad_widen is 0, 1 or 2");
     if (grad_narrow != 0 && grad_narrow != 1) fail("E1101: grad_narrow is 0 or 1");
-    if (grad_chunk != 2 || grad_minb != 7) fail("E1101: mode 4 takes grad_chunk 2, grad_minb 7");
+    if (!((grad_chunk == 2 && (grad_minb == 7 || grad_minb == 6)) || (grad_chunk == 4 && grad_minb == 5)))
+      fail("E1101: mode 4 takes grad_chunk 2 with grad_minb 7 or 6, or grad_chunk 4 with grad_minb 5");
   }
   if (grad_mode == 3 && grad_block > 128) fail("E1101: the ring gradient kernel takes <= 128 threads");
   if (grad_mode == 1 && grad_block > 128) fail("E1101: the staged gradient kernel takes <= 128 threads");
@@ -2977,6 +2978,7 @@ class Impl final : public Stepper {
               }
             }
       if (sizeof(C) == 4 && limiter_)
+        for (int shape = 0; shape < 3; ++shape)  // (entries in flight, register bound)
         for (int widen : {0, 1, 2})
           for (int narrow : {0, 1})
             {
@@ -2985,8 +2987,8 @@ class Impl final : public Stepper {
               t.grad_block = 128;
               t.grad_widen = widen;
               t.grad_narrow = narrow;
-              t.grad_chunk = 2;
-              t.grad_minb = 7;
+              t.grad_chunk = shape == 2 ? 4 : 2;
+              t.grad_minb = shape == 0 ? 7 : (shape == 1 ? 6 : 5);
               const double ms = measure(t, kGradients);
               if (ms < best_ms) {
                 best_ms = ms;
@@ -3524,7 +3526,12 @@ class Impl final : public Stepper {
       auto shape = [&](auto wide, auto narrow) {
         constexpr int W = decltype(wide)::value;
         constexpr bool G = decltype(narrow)::value;
-        launch_as(kGradients, k_gradients_w<true, D, W, G, 2, 7>, gs, 128, d, cfl, loc);
+        if (tuning_.grad_chunk == 4)
+          launch_as(kGradients, k_gradients_w<true, D, W, G, 4, 5>, gs, 128, d, cfl, loc);
+        else if (tuning_.grad_minb == 6)
+          launch_as(kGradients, k_gradients_w<true, D, W, G, 2, 6>, gs, 128, d, cfl, loc);
+        else
+          launch_as(kGradients, k_gradients_w<true, D, W, G, 2, 7>, gs, 128, d, cfl, loc);
       };
       auto narrow = [&](auto wide) {
         if (tuning_.grad_narrow) shape(wide, std::true_type{});

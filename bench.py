@@ -57,6 +57,10 @@ def measured_hbm_peak() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+# The step result a step call reads back: the head of the device's control block (dt bits, the
+# invalid-cell marks, step count, dt, fault and special words, the five RMS values).
+CONTROL_HEAD = 96
+
 # ------------------------------------------------------------------ algorithmic bytes
 
 
@@ -733,6 +737,15 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
     t1 = time.perf_counter()
     e2e_s = max_over_ranks(t1 - t0)
     e2e = total * e2e_steps / e2e_s
+    # -- the reference's own device loop (EulerPhysics::device_step, euler_physics.cpp:1538-1570):
+    # one DeviceStepper::step call per step, the state kept on the device (the host copy is
+    # refreshed only by sync()), each call's result (RMS, dt, invalid cell) read back
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=1, graph=True)
+    t1 = time.perf_counter()
+    march_rate = total * e2e_steps / max_over_ranks(t1 - t0)
 
     # -- per-kernel times (CUDA events around every launch on the stepper's stream)
     kt = dev.kernel_times(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=3)
@@ -766,8 +779,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
             "dtype": "f32 (f64 accumulation)" if case.scheme.precision != "fp64" else "f64",
             "data": "synthetic",
             "config": dict(workload_config(args), tuning=tuned),
+            "e2e_device_loop": {"value": march_rate, "unit": "cell-iterations/s",
+                                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": CONTROL_HEAD,
+                                "note": "one step call per step through the C ABI, the state on "
+                                        "the device, the step result (RMS, dt, invalid cell) read "
+                                        "back, as the reference's device_step loop"},
             "e2e": {"value": e2e, "unit": "cell-iterations/s",
-                    "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 40 * n + 128},  # fmt: skip
+                    "h2d_bytes_per_step": 40 * n, "d2h_bytes_per_step": 40 * n + CONTROL_HEAD},  # fmt: skip
             "gpu_launches": int(launches),
             "roofline": {
                 "bound": "hbm",

@@ -177,8 +177,9 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * or 8, at most 128 threads per block; 4, fp32+acc64 only: as 0 with [0] entries loaded together,
  * 128 threads per block, and [6] 0, 1 or 2: none, the x and y, or all of each entry's 15 products
  * widened to FP64 on the integer pipe, exactly (2^-896-scaled bit moves) instead of by cvt; [7]
- * 1: neighbours gathered as 16 + 4 bytes instead of one 32-byte load; [8] 7, the blocks of 128
- * threads per SM the registers are bounded for, with [0] = 2; 5, fp32+acc64 only: each warp's
+ * 1: neighbours gathered as 16 + 4 bytes instead of one 32-byte load; [8] the blocks of 128
+ * threads per SM the registers are bounded for: 7 or 6 with [0] = 2, 5 with [0] = 4; 5,
+ * fp32+acc64 only: each warp's
  * stencil rows streamed by TMA bulk copies into a ring of [9] (4 or 8) shared-memory slots ahead of
  * the warp, [0] (2 or 3) gathers in flight, [7] as for 4, 128 threads per block).
  * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum

@@ -214,10 +214,11 @@ def test_tuning_variants_are_bit_identical(precision):
                 assert bits_equal(rms, rms_o), (gmode, chunk, mode, block)
     if precision == "fp64":
         return
-    # mode 4: the products widened on the integer pipe (none, x and y, all), 5-word gathers;
+    # mode 4: the products widened on the integer pipe (none, x and y, all), 5-word gathers,
+    # two entries in flight bounded for 7 or 6 blocks per SM or four for 5;
     # mode 5: the per-warp TMA row ring of 4 or 8 slots with 2 or 3 gathers in flight
-    variants = [dict(grad_mode=4, grad_chunk=2, grad_widen=w, grad_narrow=g, grad_minb=7)
-                for w in (0, 1, 2) for g in (0, 1)]
+    variants = [dict(grad_mode=4, grad_chunk=ch, grad_widen=w, grad_narrow=g, grad_minb=mb)
+                for ch, mb in ((2, 7), (2, 6), (4, 5)) for w in (0, 1, 2) for g in (0, 1)]
     variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
                  for r in (4, 8) for ch in (2, 3) for g in (0, 1)]
     for i, v in enumerate(variants):
@@ -249,8 +250,9 @@ def test_gradient_stagings_agree_on_the_channel(precision):
             norms[(gmode, chunk, block)] = dev.history(case.steps)[0]
             out[(gmode, chunk, block)] = dev.download()
     if precision != "fp64":
-        variants = [dict(grad_mode=4, grad_chunk=2, grad_widen=w, grad_narrow=g, grad_minb=7)
-                    for w, g in ((0, 1), (1, 0), (2, 1))]
+        variants = [dict(grad_mode=4, grad_chunk=ch, grad_widen=w, grad_narrow=g, grad_minb=mb)
+                    for ch, mb, w, g in ((2, 7, 0, 1), (2, 7, 1, 0), (2, 6, 2, 1), (4, 5, 0, 0),
+                                         (4, 5, 1, 1))]
         variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
                      for r, ch, g in ((4, 2, 0), (8, 3, 1), (4, 3, 1), (8, 2, 0))]
         for v in variants:
