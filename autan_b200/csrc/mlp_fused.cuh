@@ -26,19 +26,24 @@
 namespace fused {
 
 constexpr int kLayersMax = 8;
-constexpr int kThreads = 256;             // warp w: TMEM lanes 32 (w % 4), column half w / 4
+constexpr int kThreads = 512;             // warp w: TMEM lanes 32 (w % 4), column group w / 4
+constexpr int kGroups = kThreads / 128;   // column groups of an accumulator's epilogue
 constexpr int kImg = 128 * 128 * 2;       // bytes of a 128 x 128 BF16 operand image
 constexpr int kTmemCols = 256;            // [0, 128) forward / dA accumulator, [128, 256) dW
 constexpr int kWgradCol = 128;
 // shared memory: A / dZ image, dZ^T (and the forward's A^T staging), W images x 2, A^T images x 2,
-// column sums [4][128] and the squared-error halves [2][128] (FP32)
+// column sums [4 lane quarters][128] and the squared-error parts [kGroups][128] (FP32)
 constexpr int kOffA = 0;
 constexpr int kOffDzt = kImg;
 constexpr int kOffW = 2 * kImg;
 constexpr int kOffAt = 4 * kImg;
 constexpr int kOffCol = 6 * kImg;
 constexpr int kOffSe = kOffCol + 4 * 128 * 4;
-constexpr int kSmem = kOffSe + 2 * 128 * 4;
+constexpr int kSmem = kOffSe + kGroups * 128 * 4;
+
+// The columns [c0, c1) of an N-column accumulator that column group h reads in the epilogues: N
+// split into kGroups parts of at least 8 (groups past N read none).
+__device__ __forceinline__ int group_cols(int N) { return N / kGroups > 8 ? N / kGroups : 8; }
 
 struct Layout {
   int layers;  // weight layers: hidden layers + the output layer
@@ -197,14 +202,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ __align__(8) unsigned long long mma_bar, ld_bar[2], dead_bar;
   __shared__ uint32_t tmem_slot;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int q = warp & 3, h = warp >> 2;  // TMEM lane quarter, column half
+  const int q = warp & 3, h = warp >> 2;  // TMEM lane quarter, column group
   const int row = 32 * q + lane;          // this thread's row of the tile
   unsigned char* const aimg = sm + kOffA;  // A_l (forward), dZ_l (backward)
   unsigned char* const dzt = sm + kOffDzt;
   auto wimg = [&](int b) { return sm + kOffW + b * kImg; };    // W_l / W_l^T, double-buffered
   auto atimg = [&](int b) { return sm + kOffAt + b * kImg; };  // A_l^T, double-buffered
   float* const colsum = reinterpret_cast<float*>(sm + kOffCol);  // [4][128]
-  float* const sehalf = reinterpret_cast<float*>(sm + kOffSe);   // [2][128]
+  float* const separt = reinterpret_cast<float*>(sm + kOffSe);   // [kGroups][128]
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&tmem_slot)),
@@ -350,6 +355,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_commit(&mma_bar);
       }
       mma_pending = true;
+      // the backward epilogue's GELU'(Z_{l-1}) of this thread's 32 columns (128 / kGroups: the
+      // input of a layer l > 0 is 128 wide), loaded while the MMAs run
+      float gp[128 / kGroups];
+      if constexpr (TRAIN) {
+        if (!forward && l > 0) {
+#pragma unroll
+          for (int e = 0; e < 128 / kGroups; ++e)
+            gp[e] = zc[(static_cast<long long>(l - 1) * 128 + h * (128 / kGroups) + e) * 128 + row];
+        }
+      }
       ok = wait_all(&mma_bar, mma_par);
       if (!ok) break;
       mma_par ^= 1u;
@@ -361,15 +376,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool last = l == L - 1;
         const float* bias = P.params + P.w0[l] + static_cast<long long>(P.out[l]) * P.in[l];
         float s_err = 0.0f;
-        for (int c0 = h * (N >> 1); c0 < (h + 1) * (N >> 1); c0 += 8) {
+        const int cw = group_cols(N);
+        for (int c0 = h * cw; c0 < min(N, (h + 1) * cw); c0 += 8) {
           float z[8];
           tmem_ld8(tmem + lane_base + static_cast<uint32_t>(c0), z);
 #pragma unroll
-          for (int e = 0; e < 8; ++e) z[e] += c0 + e < P.out[l] ? bias[c0 + e] : 0.0f;
+          for (int e = 0; e < 8; ++e) z[e] += c0 + e < P.out[l] ? __ldg(bias + c0 + e) : 0.0f;
           if (!last) {
             if constexpr (TRAIN) {
+              // GELU'(Z) for the backward pass (the same erf as the activation's)
 #pragma unroll
-              for (int e = 0; e < 8; ++e) zc[(static_cast<long long>(l) * 128 + c0 + e) * 128 + row] = z[e];
+              for (int e = 0; e < 8; ++e)
+                zc[(static_cast<long long>(l) * 128 + c0 + e) * 128 + row] = gelu_grad(z[e]);
             }
             float a[8];
 #pragma unroll
@@ -403,9 +421,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!last) {
           if (TRAIN) save_at(l + 1, N);
         } else if constexpr (TRAIN) {
-          sehalf[h * 128 + row] = s_err;
+          separt[h * 128 + row] = s_err;
           bias_grad(l, first);  // synchronises first
-          if (h == 0 && valid) se[r0 + row] = sehalf[row] + sehalf[128 + row];
+          if (h == 0 && valid) {
+            float t = separt[row];
+            for (int g = 1; g < kGroups; ++g) t += separt[g * 128 + row];
+            se[r0 + row] = t;
+          }
           if (threadIdx.x == 0) bulk_store_read_done();  // dzt free of the last A^T store
           __syncthreads();
           transpose_img(aimg, dzt, N);
@@ -415,7 +437,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool direct = P.np[l] == 128;
         const int nw = direct ? P.kp[l] : P.np[l];
         float* const pw = part + P.w0[l];
-        for (int c0 = h * (nw >> 1); c0 < (h + 1) * (nw >> 1); c0 += 8) {
+        const int cw = group_cols(nw);
+        for (int c0 = h * cw; c0 < min(nw, (h + 1) * cw); c0 += 8) {
           float v[8];
           tmem_ld8(tmem + lane_base + static_cast<uint32_t>(kWgradCol + c0), v);
 #pragma unroll
@@ -429,13 +452,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (l > 0) {
           // dZ_{l-1} = dA_l GELU'(Z_{l-1}), its column sums (bias gradient of layer l - 1)
-          const int N = P.kp[l];  // = np[l - 1]
-          for (int c0 = h * (N >> 1); c0 < (h + 1) * (N >> 1); c0 += 8) {
+          constexpr int N = 128;  // = kp[l] = np[l - 1] at width 128
+#pragma unroll
+          for (int j = 0; j < N / kGroups / 8; ++j) {
+            const int c0 = h * (N / kGroups) + 8 * j;
             float g[8];
             tmem_ld8(tmem + lane_base + static_cast<uint32_t>(c0), g);
 #pragma unroll
-            for (int e = 0; e < 8; ++e)
-              g[e] *= gelu_grad(zc[(static_cast<long long>(l - 1) * 128 + c0 + e) * 128 + row]);
+            for (int e = 0; e < 8; ++e) g[e] *= gp[8 * j + e];
             colsum_chunk(c0, g);
             put8(aimg, row, c0, g);
           }
