@@ -1849,8 +1849,6 @@ __device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typena
                                             double* res_out) {
   using C = typename P::C;
   const double vol = __ldg(d.volume + c);
-  CellIn in;
-  load_cell_in(d, c, mode, stage, local, in);
   double res[5];
   {
     const C nv = -static_cast<C>(vol);  // sources (:611-616): res = -V s
@@ -1888,6 +1886,9 @@ __device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typena
       }
     }
   }
+  // the cell's RK inputs after the faces (not held in registers through the face loop)
+  CellIn in;
+  load_cell_in(d, c, mode, stage, local, in);
   finish_cell(d, c, res, vol, mode, stage, wa, wb, last, in, !NORMS);
   if constexpr (NORMS) {
 #pragma unroll

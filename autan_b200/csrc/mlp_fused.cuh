@@ -39,7 +39,8 @@ constexpr int kOffW = 2 * kImg;
 constexpr int kOffAt = 4 * kImg;
 constexpr int kOffCol = 6 * kImg;
 constexpr int kOffSe = kOffCol + 4 * 128 * 4;
-constexpr int kSmem = kOffSe + kGroups * 128 * 4;
+constexpr int kOffBias = kOffSe + kGroups * 128 * 4;  // the current layer's bias, 128 FP32
+constexpr int kSmem = kOffBias + 128 * 4;
 
 // The columns [c0, c1) of an N-column accumulator that column group h reads in the epilogues: N
 // split into kGroups parts of at least 8 (groups past N read none).
@@ -119,6 +120,50 @@ __device__ __forceinline__ void tmem_ld8(uint32_t addr, float* out) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int j = 0; j < 8; ++j) out[j] = __uint_as_float(v[j]);
+}
+
+// 32 FP32 accumulator columns [col, col + 32) of this warp's 32 TMEM lanes: one load, one wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float* out) {
+  uint32_t v[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+        "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+        "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) out[j] = __uint_as_float(v[j]);
+}
+
+// 16 FP32 accumulator columns [col, col + 16) of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float* out) {
+  uint32_t v[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) out[j] = __uint_as_float(v[j]);
+}
+
+// This warp's part of an accumulator: columns [c, c + 8 n) for n = cw / 8 (cw 32: one 32-column
+// load; cw 8: one 8-column load; columns at or past `end`: none).
+__device__ __forceinline__ void tmem_part(uint32_t addr, int cw, int c, int end, float* out) {
+  if (c >= end) return;
+  if (cw == 32) {
+    tmem_ld32(addr + static_cast<uint32_t>(c), out);
+  } else {
+    tmem_ld8(addr + static_cast<uint32_t>(c), out);
+  }
 }
 
 // A bounded wait on `bar`'s phase `parity` by every thread; true (uniformly) when it completed.
@@ -210,6 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   auto atimg = [&](int b) { return sm + kOffAt + b * kImg; };  // A_l^T, double-buffered
   float* const colsum = reinterpret_cast<float*>(sm + kOffCol);  // [4][128]
   float* const separt = reinterpret_cast<float*>(sm + kOffSe);   // [kGroups][128]
+  float* const sbias = reinterpret_cast<float*>(sm + kOffBias);  // [128]
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&tmem_slot)),
@@ -355,14 +401,20 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc_commit(&mma_bar);
       }
       mma_pending = true;
-      // the backward epilogue's GELU'(Z_{l-1}) of this thread's 32 columns (128 / kGroups: the
-      // input of a layer l > 0 is 128 wide), loaded while the MMAs run
-      float gp[128 / kGroups];
-      if constexpr (TRAIN) {
-        if (!forward && l > 0) {
+      // loaded while the MMAs run: the forward epilogue's bias into shared memory (visible after
+      // the wait's barrier); the backward epilogue's GELU'(Z_{l-1}) of this thread's 32 columns
+      // (the input of a layer l > 0 is 128 wide) into registers
+      float pre[32];
+      if (forward) {
+        if (threadIdx.x < 128) {
+          const float* bias = P.params + P.w0[l] + static_cast<long long>(P.out[l]) * P.in[l];
+          sbias[threadIdx.x] = static_cast<int>(threadIdx.x) < P.out[l] ? __ldg(bias + threadIdx.x) : 0.0f;
+        }
+      } else if constexpr (TRAIN) {
+        if (l > 0) {
 #pragma unroll
-          for (int e = 0; e < 128 / kGroups; ++e)
-            gp[e] = zc[(static_cast<long long>(l - 1) * 128 + h * (128 / kGroups) + e) * 128 + row];
+          for (int e = 0; e < 32; ++e)
+            pre[e] = zc[(static_cast<long long>(l - 1) * 128 + h * 32 + e) * 128 + row];
         }
       }
       ok = wait_all(&mma_bar, mma_par);
@@ -374,14 +426,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (forward) {
         const int N = P.np[l];
         const bool last = l == L - 1;
-        const float* bias = P.params + P.w0[l] + static_cast<long long>(P.out[l]) * P.in[l];
         float s_err = 0.0f;
         const int cw = group_cols(N);
-        for (int c0 = h * cw; c0 < min(N, (h + 1) * cw); c0 += 8) {
-          float z[8];
-          tmem_ld8(tmem + lane_base + static_cast<uint32_t>(c0), z);
+        float acc[32];
+        tmem_part(tmem + lane_base, cw, h * cw, N, acc);
 #pragma unroll
-          for (int e = 0; e < 8; ++e) z[e] += c0 + e < P.out[l] ? __ldg(bias + c0 + e) : 0.0f;
+        for (int j = 0; j < 4; ++j) {
+          const int c0 = h * cw + 8 * j;
+          if (8 * j >= cw || c0 >= N) break;
+          float z[8];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) z[e] = acc[8 * j + e] + sbias[c0 + e];
           if (!last) {
             if constexpr (TRAIN) {
               // GELU'(Z) for the backward pass (the same erf as the activation's)
@@ -438,28 +493,43 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int nw = direct ? P.kp[l] : P.np[l];
         float* const pw = part + P.w0[l];
         const int cw = group_cols(nw);
-        for (int c0 = h * cw; c0 < min(nw, (h + 1) * cw); c0 += 8) {
-          float v[8];
-          tmem_ld8(tmem + lane_base + static_cast<uint32_t>(kWgradCol + c0), v);
+        // in two loads of up to 16 columns (the GELU' values held for the next part bound the
+        // registers)
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int o = direct ? row : c0 + e, i = direct ? c0 + e : row;
-            if (o < P.out[l] && i < P.in[l]) {
-              float* dst = pw + static_cast<long long>(o) * P.in[l] + i;
-              *dst = first ? v[e] : *dst + v[e];
+        for (int half = 0; half < 2; ++half) {
+          const int cb = h * cw + 16 * half;
+          if (16 * half >= cw || cb >= nw) break;
+          float wv[16];
+          if (cw == 32) {
+            tmem_ld16(tmem + lane_base + static_cast<uint32_t>(kWgradCol + cb), wv);
+          } else {
+            tmem_ld8(tmem + lane_base + static_cast<uint32_t>(kWgradCol + cb), wv);
+          }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int c0 = cb + 8 * j;
+            if (16 * half + 8 * j >= cw || c0 >= nw) break;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const int o = direct ? row : c0 + e, i = direct ? c0 + e : row;
+              if (o < P.out[l] && i < P.in[l]) {
+                float* dst = pw + static_cast<long long>(o) * P.in[l] + i;
+                *dst = first ? wv[8 * j + e] : *dst + wv[8 * j + e];
+              }
             }
           }
         }
         if (l > 0) {
           // dZ_{l-1} = dA_l GELU'(Z_{l-1}), its column sums (bias gradient of layer l - 1)
           constexpr int N = 128;  // = kp[l] = np[l - 1] at width 128
+          float da[32];
+          tmem_ld32(tmem + lane_base + static_cast<uint32_t>(h * 32), da);
 #pragma unroll
-          for (int j = 0; j < N / kGroups / 8; ++j) {
-            const int c0 = h * (N / kGroups) + 8 * j;
+          for (int j = 0; j < 4; ++j) {
+            const int c0 = h * 32 + 8 * j;
             float g[8];
-            tmem_ld8(tmem + lane_base + static_cast<uint32_t>(c0), g);
 #pragma unroll
-            for (int e = 0; e < 8; ++e) g[e] *= gp[8 * j + e];
+            for (int e = 0; e < 8; ++e) g[e] = da[8 * j + e] * pre[8 * j + e];
             colsum_chunk(c0, g);
             put8(aimg, row, c0, g);
           }
