@@ -565,6 +565,42 @@ def run_warmstart_fp64(args) -> None:
     print(json.dumps({"metric": "bump force, warm vs freestream start, FP64 march", **res}), flush=True)
 
 
+def run_setup_times(args) -> None:
+    """The gradient set-up of the workload's mesh (face2 stencil and LSQ weights) on the GPU
+    (autan_b200.setup_device) against the host set-up: both results compared bit for bit, the
+    host time and the device times; one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    from autan_b200 import cases
+    from autan_b200.setup_device import DeviceSetup
+
+    if args.workload == "channel":
+        case = cases.bump_channel(*(int(v) for v in args.channel.split(",")))
+    elif args.workload == "tets":
+        case = cases.vortex_tets(*(int(v) for v in args.lattice.split(",")), precision="fp32+acc64")
+    else:
+        raise SystemExit("--setup-times takes --workload channel or tets")
+    m = case.mesh
+    kind = np.ascontiguousarray(case.bc_kind, np.uint8)
+    t0 = time.perf_counter()
+    wh = m.gradient_weights(kind)
+    host_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    with DeviceSetup(m) as s:
+        off, ent = s.stencil()
+        w, retried = s.weights(kind)
+        dev = s.times()
+    call_s = time.perf_counter() - t0
+    print(json.dumps({
+        "metric": "gradient set-up (face2 stencil and LSQ weights)", "workload": args.workload,
+        "cells": int(m.n_owned_cells), "entries": int(ent.size),
+        "stencil_same": bool(np.array_equal(off, m.stencil_offsets) and np.array_equal(ent, m.stencil)),
+        "weights_same": bool(np.array_equal(w.view(np.uint64), wh.view(np.uint64))),
+        "retried_cells": retried, "host_weights_s": host_s, "device_calls_s": call_s, **dev,
+    }), flush=True)  # fmt: skip
+
+
 def run_mlp_step(args) -> None:
     """The warm-start MLP's training step (7 -> 4 x 128 GELU -> 5, 8192-row minibatches of 65 536
     seeded rows, Adam) and its inference (2^20 rows) per engine: 0 mma.sync a kernel per layer,
@@ -872,6 +908,9 @@ def main() -> None:
                          "test set marched in FP64 from both starts (--load-network)")
     ap.add_argument("--warmstart-fp64-set", default="32,20000,500000",
                     help="the warm-start test set the cases are drawn from: CASES,LO,HI")
+    ap.add_argument("--setup-times", action="store_true",
+                    help="instead of the throughput line: the workload mesh's gradient set-up on "
+                         "the GPU against the host's, compared bit for bit and timed")
     ap.add_argument("--mlp-step", action="store_true",
                     help="instead of the throughput line: time the warm-start MLP's training step "
                          "and inference per engine (--steps epochs of 8 steps)")
@@ -895,6 +934,9 @@ def main() -> None:
         ap.error("at least 3 warm-up steps")
     if args.mlp_step:
         run_mlp_step(args)
+        return
+    if args.setup_times:
+        run_setup_times(args)
         return
     if args.warmstart_fp64:
         run_warmstart_fp64(args)
