@@ -1861,18 +1861,26 @@ __device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typena
   const int ib = __ldg(d.inc_start + (c >> 5)) + (c & 31);
   const int il = __ldg(d.inc_len + c);
   constexpr int kChunk = 4;
-  for (int j0 = 0; j0 < il; j0 += kChunk) {
-    int code[kChunk];
-    C fv[kChunk][5];
+  // the codes of the next chunk load with this chunk's flux records (two dependent loads a chunk
+  // otherwise: its codes, then its records)
+  int code[kChunk];
 #pragma unroll
-    for (int q = 0; q < kChunk; ++q)
-      code[q] = j0 + q < il ? __ldg(d.inc_code + ib + static_cast<long long>(j0 + q) * kSlice) : 0;
+  for (int q = 0; q < kChunk; ++q)
+    code[q] = q < il ? __ldg(d.inc_code + ib + static_cast<long long>(q) * kSlice) : 0;
+  for (int j0 = 0; j0 < il; j0 += kChunk) {
+    C fv[kChunk][5];
 #pragma unroll
     for (int q = 0; q < kChunk; ++q)
       if (j0 + q < il)
         load5<P>(code[q] >= 0 ? flux + static_cast<long long>(code[q] >> 1) * kFlux
                               : bflux + static_cast<long long>(-code[q] - 1) * kFlux,
                  fv[q]);
+    int next[kChunk];
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) {
+      const int j = j0 + kChunk + q;
+      next[q] = j < il ? __ldg(d.inc_code + ib + static_cast<long long>(j) * kSlice) : 0;
+    }
 #pragma unroll
     for (int q = 0; q < kChunk; ++q) {
       if (j0 + q < il) {
@@ -1885,6 +1893,8 @@ __device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typena
         }
       }
     }
+#pragma unroll
+    for (int q = 0; q < kChunk; ++q) code[q] = next[q];
   }
   // the cell's RK inputs after the faces (not held in registers through the face loop)
   CellIn in;
