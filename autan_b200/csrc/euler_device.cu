@@ -919,12 +919,7 @@ __device__ __forceinline__ double gradient_tail_pipelined(const Dev<Fp32Acc64>& 
 // all 15, the rest through cvt; G5 gathers neighbours with load5_narrow; CHUNK entries are
 // loaded together. Where Control::special is set or a weight is out of range the cells take the
 // cvt loop instead (the same sums, bit for bit).
-// A non-blocking prefetch of the line holding `p` into L1 (no register, no scoreboard).
-__device__ __forceinline__ void prefetch_l1(const void* p) {
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
-template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK, int PF = 0>
+template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK>
 __device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, double cfl, int local) {
   using P = Fp32Acc64;
   using C = float;
@@ -948,32 +943,9 @@ __device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, doubl
     }
     const int base = __ldg(d.st_start + (c >> 5)) + (c & 31);
     const int len = __ldg(d.st_len + c);
-    auto row_at = [&](int j) { return d.st + 4 * (base + static_cast<long long>(j) * kSlice); };
     auto walk = [&](auto scaled) {
       constexpr int W = decltype(scaled)::value;
-      // PF > 0: an L1 prefetch pipeline ahead of the loads: each chunk prefetches the rows 2 PF
-      // entries ahead and the neighbour records PF entries ahead, whose index words it loaded one
-      // chunk earlier (from rows prefetched PF entries before that)
-      int pidx[CHUNK];
-      if constexpr (PF > 0) {
-#pragma unroll
-        for (int q = 0; q < CHUNK; ++q)
-          pidx[q] = PF + q < len ? __ldg(reinterpret_cast<const int*>(row_at(PF + q)) + 3) : -1;
-      }
       for (int j0 = 0; j0 < len; j0 += CHUNK) {
-        if constexpr (PF > 0) {
-#pragma unroll
-          for (int q = 0; q < CHUNK; ++q)
-            if (j0 + 2 * PF + q < len) prefetch_l1(row_at(j0 + 2 * PF + q));
-#pragma unroll
-          for (int q = 0; q < CHUNK; ++q)
-            if (pidx[q] >= 0) prefetch_l1(d.prim + static_cast<long long>(pidx[q]) * kPrimW);
-#pragma unroll
-          for (int q = 0; q < CHUNK; ++q) {
-            const int jn = j0 + CHUNK + PF + q;
-            pidx[q] = jn < len ? __ldg(reinterpret_cast<const int*>(row_at(jn)) + 3) : -1;
-          }
-        }
         C e4[CHUNK][4], wn[CHUNK][5];
 #pragma unroll
         for (int q = 0; q < CHUNK; ++q)
@@ -1018,9 +990,9 @@ __device__ __forceinline__ void gradients_w_cells(const Dev<Fp32Acc64>& d, doubl
   if constexpr (DT) block_min_dt(dt, live, &d.ctl->dt_bits);
 }
 
-template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK, int MINB, int PF = 0>
+template <bool LIMIT, bool DT, int WIDE, bool G5, int CHUNK, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_gradients_w(Dev<Fp32Acc64> d, double cfl, int local) {
-  gradients_w_cells<LIMIT, DT, WIDE, G5, CHUNK, PF>(d, cfl, local);
+  gradients_w_cells<LIMIT, DT, WIDE, G5, CHUNK>(d, cfl, local);
 }
 
 // ---------------------------------------------------------------- TMA bulk staging
@@ -2362,14 +2334,11 @@ struct Tuning {
                          // bounded for grad_minb blocks of 128 per SM (chunk 2: 7 or 6; chunk 4: 5);
                          // 5 (fp32+acc64): each warp's stencil rows streamed by TMA bulk copies
                          // into a ring of grad_depth shared-memory slots, grad_chunk gathers in
-                         // flight (5-word with grad_narrow);
-                         // 6 (fp32+acc64): mode 4 (two entries, no widening) with an L1 prefetch
-                         // pipeline grad_depth entries ahead
+                         // flight (5-word with grad_narrow)
   int grad_widen = 0;    // mode 4: products widened by widen_scaled: 0 none, 1 x and y, 2 all
   int grad_narrow = 0;   // mode 4: 1 gathers neighbours as 16 + 4 bytes instead of 32
   int grad_minb = 7;     // mode 4: blocks of 128 threads per SM the registers are bounded for
-  int grad_depth = 4;    // mode 5: entries each warp's row ring holds (4 or 8); mode 6: the
-                         // prefetch distance in entries (4 or 8)
+  int grad_depth = 4;    // mode 5: entries each warp's row ring holds (4 or 8)
   static constexpr int kCount = 10;
   static constexpr int kMinCount = 6;  // callers that predate mode 4 pass the first six
   void to(int32_t* p) const {
@@ -2415,13 +2384,7 @@ void Tuning::validate() const {
   if (face_mode < 0 || face_mode > 2) fail("E1101: face_mode is 0, 1 or 2");
   if (grad_mode == 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
-  if (grad_mode < 0 || grad_mode > 6) fail("E1101: grad_mode is 0 to 6");
-  if (grad_mode == 6) {
-    if (grad_block != 128) fail("E1101: the mode-6 gradient kernel takes 128 threads");
-    if (grad_chunk != 2 || (grad_minb != 7 && grad_minb != 6))
-      fail("E1101: mode 6 takes grad_chunk 2 with grad_minb 7 or 6");
-    if (grad_depth != 4 && grad_depth != 8) fail("E1101: grad_depth of mode 6 is 4 or 8");
-  }
+  if (grad_mode < 0 || grad_mode > 5) fail("E1101: grad_mode is 0 to 5");
   if (grad_mode == 5) {
     if (grad_block != 128) fail("E1101: the mode-5 gradient kernel takes 128 threads");
     if (grad_chunk != 2 && grad_chunk != 3) fail("E1101: grad_chunk of mode 5 is 2 or 3");
@@ -3026,21 +2989,6 @@ class Impl final : public Stepper {
               }
             }
       if (sizeof(C) == 4 && limiter_)
-        for (int depth : {4, 8})
-          for (int minb : {7, 6}) {
-            Tuning t = keep;
-            t.grad_mode = 6;
-            t.grad_block = 128;
-            t.grad_chunk = 2;
-            t.grad_minb = minb;
-            t.grad_depth = depth;
-            const double ms = measure(t, kGradients);
-            if (ms < best_ms) {
-              best_ms = ms;
-              best = t;
-            }
-          }
-      if (sizeof(C) == 4 && limiter_)
         for (int shape = 0; shape < 3; ++shape)  // (entries in flight, register bound)
         for (int widen : {0, 1, 2})
           for (int narrow : {0, 1})
@@ -3514,10 +3462,9 @@ class Impl final : public Stepper {
           launch_as(kGradients, k_gradients_tiles<P, L, D>, cell_grid(128), 128, d, cfl, loc);
           return;
         }
-        if (tuning_.grad_mode >= 4) {
+        if (tuning_.grad_mode == 4 || tuning_.grad_mode == 5) {
           if constexpr (std::is_same_v<P, Fp32Acc64> && L) {
             if (tuning_.grad_mode == 5) launch_gradients_ring<D>(d, cfl, loc);
-            else if (tuning_.grad_mode == 6) launch_gradients_pf<D>(d, cfl, loc);
             else launch_gradients_w<D>(d, cfl, loc);
             return;
           }
@@ -3604,27 +3551,6 @@ class Impl final : public Stepper {
       if (tuning_.grad_widen == 2) narrow(std::integral_constant<int, 2>{});
       else if (tuning_.grad_widen == 1) narrow(std::integral_constant<int, 1>{});
       else narrow(std::integral_constant<int, 0>{});
-    }
-  }
-
-  // The mode-6 gradient kernel: mode 4's two entries in flight (no widening, 32-byte gathers)
-  // with the L1 prefetch pipeline grad_depth entries ahead, registers bounded for grad_minb
-  // blocks of 128 per SM.
-  template <bool D>
-  void launch_gradients_pf(const Dev<P>& d, double cfl, int loc) {
-    if constexpr (std::is_same_v<P, Fp32Acc64>) {
-      const int gs = cell_grid(128);
-      if (tuning_.grad_depth == 8) {
-        if (tuning_.grad_minb == 6)
-          launch_as(kGradients, k_gradients_w<true, D, 0, false, 2, 6, 8>, gs, 128, d, cfl, loc);
-        else
-          launch_as(kGradients, k_gradients_w<true, D, 0, false, 2, 7, 8>, gs, 128, d, cfl, loc);
-      } else {
-        if (tuning_.grad_minb == 6)
-          launch_as(kGradients, k_gradients_w<true, D, 0, false, 2, 6, 4>, gs, 128, d, cfl, loc);
-        else
-          launch_as(kGradients, k_gradients_w<true, D, 0, false, 2, 7, 4>, gs, 128, d, cfl, loc);
-      }
     }
   }
 
