@@ -1992,22 +1992,20 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
                                                            const int* case_of,
                                                            const unsigned char* active,
                                                            unsigned long long* words) {
-  // the current case's words of the block; each thread's squares of that case in ThreadWindows
-  __shared__ unsigned long long sh[5 * kWords];
-  ThreadWindow win[5];
+  constexpr int kWarps = kBlock / 32;
+  __shared__ unsigned long long sh[kWarps][5 * kWords];
+  unsigned long long* mine = sh[threadIdx.x >> 5];
   auto clear = [&]() {
-    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
+    for (int i = threadIdx.x; i < kWarps * 5 * kWords; i += blockDim.x) (&sh[0][0])[i] = 0;
   };
-  auto flush = [&](int kc) {  // every thread: windows, then the block's words into case kc's
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      win[k].flush_warp(sh + k * kWords);
-      win[k].reset();
-    }
-    __syncthreads();
+  auto flush = [&](int kc) {
     unsigned long long* dst = words + static_cast<long long>(kc) * 5 * kWords;
-    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x)
-      if (sh[i] != 0) atomicAdd(&dst[i], sh[i]);
+    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+      unsigned long long v = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) v += sh[w][i];
+      if (v != 0) atomicAdd(&dst[i], v);
+    }
   };
   clear();
   __syncthreads();
@@ -2022,6 +2020,7 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
       if (active[first] == 0) continue;  // a stopped case: nothing to add
       if (first != cur) {
         if (cur >= 0) {
+          __syncthreads();
           flush(cur);
           __syncthreads();
           clear();
@@ -2029,12 +2028,10 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
         }
         cur = first;
       }
-      if (c < n) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k) {
-          const double r = res[k * static_cast<long long>(n) + c];
-          win[k].add(r * r, sh + k * kWords);
-        }
+      for (int k = 0; k < 5; ++k) {
+        const double r = c < n ? res[k * static_cast<long long>(n) + c] : 0.0;
+        warp_exact_add_nonneg<true>(mine + k * kWords, r * r);
       }
     } else {
       const unsigned full = 0xffffffffu;
@@ -2054,18 +2051,8 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
       }
     }
   }
-  if (cur >= 0) flush(cur);  // uniform over the block
-}
-
-// The global exact words of a batched step from its cases' words (a sum of integers: the same
-// total as a pass over the active cells), before k_case_norm_finish clears them.
-__global__ void k_case_words_total(const unsigned long long* case_words, int n_cases,
-                                   Control* ctl) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 5 * kWords; i += gridDim.x * blockDim.x) {
-    unsigned long long v = 0;
-    for (int kc = 0; kc < n_cases; ++kc) v += case_words[static_cast<long long>(kc) * 5 * kWords + i];
-    (&ctl->words[0][0])[i] = v;
-  }
+  __syncthreads();
+  if (cur >= 0) flush(cur);
 }
 
 // Per case and equation (q = 5 case + k): rms = sqrt(sum / cells of the case) into this step's
@@ -3643,26 +3630,24 @@ class Impl final : public Stepper {
           launch_as(kNorms, k_norm_collect, 1, 512,
                     static_cast<const unsigned long long*>(norm_words_.as<unsigned long long>()),
                     d_.ctl);
-        } else if (n_cases_ > 0) {
-          // per case, then the global words as the cases' total (one pass over the residual)
+        } else {
+          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
+                    static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
+                    n_cases_ > 0 ? static_cast<const int*>(case_of_.as<int>()) : nullptr,
+                    n_cases_ > 0 ? static_cast<const unsigned char*>(active_.as<unsigned char>())
+                                 : nullptr);
+        }
+        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        if (n_cases_ > 0) {
           launch_as(kNorms, k_case_norm_sums, blocks(n_, kBlock * kCaseSpan), kBlock,
                     static_cast<const double*>(res_.as<double>()), n_,
                     static_cast<const int*>(case_of_.as<int>()),
                     static_cast<const unsigned char*>(active_.as<unsigned char>()),
                     case_words_.as<unsigned long long>());
-          launch_as(kNorms, k_case_words_total, 2, 256,
-                    static_cast<const unsigned long long*>(case_words_.as<unsigned long long>()),
-                    n_cases_, d_.ctl);
-        } else {
-          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
-                    static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
-                    static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
-        }
-        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
-        if (n_cases_ > 0)
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
                     case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
                     n_cases_, static_cast<const Control*>(d_.ctl), case_hist_.as<double>());
+        }
       }
     }
     launch(k_end_step, 1, 32, d_.ctl);

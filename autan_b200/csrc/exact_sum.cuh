@@ -165,11 +165,6 @@ struct ThreadWindow {
     w[3] += (o1 ? p2 : 0ULL) + (o2 ? p1 : 0ULL);
     w[4] += o2 ? p2 : 0ULL;
   }
-  __device__ __forceinline__ void reset() {
-    base = -1;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) w[i] = 0ULL;
-  }
   // The windows of the warp's lanes into `words` (shared words of the block): the lanes with the
   // same base add their words exactly (three 16-bit chunks a word, one redux.sync each; a word
   // holds at most 2^16 terms' parts, below 2^48) and one lane adds the sums atomically. Every
