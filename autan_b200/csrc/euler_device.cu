@@ -1801,9 +1801,9 @@ __device__ __forceinline__ void gather_cell(const Dev<P>& d, int c, const typena
 
 // Store-gather sum: each cell's face fluxes added in increasing face index from the source term,
 // then the RK stage (finish_cell). NORMS (face mode 2, a step's stage 0 without batched cases):
-// the squares of the stage-0 residual also go into the exact sums of the RMS norms here (per-thread
-// windows, per block in shared memory, per block into a replica of norm_words) instead of a
-// separate pass over a stored residual (which is then not stored).
+// the squares of the stage-0 residual also go into the exact sums of the RMS norms here, per warp
+// in shared memory and per block into a replica of norm_words, instead of a separate pass over a
+// stored residual (which is then not stored).
 template <class P, bool NORMS>
 __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* flux,
                                                 const typename P::C* bflux, int mode, int stage,
@@ -1814,34 +1814,31 @@ __global__ void __launch_bounds__(256) k_gather(Dev<P> d, const typename P::C* f
     if (c >= 0 && c < d.n && cell_active(d, c))
       gather_cell<P, false>(d, c, flux, bflux, mode, stage, wa, wb, local, last, nullptr);
   } else {
-    // a contiguous run of cells per warp over the resident grid (never re-packed: fused only
-    // without batched cases; a warp's 32 consecutive cells are one slice), each thread's squares
-    // in one ThreadWindow per component, merged once per warp into the block's shared words and
-    // once per block into a replica of norm_words
-    __shared__ unsigned long long block_words[5 * kWords];
-    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) block_words[i] = 0ULL;
+    // grid-stride over the cells (never re-packed: fused only without batched cases), so that
+    // each block clears and flushes its shared words once for many cells
+    extern __shared__ unsigned long long warp_words[];  // (blockDim.x / 32) x 5 x kWords
+    const int nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < nw * 5 * kWords; i += blockDim.x) warp_words[i] = 0ULL;
     __syncthreads();
-    const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
-    const long long warp = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const long long per = ((d.n + warps - 1) / warps + 31) / 32 * 32;  // at most 2^16 per lane
-    const long long c0 = warp * per;
-    const long long c1 = min(c0 + per, static_cast<long long>(d.n));
-    ThreadWindow win[5];
-    for (long long c = c0 + lane; c < c1; c += 32) {
-      if (!cell_active(d, static_cast<int>(c))) continue;
-      double res[5];
-      gather_cell<P, true>(d, static_cast<int>(c), flux, bflux, mode, stage, wa, wb, local, last,
-                           res);
+    unsigned long long* mine = warp_words + (threadIdx.x >> 5) * 5 * kWords;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < d.n;
+         base += stride) {  // block-uniform trip count: every lane reaches the warp adds
+      const long long c = base + threadIdx.x;
+      double res[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      if (c < d.n && cell_active(d, static_cast<int>(c)))
+        gather_cell<P, true>(d, static_cast<int>(c), flux, bflux, mode, stage, wa, wb, local,
+                             last, res);
 #pragma unroll
-      for (int k = 0; k < 5; ++k) win[k].add(res[k] * res[k], block_words + k * kWords);
+      for (int k = 0; k < 5; ++k) warp_exact_add_nonneg<true>(mine + k * kWords, res[k] * res[k]);
     }
-#pragma unroll
-    for (int k = 0; k < 5; ++k) win[k].flush_warp(block_words + k * kWords);
     __syncthreads();
     unsigned long long* replica = norm_words + (blockIdx.x % kNormReplicas) * 5 * kWords;
-    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x)
-      if (block_words[i] != 0) atomicAdd(&replica[i], block_words[i]);
+    for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+      unsigned long long v = 0;
+      for (int w = 0; w < nw; ++w) v += warp_words[w * 5 * kWords + i];
+      if (v != 0) atomicAdd(&replica[i], v);
+    }
   }
 }
 
@@ -1918,40 +1915,35 @@ __global__ void k_norm_collect(const unsigned long long* replicas, Control* ctl)
   }
 }
 
-// The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176): each warp
-// takes a contiguous run of cells (its lanes 32 cells apart, coalesced), each thread adds its
-// cells' squares into one ThreadWindow per component (neighbouring cells' residuals share their
-// limbs, so the adds are integer selects with no warp-collective step), the warp merges its
-// lanes' windows into the block's shared words, and the block adds its non-zero words to the
-// global words. Integer sums: the words' total, and so the rounded norm, do not depend on the
-// order. With batched cases (case_of, active not null) the cells of stopped cases are left out.
+// The exact sums of R_k^2 over the owned cells (SquareTerm, device_stepper.cuh:168-176): each
+// warp adds into words of its own in shared memory, the block then sums its warps' words and adds
+// the non-zero ones to the global words.
+// With batched cases (case_of, active not null) the cells of stopped cases are left out.
 __global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, Control* ctl,
                                                       const int* case_of,
                                                       const unsigned char* active) {
-  __shared__ unsigned long long sh[5 * kWords];
-  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) sh[i] = 0;
+  constexpr int kWarps = kBlock / 32;
+  __shared__ unsigned long long sh[kWarps][5 * kWords];
+  for (int i = threadIdx.x; i < kWarps * 5 * kWords; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
-  const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
-  const long long warp = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  // cells per warp, a multiple of 32; at most 2^16 per lane (ThreadWindow's word bound)
-  const long long per = ((n + warps - 1) / warps + 31) / 32 * 32;
-  const long long c0 = warp * per;
-  const long long c1 = min(c0 + per, static_cast<long long>(n));
-  ThreadWindow win[5];
-  for (long long c = c0 + lane; c < c1; c += 32) {
-    if (active != nullptr && active[case_of[c]] == 0) continue;
+  unsigned long long* mine = sh[threadIdx.x >> 5];
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x; base < n; base += stride) {
+    const long long c = base + threadIdx.x;
+    double r[5];
+    const bool in = c < n && (active == nullptr || active[case_of[c]] != 0);
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const double r = res[k * static_cast<long long>(n) + c];
-      win[k].add(r * r, sh + k * kWords);
-    }
+    for (int k = 0; k < 5; ++k) r[k] = in ? res[k * static_cast<long long>(n) + c] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) warp_exact_add_nonneg<true>(mine + k * kWords, r[k] * r[k]);
   }
-#pragma unroll
-  for (int k = 0; k < 5; ++k) win[k].flush_warp(sh + k * kWords);
   __syncthreads();
-  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x)
-    if (sh[i] != 0) atomicAdd(&ctl->words[i / kWords][i % kWords], sh[i]);
+  for (int i = threadIdx.x; i < 5 * kWords; i += blockDim.x) {
+    unsigned long long v = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) v += sh[w][i];
+    if (v != 0) atomicAdd(&ctl->words[i / kWords][i % kWords], v);
+  }
 }
 
 // record_norms (euler_physics.cpp:1040-1054): rms_k = sqrt(sum / N); the step's history entry.
@@ -3183,7 +3175,8 @@ class Impl final : public Stepper {
     C* bfl = bflux_.as<C>();
     const int gb = tuning_.gather_block;
     if (norms) {
-      launch_smem(kFaces, k_gather<P, true>, norm_gather_grid(gb, 0), gb, 0, d,
+      const size_t sm = static_cast<size_t>(gb / 32) * 5 * kWords * sizeof(unsigned long long);
+      launch_smem(kFaces, k_gather<P, true>, norm_gather_grid(gb, sm), gb, sm, d,
                   static_cast<const C*>(fl),
                   static_cast<const C*>(bfl), mode, stage, wa, wb, local, last,
                   norm_words_.as<unsigned long long>());

@@ -125,75 +125,6 @@ __device__ __forceinline__ void warp_exact_add_nonneg(unsigned long long* words,
   }
 }
 
-// One thread's exact sum of non-negative terms that cluster in magnitude (the squares of the
-// residuals of a run of neighbouring cells): five words at limbs base .. base + 4, base set by the
-// first non-zero term (its limb - 1); a term's three 32-bit parts land in three of them by
-// selects, with no warp-collective step. A term outside the window, +inf or NaN goes to `spill`
-// (shared words of the block) with atomics. Each part is below 2^32, so a word holds 2^31 terms.
-struct ThreadWindow {
-  int base = -1;  // no term yet
-  unsigned long long w[5] = {0ULL, 0ULL, 0ULL, 0ULL, 0ULL};
-
-  __device__ __forceinline__ void add(double t, unsigned long long* spill) {
-    const unsigned long long bits = static_cast<unsigned long long>(__double_as_longlong(t));
-    const int biased = static_cast<int>((bits >> 52) & 0x7ff);
-    const unsigned long long fraction = bits & ((1ULL << 52) - 1);
-    if (biased == 0x7ff) {
-      atomicAdd(&spill[fraction != 0 ? kLimbs + 2 : kLimbs], 1ULL);
-      return;
-    }
-    if (biased == 0 && fraction == 0) return;
-    const unsigned long long m = biased == 0 ? fraction : (fraction | (1ULL << 52));
-    const int e = biased == 0 ? -1074 : biased - 1075;
-    const int p = e + kOffset;
-    const int limb = p >> 5;
-    const int s = p & 31;
-    const unsigned long long lo = m << s, hi = s == 0 ? 0ULL : m >> (64 - s);
-    const unsigned long long p0 = lo & 0xffffffffULL, p1 = lo >> 32, p2 = hi & 0xffffffffULL;
-    if (base < 0) base = limb > 0 ? limb - 1 : 0;
-    const int off = limb - base;
-    if (off < 0 || off > 2) {
-      atomicAdd(&spill[limb], p0);
-      atomicAdd(&spill[limb + 1], p1);
-      atomicAdd(&spill[limb + 2], p2);
-      return;
-    }
-    const bool o0 = off == 0, o1 = off == 1, o2 = off == 2;
-    w[0] += o0 ? p0 : 0ULL;
-    w[1] += (o0 ? p1 : 0ULL) + (o1 ? p0 : 0ULL);
-    w[2] += (o0 ? p2 : 0ULL) + (o1 ? p1 : 0ULL) + (o2 ? p0 : 0ULL);
-    w[3] += (o1 ? p2 : 0ULL) + (o2 ? p1 : 0ULL);
-    w[4] += o2 ? p2 : 0ULL;
-  }
-  // The windows of the warp's lanes into `words` (shared words of the block): the lanes with the
-  // same base add their words exactly (three 16-bit chunks a word, one redux.sync each; a word
-  // holds at most 2^16 terms' parts, below 2^48) and one lane adds the sums atomically. Every
-  // lane of the warp calls it.
-  __device__ __forceinline__ void flush_warp(unsigned long long* words) const {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    unsigned todo = __ballot_sync(full, base >= 0);
-    while (todo != 0) {
-      const int leader = __ffs(todo) - 1;
-      const int lb = __shfl_sync(full, base, leader);
-      const bool mine = base >= 0 && base == lb;
-      const unsigned group = __ballot_sync(full, mine);
-#pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const unsigned long long v = mine ? w[i] : 0ULL;
-        const unsigned a = __reduce_add_sync(full, static_cast<unsigned>(v & 0xffff));
-        const unsigned b = __reduce_add_sync(full, static_cast<unsigned>((v >> 16) & 0xffff));
-        const unsigned c = __reduce_add_sync(full, static_cast<unsigned>((v >> 32) & 0xffff));
-        const unsigned long long sum = static_cast<unsigned long long>(a) +
-                                       (static_cast<unsigned long long>(b) << 16) +
-                                       (static_cast<unsigned long long>(c) << 32);
-        if (lane == leader && sum != 0ULL) atomicAdd(&words[lb + i], sum);
-      }
-      todo &= ~group;
-    }
-  }
-};
-
 // The rounded value of a word array (ExactSum::value, runtime/src/exact_sum.cpp:99-140).
 __device__ inline double exact_value(const unsigned long long* in) {
   long long w[kWords];
