@@ -2047,6 +2047,17 @@ __global__ void __launch_bounds__(kBlock) k_case_norm_sums(const double* res, in
   if (cur >= 0) flush(cur);
 }
 
+// The global exact words of a batched step from its cases' words (a sum of integers: the same
+// total as a pass over the active cells), before k_case_norm_finish clears them.
+__global__ void k_case_words_total(const unsigned long long* case_words, int n_cases,
+                                   Control* ctl) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 5 * kWords; i += gridDim.x * blockDim.x) {
+    unsigned long long v = 0;
+    for (int kc = 0; kc < n_cases; ++kc) v += case_words[static_cast<long long>(kc) * 5 * kWords + i];
+    (&ctl->words[0][0])[i] = v;
+  }
+}
+
 // Per case and equation (q = 5 case + k): rms = sqrt(sum / cells of the case) into this step's
 // row of the case history; the words are cleared for the next step.
 __global__ void k_case_norm_finish(unsigned long long* words, const double* cells, int n_cases,
@@ -3623,24 +3634,26 @@ class Impl final : public Stepper {
           launch_as(kNorms, k_norm_collect, 1, 512,
                     static_cast<const unsigned long long*>(norm_words_.as<unsigned long long>()),
                     d_.ctl);
-        } else {
-          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
-                    static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
-                    n_cases_ > 0 ? static_cast<const int*>(case_of_.as<int>()) : nullptr,
-                    n_cases_ > 0 ? static_cast<const unsigned char*>(active_.as<unsigned char>())
-                                 : nullptr);
-        }
-        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
-        if (n_cases_ > 0) {
+        } else if (n_cases_ > 0) {
+          // per case, then the global words as the cases' total (one pass over the residual)
           launch_as(kNorms, k_case_norm_sums, blocks(n_, kBlock * kCaseSpan), kBlock,
                     static_cast<const double*>(res_.as<double>()), n_,
                     static_cast<const int*>(case_of_.as<int>()),
                     static_cast<const unsigned char*>(active_.as<unsigned char>()),
                     case_words_.as<unsigned long long>());
+          launch_as(kNorms, k_case_words_total, 2, 256,
+                    static_cast<const unsigned long long*>(case_words_.as<unsigned long long>()),
+                    n_cases_, d_.ctl);
+        } else {
+          launch_as(kNorms, k_norm_sums, norm_blocks(), kBlock,
+                    static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
+                    static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
+        }
+        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        if (n_cases_ > 0)
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
                     case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
                     n_cases_, static_cast<const Control*>(d_.ctl), case_hist_.as<double>());
-        }
       }
     }
     launch(k_end_step, 1, 32, d_.ctl);
