@@ -1324,132 +1324,6 @@ __global__ void __launch_bounds__(128, 7) k_gradients_wring(Dev<Fp32Acc64> d, do
   if constexpr (DT) block_min_dt(dt, live && ok, &d.ctl->dt_bits);
 }
 
-// ---------------------------------------------------------------- warp-specialised gather
-//
-// Mode 6 (fp32+acc64 with the limiter): blocks of kWsPairs consumer warps (128 cells, one each)
-// and as many producer warps. Producer warp p streams, for the 32 cells of consumer warp p, every
-// stencil entry's three weights and its neighbour's five primitives (32 bytes) into a ring of
-// kWsSlots shared-memory slots, kWsGroup entries at a time (their row loads, then their record
-// loads, all in flight together); consumer warp p adds each entry from the ring in stencil order
-// (the FP64 sums of every other form, so the same bits) and then does the limiter's pass itself.
-// A full and an empty mbarrier per slot; every wait is bounded and a wait that runs out sets the
-// fault word (E1201) and ends the warp's work.
-
-constexpr int kWsPairs = 4;
-constexpr int kWsGroup = 4;                   // entries a producer warp loads together
-constexpr int kWsSlots = 2 * kWsGroup;        // slots per warp pair: two groups
-constexpr int kWsSlotF4 = 64;                 // a slot: two 16-byte halves x 32 lanes
-constexpr int kWsSmem = kWsPairs * kWsSlots * kWsSlotF4 * 16;  // 32 KB
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-template <bool DT, int MINB>
-__global__ void __launch_bounds__(2 * 32 * kWsPairs, MINB) k_gradients_ws(Dev<Fp32Acc64> d,
-                                                                       double cfl, int local) {
-  using P = Fp32Acc64;
-  using C = float;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) unsigned long long full_bar[kWsPairs * kWsSlots];
-  __shared__ __align__(8) unsigned long long empty_bar[kWsPairs * kWsSlots];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool producer = warp >= kWsPairs;
-  const int pair = producer ? warp - kWsPairs : warp;
-  const int c = blockIdx.x * (32 * kWsPairs) + pair * 32 + lane;
-  const bool live = c < d.n && cell_active(d, c);
-  if (threadIdx.x < kWsPairs * kWsSlots) {
-    mbar_init(&full_bar[threadIdx.x], 1);
-    mbar_init(&empty_bar[threadIdx.x], 1);
-  }
-  __syncthreads();
-  float4* const ring = reinterpret_cast<float4*>(smem_raw) + pair * kWsSlots * kWsSlotF4;
-  unsigned long long* const full = full_bar + pair * kWsSlots;
-  unsigned long long* const empty = empty_bar + pair * kWsSlots;
-  const int len = live ? __ldg(d.st_len + c) : 0;
-  const int maxlen = static_cast<int>(__reduce_max_sync(0xffffffffu, static_cast<unsigned>(len)));
-  const long long base = c < d.n ? __ldg(d.st_start + (c >> 5)) + (c & 31) : 0;
-  bool ok = true;
-  double dt = 0.0;
-  if (producer) {
-    for (int g = 0; g * kWsGroup < maxlen; ++g) {
-      const int j0 = g * kWsGroup;
-      const int s0 = (g & 1) * kWsGroup;
-      const unsigned par = ((g >> 1) & 1) ^ 1u;  // the consumer's release of the slots' last use
-      bool got = true;
-#pragma unroll
-      for (int q = 0; q < kWsGroup; ++q) got = got && slot_wait(&empty[s0 + q], par);
-      if (!__all_sync(0xffffffffu, got)) {
-        ok = false;
-        break;
-      }
-      float4 row[kWsGroup];
-      C rec[kWsGroup][8];
-#pragma unroll
-      for (int q = 0; q < kWsGroup; ++q)
-        if (j0 + q < len)
-          row[q] = __ldg(reinterpret_cast<const float4*>(d.st + 4 * (base + static_cast<long long>(j0 + q) * kSlice)));
-#pragma unroll
-      for (int q = 0; q < kWsGroup; ++q)
-        if (j0 + q < len)
-          ld32(d.prim + static_cast<long long>(index_of(row[q].w)) * kPrimW, rec[q]);
-#pragma unroll
-      for (int q = 0; q < kWsGroup; ++q) {
-        if (j0 + q < len) {
-          ring[(s0 + q) * kWsSlotF4 + lane] = make_float4(row[q].x, row[q].y, row[q].z, rec[q][0]);
-          ring[(s0 + q) * kWsSlotF4 + 32 + lane] = make_float4(rec[q][1], rec[q][2], rec[q][3], rec[q][4]);
-        }
-      }
-      __syncwarp();
-      if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < kWsGroup; ++q) mbar_arrive(&full[s0 + q]);
-    }
-  } else {
-    C wc[5] = {C(0), C(0), C(0), C(0), C(0)};
-    if (live) load5<P>(d.prim + static_cast<long long>(c) * kPrimW, wc);
-    double acc[15];
-#pragma unroll
-    for (int k = 0; k < 15; ++k) acc[k] = 0.0;
-    C lo[5], hi[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      lo[k] = C(INFINITY);
-      hi[k] = -C(INFINITY);
-    }
-    for (int j = 0; j < maxlen; ++j) {
-      const int s = j % kWsSlots;
-      if (!__all_sync(0xffffffffu, slot_wait(&full[s], (j / kWsSlots) & 1))) {
-        ok = false;
-        break;
-      }
-      const float4 a = ring[s * kWsSlotF4 + lane];
-      const float4 b = ring[s * kWsSlotF4 + 32 + lane];
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-      if (j < len) {
-        const C e[3] = {a.x, a.y, a.z};
-        const C wn[5] = {a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          const C dw = wn[i] - wc[i];
-          acc[3 * i] += static_cast<double>(dw * e[0]);
-          acc[3 * i + 1] += static_cast<double>(dw * e[1]);
-          acc[3 * i + 2] += static_cast<double>(dw * e[2]);
-        }
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-          lo[i] = bound_min(lo[i], wn[i]);
-          hi[i] = bound_max(hi[i], wn[i]);
-        }
-      }
-    }
-    if (ok && live) dt = gradient_tail_pipelined<true, DT, false>(d, c, wc, acc, lo, hi, cfl, local);
-  }
-  if (!ok && lane == 0) atomicExch(&d.ctl->fault, 1ULL);
-  if constexpr (DT) block_min_dt(dt, live && ok && !producer, &d.ctl->dt_bits);
-}
-
 // fp32+acc64 with up to 4 entries in flight, registers sized for 6 blocks of 128 per SM: the
 // stage-0 form (with the time step) drops from 94 to 80 registers. The 8-entry form and the FP64
 // policy spill under that bound and keep k_gradients_tma.
@@ -2471,10 +2345,7 @@ struct Tuning {
                          // bounded for grad_minb blocks of 128 per SM (chunk 2: 7 or 6; chunk 4: 5);
                          // 5 (fp32+acc64): each warp's stencil rows streamed by TMA bulk copies
                          // into a ring of grad_depth shared-memory slots, grad_chunk gathers in
-                         // flight (5-word with grad_narrow);
-                         // 6 (fp32+acc64): producer warps gather each stencil entry's weights and
-                         // neighbour record into a shared-memory ring for consumer warps,
-                         // registers bounded for grad_minb (4 or 3) blocks of 256 per SM
+                         // flight (5-word with grad_narrow)
   int grad_widen = 0;    // mode 4: products widened by widen_scaled: 0 none, 1 x and y, 2 all
   int grad_narrow = 0;   // mode 4: 1 gathers neighbours as 16 + 4 bytes instead of 32
   int grad_minb = 7;     // mode 4: blocks of 128 threads per SM the registers are bounded for
@@ -2524,11 +2395,7 @@ void Tuning::validate() const {
   if (face_mode < 0 || face_mode > 2) fail("E1101: face_mode is 0, 1 or 2");
   if (grad_mode == 3 && grad_chunk != 2 && grad_chunk != 4 && grad_chunk != 8)
     fail("E1101: grad_chunk of the ring kernel is 2, 4 or 8");
-  if (grad_mode < 0 || grad_mode > 6) fail("E1101: grad_mode is 0 to 6");
-  if (grad_mode == 6) {
-    if (grad_block != 128) fail("E1101: the mode-6 gradient kernel takes 128 cells a block");
-    if (grad_minb != 4 && grad_minb != 3) fail("E1101: grad_minb of mode 6 is 4 or 3");
-  }
+  if (grad_mode < 0 || grad_mode > 5) fail("E1101: grad_mode is 0 to 5");
   if (grad_mode == 5) {
     if (grad_block != 128) fail("E1101: the mode-5 gradient kernel takes 128 threads");
     if (grad_chunk != 2 && grad_chunk != 3) fail("E1101: grad_chunk of mode 5 is 2 or 3");
@@ -3133,18 +3000,6 @@ class Impl final : public Stepper {
               }
             }
       if (sizeof(C) == 4 && limiter_)
-        for (int minb : {4, 3}) {
-          Tuning t = keep;
-          t.grad_mode = 6;
-          t.grad_block = 128;
-          t.grad_minb = minb;
-          const double ms = measure(t, kGradients);
-          if (ms < best_ms) {
-            best_ms = ms;
-            best = t;
-          }
-        }
-      if (sizeof(C) == 4 && limiter_)
         for (int shape = 0; shape < 3; ++shape)  // (entries in flight, register bound)
         for (int widen : {0, 1, 2})
           for (int narrow : {0, 1})
@@ -3618,10 +3473,9 @@ class Impl final : public Stepper {
           launch_as(kGradients, k_gradients_tiles<P, L, D>, cell_grid(128), 128, d, cfl, loc);
           return;
         }
-        if (tuning_.grad_mode >= 4) {
+        if (tuning_.grad_mode == 4 || tuning_.grad_mode == 5) {
           if constexpr (std::is_same_v<P, Fp32Acc64> && L) {
             if (tuning_.grad_mode == 5) launch_gradients_ring<D>(d, cfl, loc);
-            else if (tuning_.grad_mode == 6) launch_gradients_ws<D>(d, cfl, loc);
             else launch_gradients_w<D>(d, cfl, loc);
             return;
           }
@@ -3708,19 +3562,6 @@ class Impl final : public Stepper {
       if (tuning_.grad_widen == 2) narrow(std::integral_constant<int, 2>{});
       else if (tuning_.grad_widen == 1) narrow(std::integral_constant<int, 1>{});
       else narrow(std::integral_constant<int, 0>{});
-    }
-  }
-
-  // The mode-6 gradient kernel (producer and consumer warps), registers bounded for grad_minb
-  // blocks of 256 threads per SM.
-  template <bool D>
-  void launch_gradients_ws(const Dev<P>& d, double cfl, int loc) {
-    if constexpr (std::is_same_v<P, Fp32Acc64>) {
-      const int gs = blocks(n_, 32 * kWsPairs);
-      if (tuning_.grad_minb == 3)
-        launch_smem(kGradients, k_gradients_ws<D, 3>, gs, 64 * kWsPairs, kWsSmem, d, cfl, loc);
-      else
-        launch_smem(kGradients, k_gradients_ws<D, 4>, gs, 64 * kWsPairs, kWsSmem, d, cfl, loc);
     }
   }
 

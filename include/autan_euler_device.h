@@ -181,10 +181,7 @@ int autan_euler_device_kernel_times(void* handle, double cfl, double dt, int32_t
  * threads per SM the registers are bounded for: 7 or 6 with [0] = 2, 5 with [0] = 4; 5,
  * fp32+acc64 only: each warp's
  * stencil rows streamed by TMA bulk copies into a ring of [9] (4 or 8) shared-memory slots ahead of
- * the warp, [0] (2 or 3) gathers in flight, [7] as for 4, 128 threads per block; 6,
- * fp32+acc64 only: producer warps gather every stencil entry's weights and neighbour record into
- * a shared-memory ring for as many consumer warps, 128 cells and 256 threads per block, [1] =
- * 128, [8] 4 or 3 the blocks per SM the registers are bounded for).
+ * the warp, [0] (2 or 3) gathers in flight, [7] as for 4, 128 threads per block).
  * Every choice gives the same bits. No counterpart in the reference beyond its Strategy enum
  * (codegen/include/autan/kernels/strategy.hpp:14-21). */
 int autan_euler_device_set_tuning(void* handle, const int32_t* params, int32_t count, char* err,

@@ -219,8 +219,6 @@ def test_tuning_variants_are_bit_identical(precision):
     # mode 5: the per-warp TMA row ring of 4 or 8 slots with 2 or 3 gathers in flight
     variants = [dict(grad_mode=4, grad_chunk=ch, grad_widen=w, grad_narrow=g, grad_minb=mb)
                 for ch, mb in ((2, 7), (2, 6), (4, 5)) for w in (0, 1, 2) for g in (0, 1)]
-    # mode 6: producer warps gather into a shared-memory ring for consumer warps
-    variants += [dict(grad_mode=6, grad_minb=mb) for mb in (4, 3)]
     variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
                  for r in (4, 8) for ch in (2, 3) for g in (0, 1)]
     for i, v in enumerate(variants):
@@ -257,7 +255,6 @@ def test_gradient_stagings_agree_on_the_channel(precision):
                                          (4, 5, 1, 1))]
         variants += [dict(grad_mode=5, grad_chunk=ch, grad_depth=r, grad_narrow=g)
                      for r, ch, g in ((4, 2, 0), (8, 3, 1), (4, 3, 1), (8, 2, 0))]
-        variants += [dict(grad_mode=6, grad_minb=mb) for mb in (4, 3)]
         for v in variants:
             with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
                 dev.set_tuning(grad_block=128, face_mode=1, face_block=128, gather_block=128, **v)
