@@ -60,7 +60,7 @@ int autan_mlp_train(void* handle, int32_t epochs, int32_t batch, float lr, uint6
                     float* loss, char* err, size_t err_len);
 /* One forward and backward pass on n rows (host x, y as set_data's), no update: *loss and the
  * gradient of the loss with respect to every parameter (parameter_count floats, as
- * get_parameters); n at most 65535 x 128. For checks against a CPU restatement. */
+ * get_parameters); n from 1 to 2^20. For checks against a CPU restatement. */
 int autan_mlp_gradient(void* handle, const float* x, const float* y, int64_t n, float* loss,
                        float* grad, char* err, size_t err_len);
 /* Prediction of n rows: x (n x inputs) to y (n x outputs), raw units. device_ptrs != 0: x and y
