@@ -866,7 +866,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 # (stage 0 + 2 x stage 1) / 3 (stages 1 and 2 do the same work).
 TRAFFIC = {
     ("gradients", "tets"): (452191659, 1016064, "gradients_occ7_tets_and_channel_1M.md"),
-    ("gradients", "channel"): (700893355, 994600, "gradients_w_channel_1M.md"),
+    ("gradients", "channel"): (702985984, 994600, "gradients_occ7_channel_1M.md"),
 }
 
 
