@@ -859,14 +859,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel
 # kind, averaged over a step's launches, from one ncu capture per mesh family on a smaller case
-# of that family (the capture named beside each entry, under profiles/): (kernel kind, mesh
-# family) -> (bytes per launch, cells of the capture, capture). The bytes per cell do not depend
+# of that family (its summary is under profiles/): (kernel kind, mesh family) -> (bytes per
+# launch, cells of the capture, the captured kernel and case). The bytes per cell do not depend
 # on the lattice size (same stencil, record sizes and cell ordering), so a workload's traffic is
 # the entry scaled to its cells. Where the capture holds stages 0 and 1, the step's average is
 # (stage 0 + 2 x stage 1) / 3 (stages 1 and 2 do the same work).
 TRAFFIC = {
-    ("gradients", "tets"): (452191659, 1016064, "gradients_occ7_tets_and_channel_1M.md"),
-    ("gradients", "channel"): (702985984, 994600, "gradients_occ7_channel_1M.md"),
+    ("gradients", "tets"): (452191659, 1016064, "k_gradients_occ7, 1 016 064-cell tets lattice"),
+    ("gradients", "channel"): (702985984, 994600, "k_gradients_occ7, 994 600-cell bump channel"),
 }
 
 
