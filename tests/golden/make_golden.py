@@ -616,7 +616,7 @@ def main():
                      prim=drv.prim.astype(np.float64), grad=drv.grad.astype(np.float64),
                      phi=drv.phi.astype(np.float64), wmin=drv.wmin.astype(np.float64),
                      wmax=drv.wmax.astype(np.float64), prim_b=drv.prim_b.astype(np.float64))  # fmt: skip
-        if name in ("hex_roe1_f64", "tet_hllc2_f64", "tet_hllc2_f32"):
+        if name not in ("chan_ausm2_f64", "chan_roe2_f64"):  # steps where no exp/log enters
             for rk in (3, 4):
                 drv2 = Driver(ref, md, scheme, bkind, bc, source)
                 un, norms, dt = drv2.step(u, rk, 0.5)
