@@ -1614,7 +1614,8 @@ __device__ __forceinline__ void load_cell_in(const Dev<P>& d, int c, int mode, i
 #pragma unroll
     for (int k = 0; k < 5; ++k) in.x[k] = 0.0;
   }
-  in.h = local ? d.dt_local[c] : d.ctl->dt;
+  // the global step from its minimum's bits (final once the stage-0 cell kernel has run)
+  in.h = local ? d.dt_local[c] : __longlong_as_double(static_cast<long long>(d.ctl->dt_bits));
 }
 
 template <class P>
@@ -1947,7 +1948,10 @@ __global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, 
 }
 
 // record_norms (euler_physics.cpp:1040-1054): rms_k = sqrt(sum / N); the step's history entry.
-__global__ void k_norm_finish(Control* ctl, int n, int record) {
+// With record (a step's stage 0): the step's dt from its minimum's bits (for the host and the
+// history; the gathers read the bits themselves) and the history entry; with advance, the step
+// count too (in place of k_end_step, where nothing later in the step reads it).
+__global__ void k_norm_finish(Control* ctl, int n, int record, int advance) {
   const int k = threadIdx.x;
   __shared__ double rms[5];
   if (k < 5) rms[k] = sqrt(exact_value(ctl->words[k]) / static_cast<double>(n));
@@ -1958,7 +1962,11 @@ __global__ void k_norm_finish(Control* ctl, int n, int record) {
       ctl->rms[q] = rms[q];
       if (record) ctl->hist_rms[slot][q] = rms[q];
     }
-    if (record) ctl->hist_dt[slot] = ctl->dt;
+    if (record) {
+      ctl->dt = __longlong_as_double(static_cast<long long>(ctl->dt_bits));
+      ctl->hist_dt[slot] = ctl->dt;
+    }
+    if (advance) ctl->step += 1;
   }
 }
 
@@ -2083,11 +2091,6 @@ __global__ void k_begin(Control* ctl, double dt_fixed, unsigned long long* norm_
     ctl->bad_state = ~0ULL;
     ctl->bad_res = ~0ULL;
   }
-}
-
-// The global step from its minimum's bits.
-__global__ void k_take_dt(Control* ctl) {
-  if (threadIdx.x == 0) ctl->dt = __longlong_as_double(static_cast<long long>(ctl->dt_bits));
 }
 
 __global__ void k_end_step(Control* ctl) {
@@ -2815,7 +2818,7 @@ class Impl final : public Stepper {
     enqueue_residual(0);
     launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
            static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
-    launch(k_norm_finish, 1, 32, d_.ctl, n_, 0);
+    launch(k_norm_finish, 1, 32, d_.ctl, n_, 0, 0);
     // invalid(): the state, then the residual, marked on the device
     launch(k_invalid<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
            static_cast<const double*>(res_.as<double>()));
@@ -2887,7 +2890,7 @@ class Impl final : public Stepper {
   void time_steps(double cfl, double* dt) override {
     Buffer tmp(std::max(n_, 1) * sizeof(double));
     Dev<P> d = with_rec(0, 0);
-    launch(k_boundary_states<P>, blocks(nb_), kBlock, d);
+    if (nb_ > 0) launch(k_boundary_states<P>, blocks(nb_), kBlock, d);
     d.ctl = nullptr;
     launch(k_spectral<P>, blocks(n_), kBlock, d, cfl, 0, tmp.as<double>());
     check(cudaMemcpyAsync(dt, tmp.ptr(), n_ * sizeof(double), cudaMemcpyDeviceToHost, stream), "dt");
@@ -3461,7 +3464,7 @@ class Impl final : public Stepper {
   // with `dt`, the spectral radius and the CFL step of the step too.
   void enqueue_cells(int in, bool dt, double cfl, bool local) {
     const Dev<P> d = with_rec(in, in);
-    launch_as(kBoundary, k_boundary_states<P>, bface_grid(kBlock, nb_), kBlock, d);
+    if (nb_ > 0) launch_as(kBoundary, k_boundary_states<P>, bface_grid(kBlock, nb_), kBlock, d);
     const int g = cell_grid(kBlock);
     const int loc = local ? 1 : 0;
     if (second_) {
@@ -3624,7 +3627,6 @@ class Impl final : public Stepper {
       const int in = k.rk == 3 ? in3[st] : in4[st];
       const int out = k.rk == 3 ? out3[st] : out4[st];
       enqueue_cells(in, st == 0 && cfl_dt, k.cfl, local);
-      if (st == 0) launch(k_take_dt, 1, 32, d_.ctl);
       const double wa = k.rk == 3 ? w3[st][0] : c4[st];
       const double wb = k.rk == 3 ? w3[st][1] : 0.0;
       launch_faces(with_rec(in, out), k.rk == 3 ? kRk3 : kRk4, st, wa, wb, local ? 1 : 0,
@@ -3649,14 +3651,14 @@ class Impl final : public Stepper {
                     static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
                     static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
         }
-        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1);
+        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1, n_cases_ == 0 ? 1 : 0);
         if (n_cases_ > 0)
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
                     case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
                     n_cases_, static_cast<const Control*>(d_.ctl), case_hist_.as<double>());
       }
     }
-    launch(k_end_step, 1, 32, d_.ctl);
+    if (n_cases_ > 0) launch(k_end_step, 1, 32, d_.ctl);  // after the per-case history
   }
 
   void capture(const StepKey& k) {
