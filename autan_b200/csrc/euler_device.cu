@@ -1763,9 +1763,15 @@ __device__ __forceinline__ void bface_flux_body(const Dev<P>& d, int b, typename
 }
 
 // Store-gather, first half (the reference's store strategy, emit_gpu.py): the flux of every owned
-// interior face, once, in its orientation, into the face scratch.
+// interior face, once, in its orientation, into the face scratch. The fp32+acc64 forms that fit 48
+// registers without spilling (planar faces, or first order) are bounded for it: 42 warps per SM at
+// 64 threads a block instead of 36 at 50 registers. The non-planar second-order and fp64 forms
+// spill under that bound and keep their own allocation.
+template <class P, bool PLANAR, bool SECOND>
+constexpr int kFaceMinBlocks = (sizeof(typename P::C) == 4 && (PLANAR || !SECOND)) ? 5 : 1;
 template <class P, int FLUX, bool PLANAR, bool SECOND>
-__global__ void __launch_bounds__(256) k_face_flux(Dev<P> d, typename P::C* flux) {
+__global__ void __launch_bounds__(256, (kFaceMinBlocks<P, PLANAR, SECOND>))
+    k_face_flux(Dev<P> d, typename P::C* flux) {
   const int f = tile_item(d.face_tiles, d.n_face_tiles);
   if (f < 0 || f >= d.n_if) return;
   if (d.face_warp_case != nullptr) {
