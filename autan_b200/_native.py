@@ -147,6 +147,27 @@ class MarchResult(C.Structure):
     ]
 
 
+# Callbacks of struct autan_euler_ranks.
+EXCHANGE_FN = C.CFUNCTYPE(i32, vp, i32, i64, vp)
+REDUCE_FN = C.CFUNCTYPE(i32, vp, i32, i64, vp)
+
+
+class Ranks(C.Structure):
+    """struct autan_euler_ranks of include/autan_euler_device.h."""
+
+    _fields_ = [
+        ("user", vp),
+        ("exchange", EXCHANGE_FN),
+        ("reduce", REDUCE_FN),
+        ("send", vp),
+        ("recv", vp),
+        ("words", vp),
+        ("n_send", i64),
+        ("send_cells", P(i32)),
+        ("global_cells", f64),
+    ]
+
+
 def _bind(lib: C.CDLL) -> None:
     def fn(name: str, res, *args):
         f = getattr(lib, name)
@@ -179,6 +200,8 @@ def _bind(lib: C.CDLL) -> None:
         fn("autan_euler_device_evaluate", C.c_int, vp, P(StepResult), C.c_char_p, sz)
         fn("autan_euler_device_sync", C.c_int, vp, C.c_char_p, sz)
         fn("autan_euler_device_set_stall_test", C.c_int, vp, i32, C.c_char_p, sz)
+        fn("autan_euler_device_set_ranks", C.c_int, vp, P(Ranks), C.c_char_p, sz)
+        fn("autan_euler_device_external_ghosts", C.c_int, vp, P(i64), C.c_char_p, sz)
         fn("autan_euler_device_stream", vp, vp)
         fn("autan_euler_device_counters", C.c_int, vp, P(i64), C.c_char_p, sz)
         fn("autan_euler_device_gradients", C.c_int, vp, P(f64), P(f64), C.c_char_p, sz)

@@ -1953,14 +1953,15 @@ __global__ void __launch_bounds__(kBlock) k_norm_sums(const double* res, int n, 
   }
 }
 
-// record_norms (euler_physics.cpp:1040-1054): rms_k = sqrt(sum / N); the step's history entry.
+// record_norms (euler_physics.cpp:1040-1054): rms_k = sqrt(sum / N), N the owned cells (of all
+// ranks on a partitioned mesh); the step's history entry.
 // With record (a step's stage 0): the step's dt from its minimum's bits (for the host and the
 // history; the gathers read the bits themselves) and the history entry; with advance, the step
 // count too (in place of k_end_step, where nothing later in the step reads it).
-__global__ void k_norm_finish(Control* ctl, int n, int record, int advance) {
+__global__ void k_norm_finish(Control* ctl, double n, int record, int advance) {
   const int k = threadIdx.x;
   __shared__ double rms[5];
-  if (k < 5) rms[k] = sqrt(exact_value(ctl->words[k]) / static_cast<double>(n));
+  if (k < 5) rms[k] = sqrt(exact_value(ctl->words[k]) / n);
   __syncthreads();
   if (k == 0) {
     const long long slot = ctl->step % kHistory;
@@ -2103,13 +2104,39 @@ __global__ void k_end_step(Control* ctl) {
   if (threadIdx.x == 0) ctl->step += 1;
 }
 
+// Ghost exchange of a partitioned mesh (the forward halo exchange's pack and unpack,
+// partition/include/autan/partition/halo_exchange.hpp:18-31): records of `groups` groups of
+// kGroup words, group g of cell c at base + g gstride + kGroup c. PACK: the records of cells[i]
+// into buf record after record; else the records buf[i] into the cells first + i. One thread per
+// 16-byte piece (group strides, records and buf are 16-byte aligned).
+template <class C, bool PACK>
+__global__ void k_halo_records(C* base, long long gstride, int groups, const int* cells,
+                               long long count, int first, C* buf) {
+  constexpr int kPieces = kGroup * static_cast<int>(sizeof(C)) / 16;
+  const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long per = static_cast<long long>(groups) * kPieces;
+  if (t >= count * per) return;
+  const long long i = t / per;
+  const int r = static_cast<int>(t - i * per);
+  const int g = r / kPieces, q = r % kPieces;
+  const long long c = PACK ? static_cast<long long>(cells[i]) : first + i;
+  uint4* rec = reinterpret_cast<uint4*>(base + g * gstride + c * kGroup) + q;
+  uint4* packed = reinterpret_cast<uint4*>(buf + (i * groups + g) * kGroup) + q;
+  if constexpr (PACK) {
+    *packed = *rec;
+  } else {
+    *rec = *packed;
+  }
+}
+
 // Gradients and limiter of the reconstruction array, as FP64 SoA (15 x n, 5 x n).
 template <class P>
-__global__ void k_unpack(const typename P::C* recon, int n, double* grad, double* phi) {
+__global__ void k_unpack(const typename P::C* recon, int n, long long rstride, double* grad,
+                         double* phi) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   auto word = [&](int w) {
-    return static_cast<double>(recon[(w / kGroup) * static_cast<long long>(kGroup) * n +
+    return static_cast<double>(recon[(w / kGroup) * rstride +
                                      static_cast<long long>(c) * kGroup + w % kGroup]);
   };
   for (int k = 0; k < 15; ++k) grad[static_cast<long long>(k) * n + c] = word(5 + k);
@@ -2455,6 +2482,8 @@ class Stepper {
   virtual void case_history(long long count, double* rms) = 0;
   virtual int n_cases() const = 0;
   virtual void set_stall_test(int polls) = 0;
+  virtual void set_ranks(const autan_euler_ranks* ranks) = 0;
+  virtual long long external_ghosts() const = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
@@ -2477,11 +2506,16 @@ class Impl final : public Stepper {
     nif_ = m.n_owned_interior_faces;
     nb_ = m.n_faces - m.n_interior_faces;
     validate(m);
-    // Value index of every mesh cell: owned cells themselves, images their owned cell.
+    // Value index of every mesh cell: owned cells themselves, images their owned cell, external
+    // ghosts (ghost_owner -1: another rank's cell) records of their own after the owned cells'.
     std::vector<int> val(nc_);
     for (int c = 0; c < n_; ++c) val[c] = c;
+    for (int g = n_; g < nc_; ++g)
+      if (m.ghost_owner[g - n_] == -1) val[g] = n_ + n_ext_++;
+    nv_ = n_ + n_ext_;
     for (int g = n_; g < nc_; ++g) {
       const int o = m.ghost_owner[g - n_];
+      if (o == -1) continue;
       if (o < 0 || o >= n_) fail("E1101: a ghost cell's owner is not an owned cell");
       val[g] = o;
     }
@@ -2585,12 +2619,12 @@ class Impl final : public Stepper {
         // The other side: the owner for the neighbour's incidence and the reverse, or the face.
         const C* q = v >= 0 ? face.data() + static_cast<long long>(f) * kFace
                             : bface_host_.data() + static_cast<long long>(f - ni_) * kBface;
-        irec[4 * at + 3] = v >= 0 ? ((v & 1) ? q[7] : q[11]) : index_bits<C>(n_ + (f - ni_));
+        irec[4 * at + 3] = v >= 0 ? ((v & 1) ? q[7] : q[11]) : index_bits<C>(nv_ + (f - ni_));
         for (int a = 0; a < 4; ++a) idt[4 * at + a] = q[a];
       }
     }
     // Stencil of owned cells, sliced, each entry {w_x, w_y, w_z, record}: the record of a cell
-    // value (its value index) or of boundary face b's state (n + b).
+    // value (its value index) or of boundary face b's state (n + external ghosts + b).
     const bool has_stencil =
         m.stencil != nullptr && m.stencil_offsets != nullptr && m.stencil_lsq_weight != nullptr;
     std::vector<long long> soff(n_ + 1, 0);
@@ -2610,7 +2644,7 @@ class Impl final : public Stepper {
         } else {
           const int f = -e - 1;
           if (f < ni_ || f >= nf_) fail("E1101: a stencil entry is not a boundary face");
-          v = n_ + (f - ni_);  // the boundary state's record, after the cells' records
+          v = nv_ + (f - ni_);  // the boundary state's record, after the cells' records
         }
         C* q = ste.data() + 4 * st_.at(c, static_cast<int>(k - m.stencil_offsets[c]));
         for (int a = 0; a < 3; ++a) {
@@ -2638,9 +2672,10 @@ class Impl final : public Stepper {
       max_faces_ = std::max<int>(max_faces_, static_cast<int>(m.cell_face_offsets[c + 1] - m.cell_face_offsets[c]));
     // Device arrays.
     const size_t n5 = 5ULL * n_;
-    // each primitive buffer holds the owned cells' records, then the boundary faces' states
-    for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * (n_ + std::max(nb_, 1)) * sizeof(C));
-    recon_.alloc(static_cast<size_t>(kRecon) * n_ * sizeof(C));
+    // each primitive buffer holds the owned cells' records, the external ghosts', then the
+    // boundary faces' states; the reconstruction array the cells' and the external ghosts'
+    for (auto& b : prim_) b.alloc(static_cast<size_t>(kPrimW) * (nv_ + std::max(nb_, 1)) * sizeof(C));
+    recon_.alloc(static_cast<size_t>(kRecon) * nv_ * sizeof(C));
     u_.alloc(n5 * sizeof(double));
     stage_.alloc(n5 * sizeof(double));
     racc_.alloc(n5 * sizeof(double));
@@ -2672,9 +2707,9 @@ class Impl final : public Stepper {
     d_.n = n_;
     d_.nb = nb_;
     d_.n_if = nif_;
-    d_.prim_b = prim_[0].as<C>() + static_cast<long long>(kPrimW) * n_;
+    d_.prim_b = prim_[0].as<C>() + static_cast<long long>(kPrimW) * nv_;
     d_.recon = recon_.as<C>();
-    d_.rstride = static_cast<long long>(kGroup) * n_;
+    d_.rstride = static_cast<long long>(kGroup) * nv_;
     d_.u = u_.as<double>();
     d_.stage = stage_.as<double>();
     d_.racc = racc_.as<double>();
@@ -2706,6 +2741,7 @@ class Impl final : public Stepper {
     d_.cell_tiles = d_.face_tiles = d_.bface_tiles = nullptr;
     d_.n_cell_tiles = d_.n_face_tiles = d_.n_bface_tiles = 0;
     d_.wide_ok = (sizeof(C) == 4 && weights_in_range) ? 1 : 0;
+    wide_ok_mesh_ = d_.wide_ok;
     d_.stall_polls = 0;
     check(cudaMallocHost(reinterpret_cast<void**>(&head_), kControlHead), "cudaMallocHost");
     if (tuning_.face_mode != 0) ensure_flux_scratch();
@@ -2790,7 +2826,8 @@ class Impl final : public Stepper {
     check(cudaStreamSynchronize(stream), "download");
     for (int k = 0; k < 5; ++k)
       for (int g = n_; g < nc_; ++g)
-        host[k * static_cast<long long>(nc_) + g] = host[k * static_cast<long long>(nc_) + ghost_owner_[g - n_]];
+        if (ghost_owner_[g - n_] >= 0)  // an external ghost's entry is left as it is
+          host[k * static_cast<long long>(nc_) + g] = host[k * static_cast<long long>(nc_) + ghost_owner_[g - n_]];
   }
 
   // The primitives of the device state u_ into record buffer 0, where every step starts: a new
@@ -2810,6 +2847,7 @@ class Impl final : public Stepper {
   void download_state(double* u) override { copy_out(u_.as<double>(), u); }
 
   void residual(const double* u, double* res) override {
+    single_rank_only("residual");
     copy_in(u, stage_.as<double>());
     launch(k_store<P>, blocks(n_), kBlock, d_, static_cast<const double*>(stage_.as<double>()),
            prim_[1].as<C>());
@@ -2820,11 +2858,22 @@ class Impl final : public Stepper {
   }
 
   void evaluate(autan_euler_step_result* out) override {
+    need_ranks();
     launch(k_begin, 1, 256, d_.ctl, 1.0, static_cast<unsigned long long*>(nullptr));
-    enqueue_residual(0);
+    if (ranked()) {
+      halo(0, prim_[0].as<C>());
+      enqueue_cells(0, false, 0.0, false);
+      if (second_) halo(1, recon_.as<C>());
+      launch_faces(with_rec(0, 0), kResidual, 0, 0.0, 0.0, 0, 0);
+      last_rec_ = 0;
+      ++counters.residuals;
+    } else {
+      enqueue_residual(0);
+    }
     launch(k_norm_sums, norm_blocks(), kBlock, static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
            static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
-    launch(k_norm_finish, 1, 32, d_.ctl, n_, 0, 0);
+    if (ranked()) reduce_words(&d_.ctl->words[0][0], 5 * kWords, 0);
+    launch(k_norm_finish, 1, 32, d_.ctl, rms_cells(), 0, 0);
     // invalid(): the state, then the residual, marked on the device
     launch(k_invalid<P>, blocks(n_), kBlock, d_, static_cast<const double*>(u_.as<double>()),
            static_cast<const double*>(res_.as<double>()));
@@ -2843,6 +2892,8 @@ class Impl final : public Stepper {
     if (rk != 3 && rk != 4) fail("E1101: rk must be 3 or 4");
     if (n < 1) fail("E1101: n_steps must be positive");
     if (!(dt > 0.0) && !(cfl > 0.0)) fail("E1101: a positive dt or CFL is needed");
+    need_ranks();
+    if (ranked()) graph = false;  // the exchange callbacks run on the host between launches
     // Reset the step count so that the history holds this call's steps, and the fault word.
     check(cudaMemsetAsync(&d_.ctl->step, 0, sizeof(long long), stream), "reset");
     check(cudaMemsetAsync(&d_.ctl->fault, 0, sizeof(unsigned long long), stream), "reset");
@@ -2884,7 +2935,7 @@ class Impl final : public Stepper {
 
   void gradients(double* grad, double* phi) override {
     Buffer g(15ULL * n_ * sizeof(double)), f(5ULL * n_ * sizeof(double));
-    launch(k_unpack<P>, blocks(n_), kBlock, static_cast<const C*>(recon_.as<C>()), n_,
+    launch(k_unpack<P>, blocks(n_), kBlock, static_cast<const C*>(recon_.as<C>()), n_, d_.rstride,
            g.as<double>(), f.as<double>());
     if (grad != nullptr)
       check(cudaMemcpyAsync(grad, g.ptr(), 15ULL * n_ * 8, cudaMemcpyDeviceToHost, stream), "grad");
@@ -2894,6 +2945,7 @@ class Impl final : public Stepper {
   }
 
   void time_steps(double cfl, double* dt) override {
+    single_rank_only("time_steps");
     Buffer tmp(std::max(n_, 1) * sizeof(double));
     Dev<P> d = with_rec(0, 0);
     if (nb_ > 0) launch(k_boundary_states<P>, blocks(nb_), kBlock, d);
@@ -2907,6 +2959,7 @@ class Impl final : public Stepper {
   // milliseconds and the launches.
   void kernel_times(double cfl, double dt, bool local, int rk, long long n, double* ms,
                     long long* launches) override {
+    need_ranks();
     for (int k = 0; k < 6; ++k) {
       ms[k] = 0.0;
       launches[k] = 0;
@@ -2948,6 +3001,7 @@ class Impl final : public Stepper {
   // face mode 2 sums inside its gather). The state is restored after
   // every trial, so tuning leaves the solution unchanged. Returns the tuned ms per step.
   double autotune(double cfl, double dt, bool local, int rk, int trial_steps) override {
+    single_rank_only("autotune");
     if (trial_steps < 1) fail("E1101: trial_steps must be positive");
     Buffer saved(5ULL * n_ * sizeof(double));
     check(cudaMemcpyAsync(saved.ptr(), u_.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),
@@ -3173,7 +3227,7 @@ class Impl final : public Stepper {
       d.n_bface_tiles = n_bface_tiles_;
     }
     d.prim = prim_[in].as<C>();
-    d.prim_b = prim_[in].as<C>() + static_cast<long long>(kPrimW) * n_;  // this stage's boundary states
+    d.prim_b = prim_[in].as<C>() + static_cast<long long>(kPrimW) * nv_;  // this stage's boundary states
     d.prim_next = prim_[out].as<C>();
     return d;
   }
@@ -3245,6 +3299,7 @@ class Impl final : public Stepper {
   }
 
   void face_parts(const double* u, double* res_faces, double* face_flux) override {
+    single_rank_only("face_parts");
     prepare(u);
     enqueue_face_parts();
     if (res_faces != nullptr) {
@@ -3265,6 +3320,7 @@ class Impl final : public Stepper {
   }
 
   void boundary_pressure(const double* u, double* p, double* force) override {
+    single_rank_only("boundary_pressure");
     prepare(u);
     Buffer pb(std::max<size_t>(1, static_cast<size_t>(nb_)) * sizeof(double));
     Buffer fb(force != nullptr ? 3ULL * std::max(nb_, 1) * sizeof(double) : 0);
@@ -3280,6 +3336,7 @@ class Impl final : public Stepper {
   }
 
   int conservation(double* sums) override {
+    single_rank_only("conservation");
     prepare(nullptr);
     enqueue_face_parts();
     check(cudaMemsetAsync(cons_words_.ptr(), 0, cons_words_.bytes(), stream), "conservation");
@@ -3300,6 +3357,8 @@ class Impl final : public Stepper {
 
   // Batched cases: owned cells [cell_offsets[k], cell_offsets[k + 1]) form case k.
   void set_cases(int n_cases, const int64_t* off) override {
+    single_rank_only("set_cases");
+    if (ranked()) fail("E1101: ranks and batched cases do not go together");
     if (n_cases < 1 || off == nullptr) fail("E1101: at least one case and its cell offsets");
     if (off[0] != 0 || off[n_cases] != n_) fail("E1101: case offsets must span the owned cells");
     std::vector<int> case_of(std::max(n_, 1), 0);
@@ -3435,6 +3494,86 @@ class Impl final : public Stepper {
     if (polls < 0) fail("E1101: polls must be >= 0");
     d_.stall_polls = polls;
     drop_graph();
+  }
+
+  // ---- ranks of a partitioned mesh
+
+  long long external_ghosts() const override { return n_ext_; }
+
+  void set_ranks(const autan_euler_ranks* r) override {
+    drop_graph();
+    if (r == nullptr) {
+      ranks_ = autan_euler_ranks{};
+      send_cells_ = Buffer();
+      d_.wide_ok = wide_ok_mesh_;
+      return;
+    }
+    if (n_cases_ > 0) fail("E1101: ranks and batched cases do not go together");
+    if (r->exchange == nullptr || r->reduce == nullptr) fail("E1101: ranks need both callbacks");
+    if (r->n_send < 0 || (r->n_send > 0 && (r->send_cells == nullptr || r->send == nullptr)))
+      fail("E1101: a send list needs its cells and its buffer");
+    if (n_ext_ > 0 && r->recv == nullptr) fail("E1101: external ghosts need a receive buffer");
+    if (r->words == nullptr) fail("E1101: ranks need the reduction words");
+    auto misaligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; };
+    if (misaligned(r->send) || misaligned(r->recv) || misaligned(r->words))
+      fail("E1101: the exchange buffers must be 16-byte aligned");
+    if (!(r->global_cells >= static_cast<double>(n_))) fail("E1101: global_cells below the owned cells");
+    std::vector<int> cells(static_cast<size_t>(std::max<long long>(r->n_send, 1)), 0);
+    for (long long i = 0; i < r->n_send; ++i) {
+      if (r->send_cells[i] < 0 || r->send_cells[i] >= n_) fail("E1101: a send cell is not an owned cell");
+      cells[i] = r->send_cells[i];
+    }
+    send_cells_ = upload(cells, stream);
+    check(cudaStreamSynchronize(stream), "ranks");
+    ranks_ = *r;
+    d_.wide_ok = 0;
+  }
+
+  bool ranked() const { return ranks_.exchange != nullptr; }
+  double rms_cells() const { return ranked() ? ranks_.global_cells : static_cast<double>(n_); }
+
+  // An entry point that evaluates from a host state or tunes itself: owned cells only.
+  void single_rank_only(const char* what) const {
+    if (n_ext_ > 0) {
+      std::string m = "E1101: ";
+      m += what;
+      m += " is not available on a mesh with external ghosts";
+      fail(m.c_str());
+    }
+  }
+  // A step or evaluation of a mesh with external ghosts needs the ranks' exchange.
+  void need_ranks() const {
+    if (n_ext_ > 0 && !ranked())
+      fail("E1101: a mesh with external ghosts steps only with its ranks set");
+  }
+
+  // The forward ghost exchange of the primitive records in `prim` (what 0) or of the
+  // reconstruction array (what 1): pack the send cells' records, the exchange callback, unpack
+  // the external ghosts' records.
+  void halo(int what, C* base) {
+    const int groups = what == 0 ? 1 : kRecon / kGroup;
+    const long long gstride = what == 0 ? 0 : d_.rstride;
+    const long long per = static_cast<long long>(groups) * kGroup * static_cast<long long>(sizeof(C)) / 16;
+    if (ranks_.n_send > 0)
+      launch(k_halo_records<C, true>, blocks(ranks_.n_send * per), kBlock, base, gstride, groups,
+             static_cast<const int*>(send_cells_.as<int>()), static_cast<long long>(ranks_.n_send), 0,
+             static_cast<C*>(ranks_.send));
+    const long long bytes = static_cast<long long>(groups) * kGroup * static_cast<long long>(sizeof(C));
+    if (ranks_.exchange(ranks_.user, what, bytes, static_cast<void*>(stream)) != 0)
+      fail("E1301: the ranks' ghost exchange failed");
+    if (n_ext_ > 0)
+      launch(k_halo_records<C, false>, blocks(static_cast<long long>(n_ext_) * per), kBlock, base,
+             gstride, groups, static_cast<const int*>(nullptr), static_cast<long long>(n_ext_), n_,
+             static_cast<C*>(ranks_.recv));
+  }
+
+  // `count` words of the control block combined over the ranks in place (op 0 sum, 1 min).
+  void reduce_words(unsigned long long* dev, int count, int op) {
+    const size_t bytes = static_cast<size_t>(count) * sizeof(unsigned long long);
+    check(cudaMemcpyAsync(ranks_.words, dev, bytes, cudaMemcpyDeviceToDevice, stream), "ranks");
+    if (ranks_.reduce(ranks_.user, op, count, static_cast<void*>(stream)) != 0)
+      fail("E1301: the ranks' reduction failed");
+    check(cudaMemcpyAsync(dev, ranks_.words, bytes, cudaMemcpyDeviceToDevice, stream), "ranks");
   }
 
   // Calls body(flux, planar, second) with the scheme's compile-time choices.
@@ -3632,7 +3771,12 @@ class Impl final : public Stepper {
     for (int st = 0; st < stages; ++st) {
       const int in = k.rk == 3 ? in3[st] : in4[st];
       const int out = k.rk == 3 ? out3[st] : out4[st];
+      if (ranked()) halo(0, prim_[in].as<C>());
       enqueue_cells(in, st == 0 && cfl_dt, k.cfl, local);
+      if (ranked()) {
+        if (st == 0 && cfl_dt) reduce_words(&d_.ctl->dt_bits, 1, 1);
+        if (second_) halo(1, recon_.as<C>());
+      }
       const double wa = k.rk == 3 ? w3[st][0] : c4[st];
       const double wb = k.rk == 3 ? w3[st][1] : 0.0;
       launch_faces(with_rec(in, out), k.rk == 3 ? kRk3 : kRk4, st, wa, wb, local ? 1 : 0,
@@ -3657,7 +3801,8 @@ class Impl final : public Stepper {
                     static_cast<const double*>(res_.as<double>()), n_, d_.ctl,
                     static_cast<const int*>(nullptr), static_cast<const unsigned char*>(nullptr));
         }
-        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, n_, 1, n_cases_ == 0 ? 1 : 0);
+        if (ranked()) reduce_words(&d_.ctl->words[0][0], 5 * kWords, 0);
+        launch_as(kNorms, k_norm_finish, 1, 32, d_.ctl, rms_cells(), 1, n_cases_ == 0 ? 1 : 0);
         if (n_cases_ > 0)
           launch_as(kNorms, k_case_norm_finish, blocks(5LL * n_cases_, 128), 128,
                     case_words_.as<unsigned long long>(), static_cast<const double*>(case_cells_.as<double>()),
@@ -3696,6 +3841,13 @@ class Impl final : public Stepper {
   autan_euler_scheme scheme_;
   bool planar_, second_, limiter_;
   int nc_ = 0, n_ = 0, nf_ = 0, ni_ = 0, nif_ = 0, nb_ = 0;
+  int n_ext_ = 0, nv_ = 0;  // external ghosts; owned cells + external ghosts (value records)
+  // The ranks of a partitioned mesh (null exchange: one rank), the send list on the device and
+  // the widening choice of the mesh's own weights (off while ranks are set: the special-value word
+  // would not see the other ranks' records).
+  autan_euler_ranks ranks_{};
+  Buffer send_cells_;
+  int wide_ok_mesh_ = 0;
   Sliced st_, inc_;
   Dev<P> d_{};
   Buffer prim_[3];  // primitive records, rotated through the stages
@@ -4193,6 +4345,18 @@ int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t 
 
 int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len) {
   AUTAN_CALL({ h->set_stall_test(polls); });
+}
+
+int autan_euler_device_set_ranks(void* handle, const autan_euler_ranks* ranks, char* err,
+                                 size_t err_len) {
+  AUTAN_CALL({ h->set_ranks(ranks); });
+}
+
+int autan_euler_device_external_ghosts(void* handle, int64_t* count, char* err, size_t err_len) {
+  AUTAN_CALL({
+    if (count == nullptr) fail("E1101: null count");
+    *count = h->external_ghosts();
+  });
 }
 
 int autan_euler_device_sync(void* handle, char* err, size_t err_len) {

@@ -282,6 +282,43 @@ int autan_euler_device_march_cases(void* handle, double cfl, double dt, int32_t 
  * for the copies it has issued and stores nothing, and the step call returns E1201. 0 turns the
  * hook off; the handle stays usable either way. */
 int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, size_t err_len);
+
+/* One rank's share of a partitioned mesh (the reference's GhostFill / HaloExchange forward and
+ * Ranks::sum / min, partition/include/autan/partition/halo_exchange.hpp:14-66,
+ * physics/src/euler.cpp:96-136). The handle's mesh then holds external ghosts: ghost cells whose
+ * ghost_owner is -1, whose values another rank owns. Their records are filled by `exchange` at
+ * the start of every RK stage (primitives: what 0, 8 words a cell) and, second order, after its
+ * gradient loop (phi then grad: what 1, 24 words a cell; words of the precision's storage type,
+ * 4 bytes in fp32+acc64, 8 in fp64). Before each call the library has enqueued on `stream` the
+ * packing of the records of send_cells[0 .. n_send) into `send`, record after record; the
+ * callee leaves in `recv`, for the work the library enqueues on `stream` after the call returns,
+ * the records of the external ghosts in their order in the mesh. `reduce` combines `count` words
+ * at `words` over the ranks in place, for the work enqueued after it returns: op 0 the sum
+ * modulo 2^64 (the 5 x 71 exact-sum words of the stage-0 residual norms), op 1 the minimum as
+ * signed 64-bit integers (the bits of the CFL step, a positive double). The RMS norms divide by
+ * global_cells. Every rank makes the same calls in the same order. A callback's nonzero return
+ * fails the step call with E1301.
+ *
+ * With ranks set, step runs eagerly (no graph) and, with evaluate, is the only evaluation entry;
+ * residual, face_parts, boundary_pressure, conservation, autotune and batched cases are refused
+ * (E1101) on a mesh with external ghosts. invalid_cell stays a local cell; the Python driver
+ * (autan_b200/partition.py) reduces it to the least global id. NULL detaches the ranks. */
+struct autan_euler_ranks {
+  void* user;
+  int32_t (*exchange)(void* user, int32_t what, int64_t record_bytes, void* stream);
+  int32_t (*reduce)(void* user, int32_t op, int64_t count, void* stream);
+  void* send;                /* device, n_send x 24 words */
+  void* recv;                /* device, external ghosts x 24 words */
+  uint64_t* words;           /* device, at least 5 x 71 words */
+  int64_t n_send;
+  const int32_t* send_cells; /* n_send owned cells (host; copied), repeats allowed */
+  double global_cells;       /* owned cells over all ranks */
+};
+int autan_euler_device_set_ranks(void* handle, const struct autan_euler_ranks* ranks, char* err,
+                                 size_t err_len);
+/* The number of external ghosts of the handle's mesh. */
+int autan_euler_device_external_ghosts(void* handle, int64_t* count, char* err, size_t err_len);
+
 /* Waits for the handle's stream. */
 int autan_euler_device_sync(void* handle, char* err, size_t err_len);
 /* The handle's cudaStream_t. */

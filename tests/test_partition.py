@@ -1,0 +1,221 @@
+"""Partitioned meshes on CPU: every rank's local mesh restates its owned cells' loops of the
+global mesh entry for entry (the same faces, orientation, stencil entries, weights and geometry,
+in the same order), the halo plan delivers each external ghost its owning rank's record, and the
+exchange and reductions of the torch.distributed backend do so over two gloo ranks (the NCCL
+path's host logic)."""
+
+import datetime
+import multiprocessing as mp
+import os
+import socket
+import sys
+import threading
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from autan_b200 import mesh as M
+from autan_b200 import partition as PT
+
+REPO = Path(__file__).resolve().parent.parent
+
+
+def meshes():
+    return [
+        ("channel", M.bump_channel(24, 12, 4)),
+        ("tets", M.jittered_tets(8, 8, 2, extent=(1.0, 1.0, 0.25))),
+        ("hex", M.periodic_box_hex(8, 8, 2)),
+    ]
+
+
+def random_parts(m, n_parts, seed):
+    rng = np.random.default_rng(seed)
+    parts = rng.integers(0, n_parts, m.n_owned_cells).astype(np.int32)
+    parts[:n_parts] = np.arange(n_parts)  # none empty
+    return parts
+
+
+def check_partition(m, w, p):
+    L = p.mesh
+    cg, fg = p.cell_global, p.face_global
+    no, ni_l = p.n_owned, L["n_interior_faces"]
+    home = np.concatenate((np.arange(m.n_owned_cells), m.ghost_owner))
+    # owned cells in global order, every one owned by this rank
+    assert np.all(np.diff(cg[:no]) > 0)
+    # faces: geometry and orientation of the global faces
+    assert np.array_equal(cg[L["owner"]], m.owner[fg])
+    assert np.array_equal(cg[L["neighbour"]], m.neighbour[fg[:ni_l]])
+    assert np.array_equal(L["face_normal"], m.face_normal[:, fg])
+    assert np.array_equal(L["face_centroid"], m.face_centroid[:, fg])
+    assert np.array_equal(L["face_area_magnitude"], m.face_area_magnitude[fg])
+    assert np.array_equal(L["cell_centroid"], m.cell_centroid[:, cg])
+    assert np.all(fg[:ni_l] < m.n_owned_interior_faces)
+    assert np.all(fg[ni_l:] >= m.n_interior_faces)
+    # each owned cell: its faces and stencil entries, in the global order
+    cfo, so = L["cell_face_offsets"], L["stencil_offsets"]
+    gcfo, gso = m.cell_face_offsets, m.stencil_offsets
+    for c in range(no):
+        g = cg[c]
+        lf = L["cell_faces"][cfo[c] : cfo[c + 1]]
+        assert np.array_equal(fg[lf], m.cell_faces[gcfo[g] : gcfo[g + 1]])
+        assert np.all(np.diff(lf) > 0)
+        ls = L["stencil"][so[c] : so[c + 1]]
+        gs = m.stencil[gso[g] : gso[g + 1]]
+        back = np.where(ls >= 0, cg[np.maximum(ls, 0)], -(fg[np.maximum(-ls - 1, 0)] + 1))
+        assert np.array_equal(back, gs)
+        assert np.array_equal(p.weights[:, so[c] : so[c + 1]], w[:, gso[g] : gso[g + 1]])
+    # ghosts: external first, by source rank then global cell; images of this rank's cells after
+    gown = L["ghost_owner"]
+    assert np.all(gown[: p.n_external] == -1)
+    assert np.all(gown[p.n_external :] >= 0) and np.all(gown[p.n_external :] < no)
+    assert np.array_equal(cg[gown[p.n_external :]], home[cg[no + p.n_external :]])
+    return home
+
+
+@pytest.mark.parametrize("how", ["blocks", "random"])
+@pytest.mark.parametrize("n_parts", [2, 3, 5])
+def test_local_meshes_restate_the_global_loops(how, n_parts):
+    for name, m in meshes():
+        w = m.gradient_weights(np.full(m.n_boundary_faces, M.BC_SLIP, np.uint8))
+        parts = PT.partition_cells(m, n_parts) if how == "blocks" else random_parts(m, n_parts, 7)
+        ps = PT.extract_partitions(m, w, parts)
+        assert sum(p.n_owned for p in ps) == m.n_owned_cells
+        owned = np.concatenate([p.cell_global[: p.n_owned] for p in ps])
+        assert np.array_equal(np.sort(owned), np.arange(m.n_owned_cells))
+        for p in ps:
+            home = check_partition(m, w, p)
+            ext = p.cell_global[p.n_owned : p.n_owned + p.n_external]
+            r = parts[home[ext]]
+            assert np.all(r != p.rank)
+            assert np.all(np.diff(r) >= 0)  # grouped by source rank
+            assert np.array_equal(np.bincount(r, minlength=n_parts), p.recv_counts)
+        # the halo plan: what each rank sends is what its receivers' ghosts hold
+        for q in ps:
+            got = []
+            for r in ps:
+                first = int(r.send_counts[: q.rank].sum())
+                cells = r.send_cells[first : first + int(r.send_counts[q.rank])]
+                assert int(q.recv_counts[r.rank]) == cells.size
+                got.append(r.cell_global[cells])
+            ext = q.cell_global[q.n_owned : q.n_owned + q.n_external]
+            home = np.concatenate((np.arange(m.n_owned_cells), m.ghost_owner))
+            assert np.array_equal(np.concatenate(got), home[ext]), name
+
+
+def test_blocks_balance_the_face_cost():
+    m = M.bump_channel(48, 24, 4)
+    parts = PT.partition_cells(m, 4)
+    cost = PT.cell_cost(m)
+    share = np.array([cost[parts == r].sum() for r in range(4)]) / cost.sum()
+    assert np.all(np.abs(share - 0.25) < 0.01)
+    assert np.all(np.diff(parts) >= 0)
+
+
+class _Member:
+    """One rank's exchange buffers on the host, standing in for a stepper."""
+
+    def __init__(self, part):
+        self.part = part
+        self.buf = PT._Buffers(part, 4, "cpu")
+
+
+def _fill_and_check(member, ranks, m, record_bytes, stream=None):
+    """Pack each sent cell's global home id into its record, exchange, and check every external
+    ghost's record; then a sum and a min of the words over the ranks."""
+    import torch
+
+    p = member.part
+    home = np.concatenate((np.arange(m.n_owned_cells), m.ghost_owner))
+    rows = member.buf.send_rows(int(p.send_cells.size), record_bytes)
+    ids = p.cell_global[p.send_cells].astype(np.int64)
+    rec = np.zeros((ids.size, record_bytes // 8), dtype=np.int64)
+    rec[:, 0] = ids
+    rec[:, -1] = p.rank
+    rows.copy_(torch.from_numpy(rec.view(np.uint8).reshape(ids.size, record_bytes)))
+    ranks.exchange(member, 0, record_bytes, stream)
+    got = member.buf.recv_rows(p.n_external, record_bytes).numpy().copy().view(np.int64)
+    ext = p.cell_global[p.n_owned : p.n_owned + p.n_external]
+    assert np.array_equal(got[:, 0], home[ext])
+    member.buf.words[:5].copy_(torch.tensor([p.rank + 1, -1, 2**62, 7 * p.rank, 3 - p.rank]))
+    ranks.reduce(member, 0, 5, stream)
+    n = p.n_parts
+    want = [n * (n + 1) // 2, -n, (n * 2**62 + 2**63) % 2**64 - 2**63, 7 * n * (n - 1) // 2,
+            sum(3 - r for r in range(n))]  # fmt: skip
+    assert member.buf.words[:5].tolist() == want
+    member.buf.words[:2].copy_(torch.tensor([10 + p.rank, 4 - p.rank]))
+    ranks.reduce(member, 1, 2, stream)
+    assert member.buf.words[:2].tolist() == [10, 4 - (n - 1)]
+    assert ranks.min_host(member, 100 - p.rank) == 100 - (n - 1)
+
+
+@pytest.mark.parametrize("record_bytes", [32, 96])
+def test_thread_ranks_exchange_and_reduce_on_host(record_bytes):
+    m = M.jittered_tets(8, 8, 2, extent=(1.0, 1.0, 0.25))
+    ps = PT.extract_partitions(m, None, random_parts(m, 3, 1))
+    ranks = PT.ThreadRanks(3, timeout=60)
+    members = [_Member(p) for p in ps]
+    for mb in members:
+        ranks.join(mb)
+    errors = []
+
+    def run(mb):
+        try:
+            _fill_and_check(mb, ranks, m, record_bytes)
+        except BaseException as e:  # noqa: BLE001 (reported below)
+            errors.append(e)
+            ranks.barrier.abort()
+
+    threads = [threading.Thread(target=run, args=(mb,)) for mb in members]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=120)
+    assert not errors, errors
+
+
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _torch_rank(rank: int, world: int, port: int, out) -> None:
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, str(REPO))
+    import torch.distributed as dist
+
+    from autan_b200 import mesh as M2
+    from autan_b200 import partition as PT2
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))  # fmt: skip
+    try:
+        m = M2.bump_channel(24, 12, 4)
+        parts = PT2.partition_cells(m, world)
+        (p,) = PT2.extract_partitions(m, None, parts, ranks=[rank])
+        ranks = PT2.TorchRanks()
+        member = _Member(p)
+        for rb in (32, 96):
+            _fill_and_check(member, ranks, m, rb)
+        dist.barrier()
+        out.put((rank, "ok"))
+    except BaseException as e:  # noqa: BLE001
+        out.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_torch_ranks_exchange_and_reduce_gloo():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_torch_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted(out.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert got == [(0, "ok"), (1, "ok")]
