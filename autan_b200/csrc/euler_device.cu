@@ -3001,7 +3001,7 @@ class Impl final : public Stepper {
   // face mode 2 sums inside its gather). The state is restored after
   // every trial, so tuning leaves the solution unchanged. Returns the tuned ms per step.
   double autotune(double cfl, double dt, bool local, int rk, int trial_steps) override {
-    single_rank_only("autotune");
+    need_ranks();  // with ranks, every rank tunes together: the trials make the same exchanges
     if (trial_steps < 1) fail("E1101: trial_steps must be positive");
     Buffer saved(5ULL * n_ * sizeof(double));
     check(cudaMemcpyAsync(saved.ptr(), u_.ptr(), saved.bytes(), cudaMemcpyDeviceToDevice, stream),

@@ -491,6 +491,17 @@ class PartitionedEuler:
     def history(self, count: int):
         return self.dev.history(count)
 
+    def autotune(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
+                 trial_steps: int = 2) -> tuple[dict, float]:  # fmt: skip
+        """The autotuner on this rank's mesh. Every rank calls it together: its trials step and
+        so exchange; each rank keeps its own fastest choices (no result depends on them)."""
+        return self._native(lambda: self.dev.autotune(cfl, dt, local, rk, trial_steps))
+
+    def kernel_times(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
+                     n_steps: int = 1) -> dict:  # fmt: skip
+        """EulerDevice.kernel_times of this rank (every rank calls it together)."""
+        return self._native(lambda: self.dev.kernel_times(cfl, dt, local, rk, n_steps))
+
     def close(self) -> None:
         if getattr(self, "dev", None) is not None:
             try:

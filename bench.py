@@ -857,6 +857,117 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_partitioned(args, rank: int, world: int, local_rank: int) -> None:
+    """One mesh over the ranks (strong scaling): each rank steps its partition (consecutive runs
+    of the mesh's cell order, equal face cost), the ghosts' primitive and reconstruction records
+    exchanged every RK stage and the norms' exact-sum words and the CFL step's minimum reduced,
+    through NCCL (TorchRanks) under torchrun; one rank steps the whole mesh through the same path
+    (ThreadRanks of one, no ghosts). Device time of the timed steps, max over ranks; the value is
+    the whole mesh's cells times the steps over that time."""
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from autan_b200 import cases
+    from autan_b200 import partition as PT
+
+    if args.workload == "channel":
+        case = cases.bump_channel(*(int(v) for v in args.channel.split(",")))
+    elif args.workload == "tets":
+        case = cases.vortex_tets(*(int(v) for v in args.lattice.split(",")), precision="fp32+acc64")
+    else:
+        raise SystemExit("--partitioned takes --workload channel or tets")
+    weights = case.mesh.gradient_weights(case.bc_kind)
+    parts = PT.partition_cells(case.mesh, world)
+    (part,) = PT.extract_partitions(case.mesh, weights, parts, ranks=[rank])
+    ranks = PT.TorchRanks() if dist is not None else PT.ThreadRanks(1)
+    mb = PT.PartitionedEuler(part, case.scheme, ranks, case.bc_kind, case.bc_data,
+                             device=local_rank)  # fmt: skip
+    mb.upload(case.u0)
+    if args.tuning:
+        mb.dev.set_tuning(**dict(zip(mb.dev.TUNING_KEYS, (int(v) for v in args.tuning.split(",")))))
+        tuned = mb.dev.tuning()
+    else:
+        tuned, _ = mb.autotune(cfl=case.cfl, rk=case.rk, local=case.local, trial_steps=2)
+        mb.upload(case.u0)
+    stream = torch.cuda.ExternalStream(mb.dev.stream)
+    mb.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    launches0 = mb.dev.counters()["launches"]
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clock_sampler(gpu_uuid(local_rank)) as clocks:
+        start.record(stream)
+        r = mb.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=args.steps)
+        end.record(stream)
+        end.synchronize()
+    barrier()
+    launches = mb.dev.counters()["launches"] - launches0
+    ms = reduce_max(start.elapsed_time(end), dist, "cuda")
+    n_global = case.mesh.n_owned_cells
+    value = n_global * args.steps / (ms * 1e-3)
+    if r.invalid_cell is not None:
+        raise RuntimeError(f"invalid state at cell {r.invalid_cell}")
+    # end to end: the rank's local state in from pinned host memory and out every step
+    nl = part.mesh["n_cells"]
+    u_host = torch.empty((5, nl), dtype=torch.float64, pin_memory=True).numpy()
+    mb.dev.download(out=u_host)
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        mb.dev.upload(u_host)
+        mb.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=1)
+        mb.dev.download(out=u_host)
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, "cuda")
+    ghosts = reduce_sum(float(part.n_external), dist, "cuda")
+    word = 4 if case.scheme.precision == "fp32+acc64" else 8
+    stages = 3 if case.rk == 3 else 4
+    line = {
+        "metric": "cell-iterations/s",
+        "value": value,
+        "unit": "cell-iterations/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32 (f64 accumulation)" if word == 4 else "f64",
+        "data": "synthetic",
+        "config": dict(workload_config(args), parallelism=f"partitioned x{world}",
+                       partition="consecutive runs of the cell order, equal face cost",
+                       external_ghosts_all_ranks=int(ghosts),
+                       exchange_bytes_per_step_all_ranks=int(ghosts) * stages * 32 * word,
+                       tuning_rank0=tuned),  # fmt: skip
+        "e2e": {"value": n_global * e2e_steps / e2e_s, "unit": "cell-iterations/s",
+                "h2d_bytes_per_step": 40 * part.n_owned, "d2h_bytes_per_step": 40 * part.n_owned,
+                "note": "per rank, its local state through the C ABI every step"},  # fmt: skip
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "residual_rms": list(map(float, r.residuals)),
+    }
+    mb.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant kernel
 # kind, averaged over a step's launches, from one ncu capture per mesh family on a smaller case
 # of that family (its summary is under profiles/): (kernel kind, mesh family) -> (bytes per
@@ -927,6 +1038,9 @@ def main() -> None:
                     help="with --warmstart: take the network from this .npz instead of training")
     ap.add_argument("--error-steps", type=int, default=100,
                     help="steps of the fp32+acc64 against fp64 comparison (0: skip)")
+    ap.add_argument("--partitioned", action="store_true",
+                    help="one mesh partitioned over the ranks (strong scaling; ghost exchange "
+                         "through NCCL under torchrun), channel or tets")  # fmt: skip
     ap.add_argument("--profile", action="store_true",
                     help="warm-up, then --steps eager steps only (for ncu)")
     args = ap.parse_args()
@@ -949,6 +1063,8 @@ def main() -> None:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.partitioned:
+        run_partitioned(args, rank, world, local_rank)
     else:
         run_ours(args, rank, world, local_rank)
 

@@ -18,8 +18,9 @@
  * cell first; boundary faces after the interior ones; cell_faces per cell in increasing face
  * index. Ghost cells are periodic images of owned cells (a one-rank partition with self-exchange,
  * partition/src/self_exchange.cpp:15-30): ghost g takes the values of owned cell ghost_owner[g].
- * The device holds owned cells only and reads an image's values at its owned cell, so no ghost
- * fill runs.
+ * The device reads an image's values at its owned cell, so no ghost fill runs for images. On a
+ * rank of a partitioned mesh, a ghost with ghost_owner -1 is external: another rank owns it, and
+ * the ranks' exchange fills its records (autan_euler_device_set_ranks).
  *
  * Not thread-safe per handle; distinct handles may run concurrently. Every call is ordered on the
  * handle's stream; calls that return host data synchronise it. */
@@ -118,7 +119,8 @@ int autan_euler_device_set_source(void* handle, const double* source, char* err,
 int autan_euler_device_set_second_order(void* handle, int32_t on, char* err, size_t err_len);
 
 /* DeviceStepper<P>::upload / download (euler_device.hpp:39-40): the FP64 conserved state,
- * 5 x n_cells (ghost entries ignored on upload, written as their owned cell's on download). */
+ * 5 x n_cells (ghost entries ignored on upload; on download an image's written as its owned
+ * cell's, an external ghost's left as they are). */
 int autan_euler_device_upload(void* handle, const double* u, char* err, size_t err_len);
 int autan_euler_device_download(void* handle, double* u, char* err, size_t err_len);
 
@@ -299,10 +301,13 @@ int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, si
  * global_cells. Every rank makes the same calls in the same order. A callback's nonzero return
  * fails the step call with E1301.
  *
- * With ranks set, step runs eagerly (no graph) and, with evaluate, is the only evaluation entry;
- * residual, face_parts, boundary_pressure, conservation, autotune and batched cases are refused
- * (E1101) on a mesh with external ghosts. invalid_cell stays a local cell; the Python driver
- * (autan_b200/partition.py) reduces it to the least global id. NULL detaches the ranks. */
+ * With ranks set, step runs eagerly (no graph); step, evaluate, kernel_times, march and autotune
+ * make the exchanges, so every rank calls them together (autotune's trials are the same on every
+ * rank; each rank keeps its own fastest choices, which change no result). residual, time_steps,
+ * face_parts, boundary_pressure, conservation and batched cases are refused (E1101) on a mesh
+ * with external ghosts, and every entry that steps is refused there until ranks are set.
+ * invalid_cell stays a local cell; the Python driver (autan_b200/partition.py) reduces it to the
+ * least global id. NULL detaches the ranks. */
 struct autan_euler_ranks {
   void* user;
   int32_t (*exchange)(void* user, int32_t what, int64_t record_bytes, void* stream);

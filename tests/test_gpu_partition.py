@@ -194,7 +194,9 @@ def test_a_failed_exchange_fails_the_step_with_its_cause():
         with pytest.raises(NativeError, match="E1101"):
             mb.dev.residual(np.zeros((5, p.mesh["n_cells"])))
         with pytest.raises(NativeError, match="E1101"):
-            mb.dev.autotune(case.cfl, 0.0, case.local, case.rk)
+            mb.dev.face_parts()
+        with pytest.raises(NativeError, match="E1101"):
+            mb.dev.time_steps(case.cfl)
     finally:
         mb.close()
 
@@ -212,3 +214,64 @@ def test_a_mesh_with_external_ghosts_needs_its_ranks():
         d.upload(case.u0[:, p.cell_global])
         with pytest.raises(NativeError, match="E1101"):
             d.step(case.cfl, 0.0, case.local, case.rk, 1)
+
+
+def test_partitioned_full_size_lattice():
+    """The 2 073 600-cell tetrahedral vortex on four ranks: two steps, the whole mesh's bits (the
+    ghost records' indices and the exchange buffers at a production size)."""
+    case = K.vortex_tets(240, 240, 6, precision="fp32+acc64")
+    m = case.mesh
+    assert m.n_owned_cells == 2_073_600
+    weights = m.gradient_weights(case.bc_kind)
+    check_same(case, weights, case.u0, PT.partition_cells(m, 4), 2)
+
+
+def _nccl_one_rank(port, out):
+    import datetime
+    import os
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    try:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=60))  # fmt: skip
+        case = CASES["channel"]("fp32+acc64")
+        m = case.mesh
+        weights = m.gradient_weights(case.bc_kind)
+        u0 = perturbed(case, 1e-3, 3)
+        ref_state, ref_r, ref_rms, *_ = whole(case, weights, u0, 3)
+        (p,) = PT.extract_partitions(m, weights, np.zeros(m.n_owned_cells, np.int32))
+        mb = PT.PartitionedEuler(p, case.scheme, PT.TorchRanks(), case.bc_kind, case.bc_data)
+        mb.upload(u0)
+        r = mb.step(case.cfl, 0.0, case.local, case.rk, 3)
+        rms, _ = mb.history(3)
+        ok = same_bits(mb.download(), ref_state) and same_bits(rms, ref_rms)
+        ok = ok and same_bits(r.residuals, ref_r.residuals)
+        mb.close()
+        dist.destroy_process_group()
+        out.put("ok" if ok else "different bits")
+    except BaseException as e:  # noqa: BLE001
+        out.put(repr(e))
+
+
+def test_torch_ranks_on_nccl_streams():
+    """The NCCL backend's reductions on the stepper's stream (a group of one rank: the norms and
+    the step pass through NCCL all-reduces between the step's launches)."""
+    import multiprocessing as mp
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    proc = ctx.Process(target=_nccl_one_rank, args=(port, out))
+    proc.start()
+    got = out.get(timeout=300)
+    proc.join(timeout=60)
+    assert got == "ok"
+    assert proc.exitcode == 0
