@@ -34,6 +34,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -2264,8 +2265,13 @@ struct Failure : std::runtime_error {
 
 [[noreturn]] void fail(const std::string& what) { throw Failure(what); }
 
+// A failed CUDA call: the runtime's (non-sticky) last-error state is cleared before reporting, so
+// that the next launch's check sees that launch's own result.
 void check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) fail(std::string("E1200: ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    fail(std::string("E1200: ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 
 class Buffer {
@@ -2483,6 +2489,9 @@ class Stepper {
   virtual int n_cases() const = 0;
   virtual void set_stall_test(int polls) = 0;
   virtual void set_ranks(const autan_euler_ranks* ranks) = 0;
+  // Whether any rank has `mine` set (this rank's alone without ranks): a stop every rank of a
+  // partitioned march takes together.
+  virtual bool any_rank(bool mine) = 0;
   virtual long long external_ghosts() const = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -3199,16 +3208,38 @@ class Impl final : public Stepper {
   template <class K, class... A>
   void launch_smem(int kind, K kernel, int grid, int block, size_t smem, A... args) {
     cudaEvent_t before = nullptr, after = nullptr;
-    if (smem > 48 * 1024)
+    if (smem > 48 * 1024) {
+      // The kernel's dynamic shared-memory limit raised to the device's opt-in maximum less its
+      // static shared memory, the same value from every handle and thread: a limit set to each
+      // launch's own size would race with another handle's launch of the same kernel at a larger
+      // size.
+      if (smem_optin_ == 0) {
+        int dev = 0;
+        check(cudaGetDevice(&dev), "device");
+        check(cudaDeviceGetAttribute(&smem_optin_, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+              "device");
+      }
+      cudaFuncAttributes fa{};
+      check(cudaFuncGetAttributes(&fa, kernel), "shared memory");
+      const long long limit =
+          static_cast<long long>(smem_optin_) - static_cast<long long>(fa.sharedSizeBytes);
+      if (static_cast<long long>(smem) > limit) fail("E1200: shared memory above the device's limit");
       check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)), "shared memory");
+                                 static_cast<int>(limit)), "shared memory");
+    }
     if (timing_) {
       check(cudaEventCreate(&before), "event");
       check(cudaEventCreate(&after), "event");
       check(cudaEventRecord(before, stream), "event");
     }
     kernel<<<grid, block, smem, stream>>>(args...);
-    check(cudaGetLastError(), "kernel launch");
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      char what[160];
+      std::snprintf(what, sizeof(what), "kernel launch (kind %d, grid %d, block %d, %zu bytes shared)",
+                    kind, grid, block, smem);
+      check(e, what);
+    }
     ++counters.launches;
     if (timing_) {
       check(cudaEventRecord(after, stream), "event");
@@ -3530,6 +3561,24 @@ class Impl final : public Stepper {
   }
 
   bool ranked() const { return ranks_.exchange != nullptr; }
+
+  // The CUDA runtime's last-error state after a ranks' callback: an error the callee's own CUDA
+  // calls left there (a communication library may leave one it has handled) is the callee's to
+  // report through its return code, and must not be read as the failure of the library's next
+  // launch. Sticky errors (a faulted context) stay visible to every later call.
+  static void drop_callee_error() { (void)cudaGetLastError(); }
+
+  bool any_rank(bool mine) override {
+    if (!ranked()) return mine;
+    long long word = mine ? 0 : 1;  // the minimum over the ranks is 0 where any rank has it set
+    check(cudaMemcpyAsync(ranks_.words, &word, sizeof(word), cudaMemcpyHostToDevice, stream), "ranks");
+    const int32_t rc = ranks_.reduce(ranks_.user, 1, 1, static_cast<void*>(stream));
+    drop_callee_error();
+    if (rc != 0) fail("E1301: the ranks' reduction failed");
+    check(cudaMemcpyAsync(&word, ranks_.words, sizeof(word), cudaMemcpyDeviceToHost, stream), "ranks");
+    check(cudaStreamSynchronize(stream), "ranks");
+    return word == 0;
+  }
   double rms_cells() const { return ranked() ? ranks_.global_cells : static_cast<double>(n_); }
 
   // An entry point that evaluates from a host state or tunes itself: owned cells only.
@@ -3559,8 +3608,9 @@ class Impl final : public Stepper {
              static_cast<const int*>(send_cells_.as<int>()), static_cast<long long>(ranks_.n_send), 0,
              static_cast<C*>(ranks_.send));
     const long long bytes = static_cast<long long>(groups) * kGroup * static_cast<long long>(sizeof(C));
-    if (ranks_.exchange(ranks_.user, what, bytes, static_cast<void*>(stream)) != 0)
-      fail("E1301: the ranks' ghost exchange failed");
+    const int32_t rc = ranks_.exchange(ranks_.user, what, bytes, static_cast<void*>(stream));
+    drop_callee_error();
+    if (rc != 0) fail("E1301: the ranks' ghost exchange failed");
     if (n_ext_ > 0)
       launch(k_halo_records<C, false>, blocks(static_cast<long long>(n_ext_) * per), kBlock, base,
              gstride, groups, static_cast<const int*>(nullptr), static_cast<long long>(n_ext_), n_,
@@ -3571,8 +3621,9 @@ class Impl final : public Stepper {
   void reduce_words(unsigned long long* dev, int count, int op) {
     const size_t bytes = static_cast<size_t>(count) * sizeof(unsigned long long);
     check(cudaMemcpyAsync(ranks_.words, dev, bytes, cudaMemcpyDeviceToDevice, stream), "ranks");
-    if (ranks_.reduce(ranks_.user, op, count, static_cast<void*>(stream)) != 0)
-      fail("E1301: the ranks' reduction failed");
+    const int32_t rc = ranks_.reduce(ranks_.user, op, count, static_cast<void*>(stream));
+    drop_callee_error();
+    if (rc != 0) fail("E1301: the ranks' reduction failed");
     check(cudaMemcpyAsync(dev, ranks_.words, bytes, cudaMemcpyDeviceToDevice, stream), "ranks");
   }
 
@@ -3842,6 +3893,7 @@ class Impl final : public Stepper {
   bool planar_, second_, limiter_;
   int nc_ = 0, n_ = 0, nf_ = 0, ni_ = 0, nif_ = 0, nb_ = 0;
   int n_ext_ = 0, nv_ = 0;  // external ghosts; owned cells + external ghosts (value records)
+  int smem_optin_ = 0;      // the device's opt-in shared memory per block (queried on first use)
   // The ranks of a partitioned mesh (null exchange: one rank), the send list on the device and
   // the widening choice of the mesh's own weights (off while ranks are set: the special-value word
   // would not see the other ranks' records).
@@ -3951,7 +4003,8 @@ void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_
   check(cudaEventCreate(&t1), "event");
   check(cudaEventRecord(t0, h->stream), "event");
   long long taken = 0;
-  while (taken < max_steps && !res.converged && res.invalid_cell < 0) {
+  bool invalid = false;  // on any rank of a partitioned mesh
+  while (taken < max_steps && !res.converged && !invalid) {
     const long long n = std::min<long long>(batch, max_steps - taken);
     autan_euler_step_result r{};
     h->step(cfl, dt, local, rk, n, true, &r);
@@ -3968,6 +4021,7 @@ void march(Stepper* h, double cfl, double dt, bool local, int rk, long long max_
     }
     taken += n;
     res.invalid_cell = r.invalid_cell;
+    invalid = h->any_rank(r.invalid_cell >= 0);
   }
   check(cudaEventRecord(t1, h->stream), "event");
   check(cudaEventSynchronize(t1), "event");

@@ -36,8 +36,30 @@ struct Failure : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 [[noreturn]] void fail(const std::string& what) { throw Failure(what); }
+// A failed CUDA call: the runtime's (non-sticky) last-error state is cleared before reporting, so
+// that the next launch's check sees that launch's own result.
 void check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) fail(std::string("E1300: ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    fail(std::string("E1300: ") + what + ": " + cudaGetErrorString(e));
+  }
+}
+
+// Allows `kernel` launches with up to `bytes` of dynamic shared memory: its limit raised to the
+// device's opt-in maximum less the kernel's static shared memory, the same value from every
+// handle and thread (a limit set to each
+// launch's own size would race with another handle's launch of the same kernel at a larger size).
+template <class K>
+void allow_smem(K kernel, size_t bytes) {
+  int dev = 0, optin = 0;
+  check(cudaGetDevice(&dev), "device");
+  check(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device");
+  cudaFuncAttributes fa{};
+  check(cudaFuncGetAttributes(&fa, kernel), "smem");
+  const long long limit = static_cast<long long>(optin) - static_cast<long long>(fa.sharedSizeBytes);
+  if (static_cast<long long>(bytes) > limit) fail("E1300: shared memory above the device's limit");
+  check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(limit)), "smem");
 }
 
 constexpr int kMaxWidth = 128;
@@ -745,15 +767,13 @@ class Net {
       ensure(wfull_, static_cast<size_t>(size) * 4);
       if (tc_) {
         const size_t smem = static_cast<size_t>(kTcRows + Ly.kp) * kTcRows * 2;
-        check(cudaFuncSetAttribute(k_tc_gemm<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(smem)), "smem");
+        allow_smem(k_tc_gemm<1, false>, smem);
         k_tc_gemm<1, false><<<chunks, 128, smem, stream_>>>(
             dzb_.as<bf16>(), Ly.np, rows, kTcRows, a_prev, lda, Ly.kp, Ly.np, nullptr, nullptr, 0,
             nullptr, partial_.as<float>(), 0, tmem_cols(Ly.kp), fault_.as<unsigned int>());
       } else {
         if (!wgrad_attr_) {
-          check(cudaFuncSetAttribute(k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgradSmem),
-                "smem");
+          allow_smem(k_wgrad, kWgradSmem);
           wgrad_attr_ = true;
         }
         k_wgrad<<<chunks, 256, kWgradSmem, stream_>>>(dzb_.as<bf16>(), Ly.np, a_prev, lda, rows, Ly.np,
@@ -831,10 +851,8 @@ class Net {
   }
   void fused_attrs() {
     if (fused_attr_) return;
-    check(cudaFuncSetAttribute(fused::k_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               fused::kSmem), "smem");
-    check(cudaFuncSetAttribute(fused::k_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               fused::kSmem), "smem");
+    allow_smem(fused::k_fused<true>, fused::kSmem);
+    allow_smem(fused::k_fused<false>, fused::kSmem);
     fused_attr_ = true;
   }
 
@@ -963,8 +981,7 @@ class Net {
                     const float* bias, float* Z, int ldz, bf16* Y, float* Yf, int ldy) {
     if (tc_) {
       const size_t smem = static_cast<size_t>(kTcRows + N) * K * 2;
-      check(cudaFuncSetAttribute(k_tc_gemm<0, ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)), "smem");
+      allow_smem(k_tc_gemm<0, ACT>, smem);
       k_tc_gemm<0, ACT><<<blocks(M, kTcRows), 128, smem, stream_>>>(A, lda, M, K, B, ldb, N, N, bias,
                                                                    Z, ldz, Y, Yf, ldy, tmem_cols(N),
                                                                    fault_.as<unsigned int>());
@@ -973,8 +990,7 @@ class Net {
     }
     const size_t smem = static_cast<size_t>(kRowsPerBlock + N) * (K + 8) * 2;
     if (smem > 48 * 1024)
-      check(cudaFuncSetAttribute(k_dense<ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(smem)), "smem");
+      allow_smem(k_dense<ACT>, smem);
     k_dense<ACT><<<blocks(M, kRowsPerBlock), 128, smem, stream_>>>(A, lda, M, K, B, ldb, N, bias, Z,
                                                                   ldz, Y, Yf, ldy);
     check(cudaGetLastError(), "dense");

@@ -36,8 +36,13 @@ struct Failure : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 [[noreturn]] void fail(const std::string& what) { throw Failure(what); }
+// A failed CUDA call: the runtime's (non-sticky) last-error state is cleared before reporting, so
+// that the next launch's check sees that launch's own result.
 void check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) fail(std::string("E1300: ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    fail(std::string("E1300: ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 
 // Status words of a set-up: [0] cells whose candidates overflowed the buffer, [1] cells whose

@@ -288,6 +288,8 @@ class ThreadRanks:
             s.synchronize()
 
     def exchange(self, member, what: int, record_bytes: int, stream) -> None:
+        if self.n == 1:
+            return  # one rank: no ghost of another rank, nothing to wait for
         s = self._stream(stream)
         self._sync(s)  # the packing
         self.barrier.wait()
@@ -308,6 +310,8 @@ class ThreadRanks:
         self.barrier.wait()  # nobody packs again while a peer still reads its buffer
 
     def reduce(self, member, op: int, count: int, stream) -> None:
+        if self.n == 1:
+            return  # the sum and the minimum over one rank are its own words
         s = self._stream(stream)
         self._sync(s)
         mine = member.buf.words[:count].cpu().numpy().view(np.uint64)
@@ -328,6 +332,8 @@ class ThreadRanks:
         self._sync(s)
 
     def min_host(self, member, value: int) -> int:
+        if self.n == 1:
+            return int(value)
         self.slots[member.part.rank] = int(value)
         self.barrier.wait()
         out = min(self.slots)
@@ -490,6 +496,17 @@ class PartitionedEuler:
 
     def history(self, count: int):
         return self.dev.history(count)
+
+    def march(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
+              max_steps: int = 1000, batch: int = 50, orders: float = 8.0, floors=None) -> dict:  # fmt: skip
+        """EulerDevice.march on every rank together: the whole mesh's norms drive the same
+        convergence decision on every rank, so all take the same steps; invalid_cell global."""
+        out = self._native(lambda: self.dev.march(cfl, dt, local, rk, max_steps, batch, orders,
+                                                  floors))  # fmt: skip
+        bad = out["invalid_cell"]
+        least = self.ranks.min_host(self, _NONE if bad is None else int(self.part.cell_global[bad]))
+        out["invalid_cell"] = None if least == _NONE else least
+        return out
 
     def autotune(self, cfl: float = 0.8, dt: float = 0.0, local: bool = False, rk: int = 3,
                  trial_steps: int = 2) -> tuple[dict, float]:  # fmt: skip

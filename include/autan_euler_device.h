@@ -307,7 +307,8 @@ int autan_euler_device_set_stall_test(void* handle, int32_t polls, char* err, si
  * face_parts, boundary_pressure, conservation and batched cases are refused (E1101) on a mesh
  * with external ghosts, and every entry that steps is refused there until ranks are set.
  * invalid_cell stays a local cell; the Python driver (autan_b200/partition.py) reduces it to the
- * least global id. NULL detaches the ranks. */
+ * least global id. A march stops on every rank when any rank meets an invalid cell (one more
+ * minimum over the ranks after each batch). NULL detaches the ranks. */
 struct autan_euler_ranks {
   void* user;
   int32_t (*exchange)(void* user, int32_t what, int64_t record_bytes, void* stream);

@@ -275,3 +275,52 @@ def test_torch_ranks_on_nccl_streams():
     proc.join(timeout=60)
     assert got == "ok"
     assert proc.exitcode == 0
+
+
+@pytest.mark.parametrize("bad", [False, True])
+def test_partitioned_march_takes_the_whole_mesh_steps(bad):
+    """A steady march to the convergence rule on three ranks: the same iterations, decision and
+    final state as on the whole mesh (the rule reads the whole mesh's norms on every rank). With a
+    non-positive density planted in one rank's cell, every rank stops after the first batch and
+    reports the whole mesh's least invalid cell."""
+    case = K.bump_channel(24, 12, 4, steps=1)
+    m = case.mesh
+    weights = m.gradient_weights(case.bc_kind)
+    parts = PT.partition_cells(m, 3)
+    u0 = case.u0.copy()
+    if bad:
+        u0[0, int(np.nonzero(parts == 2)[0][7])] = -1.0
+    with EulerDevice(m, case.scheme, case.bc_kind, case.bc_data, weights=weights) as d:
+        d.upload(u0)
+        ref = d.march(case.cfl, 0.0, True, 3, max_steps=400, batch=50, orders=3.0)
+        ref_state = d.download()[:, : m.n_owned_cells]
+    assert (ref["invalid_cell"] is not None) == bad
+    ps = PT.extract_partitions(m, weights, parts)
+    ranks = PT.ThreadRanks(len(ps), timeout=300)
+    members = [PT.PartitionedEuler(p, case.scheme, ranks, case.bc_kind, case.bc_data) for p in ps]
+    out, errors = [None] * len(ps), []
+
+    def run(i):
+        try:
+            members[i].upload(u0)
+            r = members[i].march(case.cfl, 0.0, True, 3, max_steps=400, batch=50, orders=3.0)
+            out[i] = (r, members[i].download())
+        except BaseException as e:  # noqa: BLE001 (reported below)
+            errors.append(e)
+            ranks.barrier.abort()
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(ps))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=600)
+    for mb in members:
+        mb.close()
+    assert not errors, errors
+    state = PT.gather_state(ps, [o[1] for o in out], m.n_owned_cells)
+    assert same_bits(state, ref_state)
+    for r, _ in out:
+        assert (r["iterations"], r["steps"], r["converged"]) == (ref["iterations"], ref["steps"],
+                                                                   ref["converged"])  # fmt: skip
+        assert same_bits(r["last"], ref["last"])
+        assert r["invalid_cell"] == ref["invalid_cell"]
