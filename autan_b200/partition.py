@@ -2,8 +2,11 @@
 with its ghosts, and the forward ghost exchange and reductions a partitioned step makes.
 
     partition_cells(mesh, n_parts)          (partition/include/autan/partition/partition.hpp:38-53)
-    extract_partitions(mesh, weights, ...)  extract_partition (partition.hpp:132-145), every rank
-    Partition.send_cells / recv_counts      HaloPattern (partition.hpp:94-110)
+    extract_partition(mesh, weights, ...)   extract_partition (partition.hpp:132-145), one rank;
+    extract_partitions                      every rank in one process
+    Partition.send_cells / recv_counts      HaloPattern (partition.hpp:94-110); the send side set
+                                            from the other ranks' requests (set_send_lists,
+                                            TorchRanks.set_send_lists over a group)
     ThreadRanks, TorchRanks                 HaloExchange forward (halo_exchange.hpp:14-66) and
                                             Ranks::sum / min
     PartitionedEuler                        the device stepper of one rank (autan_euler_ranks)
@@ -194,39 +197,64 @@ def _extract(mesh: Mesh, weights: np.ndarray | None, parts: np.ndarray, rank: in
                      _sources=home[ext])  # fmt: skip
 
 
-def extract_partitions(mesh: Mesh, weights: np.ndarray | None, parts: np.ndarray,
-                       ranks=None) -> list[Partition]:  # fmt: skip
-    """The local meshes of `ranks` (default: every part) with their send lists. `weights`: the
-    global mesh's LSQ weights (3 x stencil entries) for its boundary kinds. Every rank's ghosts
-    are derived to build the send lists, so each rank calling this for itself gets the same
-    halo as its neighbours."""
+def _check_parts(mesh: Mesh, parts) -> np.ndarray:
     parts = np.ascontiguousarray(parts, dtype=np.int32)
     if parts.size != mesh.n_owned_cells or parts.min() < 0:
         raise ValueError("one part per owned cell, from 0")
+    return parts
+
+
+def extract_partition(mesh: Mesh, weights: np.ndarray | None, parts: np.ndarray,
+                      rank: int) -> Partition:  # fmt: skip
+    """The local mesh of `rank` with its receive side (the ghosts it needs from each rank), but no
+    send list yet: `set_send_lists` completes it from the other ranks' requests, which
+    `TorchRanks.set_send_lists` gathers over a process group. `weights`: the global mesh's LSQ
+    weights (3 x stencil entries) for its boundary kinds."""
+    parts = _check_parts(mesh, parts)
+    p = _extract(mesh, weights, parts, rank)
+    p.n_parts = int(parts.max()) + 1
+    if p.recv_counts.size < p.n_parts:
+        p.recv_counts = np.pad(p.recv_counts, (0, p.n_parts - p.recv_counts.size))
+    return p
+
+
+def requests(part: Partition) -> list[np.ndarray]:
+    """Per rank r, the global owned cells whose records this rank's external ghosts take from r,
+    in ghost order (the receive side of the halo)."""
+    ends = np.cumsum(part.recv_counts)
+    return [part._sources[e - c : e] for c, e in zip(part.recv_counts, ends)]
+
+
+def set_send_lists(part: Partition, wanted: list[np.ndarray]) -> None:
+    """The send side of the halo from each rank q's request to this rank (`wanted[q]`: global
+    owned cells of this rank, in q's ghost order): send_cells as local cells, by receiver."""
+    owned = part.cell_global[: part.n_owned]  # ascending
+    cells, counts = [], np.zeros(part.n_parts, dtype=np.int64)
+    for q, g in enumerate(wanted):
+        g = np.asarray(g, dtype=np.int64)
+        at = np.searchsorted(owned, g)
+        if g.size and (at.max() >= owned.size or not np.array_equal(owned[at], g)):
+            raise ValueError(f"rank {q} asks for a cell rank {part.rank} does not own")
+        cells.append(at)
+        counts[q] = g.size
+    part.send_cells = (np.concatenate(cells) if cells else np.zeros(0)).astype(np.int32)
+    part.send_counts = counts
+
+
+def extract_partitions(mesh: Mesh, weights: np.ndarray | None, parts: np.ndarray,
+                       ranks=None) -> list[Partition]:  # fmt: skip
+    """The local meshes of `ranks` (default: every part) with their send lists, all built in
+    this process: every part's receive side is derived to build the send lists. A rank of a
+    process group builds only its own (`extract_partition`, then `TorchRanks.set_send_lists`)."""
+    parts = _check_parts(mesh, parts)
     n_parts = int(parts.max()) + 1
-    every = [_extract(mesh, weights, parts, r) for r in range(n_parts)]
+    every = [extract_partition(mesh, weights, parts, r) for r in range(n_parts)]
+    asked = [requests(p) for p in every]  # asked[q][r]: what q wants from r
     want = range(n_parts) if ranks is None else ranks
     out = []
     for r in want:
-        p = every[r]
-        # local index of each owned global cell of rank r
-        mine = np.nonzero(parts == r)[0]
-        lmap = np.full(mesh.n_owned_cells, -1, dtype=np.int64)
-        lmap[mine] = np.arange(mine.size)
-        cells, counts = [], np.zeros(n_parts, dtype=np.int64)
-        for q in range(n_parts):
-            o = every[q]
-            start = int(o.recv_counts[:r].sum())
-            src = o._sources[start : start + int(o.recv_counts[r])] if r < o.recv_counts.size else []
-            cells.append(lmap[src])
-            counts[q] = len(src)
-        p.send_cells = (np.concatenate(cells) if cells else np.zeros(0)).astype(np.int32)
-        p.send_counts = counts
-        if p.recv_counts.size < n_parts:
-            p.recv_counts = np.pad(p.recv_counts, (0, n_parts - p.recv_counts.size))
-        if (p.send_cells < 0).any():
-            raise AssertionError("a sent cell is not owned by its rank")
-        out.append(p)
+        set_send_lists(every[r], [asked[q][r] for q in range(n_parts)])
+        out.append(every[r])
     return out
 
 
@@ -351,6 +379,36 @@ class TorchRanks:
 
     def join(self, member):
         return self
+
+    def set_send_lists(self, part: Partition, device=None) -> Partition:
+        """Completes `part` (from extract_partition) with its send lists: every rank's requests
+        gathered over the group (counts by all-gather, the cells by point-to-point pairs), so
+        that no rank derives another's ghosts. `device`: where the group's tensors live (a CUDA
+        device for NCCL, None for the CPU)."""
+        import torch
+        import torch.distributed as dist
+
+        n = part.n_parts
+        asked = requests(part)
+        mine = torch.tensor([a.size for a in asked], dtype=torch.int64, device=device)
+        table = [torch.zeros_like(mine) for _ in range(n)]
+        dist.all_gather(table, mine, group=self.group)
+        from_q = [int(table[q][part.rank]) for q in range(n)]  # what q asks of this rank
+        recv = [torch.zeros(c, dtype=torch.int64, device=device) for c in from_q]
+        ops = []
+        for q in range(n):
+            if q == part.rank:
+                continue
+            if from_q[q]:
+                ops.append(dist.P2POp(dist.irecv, recv[q], q, self.group))
+            if asked[q].size:
+                t = torch.from_numpy(np.ascontiguousarray(asked[q], dtype=np.int64)).to(device or "cpu")
+                ops.append(dist.P2POp(dist.isend, t, q, self.group))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        set_send_lists(part, [r.cpu().numpy() for r in recv])
+        return part
 
     @staticmethod
     def _ctx(stream):

@@ -885,8 +885,13 @@ def run_partitioned(args, rank: int, world: int, local_rank: int) -> None:
         raise SystemExit("--partitioned takes --workload channel or tets")
     weights = case.mesh.gradient_weights(case.bc_kind)
     parts = PT.partition_cells(case.mesh, world)
-    (part,) = PT.extract_partitions(case.mesh, weights, parts, ranks=[rank])
-    ranks = PT.TorchRanks() if dist is not None else PT.ThreadRanks(1)
+    part = PT.extract_partition(case.mesh, weights, parts, rank)
+    if dist is not None:
+        ranks = PT.TorchRanks()
+        ranks.set_send_lists(part, device=torch.device("cuda", local_rank))
+    else:
+        ranks = PT.ThreadRanks(1)
+        PT.set_send_lists(part, [np.zeros(0, dtype=np.int64)])
     mb = PT.PartitionedEuler(part, case.scheme, ranks, case.bc_kind, case.bc_data,
                              device=local_rank)  # fmt: skip
     mb.upload(case.u0)

@@ -193,9 +193,16 @@ def _torch_rank(rank: int, world: int, port: int, out) -> None:
                             timeout=datetime.timedelta(seconds=60))  # fmt: skip
     try:
         m = M2.bump_channel(24, 12, 4)
-        parts = PT2.partition_cells(m, world)
-        (p,) = PT2.extract_partitions(m, None, parts, ranks=[rank])
+        parts = random_parts(m, world, 3)
+        # this rank's share alone, its send lists from the other rank's requests over the group,
+        # equal to the ones one process derives from every rank's ghosts
+        p = PT2.extract_partition(m, None, parts, rank)
         ranks = PT2.TorchRanks()
+        ranks.set_send_lists(p)
+        (q,) = PT2.extract_partitions(m, None, parts, ranks=[rank])
+        assert np.array_equal(p.send_cells, q.send_cells)
+        assert np.array_equal(p.send_counts, q.send_counts)
+        assert np.array_equal(p.recv_counts, q.recv_counts)
         member = _Member(p)
         for rb in (32, 96):
             _fill_and_check(member, ranks, m, rb)
