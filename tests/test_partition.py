@@ -226,3 +226,38 @@ def test_torch_ranks_exchange_and_reduce_gloo():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert got == [(0, "ok"), (1, "ok")]
+
+
+def test_one_part_keeps_only_its_images():
+    """A partition into one part is the whole mesh: no external ghost, no send list, and the
+    periodic images stay images of their owned cells."""
+    m = M.periodic_box_hex(8, 8, 2)
+    w = m.gradient_weights(np.full(m.n_boundary_faces, M.BC_SLIP, np.uint8))
+    (p,) = PT.extract_partitions(m, w, np.zeros(m.n_owned_cells, np.int32))
+    assert p.n_external == 0 and p.send_cells.size == 0
+    assert p.n_owned == m.n_owned_cells
+    assert np.all(p.mesh["ghost_owner"] >= 0)
+    check_partition(m, w, p)
+
+
+def test_a_request_for_a_cell_the_rank_does_not_own_is_refused():
+    m = M.bump_channel(24, 12, 4)
+    parts = PT.partition_cells(m, 2)
+    p = PT.extract_partition(m, None, parts, 0)
+    foreign = np.nonzero(parts == 1)[0][:3]
+    with pytest.raises(ValueError, match="does not own"):
+        PT.set_send_lists(p, [np.zeros(0, np.int64), foreign])
+
+
+def test_requests_and_send_lists_pair_up():
+    """What each rank requests of another (in its ghost order) is what that rank's send list
+    holds for it, cell for cell."""
+    m = M.jittered_tets(8, 8, 2, extent=(1.0, 1.0, 0.25))
+    parts = random_parts(m, 4, 9)
+    ps = PT.extract_partitions(m, None, parts)
+    for q in ps:
+        asked = PT.requests(q)
+        for r in ps:
+            first = int(r.send_counts[: q.rank].sum())
+            sent = r.cell_global[r.send_cells[first : first + int(r.send_counts[q.rank])]]
+            assert np.array_equal(sent, asked[r.rank])
