@@ -478,6 +478,8 @@ class PartitionedEuler:
 
         if part.weights is None and scheme.second_order:
             raise ValueError("a second-order scheme needs the partition's LSQ weights")
+        if part.send_cells is None:
+            raise ValueError("the partition has no send lists yet (set_send_lists)")
         self.part = part
         kind = None if bc_kind is None else np.asarray(bc_kind, dtype=np.uint8)[part.bc_index]
         data = None if bc_data is None else np.asarray(bc_data, dtype=np.float64).reshape(5, -1)[:, part.bc_index]
