@@ -356,6 +356,19 @@ void oracle_arrays(const oracle* o, double* prim, double* grad, double* phi, dou
   }
 }
 
+/* The values of a rank's external ghosts for the next residual (see the data's ext_* fields):
+ * 5, 15 and 5 x ghosts, ghost order, entries of periodic images unused; the arrays stay the
+ * caller's and must outlive the evaluations that read them. */
+void oracle_set_external(oracle* o, const double* prim, const double* grad, const double* phi) {
+  if (o->precision == 0) {
+    data_f64* d = (data_f64*)o->data;
+    d->ext_prim = prim, d->ext_grad = grad, d->ext_phi = phi;
+  } else {
+    data_f32* d = (data_f32*)o->data;
+    d->ext_prim = prim, d->ext_grad = grad, d->ext_phi = phi;
+  }
+}
+
 void oracle_spectral_radius(oracle* o, double* lambda) {
   const size_t nc = (size_t)o->m.n_cells;
   if (o->precision == 0) {

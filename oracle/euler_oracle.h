@@ -62,6 +62,9 @@ void oracle_set_second_order(oracle* o, int32_t on);
 void oracle_residual(oracle* o, const double* u, double* res);
 /* The arrays of the last evaluation, as FP64: prim 5 x nc, grad 15 x nc, phi 5 x nc, wmin/wmax
  * 5 x nc, prim_b 5 x nf (any may be NULL). */
+/* A rank's external ghosts (ghost_owner -1): their primitives, gradients and limiter values
+ * (5, 15 and 5 x ghosts in ghost order) for the ghost fills of the following residuals. */
+void oracle_set_external(oracle* o, const double* prim, const double* grad, const double* phi);
 void oracle_arrays(const oracle* o, double* prim, double* grad, double* phi, double* wmin,
                    double* wmax, double* prim_b);
 /* After a residual: the spectral radius of each cell (n_cells, FP64 of the stored value). */

@@ -46,6 +46,7 @@ def lib():
         L.oracle_face_parts.argtypes = [vp, P(f64), P(f64), P(f64)]
         L.oracle_boundary_pressure.argtypes = [vp, P(f64), P(f64)]
         L.oracle_arrays.argtypes = [vp] + [P(f64)] * 6
+        L.oracle_set_external.argtypes = [vp, P(f64), P(f64), P(f64)]
         L.oracle_spectral_radius.argtypes = [vp, P(f64)]
         L.oracle_step.restype = i64
         L.oracle_step.argtypes = [vp, P(f64), i32, f64, f64, i32, P(f64), P(f64)]
@@ -184,6 +185,13 @@ class Oracle:
         force = np.zeros((3, nb))
         lib().oracle_boundary_pressure(self.h, _p(p), _p(force))
         return p, force
+
+    def set_external(self, prim, grad, phi):
+        """The external ghosts' values (5, 15, 5 x ghosts, ghost order) for the next residuals:
+        what the halo exchange of a partitioned mesh delivers."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (prim, grad, phi)]
+        self.keep["external"] = arrs
+        lib().oracle_set_external(self.h, *[_p(a) for a in arrs])
 
     def arrays(self):
         nc, nf = self.n_cells, self.n_faces

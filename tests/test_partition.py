@@ -261,3 +261,55 @@ def test_requests_and_send_lists_pair_up():
             first = int(r.send_counts[: q.rank].sum())
             sent = r.cell_global[r.send_cells[first : first + int(r.send_counts[q.rank])]]
             assert np.array_equal(sent, asked[r.rank])
+
+
+def _oracle_cases():
+    from autan_b200 import cases as K
+
+    return [
+        K.bump_channel(24, 12, 4, precision="fp32+acc64", steps=1),
+        K.bump_channel(24, 12, 4, precision="fp64", steps=1),
+        K.vortex_tets(8, 8, 2, steps=1, precision="fp32+acc64", extent=(10.0, 10.0, 2.5)),
+        K.vortex_hex(8, 8, 2, steps=1, precision="fp64"),
+    ]
+
+
+@pytest.mark.parametrize("index", range(4))
+def test_partitions_restate_the_whole_mesh_residual_on_the_oracle(index):
+    """The CPU oracle over each rank's local mesh, its external ghosts given the values the owning
+    ranks hold (the whole mesh's primitives, gradients and limiter values), gives every owned
+    cell the whole mesh's residual bit for bit, second order with the limiter: the local meshes
+    keep the global loop order, orientation, geometry, stencils, weights and boundary faces."""
+    import oracle as O
+    from autan_b200 import cases as K
+
+    case = _oracle_cases()[index]
+    case.scheme.second_order = True
+    case.scheme.limiter = True
+    m = case.mesh
+    rng = np.random.default_rng(4)
+    u = case.u0 * (1.0 + 1e-3 * rng.uniform(-1.0, 1.0, case.u0.shape))
+    if m.n_cells > m.n_owned_cells:
+        u[:, m.n_owned_cells :] = u[:, m.ghost_owner]
+    md = K.oracle_mesh_dict(case)
+    whole = O.Oracle(md, case.scheme.as_dict(), case.bc_kind, case.bc_data)
+    r_whole = whole.residual(u)
+    fields = whole.arrays()
+    for parts in (PT.partition_cells(m, 3), random_parts(m, 4, 2)):
+        for p in PT.extract_partitions(m, md["stencil_lsq_weight"], parts):
+            local = dict(p.mesh, stencil_lsq_weight=p.weights)
+            o = O.Oracle(local, case.scheme.as_dict(), case.bc_kind[p.bc_index],
+                         case.bc_data[:, p.bc_index])  # fmt: skip
+            ng = p.mesh["n_cells"] - p.n_owned
+            ext = p.cell_global[p.n_owned : p.n_owned + p.n_external]
+
+            def ghosts(a, comps):
+                out = np.zeros((comps, ng))
+                out[:, : p.n_external] = a[:, ext]
+                return out
+
+            o.set_external(ghosts(fields["prim"], 5), ghosts(fields["grad"], 15),
+                           ghosts(fields["phi"], 5))  # fmt: skip
+            r = o.residual(np.ascontiguousarray(u[:, p.cell_global]))
+            want = r_whole[:, p.cell_global[: p.n_owned]]
+            assert np.array_equal(r[:, : p.n_owned].view(np.int64), want.view(np.int64)), p.rank
