@@ -421,25 +421,31 @@ class TorchRanks:
         return contextlib.nullcontext()
 
     def exchange(self, member, what: int, record_bytes: int, stream) -> None:
-        import torch.distributed as dist
-
         p = member.part
         send = member.buf.send_rows(int(p.send_cells.size), record_bytes)
         recv = member.buf.recv_rows(p.n_external, record_bytes)
+        with self._ctx(stream):
+            self.exchange_rows(p, send, recv)
+
+    def exchange_rows(self, part: Partition, send, recv) -> None:
+        """The forward halo exchange of one row per cell: `send` holds the rows of
+        part.send_cells (by receiver), `recv` receives the external ghosts' rows (by source rank,
+        ghost order); tensors of any dtype and row width on the group's device."""
+        import torch.distributed as dist
+
         ops = []
         s_at = r_at = 0
-        for q in range(p.n_parts):
-            sc, rc = int(p.send_counts[q]), int(p.recv_counts[q])
+        for q in range(part.n_parts):
+            sc, rc = int(part.send_counts[q]), int(part.recv_counts[q])
             if rc:
                 ops.append(dist.P2POp(dist.irecv, recv[r_at : r_at + rc], q, self.group))
             if sc:
                 ops.append(dist.P2POp(dist.isend, send[s_at : s_at + sc], q, self.group))
             s_at += sc
             r_at += rc
-        with self._ctx(stream):
-            if ops:
-                for w in dist.batch_isend_irecv(ops):
-                    w.wait()
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
 
     def reduce(self, member, op: int, count: int, stream) -> None:
         import torch.distributed as dist

@@ -232,6 +232,8 @@ struct oracle {
   int32_t precision;
   void* data;
   double *res, *stage, *base, *acc, *dt;
+  oracle_min_fn min; /* a partitioned mesh's minimum over the ranks, or NULL */
+  void* rank_user;
 };
 
 oracle* oracle_create(const oracle_mesh* mesh, const oracle_scheme* scheme, const uint8_t* bc_kind,
@@ -369,6 +371,18 @@ void oracle_set_external(oracle* o, const double* prim, const double* grad, cons
   }
 }
 
+void oracle_set_ranks(oracle* o, oracle_halo_fn halo, oracle_min_fn min, void* user) {
+  o->min = min;
+  o->rank_user = user;
+  if (o->precision == 0) {
+    data_f64* d = (data_f64*)o->data;
+    d->halo = halo, d->halo_user = user;
+  } else {
+    data_f32* d = (data_f32*)o->data;
+    d->halo = halo, d->halo_user = user;
+  }
+}
+
 void oracle_spectral_radius(oracle* o, double* lambda) {
   const size_t nc = (size_t)o->m.n_cells;
   if (o->precision == 0) {
@@ -423,6 +437,7 @@ int64_t oracle_step(oracle* o, double* u, int32_t rk, double cfl, double dt, int
       lam[c] = t;
       h = fmin(h, t);
     }
+    if (o->min != NULL) o->min(o->rank_user, &h);  /* Ranks::min of the step */
   }
   if (dt_out != NULL) *dt_out = h;
   const int use_local = !(dt > 0.0) && local;

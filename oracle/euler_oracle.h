@@ -54,6 +54,15 @@ typedef struct oracle_scheme {
 
 typedef struct oracle oracle;
 
+/* The ranks of a partitioned mesh, for the oracle's steps (test infrastructure: the checker of the
+ * partitioned device path). halo: at each ghost fill (kind 0 primitives, 1 gradients, 2 limiter
+ * values), `send` holds this rank's owned values (comps x owned cells) and the callee writes the
+ * external ghosts' values into `recv` (comps x ghost cells, ghost order; images' entries unused).
+ * min: the minimum over the ranks, in place (the global CFL step). */
+typedef void (*oracle_halo_fn)(void* user, int32_t kind, int32_t comps, const double* send,
+                               double* recv);
+typedef void (*oracle_min_fn)(void* user, double* value);
+
 oracle* oracle_create(const oracle_mesh* mesh, const oracle_scheme* scheme, const uint8_t* bc_kind,
                       const double* bc, const double* source);
 void oracle_free(oracle* o);
@@ -65,6 +74,8 @@ void oracle_residual(oracle* o, const double* u, double* res);
 /* A rank's external ghosts (ghost_owner -1): their primitives, gradients and limiter values
  * (5, 15 and 5 x ghosts in ghost order) for the ghost fills of the following residuals. */
 void oracle_set_external(oracle* o, const double* prim, const double* grad, const double* phi);
+/* A rank of a partitioned mesh: its exchange and minimum over the ranks (NULL: one rank). */
+void oracle_set_ranks(oracle* o, oracle_halo_fn halo, oracle_min_fn min, void* user);
 void oracle_arrays(const oracle* o, double* prim, double* grad, double* phi, double* wmin,
                    double* wmax, double* prim_b);
 /* After a residual: the spectral radius of each cell (n_cells, FP64 of the stored value). */

@@ -32,6 +32,10 @@ class OracleScheme(C.Structure):
 
 _lib = None
 
+# Callbacks of oracle_set_ranks.
+HALO_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.c_int32, P(f64), P(f64))
+MIN_FN = C.CFUNCTYPE(None, C.c_void_p, P(f64))
+
 
 def lib():
     global _lib
@@ -47,6 +51,7 @@ def lib():
         L.oracle_boundary_pressure.argtypes = [vp, P(f64), P(f64)]
         L.oracle_arrays.argtypes = [vp] + [P(f64)] * 6
         L.oracle_set_external.argtypes = [vp, P(f64), P(f64), P(f64)]
+        L.oracle_set_ranks.argtypes = [vp, HALO_FN, MIN_FN, vp]
         L.oracle_spectral_radius.argtypes = [vp, P(f64)]
         L.oracle_step.restype = i64
         L.oracle_step.argtypes = [vp, P(f64), i32, f64, f64, i32, P(f64), P(f64)]
@@ -186,6 +191,32 @@ class Oracle:
         lib().oracle_boundary_pressure(self.h, _p(p), _p(force))
         return p, force
 
+    def set_ranks(self, halo, minimum):
+        """This oracle as one rank of a partitioned mesh: halo(kind, send, recv) fills recv
+        (comps x ghosts) with the external ghosts' values from this rank's owned values send
+        (comps x owned) at each ghost fill (kind 0 primitives, 1 gradients, 2 limiter values);
+        minimum(x) returns the minimum of x over the ranks. An exception in either is re-raised
+        by the next step."""
+        no, ng = self.n_owned, self.n_cells - self.n_owned
+        self.rank_errors = []
+
+        def h(user, kind, comps, send, recv):
+            try:
+                sv = np.ctypeslib.as_array(send, shape=(comps * max(no, 1),))
+                rv = np.ctypeslib.as_array(recv, shape=(comps * max(ng, 1),))
+                halo(int(kind), sv[: comps * no].reshape(comps, no), rv[: comps * ng].reshape(comps, ng))
+            except BaseException as e:  # noqa: BLE001 (re-raised by step)
+                self.rank_errors.append(e)
+
+        def mn(user, value):
+            try:
+                value[0] = float(minimum(float(value[0])))
+            except BaseException as e:  # noqa: BLE001
+                self.rank_errors.append(e)
+
+        self.keep["ranks"] = (HALO_FN(h), MIN_FN(mn))
+        lib().oracle_set_ranks(self.h, *self.keep["ranks"], None)
+
     def set_external(self, prim, grad, phi):
         """The external ghosts' values (5, 15, 5 x ghosts, ghost order) for the next residuals:
         what the halo exchange of a partitioned mesh delivers."""
@@ -212,6 +243,11 @@ class Oracle:
         norms = np.zeros(5)
         h = np.zeros(1)
         bad = lib().oracle_step(self.h, _p(u), rk, cfl, dt, int(local), _p(norms), _p(h))
+        errors = getattr(self, "rank_errors", None)
+        if errors:
+            e = errors[0]
+            errors.clear()
+            raise RuntimeError("a rank callback failed") from e
         return norms, float(h[0]), int(bad)
 
     def first_invalid(self, u, res):

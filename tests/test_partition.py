@@ -313,3 +313,90 @@ def test_partitions_restate_the_whole_mesh_residual_on_the_oracle(index):
             r = o.residual(np.ascontiguousarray(u[:, p.cell_global]))
             want = r_whole[:, p.cell_global[: p.n_owned]]
             assert np.array_equal(r[:, : p.n_owned].view(np.int64), want.view(np.int64)), p.rank
+
+
+def _oracle_step_rank(rank: int, world: int, port: int, out) -> None:
+    """One gloo rank: each case's partition stepped by the CPU oracle, its ghost fills and the
+    CFL step's minimum through TorchRanks (the exchange code of the NCCL path), against the whole
+    mesh stepped by the oracle alone."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, str(REPO))
+    sys.path.insert(0, str(REPO / "tests"))
+    import torch
+    import torch.distributed as dist
+
+    import oracle as O
+    from autan_b200 import cases as K
+    from autan_b200 import partition as PT2
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))  # fmt: skip
+    try:
+        results = []
+        for index, case in enumerate(_oracle_cases()):
+            m = case.mesh
+            md = K.oracle_mesh_dict(case)
+            rng = np.random.default_rng(6)
+            u = case.u0 * (1.0 + 1e-3 * rng.uniform(-1.0, 1.0, case.u0.shape))
+            if m.n_cells > m.n_owned_cells:
+                u[:, m.n_owned_cells :] = u[:, m.ghost_owner]
+            steps = 3
+            whole = O.Oracle(md, case.scheme.as_dict(), case.bc_kind, case.bc_data)
+            ug = np.ascontiguousarray(u.copy())
+            dts = [whole.step(ug, rk=case.rk, cfl=case.cfl, local=case.local)[1] for _ in range(steps)]
+            for split in ("blocks", "random"):
+                parts = PT2.partition_cells(m, world) if split == "blocks" else random_parts(m, world, 5)
+                p = PT2.extract_partition(m, md["stencil_lsq_weight"], parts, rank)
+                ranks = PT2.TorchRanks()
+                ranks.set_send_lists(p)
+                o = O.Oracle(dict(p.mesh, stencil_lsq_weight=p.weights), case.scheme.as_dict(),
+                             case.bc_kind[p.bc_index], case.bc_data[:, p.bc_index])  # fmt: skip
+
+                def halo(kind, send, recv, p=p, ranks=ranks):
+                    comps = send.shape[0]
+                    rows = torch.from_numpy(np.ascontiguousarray(send[:, p.send_cells].T))
+                    got = torch.zeros((p.n_external, comps), dtype=torch.float64)
+                    ranks.exchange_rows(p, rows, got)
+                    recv[:, : p.n_external] = got.numpy().T
+
+                def minimum(x):
+                    t = torch.tensor([x], dtype=torch.float64)
+                    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+                    return float(t.item())
+
+                o.set_ranks(halo, minimum)
+                ul = np.ascontiguousarray(u[:, p.cell_global])
+                got_dt = [o.step(ul, rk=case.rk, cfl=case.cfl, local=case.local)[1]
+                          for _ in range(steps)]  # fmt: skip
+                want = ug[:, p.cell_global[: p.n_owned]]
+                same = np.array_equal(ul[:, : p.n_owned].view(np.int64), want.view(np.int64))
+                results.append((index, split, bool(same), got_dt == dts, p.n_external))
+        out.put((rank, results))
+    except BaseException as e:  # noqa: BLE001
+        out.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partitioned_oracle_steps_over_gloo_ranks():
+    """Two gloo ranks step their partitions on the CPU oracle, exchanging ghost values and the
+    step's minimum through TorchRanks: three steps of the channel (fp32+acc64 and fp64, local
+    steps), the periodic tets (global CFL step) and the periodic hex (first order, RK4) equal the
+    whole mesh's bit for bit, over block and random partitions."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_oracle_step_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted((out.get(timeout=300) for _ in procs), key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, results in got:
+        assert isinstance(results, list), results
+        assert len(results) == 8
+        for index, split, same, same_dt, n_ext in results:
+            assert n_ext > 0, (rank, index, split)
+            assert same and same_dt, (rank, index, split)
