@@ -379,15 +379,16 @@ def _oracle_step_rank(rank: int, world: int, port: int, out) -> None:
         dist.destroy_process_group()
 
 
-def test_partitioned_oracle_steps_over_gloo_ranks():
-    """Two gloo ranks step their partitions on the CPU oracle, exchanging ghost values and the
-    step's minimum through TorchRanks: three steps of the channel (fp32+acc64 and fp64, local
-    steps), the periodic tets (global CFL step) and the periodic hex (first order, RK4) equal the
-    whole mesh's bit for bit, over block and random partitions."""
+@pytest.mark.parametrize("world", [2, 3])
+def test_partitioned_oracle_steps_over_gloo_ranks(world):
+    """Gloo ranks step their partitions on the CPU oracle, exchanging ghost values and the step's
+    minimum through TorchRanks: three steps of the channel (fp32+acc64 and fp64, local steps),
+    the periodic tets (global CFL step) and the periodic hex (first order, RK4) equal the whole
+    mesh's bit for bit, over block and random partitions."""
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = free_port()
-    procs = [ctx.Process(target=_oracle_step_rank, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_oracle_step_rank, args=(r, world, port, out)) for r in range(world)]
     for p in procs:
         p.start()
     got = sorted((out.get(timeout=300) for _ in procs), key=lambda x: x[0])
