@@ -421,3 +421,28 @@ def test_march_to_convergence_matches_the_oracle():
     it, mask = O.convergence_iteration(np.array(norms), 2.0)
     assert (it, mask) == (res["iterations"], res["plateau_mask"])
     assert bits_equal(res["first"], norms[0]) and bits_equal(res["last"], norms[it - 1])
+
+
+@pytest.mark.parametrize("which", ["channel", "tets", "hex"])
+def test_checkpoint_and_resume_are_bit_identical(which):
+    """A checkpoint is the FP64 state downloaded from the device (DeviceStepper::download, what the
+    reference's checkpoint.cgns holds, runtime/src/run.cpp:2391-2480); resuming uploads it into a
+    new stepper. Two steps, a checkpoint, two more steps on a fresh handle give the bits of four
+    uninterrupted steps: the step carries no state beyond the conserved state."""
+    if which == "channel":
+        case = cases.bump_channel(24, 12, 4, steps=4)
+    elif which == "tets":
+        case = cases.vortex_tets(12, 12, 3, steps=4, extent=(10.0, 10.0, 2.5))
+    else:
+        case = cases.vortex_hex(16, 16, 2, steps=4)
+
+    def run(u, n):
+        with EulerDevice(case.mesh, case.scheme, case.bc_kind, case.bc_data) as dev:
+            dev.upload(u)
+            dev.step(cfl=case.cfl, rk=case.rk, local=case.local, n_steps=n)
+            return dev.download()
+
+    straight = run(case.u0, 4)
+    resumed = run(run(case.u0, 2), 2)
+    no = case.mesh.n_owned_cells
+    assert bits_equal(resumed[:, :no], straight[:, :no])

@@ -401,3 +401,94 @@ def test_partitioned_oracle_steps_over_gloo_ranks(world):
         for index, split, same, same_dt, n_ext in results:
             assert n_ext > 0, (rank, index, split)
             assert same and same_dt, (rank, index, split)
+
+
+def test_a_rank_that_fails_or_never_arrives_ends_the_others_exchange():
+    """Failure detection among thread ranks, on the host: a rank that raises before its exchange
+    aborts the barrier, and a rank that never arrives lets the barrier's timeout run out; either
+    way the waiting ranks leave their exchange with an error instead of hanging."""
+    import time
+
+    m = M.jittered_tets(8, 8, 2, extent=(1.0, 1.0, 0.25))
+    ps = PT.extract_partitions(m, None, random_parts(m, 3, 1))
+    for failure in ("raises", "absent"):
+        ranks = PT.ThreadRanks(3, timeout=1.0 if failure == "absent" else 60.0)
+        members = [_Member(p) for p in ps]
+        for mb in members:
+            ranks.join(mb)
+        errors, started = [], time.monotonic()
+
+        def run(mb):
+            try:
+                if mb.part.rank == 2:
+                    if failure == "raises":
+                        ranks.barrier.abort()  # what a failed rank's error path does
+                        raise RuntimeError("rank 2 failed")
+                    return  # rank 2 never comes to the exchange
+                ranks.exchange(mb, 0, 32, None)
+            except BaseException as e:  # noqa: BLE001 (checked below)
+                errors.append((mb.part.rank, type(e).__name__))
+
+        threads = [threading.Thread(target=run, args=(mb,)) for mb in members]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join(timeout=30)
+        assert all(not t.is_alive() for t in threads)
+        waiting = sorted(r for r, name in errors if name == "BrokenBarrierError")
+        assert waiting == [0, 1], (failure, errors)
+        assert time.monotonic() - started < 20
+
+
+def _departing_rank(rank: int, world: int, port: int, out) -> None:
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, str(REPO))
+    import time
+
+    import torch
+    import torch.distributed as dist
+
+    from autan_b200 import mesh as M2
+    from autan_b200 import partition as PT2
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=5))  # fmt: skip
+    m = M2.bump_channel(24, 12, 4)
+    parts = PT2.partition_cells(m, world)
+    p = PT2.extract_partition(m, None, parts, rank)
+    ranks = PT2.TorchRanks()
+    ranks.set_send_lists(p)
+    dist.barrier()
+    if rank == 1:
+        out.put((rank, "left"))
+        out.close()
+        out.join_thread()  # the message out before the abrupt exit
+        os._exit(0)  # leaves between steps, without its exchange
+    started = time.monotonic()
+    try:
+        send = torch.zeros((p.send_cells.size, 4), dtype=torch.float64)
+        recv = torch.zeros((p.n_external, 4), dtype=torch.float64)
+        ranks.exchange_rows(p, send, recv)
+        out.put((rank, "no error"))
+    except BaseException as e:  # noqa: BLE001
+        out.put((rank, f"error after {time.monotonic() - started:.0f} s: {type(e).__name__}"))
+    out.close()
+    out.join_thread()
+    os._exit(0)
+
+
+def test_a_departed_rank_ends_the_torch_exchange_with_an_error():
+    """A gloo rank leaves between steps; the other rank's next exchange fails (the process group's
+    short timeout or the closed connection) instead of waiting forever."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_departing_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(out.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert got[1] == "left"
+    assert got[0].startswith("error after"), got[0]
